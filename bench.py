@@ -1,0 +1,435 @@
+#!/usr/bin/env python
+"""Benchmark of the Spartan+WHIR prover hot path on B200: the WHIR commit of a
+2^20-coefficient multilinear polynomial (Reed-Solomon encode at rate 1/4 by
+coset NTT to 2^22 evaluations, then a Skyscraper Merkle tree over leaves of
+2^folding_factor Fr), bit-exact with the CPU algorithm.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs under torchrun: every rank commits its own polynomials (independent
+replicas, no data-path collective); time = max over ranks.  Prints one JSON
+line on rank 0.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("WHIR commit throughput, Spartan+WHIR prover hot path: 2^20 Fr coefficients -> "
+          "RS rate-1/4 coset NTT -> 2^22 evaluations -> Skyscraper Merkle tree (bit-exact)")
+UNIT = "commits/s"
+IMAD_PER_MONT = 264  # mad.lo/madc.hi/mul.lo per 8x32 CIOS product (fr.cuh: 8 x (16 + 16 + 1))
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--log-coeffs", type=int, default=20)
+    p.add_argument("--folding-factor", type=int, default=4)
+    p.add_argument("--log-inv-rate", type=int, default=2)
+    p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plugin-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(a):
+    return {"workload": "whir_commit", "log2_coeffs": a.log_coeffs,
+            "folding_factor": a.folding_factor, "log_inv_rate": a.log_inv_rate,
+            "leaf_fr": 1 << a.folding_factor,
+            "num_leaves": (1 << (a.log_coeffs - a.folding_factor)) << a.log_inv_rate,
+            "leaf_encoding": "canonical", "seed": a.seed,
+            "l2": "flushed: 256 MiB device write between timed steps (outside the step events)",
+            "parallelism": f"replicas x{a.gpus}"}
+
+
+# ---------------------------------------------------------------------------
+# CPU arm: the oracle restatement (the reference is Rust and cannot be built
+# here), OpenMP over all host threads.
+# ---------------------------------------------------------------------------
+def cpu_commit_once(O, coeffs_np, a):
+    import numpy as np
+    M = 1 << a.folding_factor
+    L = coeffs_np.shape[0] // M
+    cw_len = L << a.log_inv_rate
+    out = np.zeros((M * cw_len, 4), np.uint64)
+    rc = O.lib().pko_rs_interleaved_encode(O.p64(coeffs_np), M, L, O.p64(coeffs_np), 0, cw_len,
+                                           O.p64(out))
+    assert rc == 0
+    O.lib().pko_from_mont_many(O.p64(out), out.shape[0])
+    layers = np.zeros(32 * (2 * cw_len - 1), np.uint8)
+    rc = O.lib().pko_merkle_tree(O.p8(out.view(np.uint8).reshape(-1)), 32 * M, cw_len, O.p8(layers))
+    assert rc == 0
+    return layers[-32:]
+
+
+def cpu_baseline_measure(a, samples=1):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    coeffs = O.sample_fr(a.seed, 1 << a.log_coeffs)
+    t0 = time.perf_counter()
+    cpu_commit_once(O, coeffs, a)
+    dt = (time.perf_counter() - t0) / 1.0
+    times = [dt]
+    for _ in range(samples - 1):
+        t0 = time.perf_counter()
+        cpu_commit_once(O, coeffs, a)
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times), O.lib().pko_num_threads()
+
+
+def commit_products(log_coeffs, ff, lr):
+    """Montgomery products of one commit: NTT butterflies + leaf hashing
+    (14 squarings per compression, one conversion per Fr) + tree levels."""
+    n = 1 << log_coeffs
+    M = 1 << ff
+    cw_len = (n >> ff) << lr
+    ntt = (cw_len * M // 2) * (log_coeffs - ff)
+    leaves = cw_len * ((M - 1) * 14 + M)
+    levels = (cw_len - 1) * 14
+    return ntt + leaves + levels
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import copy
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    coeffs = O.sample_fr(a.seed, 1 << a.log_coeffs)
+    t0 = time.perf_counter()
+    cpu_commit_once(O, coeffs, a)
+    t_full = time.perf_counter() - t0
+    budget_s = 180.0
+    shrink = 0
+    while t_full / (1 << shrink) * (a.steps + a.warmup) > budget_s and shrink < a.log_coeffs - a.folding_factor - 2:
+        shrink += 1
+    s = copy.copy(a)
+    s.log_coeffs = a.log_coeffs - shrink
+    scale = commit_products(s.log_coeffs, a.folding_factor, a.log_inv_rate) / commit_products(
+        a.log_coeffs, a.folding_factor, a.log_inv_rate)
+    sample_coeffs = coeffs[: 1 << s.log_coeffs]
+    for _ in range(max(a.warmup - 1, 0)):
+        cpu_commit_once(O, sample_coeffs, s)
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        cpu_commit_once(O, sample_coeffs, s)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = scale * a.steps / total
+    cores = O.lib().pko_num_threads()
+    if shrink:
+        sample = (f"each step commits a 2^{s.log_coeffs}-coefficient polynomial (same folding factor "
+                  f"and rate); throughput scaled to the 2^{a.log_coeffs} workload by Montgomery-"
+                  f"product count (x{scale:.5f}); one full commit took {t_full:.2f} s")
+    else:
+        sample = "full workload per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (BN254 Fr)",
+        "data": "synthetic (ChaCha20-seeded Fr)", "config": workload_config(a),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample + "; C restatement of RSFr::interleaved_encode + the "
+                                   "SkyscraperHashEngine tree, OpenMP, not the reference binary "
+                                   "(no Rust toolchain)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region.
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def physical_gpu_index(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+# ---------------------------------------------------------------------------
+# GPU arm.
+# ---------------------------------------------------------------------------
+def run_b200(a):
+    import numpy as np
+    import torch
+
+    from provekit_b200 import _lib
+    from provekit_b200._lib import PKG_LEAF_CANONICAL, check
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != a.gpus:
+        raise SystemExit(f"--gpus {a.gpus} but WORLD_SIZE={world}")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    L = _lib.lib()
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+
+    M = 1 << a.folding_factor
+    n = 1 << a.log_coeffs
+    msg_len = n // M
+    cw_len = msg_len << a.log_inv_rate
+    total_fr = cw_len * M
+
+    h_coeffs = np.zeros((n, 4), np.uint64)
+    check(L.pkg_sample_fr(a.seed + 1000 * rank, n, h_coeffs.ctypes.data, 1))
+    pinned = torch.from_numpy(h_coeffs.view(np.int64)).pin_memory()
+    d_coeffs = pinned.to(f"cuda:{local_rank}")
+    d_cw = torch.empty((total_fr, 4), dtype=torch.int64, device=d_coeffs.device)
+    d_layers = torch.empty(32 * (2 * cw_len - 1), dtype=torch.uint8, device=d_coeffs.device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=d_coeffs.device)
+    root_host = torch.empty(32, dtype=torch.uint8).pin_memory()
+    check(L.pkg_ntt_engine_reserve(cw_len))
+
+    def step():
+        check(L.pkg_rs_interleaved_encode(d_coeffs.data_ptr(), M, msg_len, None, 0, cw_len,
+                                          d_cw.data_ptr(), sh))
+        ev[1].record(stream)
+        check(L.pkg_merkle_leaves_fr(d_cw.data_ptr(), M, cw_len, PKG_LEAF_CANONICAL,
+                                     d_layers.data_ptr(), sh))
+        ev[2].record(stream)
+        check(L.pkg_merkle_levels(d_layers.data_ptr(), cw_len, sh))
+
+    # warm-up
+    with torch.cuda.stream(stream):
+        for _ in range(max(a.warmup, 0)):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            flush.zero_()
+            step()
+    stream.synchronize()
+
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(a.steps)]
+    clocks = ClockSampler(physical_gpu_index(local_rank))
+    clocks.start()
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = L.pkg_kernel_launches()
+    with torch.cuda.stream(stream):
+        for i in range(a.steps):
+            ev = events[i]
+            flush.zero_()
+            ev[0].record(stream)
+            step()
+            ev[3].record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    launches = L.pkg_kernel_launches() - launches0
+    clk = clocks.stop()
+
+    step_ms = [e[0].elapsed_time(e[3]) for e in events]
+    enc_ms = [e[0].elapsed_time(e[1]) for e in events]
+    leaf_ms = [e[1].elapsed_time(e[2]) for e in events]
+    lvl_ms = [e[2].elapsed_time(e[3]) for e in events]
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=d_coeffs.device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms_max = float(t.item())
+
+    # ---- end to end through the C ABI: pinned host coefficients in, root out
+    e2e_events = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
+    with torch.cuda.stream(stream):
+        for i in range(a.warmup + a.steps):
+            flush.zero_()
+            if i >= a.warmup:
+                e2e_events[i - a.warmup][0].record(stream)
+            d_coeffs.copy_(pinned, non_blocking=True)
+            check(L.pkg_whir_commit(d_coeffs.data_ptr(), n, a.folding_factor, a.log_inv_rate, None,
+                                    0, PKG_LEAF_CANONICAL, d_cw.data_ptr(), d_layers.data_ptr(), sh))
+            root_host.copy_(d_layers[-32:], non_blocking=True)
+            if i >= a.warmup:
+                e2e_events[i - a.warmup][1].record(stream)
+    stream.synchronize()
+    e2e_ms = sum(e[0].elapsed_time(e[1]) for e in e2e_events)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=d_coeffs.device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms_max = float(t.item())
+
+    # ---- the trait-shaped drop-in: host slices through RSFr / HashEngine
+    plugin = None
+    if not a.no_plugin_e2e:
+        msgs = [np.ascontiguousarray(h_coeffs[j * msg_len:(j + 1) * msg_len]) for j in range(M)]
+        ptrs = (ctypes.c_void_p * M)(*[m.ctypes.data for m in msgs])
+        out_cw = np.zeros((total_fr, 4), np.uint64)
+        digests = np.zeros(32 * cw_len, np.uint8)
+
+        def plugin_commit():
+            check(L.pkg_host_rs_interleaved_encode(ctypes.cast(ptrs, ctypes.c_void_p), M, msg_len,
+                                                   None, 0, cw_len, out_cw.ctypes.data))
+            check(L.pkg_host_skyscraper_hash_many(32 * M, out_cw.ctypes.data, cw_len,
+                                                  digests.ctypes.data))
+            level = digests
+            while level.size > 32:
+                nxt = np.zeros(level.size // 2, np.uint8)
+                check(L.pkg_host_skyscraper_hash_many(64, level.ctypes.data, level.size // 64,
+                                                      nxt.ctypes.data))
+                level = nxt
+            return level
+
+        plugin_commit()
+        pt = []
+        for _ in range(min(a.steps, 5)):
+            t0 = time.perf_counter()
+            plugin_commit()
+            pt.append(time.perf_counter() - t0)
+        plugin = {"value": len(pt) / sum(pt), "unit": UNIT,
+                  "h2d_bytes_per_step": 32 * n + 32 * total_fr + 32 * cw_len,
+                  "d2h_bytes_per_step": 32 * total_fr + 32 * cw_len + 32 * (cw_len - 1),
+                  "note": "wall clock, host-slice plugin calls (pkg_host_rs_interleaved_encode + "
+                          "pkg_host_skyscraper_hash_many per level), raw Montgomery leaf bytes"}
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel (Merkle leaf fold)
+    imad = ctypes.c_double(0)
+    check(L.pkg_measure_imad_rate(ctypes.byref(imad)))
+    mont_peak = imad.value / IMAD_PER_MONT
+    num_leaves = cw_len
+    mont_per_leaf_launch = num_leaves * ((M - 1) * 14 + M)
+    leaf_avg_s = statistics.mean(leaf_ms) * 1e-3
+    achieved = mont_per_leaf_launch / leaf_avg_s
+    ntt_stages = (msg_len << a.log_inv_rate).bit_length() - 1 - a.log_inv_rate
+    ntt_mont = (total_fr // 2) * ntt_stages
+    enc_avg_s = statistics.mean(enc_ms) * 1e-3
+
+    cpu = None
+    if not a.no_cpu_baseline:
+        cpu_s, cores = cpu_baseline_measure(a)
+        cpu = {"value": 1.0 / cpu_s, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "one full 2^20-coefficient commit on the host (C restatement, OpenMP); "
+                         "not the reference binary (no Rust toolchain)"}
+
+    value = a.gpus * a.steps / (total_ms_max * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": total_ms_max / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (BN254 Fr, 8x32-bit limbs)",
+        "data": "synthetic (ChaCha20-seeded uniform Fr, Montgomery form)",
+        "config": workload_config(a),
+        "roofline": {
+            "kernel": "leaf_fold_fr_kernel (Skyscraper leaf hashing)", "bound": "int",
+            "achieved": achieved / 1e9, "peak": mont_peak / 1e9, "unit": "Gmont/s",
+            "frac": achieved / mont_peak, "traffic": None,
+            "peak_source": f"measured IMAD-class rate {imad.value / 1e12:.3f} T/s "
+                           f"(pkg_measure_imad_rate) / {IMAD_PER_MONT} per CIOS product",
+            "algorithmic": f"{num_leaves} leaves x ({M - 1} compressions x 14 squarings + {M} "
+                           f"Montgomery->canonical) = {mont_per_leaf_launch} products per launch",
+        },
+        "kernels": {
+            "rs_encode_ms": statistics.mean(enc_ms), "merkle_leaves_ms": statistics.mean(leaf_ms),
+            "merkle_levels_ms": statistics.mean(lvl_ms),
+            "share": {"rs_encode": sum(enc_ms) / total_ms, "merkle_leaves": sum(leaf_ms) / total_ms,
+                      "merkle_levels": sum(lvl_ms) / total_ms},
+            "ntt_gmont_per_s": ntt_mont / enc_avg_s / 1e9,
+            "encode_hbm_gbs": 32 * (n + 2 * total_fr) / enc_avg_s / 1e9,
+        },
+        "cpu_baseline": cpu,
+        "e2e": {"value": a.gpus * a.steps / (e2e_ms_max * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": 32,
+                "note": "pkg_whir_commit with the coefficients copied from pinned host memory and "
+                        "the root read back, every step"},
+        "e2e_plugin": plugin,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse_args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

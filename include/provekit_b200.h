@@ -1,0 +1,161 @@
+/*
+ * provekit_b200.h -- C ABI of the B200 (sm_100a) ProveKit prover hot path.
+ *
+ * Field elements are BN254 Fr as 4 x uint64_t little-endian limbs, exactly the
+ * in-memory layout of arkworks' `ark_bn254::Fr` (Montgomery form, R = 2^256,
+ * fully reduced), so a Rust caller passes `slice.as_ptr() as *const u64`.
+ * Skyscraper inputs/outputs are raw bytes, as in the reference's
+ * `HashEngine::hash_many(&[u8], &mut [Hash])`.
+ *
+ * Pointer classes:
+ *   pkg_*       device pointers, work enqueued on `stream` (NULL = legacy
+ *               default stream); the call returns once the work is enqueued
+ *               unless the entry point says otherwise.
+ *   pkg_host_*  host pointers, synchronous: copy in, compute on the current
+ *               device, copy out.  These are the drop-ins for the reference's
+ *               host-slice plugin traits.
+ *
+ * Every entry point returns 0 (PKG_OK) or a negative PKG_ERR_* code and never
+ * throws; pkg_last_error() returns the calling thread's last message
+ * (convention of tooling/provekit-ffi/src/ffi.rs:29-95).  Where the reference
+ * panics on a contract violation, the entry point returns
+ * PKG_ERR_INVALID_ARGUMENT.
+ */
+#ifndef PROVEKIT_B200_H
+#define PROVEKIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PKG_OK 0
+#define PKG_ERR_INVALID_ARGUMENT (-1)
+#define PKG_ERR_CUDA (-2)
+#define PKG_ERR_OUT_OF_MEMORY (-3)
+#define PKG_ERR_UNSUPPORTED (-4)
+#define PKG_ERR_TIMEOUT (-5)
+
+/* Leaf encodings for Merkle commits over Fr codewords. */
+#define PKG_LEAF_CANONICAL 0   /* leaf bytes = canonical LE limbs (x), the   */
+                               /* values the recursive verifier re-hashes   */
+#define PKG_LEAF_MONTGOMERY 1  /* leaf bytes = raw in-memory limbs (x*2^256) */
+
+typedef void *pkg_stream_t; /* a cudaStream_t */
+
+/* ---- library ------------------------------------------------------------ */
+/* Thread-local message of the last failing call on this thread ("" if none).
+ * Replaces pk_get_last_error (tooling/provekit-ffi/src/ffi.rs:73-89). */
+const char *pkg_last_error(void);
+/* ABI version (major*10000 + minor*100 + patch). */
+int pkg_version(void);
+
+/* Seeded ChaCha20 Fr sampler for synthetic inputs: RFC 8439 block function
+ * with a 64-bit block counter in words 12-13 and zero nonce, key = seed (LE)
+ * in the first 8 bytes; each 64-byte block yields two 32-byte candidates,
+ * masked to 254 bits and rejected if >= p.  Host memory; Montgomery form when
+ * mont != 0.  No reference counterpart (the reference samples with
+ * ark_std::rand::thread_rng). */
+int pkg_sample_fr(uint64_t seed, size_t n, uint64_t *out, int mont);
+
+/* ---- ntt crate (ntt/src/ntt.rs) ------------------------------------------ */
+/* In-place NTT, normal order in, bit-reversed order out, over
+ * len / codeword_size interleaved columns; the first log2(num_groups) stages
+ * are skipped (the caller replicated cosets).
+ * Replaces `pub fn ntt_nr(values: &mut [Fr], codeword_size, num_groups)`
+ * (ntt/src/ntt.rs:105-108, 150-248).  Device pointer. */
+int pkg_ntt_nr(uint64_t *values, size_t len, size_t codeword_size, size_t num_groups,
+               pkg_stream_t stream);
+/* Inverse NTT, bit-reversed order in, normal order out.
+ * Replaces `pub fn intt_rn(input: &mut [Fr])` (ntt/src/ntt.rs:326-348). */
+int pkg_intt_rn(uint64_t *values, size_t len, pkg_stream_t stream);
+/* Grow the device-resident twiddle table to `order` (power of two <= 2^28).
+ * Replaces `NTTEngine::with_order` (ntt/src/ntt.rs:39-45).  Growing
+ * synchronises the current device. */
+int pkg_ntt_engine_reserve(size_t order);
+/* Host-slice forms of the two calls above (synchronous). */
+int pkg_host_ntt_nr(uint64_t *values, size_t len, size_t codeword_size, size_t num_groups);
+int pkg_host_intt_rn(uint64_t *values, size_t len);
+
+/* ---- RSFr: whir ReedSolomon<Fr> plugin (provekit/common/src/ntt.rs) ----- */
+/* next_order (ntt.rs:13-20): smallest power of two >= size, if <= 2^28. */
+int pkg_rs_next_order(size_t size, size_t *order_out);
+/* generator (ntt.rs:102-104): Fr::get_root_of_unity(codeword_length), mont. */
+int pkg_rs_generator(size_t codeword_length, uint64_t out[4]);
+/* evaluation_points (ntt.rs:22-42): out[i] = generator^bitrev(indices[i]).
+ * Host memory. */
+int pkg_rs_evaluation_points(size_t codeword_length, const size_t *indices, size_t n,
+                             uint64_t *out);
+/* interleaved_encode (ntt.rs:51-100).  messages: num_messages x
+ * message_length Fr, message-major (message j at j*message_length); masks:
+ * mask_len Fr in the reference's interleaved layout; out: codeword_length x
+ * num_messages Fr (row i = the num_messages evaluations at point i).
+ * Device pointers. */
+int pkg_rs_interleaved_encode(const uint64_t *messages, size_t num_messages,
+                              size_t message_length, const uint64_t *masks, size_t mask_len,
+                              size_t codeword_length, uint64_t *out, pkg_stream_t stream);
+/* Host form with the trait's `&[&[Fr]]` message list (synchronous). */
+int pkg_host_rs_interleaved_encode(const uint64_t *const *messages, size_t num_messages,
+                                   size_t message_length, const uint64_t *masks,
+                                   size_t mask_len, size_t codeword_length, uint64_t *out);
+
+/* ---- Skyscraper (skyscraper/core, provekit/common/src/skyscraper) ------- */
+/* count two-to-one compressions of 64-byte messages into 32-byte hashes.
+ * Replaces skyscraper::simple::compress_many (skyscraper/core/src/simple.rs:3-9). */
+int pkg_skyscraper_compress_many(const uint8_t *messages, size_t count, uint8_t *hashes,
+                                 pkg_stream_t stream);
+/* SkyscraperHashEngine::hash_many (provekit/common/src/skyscraper/whir.rs:42-100):
+ * size 32 copies, 64 compresses, larger multiples of 32 left-fold the chunks. */
+int pkg_skyscraper_hash_many(size_t size, const uint8_t *input, size_t count,
+                             uint8_t *output, pkg_stream_t stream);
+int pkg_host_skyscraper_hash_many(size_t size, const uint8_t *input, size_t count,
+                                  uint8_t *output);
+/* Skyscraper PoW (skyscraper/core/src/generic.rs:42-71): smallest nonce with
+ * compress(challenge, [nonce,0,0,0]) < threshold, searched on the device with
+ * every candidate below the answer evaluated.  Host in/out, synchronous. */
+int pkg_skyscraper_pow_solve(const uint64_t challenge[4], const uint64_t threshold[4],
+                             uint64_t *nonce_out);
+
+/* ---- Merkle commit ------------------------------------------------------- */
+/* Binary Skyscraper Merkle tree over num_leaves (power of two) leaves of
+ * leaf_size bytes: leaf digests = hash_many(leaf_size), internal nodes =
+ * hash_many(64) of (left || right).  layers receives 2*num_leaves-1 digests
+ * level by level: leaf digests first, root last.  Device pointers. */
+int pkg_merkle_tree(const uint8_t *leaves, size_t leaf_size, size_t num_leaves,
+                    uint8_t *layers, pkg_stream_t stream);
+/* Same tree with leaf i = the fr_per_leaf Fr of codeword row i (the
+ * interleaved_encode output), encoded per PKG_LEAF_*.  Device pointers. */
+int pkg_merkle_tree_fr(const uint64_t *codeword, size_t fr_per_leaf, size_t num_leaves,
+                       int leaf_encoding, uint8_t *layers, pkg_stream_t stream);
+
+/* The two halves of pkg_merkle_tree_fr: leaf digests into layers[0..L), then
+ * the internal levels above them (layers must hold 2*L-1 digests). */
+int pkg_merkle_leaves_fr(const uint64_t *codeword, size_t fr_per_leaf, size_t num_leaves,
+                         int leaf_encoding, uint8_t *layers, pkg_stream_t stream);
+int pkg_merkle_levels(uint8_t *layers, size_t num_leaves, pkg_stream_t stream);
+
+/* WHIR commit of one multilinear polynomial: the coefficients are split into
+ * 2^folding_factor contiguous messages, Reed-Solomon encoded at rate
+ * 2^-log_inv_rate (interleaved_encode), and committed with
+ * pkg_merkle_tree_fr.  codeword_out: num_coeffs << log_inv_rate Fr;
+ * layers_out: 2*L-1 digests, L = (num_coeffs >> folding_factor) << log_inv_rate.
+ * Device pointers. */
+int pkg_whir_commit(const uint64_t *coeffs, size_t num_coeffs, unsigned folding_factor,
+                    unsigned log_inv_rate, const uint64_t *masks, size_t mask_len,
+                    int leaf_encoding, uint64_t *codeword_out, uint8_t *layers_out,
+                    pkg_stream_t stream);
+
+/* ---- diagnostics ---------------------------------------------------------- */
+/* Number of kernels this library has launched in this process. */
+uint64_t pkg_kernel_launches(void);
+/* Measured 32-bit IMAD-class throughput of the current device (instructions
+ * per second, from a dependent-chain-free mad.lo/madc.hi microbenchmark).
+ * Synchronous. */
+int pkg_measure_imad_rate(double *instr_per_second);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

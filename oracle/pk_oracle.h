@@ -1,0 +1,94 @@
+/*
+ * pk_oracle.h -- CPU restatement of ProveKit's Spartan+WHIR prover hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the parity oracle for the CUDA
+ * implementation in provekit_b200/.  Only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline / reference arm may load it, and only as a checker
+ * or as the timed CPU baseline -- never as a fallback for the product path.
+ *
+ * Field elements are BN254 Fr, 4 x u64 little-endian limbs.  "mont" means the
+ * arkworks in-memory form x*2^256 mod p, always fully reduced; "canonical"
+ * means x itself in [0, p).
+ *
+ * Parity pins: Skyscraper KATs (skyscraper/core/src/reference.rs:104-188),
+ * sumcheck helper KATs (provekit/common/src/utils/sumcheck.rs:229-436),
+ * Poseidon2 KATs (poseidon2/src/permutation.rs:182-195, hash.rs:53-70).
+ * The NTT root of unity is derived as arkworks does (generator 5, two-adicity
+ * 28); no reference golden output pins NTT bytes directly.
+ */
+#ifndef PK_ORACLE_H
+#define PK_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- field ---------------------------------------------------------- */
+void pko_fr_mul(uint64_t r[4], const uint64_t a[4], const uint64_t b[4]);
+void pko_fr_add(uint64_t r[4], const uint64_t a[4], const uint64_t b[4]);
+void pko_fr_sub(uint64_t r[4], const uint64_t a[4], const uint64_t b[4]);
+void pko_fr_to_mont(uint64_t r[4], const uint64_t a[4]);   /* a canonical */
+void pko_fr_from_mont(uint64_t r[4], const uint64_t a[4]);
+void pko_fr_inv(uint64_t r[4], const uint64_t a[4]);         /* mont in/out */
+void pko_fr_root_of_unity(uint64_t r[4], uint64_t n);        /* mont out    */
+void pko_to_mont_many(uint64_t *v, size_t n);
+void pko_from_mont_many(uint64_t *v, size_t n);
+
+/* Seeded ChaCha20 Fr sampler (RFC 8439 block function, 64-bit counter,
+ * key = seed LE in the first 8 bytes).  254-bit mask + rejection; output in
+ * Montgomery form when mont != 0. */
+void pko_sample_fr(uint64_t seed, size_t n, uint64_t *out, int mont);
+
+/* ---- ntt crate (ntt/src/ntt.rs) --------------------------------------- */
+int  pko_ntt_nr(uint64_t *values, size_t len, size_t codeword_size, size_t num_groups);
+int  pko_intt_rn(uint64_t *values, size_t len);
+void pko_roots_reverse_ordered(uint64_t *out, size_t order);   /* order/2 entries */
+
+/* ---- RSFr::interleaved_encode (provekit/common/src/ntt.rs:51-100) ------ */
+/* messages: num_messages x message_length, message-major. */
+int pko_rs_interleaved_encode(const uint64_t *messages, size_t num_messages,
+                              size_t message_length, const uint64_t *masks,
+                              size_t mask_len, size_t codeword_length,
+                              uint64_t *out);
+void pko_rs_evaluation_points(size_t codeword_length, const size_t *indices,
+                              size_t n, uint64_t *out);
+
+/* ---- Skyscraper (skyscraper/core/src) ---------------------------------- */
+void pko_sky_compress(uint64_t out[4], const uint64_t l[4], const uint64_t r[4]);
+int  pko_sky_compress_many(const uint8_t *messages, size_t n, uint8_t *hashes);
+void pko_sky_permute(uint64_t l[4], uint64_t r[4]);               /* canonical */
+void pko_sky_ss(int round, uint64_t l[4], uint64_t r[4]);
+void pko_sky_bb(int round, uint64_t l[4], uint64_t r[4]);
+uint8_t pko_sky_sbox(uint8_t v);
+int  pko_hash_many(size_t size, const uint8_t *input, size_t count, uint8_t *output);
+/* Merkle tree over count leaves of leaf_size bytes: writes 2*count-1
+ * digests, level by level (leaf digests first, root last). */
+int  pko_merkle_tree(const uint8_t *leaves, size_t leaf_size, size_t count,
+                     uint8_t *layers);
+/* PoW: smallest nonce with compress(challenge, [nonce,0,0,0]) < threshold. */
+uint64_t pko_sky_pow_solve(const uint64_t challenge[4], const uint64_t threshold[4]);
+
+/* ---- Spartan sumcheck (provekit/common/src/utils/sumcheck.rs) ---------- */
+void pko_calculate_eq(uint64_t out[4], const uint64_t *r, const uint64_t *alpha, size_t n);
+int  pko_eq_hypercube(const uint64_t *r, size_t nr, size_t num_entries, uint64_t *out);
+/* One round of the Spartan map-reduce over tables a,b,c,eq of length size;
+ * fold != NULL applies the quarter-layout fold first (tables halve). */
+int  pko_spartan_round(uint64_t *a, uint64_t *b, uint64_t *c, uint64_t *eq,
+                       size_t size, const uint64_t *fold, uint64_t out[12]);
+/* CSR SpMV: y[row] = sum_k vals[k] * x[cols[k]] over row_ptr[row]..row_ptr[row+1]. */
+int  pko_spmv(const uint64_t *row_ptr, const uint32_t *cols, const uint64_t *vals,
+              size_t num_rows, const uint64_t *x, uint64_t *y);
+void pko_eval_cubic(uint64_t out[4], const uint64_t poly[16], const uint64_t x[4]);
+void pko_blinding_coeffs(const uint64_t *g, size_t n, size_t compute_for,
+                         const uint64_t *alphas, uint64_t out[16]);
+void pko_dot(uint64_t out[4], const uint64_t *a, const uint64_t *b, size_t n);
+
+int pko_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

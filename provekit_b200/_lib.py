@@ -1,0 +1,97 @@
+"""ctypes binding of libprovekit_b200.so (the C ABI in include/provekit_b200.h).
+
+The library is built in-tree by provekit_b200.build; importing this module
+without it raises immediately -- there is no CPU fallback for the product path.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libprovekit_b200.so")
+
+PKG_OK = 0
+PKG_ERR_INVALID_ARGUMENT = -1
+PKG_ERR_CUDA = -2
+PKG_ERR_OUT_OF_MEMORY = -3
+PKG_ERR_UNSUPPORTED = -4
+PKG_ERR_TIMEOUT = -5
+
+PKG_LEAF_CANONICAL = 0
+PKG_LEAF_MONTGOMERY = 1
+
+_c_sz = ctypes.c_size_t
+_c_u64p = ctypes.POINTER(ctypes.c_uint64)
+_c_u8p = ctypes.POINTER(ctypes.c_uint8)
+_c_vp = ctypes.c_void_p
+_c_int = ctypes.c_int
+_c_uint = ctypes.c_uint
+
+# name -> argtypes; every entry point returns int
+SIGNATURES = {
+    "pkg_sample_fr": [ctypes.c_uint64, _c_sz, _c_vp, _c_int],
+    "pkg_ntt_nr": [_c_vp, _c_sz, _c_sz, _c_sz, _c_vp],
+    "pkg_intt_rn": [_c_vp, _c_sz, _c_vp],
+    "pkg_ntt_engine_reserve": [_c_sz],
+    "pkg_host_ntt_nr": [_c_vp, _c_sz, _c_sz, _c_sz],
+    "pkg_host_intt_rn": [_c_vp, _c_sz],
+    "pkg_rs_next_order": [_c_sz, ctypes.POINTER(_c_sz)],
+    "pkg_rs_generator": [_c_sz, _c_vp],
+    "pkg_rs_evaluation_points": [_c_sz, _c_vp, _c_sz, _c_vp],
+    "pkg_rs_interleaved_encode": [_c_vp, _c_sz, _c_sz, _c_vp, _c_sz, _c_sz, _c_vp, _c_vp],
+    "pkg_host_rs_interleaved_encode": [_c_vp, _c_sz, _c_sz, _c_vp, _c_sz, _c_sz, _c_vp],
+    "pkg_skyscraper_compress_many": [_c_vp, _c_sz, _c_vp, _c_vp],
+    "pkg_skyscraper_hash_many": [_c_sz, _c_vp, _c_sz, _c_vp, _c_vp],
+    "pkg_host_skyscraper_hash_many": [_c_sz, _c_vp, _c_sz, _c_vp],
+    "pkg_skyscraper_pow_solve": [_c_vp, _c_vp, _c_u64p],
+    "pkg_merkle_tree": [_c_vp, _c_sz, _c_sz, _c_vp, _c_vp],
+    "pkg_merkle_tree_fr": [_c_vp, _c_sz, _c_sz, _c_int, _c_vp, _c_vp],
+    "pkg_merkle_leaves_fr": [_c_vp, _c_sz, _c_sz, _c_int, _c_vp, _c_vp],
+    "pkg_merkle_levels": [_c_vp, _c_sz, _c_vp],
+    "pkg_whir_commit": [_c_vp, _c_sz, _c_uint, _c_uint, _c_vp, _c_sz, _c_int, _c_vp, _c_vp, _c_vp],
+    "pkg_measure_imad_rate": [ctypes.POINTER(ctypes.c_double)],
+    "pkg_version": [],
+}
+
+
+class PkgError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"provekit_b200 error {code}: {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m provekit_b200.build` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.pkg_last_error.restype = ctypes.c_char_p
+        L.pkg_last_error.argtypes = []
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.pkg_kernel_launches.argtypes = []
+        L.pkg_kernel_launches.restype = ctypes.c_uint64
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().pkg_last_error().decode()
+
+
+def check(rc: int):
+    if rc != PKG_OK:
+        raise PkgError(rc, last_error())
+    return rc
+
+
+def exported_symbols():
+    return sorted(SIGNATURES) + ["pkg_last_error", "pkg_kernel_launches"]

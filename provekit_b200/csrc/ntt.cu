@@ -1,0 +1,409 @@
+// ntt.cu -- BN254 Fr NTT for sm_100a: the ntt crate's ntt_nr / intt_rn
+// (ntt/src/ntt.rs:105-348) behind pkg_ntt_nr / pkg_intt_rn.
+//
+// Algorithm: the same radix-2 DIT, normal-in / bit-reversed-out transform as
+// interleaved_ntt_nr (ntt/src/ntt.rs:150-248).  At global stage t there are
+// 2^t groups; group k pairs element i with i + half and multiplies the odd
+// element by roots[k] from the bit-reversed twiddle table
+// (init_roots_reverse_ordered, ntt/src/ntt.rs:275-306).  Stages are fused into
+// passes of K <= 10 stages: a pass owns independent 2^K-point sub-transforms
+// ("lines": fixed top t row bits and fixed low row bits), stages each line in
+// shared memory, and runs its K stages there, so global memory is read and
+// written once per pass instead of once per stage.  Exact modular arithmetic
+// makes the output bit-identical to the stage-by-stage CPU order.
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "fr.cuh"
+#include "fr_host.hpp"
+#include "ntt_internal.cuh"
+#include "pk_common.cuh"
+
+namespace pk {
+
+// ---------------------------------------------------------------------------
+// Device-resident twiddle table (the NTTEngine, ntt/src/ntt.rs:24-95): one
+// grow-only table per device, roots[bitrev(i)] = w_order^i for i < order/2.
+// By the prefix property (ntt/src/ntt.rs:515-522) the first m/2 entries of
+// the table for any order >= m are the order-m table.
+// ---------------------------------------------------------------------------
+struct RootsTable {
+  uint64_t* d = nullptr;
+  size_t order = 0;
+};
+static std::mutex g_roots_mu;
+static std::vector<RootsTable> g_roots;
+
+__global__ void roots_kernel(uint64_t* __restrict__ roots, const uint64_t* __restrict__ w_lo,
+                             const uint64_t* __restrict__ w_hi, int log_half, int s) {
+  size_t n = size_t(1) << log_half;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    Fr lo = fr_load_ro(w_lo, i & ((size_t(1) << s) - 1));
+    Fr hi = fr_load_ro(w_hi, i >> s);
+    Fr w = fr_mul(lo, hi);
+    size_t r = __brevll((unsigned long long)i) >> (64 - log_half);
+    fr_store(roots, r, w);
+  }
+}
+
+int roots_reserve(size_t order, const uint64_t** out) {
+  if (order < 1024) order = 1024;  // NTTEngine::new() size (ntt/src/ntt.rs:30-33)
+  if (!is_pow2(order) || order > (size_t(1) << 28)) {
+    set_last_error("twiddle order %zu is not a power of two <= 2^28", order);
+    return PKG_ERR_INVALID_ARGUMENT;
+  }
+  int dev = 0;
+  PK_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_roots_mu);
+  if ((int)g_roots.size() <= dev) g_roots.resize(dev + 1);
+  RootsTable& tab = g_roots[dev];
+  if (tab.order >= order) {
+    *out = tab.d;
+    return PKG_OK;
+  }
+  // Grow: build the order-`order` table; in-flight users of the old table
+  // are drained first.
+  PK_CUDA(cudaDeviceSynchronize());
+  int log_half = log2_exact(order / 2);
+  int s = (log_half + 1) / 2;
+  size_t nlo = size_t(1) << s, nhi = size_t(1) << (log_half - s);
+  HostFr w = HostFr::root_of_unity(order);
+  std::vector<uint64_t> h_lo(4 * nlo), h_hi(4 * nhi);
+  HostFr acc = HostFr::one();
+  for (size_t i = 0; i < nlo; i++) {
+    memcpy(&h_lo[4 * i], acc.l, 32);
+    acc = HostFr::mul(acc, w);
+  }
+  HostFr step = acc;  // w^(2^s)
+  acc = HostFr::one();
+  for (size_t i = 0; i < nhi; i++) {
+    memcpy(&h_hi[4 * i], acc.l, 32);
+    acc = HostFr::mul(acc, step);
+  }
+  uint64_t *d_new = nullptr, *d_lo = nullptr, *d_hi = nullptr;
+  PK_CUDA(cudaMalloc(&d_new, 32 * (order / 2)));
+  cudaError_t e = cudaMalloc(&d_lo, 32 * nlo);
+  if (e == cudaSuccess) e = cudaMalloc(&d_hi, 32 * nhi);
+  if (e == cudaSuccess) e = cudaMemcpy(d_lo, h_lo.data(), 32 * nlo, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_hi, h_hi.data(), 32 * nhi, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    int blocks = (int)std::min<size_t>((order / 2 + 255) / 256, (size_t)sm_count() * 16);
+    roots_kernel<<<blocks, 256>>>(d_new, d_lo, d_hi, log_half, s);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(d_lo);
+  cudaFree(d_hi);
+  if (e != cudaSuccess) {
+    cudaFree(d_new);
+    return cuda_status(e, "twiddle table");
+  }
+  if (tab.d) cudaFree(tab.d);
+  tab.d = d_new;
+  tab.order = order;
+  *out = tab.d;
+  return PKG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Pass kernel.
+//
+// Row r of the transform (codeword position) has log2(N) bits.  A pass over
+// global stages [t, t+K) splits r = (high : j : low) with high = top t bits,
+// j = next K bits, low = remaining B bits.  With M interleaved columns, the
+// element (r, c) sits at r*M + c; "line" = (high, u) with u = low*M + c in
+// [0, U), U = 2^B * M, and line element j is at (high*2^K + j)*U + u.
+// A CTA owns T consecutive lines.  Mode A (T divides U): the lines share
+// `high` and are contiguous per j.  Mode B (U divides T, U a power of two):
+// the CTA's lines cover a contiguous memory range.
+// Stage s of the pass (global stage t+s) pairs j0 = grp*2h + pos with
+// j0 + h (h = 2^(K-1-s)) and uses twiddle roots[(high << s) | grp].
+// ---------------------------------------------------------------------------
+template <int K>
+__global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ data,
+                                                      const uint64_t* __restrict__ roots,
+                                                      uint64_t U, int log_u, int T, int log_t,
+                                                      int mode_b) {
+  extern __shared__ uint4 sm[];
+  constexpr int R = 1 << K;
+  const int E = R * T;
+  const uint64_t l0 = (uint64_t)blockIdx.x * T;
+  uint64_t high_a = 0, u0 = 0;
+  if (!mode_b) {
+    high_a = l0 / U;
+    u0 = l0 - high_a * U;
+  }
+  // ---- load ----
+  for (int e = threadIdx.x; e < E; e += blockDim.x) {
+    uint64_t g;
+    int sidx;
+    if (!mode_b) {
+      int j = e >> log_t, ll = e & (T - 1);
+      g = (high_a * R + j) * U + u0 + ll;
+      sidx = j * T + ll;
+    } else {
+      int j = (e >> log_u) & (R - 1);
+      int hl = e >> (log_u + K);
+      int u = e & ((1 << log_u) - 1);
+      g = (l0 >> log_u) * R * U + e;
+      sidx = j * T + (hl << log_u) + u;
+    }
+    const uint4* src = reinterpret_cast<const uint4*>(data + 4 * g);
+    sm[2 * sidx] = src[0];
+    sm[2 * sidx + 1] = src[1];
+  }
+  __syncthreads();
+  // ---- K radix-2 stages in shared memory ----
+#pragma unroll 1
+  for (int s = 0; s < K; s++) {
+    const int log_h = K - 1 - s;
+    for (int b = threadIdx.x; b < (E >> 1); b += blockDim.x) {
+      int ll = b & (T - 1);
+      int p = b >> log_t;
+      int grp = p >> log_h;
+      int pos = p & ((1 << log_h) - 1);
+      int j0 = (grp << (log_h + 1)) + pos;
+      int j1 = j0 + (1 << log_h);
+      uint64_t high = mode_b ? ((l0 + ll) >> log_u) : high_a;
+      Fr w = fr_load_ro(roots, (high << s) | (uint64_t)grp);
+      int i0 = j0 * T + ll, i1 = j1 * T + ll;
+      Fr x0, x1;
+      uint4 a = sm[2 * i0], bb = sm[2 * i0 + 1];
+      x0.v[0] = a.x; x0.v[1] = a.y; x0.v[2] = a.z; x0.v[3] = a.w;
+      x0.v[4] = bb.x; x0.v[5] = bb.y; x0.v[6] = bb.z; x0.v[7] = bb.w;
+      a = sm[2 * i1];
+      bb = sm[2 * i1 + 1];
+      x1.v[0] = a.x; x1.v[1] = a.y; x1.v[2] = a.z; x1.v[3] = a.w;
+      x1.v[4] = bb.x; x1.v[5] = bb.y; x1.v[6] = bb.z; x1.v[7] = bb.w;
+      Fr m = fr_mul(w, x1);
+      Fr y0 = fr_add(x0, m);
+      Fr y1 = fr_sub(x0, m);
+      sm[2 * i0] = make_uint4(y0.v[0], y0.v[1], y0.v[2], y0.v[3]);
+      sm[2 * i0 + 1] = make_uint4(y0.v[4], y0.v[5], y0.v[6], y0.v[7]);
+      sm[2 * i1] = make_uint4(y1.v[0], y1.v[1], y1.v[2], y1.v[3]);
+      sm[2 * i1 + 1] = make_uint4(y1.v[4], y1.v[5], y1.v[6], y1.v[7]);
+    }
+    __syncthreads();
+  }
+  // ---- store ----
+  for (int e = threadIdx.x; e < E; e += blockDim.x) {
+    uint64_t g;
+    int sidx;
+    if (!mode_b) {
+      int j = e >> log_t, ll = e & (T - 1);
+      g = (high_a * R + j) * U + u0 + ll;
+      sidx = j * T + ll;
+    } else {
+      int j = (e >> log_u) & (R - 1);
+      int hl = e >> (log_u + K);
+      int u = e & ((1 << log_u) - 1);
+      g = (l0 >> log_u) * R * U + e;
+      sidx = j * T + (hl << log_u) + u;
+    }
+    uint4* dst = reinterpret_cast<uint4*>(data + 4 * g);
+    dst[0] = sm[2 * sidx];
+    dst[1] = sm[2 * sidx + 1];
+  }
+}
+
+typedef void (*PassFn)(uint64_t*, const uint64_t*, uint64_t, int, int, int, int);
+static PassFn pass_fn(int k) {
+  switch (k) {
+    case 1: return ntt_pass_kernel<1>;
+    case 2: return ntt_pass_kernel<2>;
+    case 3: return ntt_pass_kernel<3>;
+    case 4: return ntt_pass_kernel<4>;
+    case 5: return ntt_pass_kernel<5>;
+    case 6: return ntt_pass_kernel<6>;
+    case 7: return ntt_pass_kernel<7>;
+    case 8: return ntt_pass_kernel<8>;
+    case 9: return ntt_pass_kernel<9>;
+    default: return ntt_pass_kernel<10>;
+  }
+}
+
+static inline uint64_t pow2_part(uint64_t x) { return x & (~x + 1); }
+
+// Run global stages [t_begin, t_end) of an N-point transform over M columns.
+int ntt_stages(uint64_t* data, size_t N, size_t M, int t_begin, int t_end, const uint64_t* roots,
+               cudaStream_t stream) {
+  const int S = log2_exact(N);
+  (void)S;
+  const int kmax = 9;
+  int total = t_end - t_begin;
+  if (total <= 0) return PKG_OK;
+  int npasses = (total + kmax - 1) / kmax;
+  int t = t_begin;
+  for (int pi = 0; pi < npasses; pi++) {
+    int K = (total - (t - t_begin) + (npasses - pi) - 1) / (npasses - pi);
+    int B = log2_exact(N) - t - K;
+    uint64_t U = (uint64_t(1) << B) * M;
+    uint64_t num_lines = (uint64_t(1) << t) * U;
+    // aim for ~512 elements per CTA
+    int log_tgt = K >= 9 ? 0 : 9 - K;
+    uint64_t T = uint64_t(1) << log_tgt;
+    if (T > num_lines) T = pow2_part(num_lines);
+    int mode_b = 0;
+    int log_u = 0;
+    if (is_pow2(U) && U < T) {
+      mode_b = 1;
+      log_u = log2_exact(U);
+    } else {
+      uint64_t pu = pow2_part(U);
+      if (T > pu) T = pu;
+    }
+    int log_t = log2_exact(T);
+    uint64_t E = (uint64_t(1) << K) * T;
+    int threads = (int)std::min<uint64_t>(E / 2, 512);
+    if (threads < 32) threads = 32;
+    size_t smem = 32 * E;
+    uint64_t grid = num_lines / T;
+    PassFn fn = pass_fn(K);
+    if (smem > 48 * 1024) {
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+    fn<<<(unsigned)grid, threads, smem, stream>>>(data, roots, U, log_u, (int)T, log_t, mode_b);
+    PK_CHECK_LAUNCH("ntt_pass_kernel");
+    t += K;
+  }
+  return PKG_OK;
+}
+
+// Validation shared by the device and host forms (reference panics ->
+// PKG_ERR_INVALID_ARGUMENT).  Returns 1 if there is nothing to do.
+int ntt_validate(size_t len, size_t codeword_size, size_t num_groups, int* noop) {
+  *noop = 0;
+  if (codeword_size <= 1) {  // ntt/src/ntt.rs:161-163
+    *noop = 1;
+    return PKG_OK;
+  }
+  PK_REQUIRE(num_groups != 0 && len % num_groups == 0,
+             "values.len() must be divisible by num_groups (len=%zu, num_groups=%zu)", len,
+             num_groups);
+  PK_REQUIRE(is_pow2(codeword_size), "codeword_size %zu is not a power of two", codeword_size);
+  PK_REQUIRE(is_pow2(num_groups), "num_groups %zu is not a power of two", num_groups);
+  PK_REQUIRE(len > 0 && len % codeword_size == 0,
+             "len %zu is not a positive multiple of codeword_size %zu", len, codeword_size);
+  PK_REQUIRE(codeword_size <= (size_t(1) << 28), "codeword_size %zu exceeds 2^28", codeword_size);
+  if (num_groups >= codeword_size) *noop = 1;
+  return PKG_OK;
+}
+
+int ntt_nr_device(uint64_t* values, size_t len, size_t codeword_size, size_t num_groups,
+                  cudaStream_t stream) {
+  int noop = 0;
+  int rc = ntt_validate(len, codeword_size, num_groups, &noop);
+  if (rc || noop) return rc;
+  PK_REQUIRE(values != nullptr, "null values pointer");
+  PK_REQUIRE(aligned16(values), "device buffers must be 16-byte aligned");
+  const uint64_t* roots = nullptr;
+  rc = roots_reserve(codeword_size, &roots);
+  if (rc) return rc;
+  size_t M = len / codeword_size;
+  return ntt_stages(values, codeword_size, M, log2_exact(num_groups), log2_exact(codeword_size),
+                    roots, stream);
+}
+
+// ---------------------------------------------------------------------------
+// intt_rn: reverse_order -> values[1..].reverse() -> ntt_nr -> * n^-1 ->
+// reverse_order (ntt/src/ntt.rs:326-348), as two gathers around the NTT:
+//   v2[i] = v0[bitrev((n - i) mod n)]             (in -> tmp)
+//   v4[i] = v3[bitrev(i)] * n^-1                   (tmp -> out)
+// ---------------------------------------------------------------------------
+__global__ void intt_gather_in(const uint64_t* __restrict__ src, uint64_t* __restrict__ dst,
+                               size_t n, int log_n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    size_t k = (n - i) & (n - 1);
+    size_t r = log_n ? (__brevll((unsigned long long)k) >> (64 - log_n)) : 0;
+    fr_store(dst, i, fr_load(src, r));
+  }
+}
+
+__global__ void intt_gather_out(const uint64_t* __restrict__ src, uint64_t* __restrict__ dst,
+                                size_t n, int log_n, Fr ninv) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    size_t r = log_n ? (__brevll((unsigned long long)i) >> (64 - log_n)) : 0;
+    fr_store(dst, i, fr_mul(fr_load(src, r), ninv));
+  }
+}
+
+int intt_rn_device(uint64_t* values, size_t len, cudaStream_t stream) {
+  PK_REQUIRE(is_pow2(len), "intt_rn length %zu is not a power of two", len);
+  PK_REQUIRE(len <= (size_t(1) << 28), "intt_rn length %zu exceeds 2^28", len);
+  PK_REQUIRE(values != nullptr, "null values pointer");
+  PK_REQUIRE(aligned16(values), "device buffers must be 16-byte aligned");
+  if (len == 1) return PKG_OK;  // both permutations and the scale are identities
+  Scratch tmp;
+  int rc = tmp.alloc(32 * len, stream);
+  if (rc) return rc;
+  uint64_t* t = static_cast<uint64_t*>(tmp.ptr);
+  int log_n = log2_exact(len);
+  int blocks = (int)std::min<size_t>((len + 255) / 256, (size_t)sm_count() * 16);
+  intt_gather_in<<<blocks, 256, 0, stream>>>(values, t, len, log_n);
+  PK_CHECK_LAUNCH("intt_gather_in");
+  rc = ntt_nr_device(t, len, len, 1, stream);
+  if (rc) return rc;
+  HostFr ninv = HostFr::inv(HostFr::from_u64(len));
+  Fr nv;
+  memcpy(nv.v, ninv.l, 32);
+  intt_gather_out<<<blocks, 256, 0, stream>>>(t, values, len, log_n, nv);
+  PK_CHECK_LAUNCH("intt_gather_out");
+  return PKG_OK;
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+extern "C" int pkg_ntt_nr(uint64_t* values, size_t len, size_t codeword_size, size_t num_groups,
+                          pkg_stream_t stream) {
+  return ntt_nr_device(values, len, codeword_size, num_groups, as_stream(stream));
+}
+
+extern "C" int pkg_intt_rn(uint64_t* values, size_t len, pkg_stream_t stream) {
+  return intt_rn_device(values, len, as_stream(stream));
+}
+
+extern "C" int pkg_ntt_engine_reserve(size_t order) {
+  const uint64_t* r = nullptr;
+  return roots_reserve(order, &r);
+}
+
+extern "C" int pkg_host_ntt_nr(uint64_t* values, size_t len, size_t codeword_size,
+                               size_t num_groups) {
+  int noop = 0;
+  int rc = ntt_validate(len, codeword_size, num_groups, &noop);
+  if (rc || noop) return rc;
+  PK_REQUIRE(values != nullptr, "null values pointer");
+  uint64_t* d = nullptr;
+  PK_CUDA(cudaMalloc(&d, 32 * len));
+  cudaError_t e = cudaMemcpy(d, values, 32 * len, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rc = ntt_nr_device(d, len, codeword_size, num_groups, 0);
+    if (!rc) e = cudaMemcpy(values, d, 32 * len, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_status(e, "pkg_host_ntt_nr");
+  return rc;
+}
+
+extern "C" int pkg_host_intt_rn(uint64_t* values, size_t len) {
+  PK_REQUIRE(is_pow2(len), "intt_rn length %zu is not a power of two", len);
+  PK_REQUIRE(values != nullptr, "null values pointer");
+  uint64_t* d = nullptr;
+  PK_CUDA(cudaMalloc(&d, 32 * len));
+  cudaError_t e = cudaMemcpy(d, values, 32 * len, cudaMemcpyHostToDevice);
+  int rc = PKG_OK;
+  if (e == cudaSuccess) {
+    rc = intt_rn_device(d, len, 0);
+    if (!rc) e = cudaMemcpy(values, d, 32 * len, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_status(e, "pkg_host_intt_rn");
+  return rc;
+}

@@ -1,0 +1,82 @@
+// pk_common.cuh -- status codes, last-error plumbing and launch helpers shared
+// by every translation unit of libprovekit_b200.
+//
+// Error conventions mirror the reference's FFI layer
+// (tooling/provekit-ffi/src/ffi.rs:29-95): every entry point returns an int
+// status (0 = ok, negative = error), nothing throws across the C ABI, and a
+// thread-local message is readable through pkg_last_error().
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/provekit_b200.h"
+
+namespace pk {
+
+void set_last_error(const char* fmt, ...);
+void clear_last_error();
+
+inline int cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return PKG_OK;
+  set_last_error("%s: %s", what, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? PKG_ERR_OUT_OF_MEMORY : PKG_ERR_CUDA;
+}
+
+#define PK_CUDA(call)                                              \
+  do {                                                             \
+    cudaError_t _e = (call);                                       \
+    if (_e != cudaSuccess) return ::pk::cuda_status(_e, #call);    \
+  } while (0)
+
+void count_launch();
+
+#define PK_CHECK_LAUNCH(name) \
+  do {                        \
+    ::pk::count_launch();     \
+    PK_CUDA(cudaGetLastError()); \
+  } while (0)
+
+#define PK_REQUIRE(cond, ...)                  \
+  do {                                         \
+    if (!(cond)) {                             \
+      ::pk::set_last_error(__VA_ARGS__);       \
+      return PKG_ERR_INVALID_ARGUMENT;         \
+    }                                          \
+  } while (0)
+
+inline bool is_pow2(size_t n) { return n && !(n & (n - 1)); }
+inline int log2_exact(size_t n) {
+  int k = 0;
+  while ((size_t(1) << k) < n) k++;
+  return k;
+}
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+inline cudaStream_t as_stream(pkg_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+// Stream-ordered scratch allocation (cudaMallocAsync), freed on scope exit
+// in stream order.
+struct Scratch {
+  void* ptr = nullptr;
+  cudaStream_t stream = nullptr;
+  Scratch() = default;
+  Scratch(const Scratch&) = delete;
+  Scratch& operator=(const Scratch&) = delete;
+  int alloc(size_t bytes, cudaStream_t s) {
+    stream = s;
+    if (bytes == 0) return PKG_OK;
+    PK_CUDA(cudaMallocAsync(&ptr, bytes, s));
+    return PKG_OK;
+  }
+  ~Scratch() {
+    if (ptr) cudaFreeAsync(ptr, stream);
+  }
+};
+
+}  // namespace pk

@@ -1,0 +1,152 @@
+// runtime.cu -- library-wide plumbing: last-error storage, version, device
+// properties, the host-side Fr sampler and the IMAD-rate microbenchmark.
+#include <atomic>
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "fr.cuh"
+#include "fr_host.hpp"
+#include "pk_common.cuh"
+
+namespace pk {
+
+static thread_local char g_last_error[512] = "";
+
+void set_last_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof g_last_error, fmt, ap);
+  va_end(ap);
+}
+
+void clear_last_error() { g_last_error[0] = 0; }
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+int sm_count() {
+  static std::mutex mu;
+  static std::vector<int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)cache.size() <= dev) cache.resize(dev + 1, 0);
+  if (!cache[dev]) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cache[dev] = n > 0 ? n : 148;
+  }
+  return cache[dev];
+}
+
+// ---------------------------------------------------------------------------
+// ChaCha20 sampler (RFC 8439 section 2.3 block function).
+// ---------------------------------------------------------------------------
+static inline uint32_t rotl32(uint32_t x, int n) { return (x << n) | (x >> (32 - n)); }
+
+static void chacha20_block(const uint32_t key[8], uint64_t counter, uint32_t out[16]) {
+  const uint32_t s[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u,
+                          key[0], key[1], key[2], key[3], key[4], key[5], key[6], key[7],
+                          (uint32_t)counter, (uint32_t)(counter >> 32), 0u, 0u};
+  uint32_t x[16];
+  memcpy(x, s, sizeof x);
+  auto qr = [&](int a, int b, int c, int d) {
+    x[a] += x[b]; x[d] ^= x[a]; x[d] = rotl32(x[d], 16);
+    x[c] += x[d]; x[b] ^= x[c]; x[b] = rotl32(x[b], 12);
+    x[a] += x[b]; x[d] ^= x[a]; x[d] = rotl32(x[d], 8);
+    x[c] += x[d]; x[b] ^= x[c]; x[b] = rotl32(x[b], 7);
+  };
+  for (int i = 0; i < 10; i++) {
+    qr(0, 4, 8, 12); qr(1, 5, 9, 13); qr(2, 6, 10, 14); qr(3, 7, 11, 15);
+    qr(0, 5, 10, 15); qr(1, 6, 11, 12); qr(2, 7, 8, 13); qr(3, 4, 9, 14);
+  }
+  for (int i = 0; i < 16; i++) out[i] = x[i] + s[i];
+}
+
+// ---------------------------------------------------------------------------
+// IMAD microbenchmark: 8 independent mad.lo.cc/madc.hi.cc chains per thread.
+// ---------------------------------------------------------------------------
+__global__ void imad_rate_kernel(uint32_t* sink, uint32_t seed, int iters) {
+  uint32_t a0 = seed ^ threadIdx.x, a1 = a0 * 3u + 1u, a2 = a1 * 5u + 7u, a3 = a2 * 9u + 3u;
+  uint32_t b = seed * 0x9e3779b9u + blockIdx.x;
+  uint32_t c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0, c7 = 0;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      asm volatile(
+          "mad.lo.cc.u32  %0, %8,  %12, %0;\n\t"
+          "madc.hi.cc.u32 %1, %8,  %12, %1;\n\t"
+          "madc.lo.cc.u32 %2, %9,  %12, %2;\n\t"
+          "madc.hi.cc.u32 %3, %9,  %12, %3;\n\t"
+          "madc.lo.cc.u32 %4, %10, %12, %4;\n\t"
+          "madc.hi.cc.u32 %5, %10, %12, %5;\n\t"
+          "madc.lo.cc.u32 %6, %11, %12, %6;\n\t"
+          "madc.hi.u32    %7, %11, %12, %7;"
+          : "+r"(c0), "+r"(c1), "+r"(c2), "+r"(c3), "+r"(c4), "+r"(c5), "+r"(c6), "+r"(c7)
+          : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b));
+    }
+  }
+  uint32_t s = c0 ^ c1 ^ c2 ^ c3 ^ c4 ^ c5 ^ c6 ^ c7;
+  if (s == 0x12345678u) sink[threadIdx.x] = s;
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+extern "C" const char* pkg_last_error(void) { return g_last_error; }
+
+extern "C" int pkg_version(void) { return 100; }
+
+extern "C" uint64_t pkg_kernel_launches(void) { return g_launches.load(); }
+
+extern "C" int pkg_sample_fr(uint64_t seed, size_t n, uint64_t* out, int mont) {
+  if (n && !out) {
+    set_last_error("pkg_sample_fr: null output");
+    return PKG_ERR_INVALID_ARGUMENT;
+  }
+  const uint32_t key[8] = {(uint32_t)seed, (uint32_t)(seed >> 32), 0, 0, 0, 0, 0, 0};
+  uint64_t counter = 0;
+  size_t got = 0;
+  uint32_t blk[16];
+  while (got < n) {
+    chacha20_block(key, counter++, blk);
+    for (int h = 0; h < 2 && got < n; h++) {
+      HostFr v;
+      for (int i = 0; i < 4; i++)
+        v.l[i] = (uint64_t)blk[8 * h + 2 * i] | ((uint64_t)blk[8 * h + 2 * i + 1] << 32);
+      v.l[3] &= 0x3fffffffffffffffULL;
+      if (!v.is_canonical()) continue;
+      if (mont) v = HostFr::to_mont(v);
+      memcpy(out + 4 * got, v.l, 32);
+      got++;
+    }
+  }
+  return PKG_OK;
+}
+
+extern "C" int pkg_measure_imad_rate(double* instr_per_second) {
+  if (!instr_per_second) return PKG_ERR_INVALID_ARGUMENT;
+  uint32_t* sink = nullptr;
+  PK_CUDA(cudaMalloc(&sink, 1024 * sizeof(uint32_t)));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int threads = 256, blocks = sm_count() * 8, iters = 4096;
+  imad_rate_kernel<<<blocks, threads>>>(sink, 1u, 64);  // warm-up
+  cudaEventRecord(e0);
+  imad_rate_kernel<<<blocks, threads>>>(sink, 2u, iters);
+  cudaEventRecord(e1);
+  cudaError_t err = cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  if (err != cudaSuccess) return cuda_status(err, "imad_rate_kernel");
+  double instr = (double)blocks * threads * iters * 8.0 * 8.0;
+  *instr_per_second = instr / (ms * 1e-3);
+  return PKG_OK;
+}

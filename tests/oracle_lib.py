@@ -1,0 +1,126 @@
+"""ctypes binding of the C oracle (oracle/libpk_oracle.so).  Test
+infrastructure: used only to check the CUDA path and as the timed CPU
+baseline."""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+from oracle.build import build as _build_oracle  # noqa: E402
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_sz = ctypes.c_size_t
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(_build_oracle())
+        L = _lib
+        L.pko_fr_mul.argtypes = [_u64p, _u64p, _u64p]
+        L.pko_sample_fr.argtypes = [ctypes.c_uint64, _sz, _u64p, ctypes.c_int]
+        L.pko_ntt_nr.argtypes = [_u64p, _sz, _sz, _sz]
+        L.pko_intt_rn.argtypes = [_u64p, _sz]
+        L.pko_roots_reverse_ordered.argtypes = [_u64p, _sz]
+        L.pko_rs_interleaved_encode.argtypes = [_u64p, _sz, _sz, _u64p, _sz, _sz, _u64p]
+        L.pko_rs_evaluation_points.argtypes = [_sz, ctypes.POINTER(_sz), _sz, _u64p]
+        L.pko_sky_compress.argtypes = [_u64p, _u64p, _u64p]
+        L.pko_sky_compress_many.argtypes = [_u8p, _sz, _u8p]
+        L.pko_sky_permute.argtypes = [_u64p, _u64p]
+        L.pko_sky_ss.argtypes = [ctypes.c_int, _u64p, _u64p]
+        L.pko_sky_bb.argtypes = [ctypes.c_int, _u64p, _u64p]
+        L.pko_sky_sbox.argtypes = [ctypes.c_uint8]
+        L.pko_sky_sbox.restype = ctypes.c_uint8
+        L.pko_hash_many.argtypes = [_sz, _u8p, _sz, _u8p]
+        L.pko_merkle_tree.argtypes = [_u8p, _sz, _sz, _u8p]
+        L.pko_sky_pow_solve.argtypes = [_u64p, _u64p]
+        L.pko_sky_pow_solve.restype = ctypes.c_uint64
+        L.pko_calculate_eq.argtypes = [_u64p, _u64p, _u64p, _sz]
+        L.pko_eq_hypercube.argtypes = [_u64p, _sz, _sz, _u64p]
+        L.pko_spartan_round.argtypes = [_u64p, _u64p, _u64p, _u64p, _sz, _u64p, _u64p]
+        L.pko_spmv.argtypes = [_u64p, _u32p, _u64p, _sz, _u64p, _u64p]
+        L.pko_eval_cubic.argtypes = [_u64p, _u64p, _u64p]
+        L.pko_blinding_coeffs.argtypes = [_u64p, _sz, _sz, _u64p, _u64p]
+        L.pko_dot.argtypes = [_u64p, _u64p, _u64p, _sz]
+        L.pko_num_threads.restype = ctypes.c_int
+    return _lib
+
+
+def p64(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u64p)
+
+
+def p8(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u8p)
+
+
+def p32(a: np.ndarray):
+    assert a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u32p)
+
+
+def sample_fr(seed: int, n: int, mont: bool = True) -> np.ndarray:
+    out = np.zeros((max(n, 1), 4), dtype=np.uint64)
+    lib().pko_sample_fr(seed, n, p64(out), int(mont))
+    return out[:n]
+
+
+def ntt_nr(values: np.ndarray, codeword_size: int, num_groups: int) -> int:
+    v = values.reshape(-1, 4)
+    return lib().pko_ntt_nr(p64(v), v.shape[0], codeword_size, num_groups)
+
+
+def intt_rn(values: np.ndarray) -> int:
+    v = values.reshape(-1, 4)
+    return lib().pko_intt_rn(p64(v), v.shape[0])
+
+
+def roots(order: int) -> np.ndarray:
+    out = np.zeros((max(order // 2, 1), 4), dtype=np.uint64)
+    lib().pko_roots_reverse_ordered(p64(out), order)
+    return out[: order // 2]
+
+
+def rs_interleaved_encode(messages: np.ndarray, masks: np.ndarray, codeword_length: int):
+    """messages: (M, L, 4) uint64; masks: (k, 4).  Returns (rc, out)."""
+    M, L = messages.shape[0], messages.shape[1]
+    out = np.zeros((max(M * codeword_length, 1), 4), dtype=np.uint64)
+    msg = np.ascontiguousarray(messages.reshape(-1, 4)) if messages.size else np.zeros((1, 4), np.uint64)
+    mk = np.ascontiguousarray(masks.reshape(-1, 4)) if masks.size else np.zeros((1, 4), np.uint64)
+    rc = lib().pko_rs_interleaved_encode(p64(msg), M, L, p64(mk), masks.reshape(-1, 4).shape[0],
+                                         codeword_length, p64(out))
+    return rc, out[: M * codeword_length]
+
+
+def hash_many(size: int, data: bytes, count: int) -> bytes:
+    inp = np.frombuffer(data, dtype=np.uint8).copy() if len(data) else np.zeros(1, np.uint8)
+    out = np.zeros(max(32 * count, 1), dtype=np.uint8)
+    rc = lib().pko_hash_many(size, p8(inp), count, p8(out))
+    assert rc == 0, rc
+    return out[: 32 * count].tobytes()
+
+
+def merkle_tree(leaves: bytes, leaf_size: int, count: int) -> bytes:
+    inp = np.frombuffer(leaves, dtype=np.uint8).copy()
+    out = np.zeros(32 * (2 * count - 1), dtype=np.uint8)
+    rc = lib().pko_merkle_tree(p8(inp), leaf_size, count, p8(out))
+    assert rc == 0, rc
+    return out.tobytes()
+
+
+def compress(l, r):
+    a = np.array(l, dtype=np.uint64)
+    b = np.array(r, dtype=np.uint64)
+    o = np.zeros(4, dtype=np.uint64)
+    lib().pko_sky_compress(p64(o), p64(a), p64(b))
+    return [int(x) for x in o]

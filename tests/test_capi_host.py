@@ -1,0 +1,95 @@
+"""CPU-side checks of the C ABI: the library loads, exports every symbol the
+header declares, and its host-only logic (sampler, RS planning, argument
+validation) agrees with the oracle.  No GPU compute is launched here."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from fieldutil import P, R, from_limbs, root_of_unity, unpack
+import oracle_lib as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def L():
+    from provekit_b200 import build
+    build.build()
+    from provekit_b200 import _lib
+    return _lib.lib()
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "provekit_b200.h")).read()
+    return sorted(set(re.findall(r"\b(pkg_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_symbols_exported(L):
+    from provekit_b200 import _lib
+    declared = header_symbols()
+    assert declared, "no declarations parsed"
+    for name in declared:
+        assert hasattr(L, name), f"{name} declared but not exported"
+    # the Python binding covers every declared entry point
+    assert set(declared) <= set(_lib.exported_symbols())
+
+
+def test_sampler_matches_oracle(L):
+    for seed, n in [(1, 1), (2, 100), (3, 4097)]:
+        a = np.zeros((n, 4), np.uint64)
+        assert L.pkg_sample_fr(seed, n, a.ctypes.data, 1) == 0
+        assert np.array_equal(a, O.sample_fr(seed, n, mont=True))
+        b = np.zeros((n, 4), np.uint64)
+        assert L.pkg_sample_fr(seed, n, b.ctypes.data, 0) == 0
+        assert np.array_equal(b, O.sample_fr(seed, n, mont=False))
+
+
+def test_rs_host_helpers_match_oracle(L):
+    from provekit_b200.rs import RSFr
+    rs = RSFr()
+    assert rs.next_order(0) == 1 and rs.next_order(5) == 8 and rs.next_order(1 << 28) == 1 << 28
+    assert rs.next_order((1 << 28) + 1) is None
+    for n in (1, 2, 1024, 1 << 20):
+        g = rs.generator(n)
+        assert unpack(g.reshape(1, 4))[0] == root_of_unity(n)
+    for cw in (1, 2, 16, 64):
+        idx = list(range(cw)) + [cw + 3]
+        got = rs.evaluation_points(0, cw, idx)
+        exp = np.zeros((len(idx), 4), np.uint64)
+        arr = (ctypes.c_size_t * len(idx))(*idx)
+        O.lib().pko_rs_evaluation_points(cw, arr, len(idx), O.p64(exp))
+        assert np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("len_,cw,groups", [(8, 6, 1), (8, 8, 0), (8, 8, 3), (6, 4, 1), (0, 4, 1)])
+def test_ntt_validation_rejects_like_reference(L, len_, cw, groups):
+    """Contract violations the reference panics on come back as
+    PKG_ERR_INVALID_ARGUMENT before any device work."""
+    assert L.pkg_ntt_nr(None, len_, cw, groups, None) == -1
+    assert L.pkg_last_error()
+
+
+def test_ntt_noop_cases_need_no_device(L):
+    assert L.pkg_ntt_nr(None, 0, 0, 1, None) == 0   # ntt_empty
+    assert L.pkg_ntt_nr(None, 4, 1, 1, None) == 0   # codeword_size <= 1
+
+
+def test_hash_many_rejects_bad_sizes(L):
+    for size in (0, 1, 31, 33):
+        assert L.pkg_skyscraper_hash_many(size, None, 1, None, None) == -1
+        assert b"unsupported message size" in L.pkg_last_error()
+
+
+def test_rs_encode_validation(L):
+    assert L.pkg_rs_interleaved_encode(None, 0, 4, None, 0, 16, None, None) == 0  # no messages
+    assert L.pkg_rs_interleaved_encode(None, 2, 32, None, 0, 16, None, None) == -1
+    assert L.pkg_rs_interleaved_encode(None, 2, 8, None, 32, 16, None, None) == -1
+    assert L.pkg_rs_interleaved_encode(None, 3, 4, None, 0, 12, None, None) == -1
+
+
+def test_merkle_requires_power_of_two_leaves(L):
+    assert L.pkg_merkle_tree_fr(None, 4, 6, 0, None, None) == -1
+    assert L.pkg_merkle_tree_fr(None, 4, 8, 7, None, None) == -1
