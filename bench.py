@@ -27,6 +27,10 @@ METRIC = ("WHIR commit throughput, Spartan+WHIR prover hot path: 2^20 Fr coeffic
           "RS rate-1/4 coset NTT -> 2^22 evaluations -> Skyscraper Merkle tree (bit-exact)")
 UNIT = "commits/s"
 IMAD_PER_MONT = 264  # mad.lo/madc.hi/mul.lo per 8x32 CIOS product (fr.cuh: 8 x (16 + 16 + 1))
+# dram__bytes_read.sum + dram__bytes_write.sum of one leaf_fold_fr_kernel launch
+# from an ncu capture of this workload (profiles/leaf_fold_fr_kernel_whir_commit_2p20.md),
+# keyed by (log2 coeffs, folding factor, log inv rate).
+LEAF_TRAFFIC_BYTES = {(20, 4, 2): 134.672896e6 + 6.241024e6}
 
 
 def parse_args():
@@ -395,7 +399,9 @@ def run_b200(a):
         "roofline": {
             "kernel": "leaf_fold_fr_kernel (Skyscraper leaf hashing)", "bound": "int",
             "achieved": achieved / 1e9, "peak": mont_peak / 1e9, "unit": "Gmont/s",
-            "frac": achieved / mont_peak, "traffic": None,
+            "frac": achieved / mont_peak,
+            "traffic": LEAF_TRAFFIC_BYTES.get((a.log_coeffs, a.folding_factor, a.log_inv_rate)),
+            "traffic_algorithmic": 32 * total_fr + 32 * num_leaves,
             "peak_source": f"measured IMAD-class rate {imad.value / 1e12:.3f} T/s "
                            f"(pkg_measure_imad_rate) / {IMAD_PER_MONT} per CIOS product",
             "algorithmic": f"{num_leaves} leaves x ({M - 1} compressions x 14 squarings + {M} "
