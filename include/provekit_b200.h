@@ -75,6 +75,21 @@ int pkg_intt_rn(uint64_t *values, size_t len, pkg_stream_t stream);
  * Replaces `NTTEngine::with_order` (ntt/src/ntt.rs:39-45).  Growing
  * synchronises the current device. */
 int pkg_ntt_engine_reserve(size_t order);
+/* pkg_intt_rn for callers that cannot let this library allocate device
+ * memory (a service that reserves all HBM for its own admission control, or
+ * an application whose framework allocator owns the free memory; cudaMalloc
+ * and cudaFree may also synchronise the device).  No counterpart in the
+ * reference.  Same result as pkg_intt_rn; calls no cudaMalloc/cudaFree or
+ * allocating library routine.  Its scratch (twiddles + gather buffer) is one
+ * fixed 3 MiB __device__ array in the library, held by every GPU that loads
+ * it until exit, so len is limited to 2^16 (larger lengths return
+ * PKG_ERR_INVALID_ARGUMENT).  All calls share that array: calls whose work
+ * overlaps on the GPU (other streams, other host threads) race; serialise
+ * them.  Each call writes every scratch word it reads, so no state carries
+ * over between calls.  The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture.  Device pointer. */
+int pkg_intt_rn_noalloc(uint64_t *values, size_t len, pkg_stream_t stream);
 /* Host-slice forms of the two calls above (synchronous). */
 int pkg_host_ntt_nr(uint64_t *values, size_t len, size_t codeword_size, size_t num_groups);
 int pkg_host_intt_rn(uint64_t *values, size_t len);

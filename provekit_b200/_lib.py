@@ -31,6 +31,7 @@ SIGNATURES = {
     "pkg_sample_fr": [ctypes.c_uint64, _c_sz, _c_vp, _c_int],
     "pkg_ntt_nr": [_c_vp, _c_sz, _c_sz, _c_sz, _c_vp],
     "pkg_intt_rn": [_c_vp, _c_sz, _c_vp],
+    "pkg_intt_rn_noalloc": [_c_vp, _c_sz, _c_vp],
     "pkg_ntt_engine_reserve": [_c_sz],
     "pkg_host_ntt_nr": [_c_vp, _c_sz, _c_sz, _c_sz],
     "pkg_host_intt_rn": [_c_vp, _c_sz],
