@@ -162,6 +162,69 @@ int pkg_whir_commit(const uint64_t *coeffs, size_t num_coeffs, unsigned folding_
                     int leaf_encoding, uint64_t *codeword_out, uint8_t *layers_out,
                     pkg_stream_t stream);
 
+/* ---- Spartan sumcheck side (provekit/common/src/utils/sumcheck.rs,
+ *      provekit/prover/src/whir_r1cs.rs) -------------------------------- */
+/* Fiat-Shamir transcript.  The reference's is spongefish's DuplexSponge over
+ * skyscraper::reference::permute (provekit/common/src/skyscraper/sponge.rs:27-41,
+ * transcript_sponge.rs:19-111); spongefish is not available, so this is a
+ * minimal duplex over the same permutation: state (l, r) canonical;
+ * init: l = domain mod p, r = 0, permute; absorb(x): l += x (canonical),
+ * permute; squeeze: permute, return l (Montgomery form).  Host only. */
+typedef struct {
+  uint64_t l[4];
+  uint64_t r[4];
+} pkg_transcript;
+int pkg_transcript_init(pkg_transcript *t, const uint64_t domain[4]);
+int pkg_transcript_absorb(pkg_transcript *t, const uint64_t x[4]);
+int pkg_transcript_squeeze(pkg_transcript *t, uint64_t out[4]);
+
+/* eq(r, x) for x < num_entries over the nr-variable hypercube, r_0 on the
+ * most significant bit (calculate_evaluations_over_boolean_hypercube_for_eq,
+ * sumcheck.rs:108-153).  r: host; out: device. */
+int pkg_eq_hypercube(const uint64_t *r, size_t nr, size_t num_entries, uint64_t *out,
+                     pkg_stream_t stream);
+/* One round of the Spartan map-reduce (the closure at whir_r1cs.rs:551-559 over
+ * sumcheck_fold_map_reduce, sumcheck.rs:14-102) on device tables a, b, c, eq of
+ * length size.  fold (host, or NULL): fold the top variable first in the
+ * quarter layout (tables then hold size/2 live entries).  out (host): f(0),
+ * f(-1), f(inf).  Synchronous. */
+int pkg_spartan_round(uint64_t *a, uint64_t *b, uint64_t *c, uint64_t *eq, size_t size,
+                      const uint64_t *fold, uint64_t out[12], pkg_stream_t stream);
+/* run_zk_sumcheck_prover (whir_r1cs.rs:519-621): m0 rounds over device tables
+ * a, b, c of length 2^m0 (modified in place), blinding polynomial g (host,
+ * m0 x 4 Fr), w1_blinding = w1[offset .. offset + 4*m0] (host).  Drives the
+ * transcript (in/out) and returns r (m0), rho, sum_g, the 4*m0 round
+ * coefficients, alpha (m0) and the blinding evaluation (all host).
+ * Synchronous (one device->host read of 3 Fr per round). */
+int pkg_spartan_sumcheck(uint64_t *a, uint64_t *b, uint64_t *c, size_t m0, const uint64_t *g,
+                         const uint64_t *w1_blinding, pkg_transcript *transcript,
+                         uint64_t *r_out, uint64_t rho_out[4], uint64_t sum_g_out[4],
+                         uint64_t *coeffs_out, uint64_t *alpha_out, uint64_t blinding_eval[4],
+                         pkg_stream_t stream);
+/* y = M x for a CSR matrix with one Fr per nonzero (HydratedSparseMatrix *
+ * &[Fr], provekit/common/src/sparse_matrix.rs:606-627); x has num_cols
+ * entries.  A column index >= num_cols (a reference panic) is skipped on the
+ * device and reported as PKG_ERR_INVALID_ARGUMENT.  Device pointers;
+ * synchronous (reads back that flag). */
+int pkg_spmv_csr(const uint64_t *row_ptr, const uint32_t *cols, const uint64_t *vals,
+                 size_t num_rows, size_t num_cols, const uint64_t *x, uint64_t *y,
+                 pkg_stream_t stream);
+/* CSR transpose (SparseMatrix::transpose, sparse_matrix.rs:409): row_ptr_t
+ * has num_cols + 1 entries; the order of entries inside a transposed row is
+ * unspecified (SpMV results do not depend on it).  Out-of-range column
+ * indices are skipped and reported as PKG_ERR_INVALID_ARGUMENT.  Device
+ * pointers; synchronous. */
+int pkg_csr_transpose(const uint64_t *row_ptr, const uint32_t *cols, const uint64_t *vals,
+                      size_t num_rows, size_t num_cols, size_t nnz, uint64_t *row_ptr_t,
+                      uint32_t *cols_t, uint64_t *vals_t, pkg_stream_t stream);
+/* c[i] = a[i] * b[i] for i < n, 0 for n <= i < padded (calculate_witness_bounds,
+ * sumcheck.rs:163-179).  Device pointers. */
+int pkg_hadamard_pad(const uint64_t *a, const uint64_t *b, size_t n, size_t padded,
+                     uint64_t *c, pkg_stream_t stream);
+/* sum_i a[i] * b[i] (whir::algebra::dot as used at whir_r1cs.rs:614-617, 637,
+ * 650).  a, b device; out host; synchronous. */
+int pkg_dot(const uint64_t *a, const uint64_t *b, size_t n, uint64_t out[4], pkg_stream_t stream);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 /* Number of kernels this library has launched in this process. */
 uint64_t pkg_kernel_launches(void);

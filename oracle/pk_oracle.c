@@ -829,3 +829,101 @@ int pko_num_threads(void) {
     return 1;
 #endif
 }
+
+/* ======================================================================= */
+/* Transcript stand-in and the Spartan zk-sumcheck driver                  */
+/* ======================================================================= */
+void pko_transcript_init(pko_transcript *t, const uint64_t domain[4]) {
+    cpy4(t->l, domain);
+    reduce_full(t->l);
+    memset(t->r, 0, 32);
+    pko_sky_permute(t->l, t->r);
+}
+
+void pko_transcript_absorb(pko_transcript *t, const uint64_t x_mont[4]) {
+    uint64_t v[4];
+    pko_fr_from_mont(v, x_mont);
+    pko_fr_add(t->l, t->l, v);
+    pko_sky_permute(t->l, t->r);
+}
+
+void pko_transcript_squeeze(pko_transcript *t, uint64_t out_mont[4]) {
+    pko_sky_permute(t->l, t->r);
+    pko_fr_to_mont(out_mont, t->l);
+}
+
+int pko_spartan_sumcheck(pko_transcript *t, uint64_t *a, uint64_t *b, uint64_t *c, size_t m0,
+                         const uint64_t *g, const uint64_t *w1, size_t blinding_offset,
+                         uint64_t *r_out, uint64_t rho_out[4], uint64_t sum_g_out[4],
+                         uint64_t *coeffs_out, uint64_t *alpha_out, uint64_t blinding_eval[4]) {
+    if (m0 < 1 || m0 > 30) return -1;
+    size_t n = (size_t)1 << m0;
+    for (size_t i = 0; i < m0; i++) pko_transcript_squeeze(t, r_out + 4 * i);   /* :529 */
+    uint64_t *eq = (uint64_t *)malloc(32 * n);
+    if (!eq) return -2;
+    pko_eq_hypercube(r_out, m0, n, eq);                                        /* :530 */
+    /* sum_over_hypercube (whir_r1cs.rs:494-501) */
+    uint64_t g0[16], t0[4], t1[4], sum_g[4];
+    static const uint64_t zero[4] = {0, 0, 0, 0};
+    pko_blinding_coeffs(g, m0, 0, NULL, g0);
+    pko_eval_cubic(t0, g0, zero);
+    pko_eval_cubic(t1, g0, ONE_MONT);
+    pko_fr_add(sum_g, t0, t1);
+    cpy4(sum_g_out, sum_g);
+    pko_transcript_absorb(t, sum_g);                                           /* :541 */
+    uint64_t rho[4];
+    pko_transcript_squeeze(t, rho);                                            /* :543 */
+    cpy4(rho_out, rho);
+    uint64_t saved[4];
+    pko_fr_mul(saved, rho, sum_g);                                             /* :546 */
+    uint64_t half[4], two[4];
+    pko_fr_add(two, ONE_MONT, ONE_MONT);
+    pko_fr_inv(half, two);
+    size_t size = n;
+    for (size_t idx = 0; idx < m0; idx++) {                                    /* :550-610 */
+        uint64_t h[12];
+        int rc = pko_spartan_round(a, b, c, eq, size, idx ? alpha_out + 4 * (idx - 1) : NULL, h);
+        if (rc) { free(eq); return rc; }
+        if (idx) size /= 2;
+        uint64_t gp[16];
+        pko_blinding_coeffs(g, m0, idx, alpha_out, gp);
+        uint64_t cf[16], tmp[4], gem1[4], cem1[4];
+        pko_fr_mul(tmp, rho, gp);
+        pko_fr_add(cf, h, tmp);                                   /* c0 */
+        pko_fr_sub(gem1, gp, gp + 4);
+        pko_fr_add(gem1, gem1, gp + 8);
+        pko_fr_sub(gem1, gem1, gp + 12);
+        pko_fr_mul(tmp, rho, gem1);
+        pko_fr_add(cem1, h + 4, tmp);
+        pko_fr_add(tmp, saved, cem1);
+        pko_fr_sub(tmp, tmp, cf);
+        pko_fr_sub(tmp, tmp, cf);
+        pko_fr_sub(tmp, tmp, cf);
+        pko_fr_mul(cf + 8, half, tmp);                            /* c2 */
+        pko_fr_mul(tmp, rho, gp + 12);
+        pko_fr_add(cf + 12, h + 8, tmp);                          /* c3 */
+        pko_fr_sub(tmp, saved, cf);
+        pko_fr_sub(tmp, tmp, cf);
+        pko_fr_sub(tmp, tmp, cf + 12);
+        pko_fr_sub(cf + 4, tmp, cf + 8);                          /* c1 */
+        memcpy(coeffs_out + 16 * idx, cf, 128);
+        for (int k = 0; k < 4; k++) pko_transcript_absorb(t, cf + 4 * k);
+        pko_transcript_squeeze(t, alpha_out + 4 * idx);
+        pko_eval_cubic(saved, cf, alpha_out + 4 * idx);
+    }
+    free(eq);
+    /* blinding_eval = <expand_powers::<4>(alpha), w1[offset..]> (:613-618) */
+    uint64_t acc[4] = {0, 0, 0, 0};
+    for (size_t i = 0; i < m0; i++) {
+        uint64_t pw[4], tt[4];
+        cpy4(pw, ONE_MONT);
+        for (int k = 0; k < 4; k++) {
+            pko_fr_mul(tt, pw, w1 + 4 * (blinding_offset + 4 * i + k));
+            pko_fr_add(acc, acc, tt);
+            pko_fr_mul(pw, pw, alpha_out + 4 * i);
+        }
+    }
+    cpy4(blinding_eval, acc);
+    pko_transcript_absorb(t, acc);
+    return 0;
+}

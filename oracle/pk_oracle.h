@@ -86,6 +86,28 @@ void pko_blinding_coeffs(const uint64_t *g, size_t n, size_t compute_for,
                          const uint64_t *alphas, uint64_t out[16]);
 void pko_dot(uint64_t out[4], const uint64_t *a, const uint64_t *b, size_t n);
 
+/* ---- Fiat-Shamir transcript stand-in ------------------------------------ */
+/* The reference's transcript is spongefish's DuplexSponge over
+ * skyscraper::reference::permute (provekit/common/src/skyscraper/sponge.rs:27-41);
+ * spongefish is not available, so its byte layout is replaced by this
+ * minimal duplex: state (l, r) canonical; init: l = domain mod p, r = 0,
+ * permute; absorb(x): l += canonical(x), permute; squeeze: permute, return l
+ * (Montgomery form out). */
+typedef struct { uint64_t l[4], r[4]; } pko_transcript;
+void pko_transcript_init(pko_transcript *t, const uint64_t domain[4]);
+void pko_transcript_absorb(pko_transcript *t, const uint64_t x_mont[4]);
+void pko_transcript_squeeze(pko_transcript *t, uint64_t out_mont[4]);
+
+/* run_zk_sumcheck_prover (provekit/prover/src/whir_r1cs.rs:519-621) over
+ * tables a, b, c of length 2^m0 (already padded; modified in place), the
+ * blinding polynomial g (m0 x 4 Fr) and the w1 polynomial (blinding
+ * coefficients at blinding_offset).  Outputs: r (m0), rho, sum_g, the 4*m0
+ * round coefficients, alpha (m0), blinding_eval. */
+int pko_spartan_sumcheck(pko_transcript *t, uint64_t *a, uint64_t *b, uint64_t *c, size_t m0,
+                         const uint64_t *g, const uint64_t *w1, size_t blinding_offset,
+                         uint64_t *r_out, uint64_t rho_out[4], uint64_t sum_g_out[4],
+                         uint64_t *coeffs_out, uint64_t *alpha_out, uint64_t blinding_eval[4]);
+
 int pko_num_threads(void);
 
 #ifdef __cplusplus

@@ -49,6 +49,17 @@ SIGNATURES = {
     "pkg_merkle_leaves_fr": [_c_vp, _c_sz, _c_sz, _c_int, _c_vp, _c_vp],
     "pkg_merkle_levels": [_c_vp, _c_sz, _c_vp],
     "pkg_whir_commit": [_c_vp, _c_sz, _c_uint, _c_uint, _c_vp, _c_sz, _c_int, _c_vp, _c_vp, _c_vp],
+    "pkg_transcript_init": [_c_vp, _c_vp],
+    "pkg_transcript_absorb": [_c_vp, _c_vp],
+    "pkg_transcript_squeeze": [_c_vp, _c_vp],
+    "pkg_eq_hypercube": [_c_vp, _c_sz, _c_sz, _c_vp, _c_vp],
+    "pkg_spartan_round": [_c_vp, _c_vp, _c_vp, _c_vp, _c_sz, _c_vp, _c_vp, _c_vp],
+    "pkg_spartan_sumcheck": [_c_vp, _c_vp, _c_vp, _c_sz, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                             _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+    "pkg_spmv_csr": [_c_vp, _c_vp, _c_vp, _c_sz, _c_sz, _c_vp, _c_vp, _c_vp],
+    "pkg_csr_transpose": [_c_vp, _c_vp, _c_vp, _c_sz, _c_sz, _c_sz, _c_vp, _c_vp, _c_vp, _c_vp],
+    "pkg_hadamard_pad": [_c_vp, _c_vp, _c_sz, _c_sz, _c_vp, _c_vp],
+    "pkg_dot": [_c_vp, _c_vp, _c_sz, _c_vp, _c_vp],
     "pkg_measure_imad_rate": [ctypes.POINTER(ctypes.c_double)],
     "pkg_version": [],
 }

@@ -1,0 +1,68 @@
+// sky_host.hpp -- host-side Skyscraper permutation (skyscraper/core/src/
+// reference.rs:49-98) on canonical values, for the Fiat-Shamir transcript.
+// ss: r += l^2 * 2^-256 + RC (the Montgomery square of a canonical value);
+// bb: r += bar(l) + RC.
+#pragma once
+#include <cstdint>
+#include <cstring>
+
+#include "fr_host.hpp"
+
+namespace pk {
+
+struct HostSky {
+  static const uint64_t* rc(int k) {
+    static const uint64_t RC[18][4] = {
+        {0, 0, 0, 0},
+        {0x903c4324270bd744ULL, 0x873125f708a7d269ULL, 0x081dd27906c83855ULL, 0x276b1823ea6d7667ULL},
+        {0x7ac8edbb4b378d71ULL, 0xe29d79f3d99e2cb7ULL, 0x751417914c1a5a18ULL, 0x0cf02bd758a484a6ULL},
+        {0xfa7adc6769e5bc36ULL, 0x1c3f8e297cca387dULL, 0x0eb7730d63481db0ULL, 0x25b0e03f18ede544ULL},
+        {0x57847e652f03cfb7ULL, 0x33440b9668873404ULL, 0x955a32e849af80bcULL, 0x002882fcbe14ae70ULL},
+        {0x979231396257d4d7ULL, 0x29989c3e1b37d3c1ULL, 0x12ef02b47f1277baULL, 0x039ad8571e2b7a9cULL},
+        {0xb5b48465abbb7887ULL, 0xa72a6bc5e6ba2d2bULL, 0x4cd48043712f7b29ULL, 0x1142d5410fc1fc1aULL},
+        {0x7ab2c156059075d3ULL, 0x17cb3594047999b2ULL, 0x44f2c93598f289f7ULL, 0x1d78439f69bc0becULL},
+        {0x05d7a965138b8edbULL, 0x36ef35a3d55c48b1ULL, 0x8ddfb8a1ac6f1628ULL, 0x258588a508f4ff82ULL},
+        {0x1596fb9afccb49e9ULL, 0x9a7367d69a09a95bULL, 0x9bc43f6984e4c157ULL, 0x13087879d2f514feULL},
+        {0x295ccd233b4109faULL, 0xe1d72f89ed868012ULL, 0x2e9e1eea4bc88a8eULL, 0x17dadee898c45232ULL},
+        {0x9a8590b4aa1f486fULL, 0xb75834b430e9130eULL, 0xb8e90b1034d5de31ULL, 0x295c6d1546e7f4a6ULL},
+        {0x850adcb74c6eb892ULL, 0x07699ef305b92fc3ULL, 0x4ef96a2ba1720f2dULL, 0x1288ca0e1d3ed446ULL},
+        {0x01960f9349d1b5eeULL, 0x8ccad30769371c69ULL, 0xe5c81e8991c98662ULL, 0x17563b4d1ae023f3ULL},
+        {0x6ba01e9476b32917ULL, 0xa1cb0a3add977bc9ULL, 0x86815a945815f030ULL, 0x2869043be91a1eeaULL},
+        {0x81776c885511d976ULL, 0x7475d34f47f414e7ULL, 0x5d090056095d96cfULL, 0x14941f0aff59e79aULL},
+        {0xbc40b4fd8fc8c034ULL, 0xbb7142c3cce4fd48ULL, 0x318356758a39005aULL, 0x1ce337a190f4379fULL},
+        {0, 0, 0, 0},
+    };
+    return RC[k];
+  }
+  static uint8_t sbox(uint8_t v) {
+    uint8_t nv = (uint8_t)~v;
+    uint8_t r1 = (uint8_t)((nv << 1) | (nv >> 7));
+    uint8_t r2 = (uint8_t)((v << 2) | (v >> 6));
+    uint8_t r3 = (uint8_t)((v << 3) | (v >> 5));
+    uint8_t t = (uint8_t)(v ^ (r1 & r2 & r3));
+    return (uint8_t)((t << 1) | (t >> 7));
+  }
+  // any 256-bit value -> [0, p)
+  static HostFr reduce(HostFr x) {
+    while (!x.is_canonical()) x = HostFr::sub_p(x);
+    return x;
+  }
+  static HostFr bar(const HostFr& x) {
+    uint64_t y[4] = {x.l[2], x.l[3], x.l[0], x.l[1]};
+    uint8_t* b = reinterpret_cast<uint8_t*>(y);
+    for (int i = 0; i < 32; i++) b[i] = sbox(b[i]);
+    return reduce(HostFr::from_limbs(y));
+  }
+  static void round(int k, bool is_bar, HostFr& l, HostFr& r) {
+    HostFr f = is_bar ? bar(l) : HostFr::mul(l, l);
+    HostFr nl = HostFr::add(HostFr::add(r, f), HostFr::from_limbs(rc(k)));
+    r = l;
+    l = nl;
+  }
+  // reference::permute (reference.rs:49-60) on canonical (l, r)
+  static void permute(HostFr& l, HostFr& r) {
+    for (int k = 0; k < 18; k++) round(k, k == 6 || k == 7 || k == 10 || k == 11, l, r);
+  }
+};
+
+}  // namespace pk

@@ -1,0 +1,630 @@
+// sumcheck.cu -- the Spartan side of the prover on the device:
+//   pkg_spartan_round      one round of run_zk_sumcheck_prover's map-reduce
+//                          (provekit/prover/src/whir_r1cs.rs:551-559 over
+//                          sumcheck_fold_map_reduce, provekit/common/src/utils/sumcheck.rs:14-102)
+//   pkg_spartan_sumcheck   the whole zk-sumcheck (whir_r1cs.rs:519-621), rounds
+//                          on the device, round-polynomial bookkeeping and the
+//                          transcript on the host
+//   pkg_eq_hypercube       calculate_evaluations_over_boolean_hypercube_for_eq (sumcheck.rs:108-153)
+//   pkg_spmv_csr           HydratedSparseMatrix * &[Fr] (sparse_matrix.rs:606-627)
+//   pkg_csr_transpose      SparseMatrix::transpose (sparse_matrix.rs:409), as a counting sort
+//   pkg_hadamard_pad       c = a o b padded with zeros (calculate_witness_bounds, sumcheck.rs:163-179)
+//   pkg_dot                whir::algebra::dot (whir_r1cs.rs:614-617, 637, 650)
+//   pkg_transcript_*       host Fiat-Shamir transcript stand-in (see the header)
+//
+// Reductions: each thread accumulates a grid-stride slice; warps combine
+// with __shfl_down_sync (8 limbs per element, field additions), warps
+// combine through shared memory, and one partial per CTA goes to a small
+// scratch array that a single-CTA kernel sums.  Field addition is exact, so
+// the result does not depend on the reduction order.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "fr.cuh"
+#include "fr_host.hpp"
+#include "pk_common.cuh"
+#include "sky_host.hpp"
+
+namespace pk {
+
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ Fr shfl_down(const Fr& x, int off) {
+  Fr r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.v[i] = __shfl_down_sync(0xffffffffu, x.v[i], off);
+  return r;
+}
+
+// Block-wide sum of K field elements per thread; thread 0 gets the result.
+template <int K>
+__device__ __forceinline__ void block_sum(Fr (&v)[K]) {
+  __shared__ Fr warp_sums[kRedThreads / 32][K];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = fr_add(v[k], shfl_down(v[k], off));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) warp_sums[warp][k] = v[k];
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = lane < nw ? warp_sums[lane][k] : fr_zero();
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = fr_add(v[k], shfl_down(v[k], off));
+  }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kRedThreads) sum_partials_kernel(const uint64_t* __restrict__ part,
+                                                                 int nparts,
+                                                                 uint64_t* __restrict__ out) {
+  Fr v[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) v[k] = fr_zero();
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = fr_add(v[k], fr_load(part, (size_t)i * K + k));
+  block_sum<K>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) fr_store(out, k, v[k]);
+}
+
+struct Tables4 {
+  uint64_t* t[4];  // a, b, c, eq
+};
+
+// The Spartan closure (whir_r1cs.rs:552-558) on one pair of each table.
+__device__ __forceinline__ void spartan_map(const Fr (&lo)[4], const Fr (&hi)[4], Fr (&acc)[3]) {
+  // f(0) = eq0 * (a0*b0 - c0)
+  Fr ab = fr_mul(lo[0], lo[1]);
+  acc[0] = fr_add(acc[0], fr_mul(lo[3], fr_sub(ab, lo[2])));
+  // f(-1) = (2eq0 - eq1) * ((2a0 - a1)(2b0 - b1) - (2c0 - c1))
+  Fr x = fr_sub(fr_add(lo[0], lo[0]), hi[0]);
+  Fr y = fr_sub(fr_add(lo[1], lo[1]), hi[1]);
+  Fr z = fr_sub(fr_add(lo[2], lo[2]), hi[2]);
+  Fr e = fr_sub(fr_add(lo[3], lo[3]), hi[3]);
+  acc[1] = fr_add(acc[1], fr_mul(e, fr_sub(fr_mul(x, y), z)));
+  // f(inf) = (eq1 - eq0)(a1 - a0)(b1 - b0)
+  Fr d = fr_mul(fr_sub(hi[3], lo[3]), fr_sub(hi[0], lo[0]));
+  acc[2] = fr_add(acc[2], fr_mul(d, fr_sub(hi[1], lo[1])));
+}
+
+// kFold: current size s = 4q; fold t[j] += f*(t[j+2q]-t[j]),
+// t[j+q] += f*(t[j+3q]-t[j+q]) in place and map (t[j], t[j+q]).
+// !kFold: size s = 2q; map (t[j], t[j+q]).
+template <bool kFold>
+__global__ void __launch_bounds__(kRedThreads) spartan_round_kernel(Tables4 tabs, size_t q, Fr fold,
+                                                                  uint64_t* __restrict__ part) {
+  Fr acc[3] = {fr_zero(), fr_zero(), fr_zero()};
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < q;
+       j += (size_t)gridDim.x * blockDim.x) {
+    Fr lo[4], hi[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint64_t* t = tabs.t[k];
+      Fr x0 = fr_load(t, j), x1 = fr_load(t, j + q);
+      if (kFold) {
+        Fr x2 = fr_load(t, j + 2 * q), x3 = fr_load(t, j + 3 * q);
+        x0 = fr_add(x0, fr_mul(fold, fr_sub(x2, x0)));
+        x1 = fr_add(x1, fr_mul(fold, fr_sub(x3, x1)));
+        fr_store(t, j, x0);
+        fr_store(t, j + q, x1);
+      }
+      lo[k] = x0;
+      hi[k] = x1;
+    }
+    spartan_map(lo, hi, acc);
+  }
+  block_sum<3>(acc);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 3; k++) fr_store(part, (size_t)blockIdx.x * 3 + k, acc[k]);
+}
+
+// eq over a block of variables: out[x] = prod_i (bit_i(x) ? r_i : 1 - r_i)
+// with r_0 on the most significant of nr bits.
+__global__ void eq_small_kernel(const uint64_t* __restrict__ r, int nr, uint64_t* __restrict__ out) {
+  size_t n = size_t(1) << nr;
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < n;
+       x += (size_t)gridDim.x * blockDim.x) {
+    Fr acc = fr_one_mont();
+    for (int i = 0; i < nr; i++) {
+      Fr ri = fr_load_ro(r, i);
+      Fr f = ((x >> (nr - 1 - i)) & 1) ? ri : fr_sub(fr_one_mont(), ri);
+      acc = fr_mul(acc, f);
+    }
+    fr_store(out, x, acc);
+  }
+}
+
+// out[x] = hi[x >> nlo] * lo[x & (2^nlo - 1)] for x < num_entries.
+__global__ void eq_combine_kernel(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo,
+                                  int nlo, size_t num_entries, uint64_t* __restrict__ out) {
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < num_entries;
+       x += (size_t)gridDim.x * blockDim.x) {
+    fr_store(out, x, fr_mul(fr_load_ro(hi, x >> nlo), fr_load_ro(lo, x & ((size_t(1) << nlo) - 1))));
+  }
+}
+
+// Column indices >= num_cols are skipped and flagged in *err (the reference
+// panics on them); the entry point turns the flag into an error status.
+__global__ void spmv_csr_kernel(const uint64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
+                                const uint64_t* __restrict__ vals, size_t num_rows, size_t num_cols,
+                                const uint64_t* __restrict__ x, uint64_t* __restrict__ y,
+                                uint32_t* __restrict__ err) {
+  for (size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x; row < num_rows;
+       row += (size_t)gridDim.x * blockDim.x) {
+    Fr acc = fr_zero();
+    for (uint64_t k = row_ptr[row]; k < row_ptr[row + 1]; k++) {
+      const uint32_t col = cols[k];
+      if (col >= num_cols) {
+        atomicOr(err, 1u);
+        continue;
+      }
+      acc = fr_add(acc, fr_mul(fr_load_ro(vals, k), fr_load_ro(x, col)));
+    }
+    fr_store(y, row, acc);
+  }
+}
+
+__global__ void hadamard_pad_kernel(const uint64_t* __restrict__ a, const uint64_t* __restrict__ b,
+                                    size_t n, size_t padded, uint64_t* __restrict__ c) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < padded;
+       i += (size_t)gridDim.x * blockDim.x)
+    fr_store(c, i, i < n ? fr_mul(fr_load_ro(a, i), fr_load_ro(b, i)) : fr_zero());
+}
+
+__global__ void __launch_bounds__(kRedThreads) dot_kernel(const uint64_t* __restrict__ a,
+                                                        const uint64_t* __restrict__ b, size_t n,
+                                                        uint64_t* __restrict__ part) {
+  Fr acc[1] = {fr_zero()};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    acc[0] = fr_add(acc[0], fr_mul(fr_load_ro(a, i), fr_load_ro(b, i)));
+  block_sum<1>(acc);
+  if (threadIdx.x == 0) fr_store(part, blockIdx.x, acc[0]);
+}
+
+// ---- CSR transpose: count, exclusive scan, scatter ------------------------
+__global__ void csr_count_cols_kernel(const uint32_t* __restrict__ cols, size_t nnz,
+                                      size_t num_cols, uint32_t* __restrict__ counts,
+                                      uint32_t* __restrict__ err) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nnz;
+       k += (size_t)gridDim.x * blockDim.x) {
+    if (cols[k] >= num_cols) {
+      atomicOr(err, 1u);
+      continue;
+    }
+    atomicAdd(&counts[cols[k]], 1u);
+  }
+}
+
+__global__ void csr_scatter_kernel(const uint64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
+                                   const uint64_t* __restrict__ vals, size_t num_rows, size_t num_cols,
+                                   unsigned long long* __restrict__ cursor,
+                                   uint32_t* __restrict__ cols_t, uint64_t* __restrict__ vals_t) {
+  for (size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x; row < num_rows;
+       row += (size_t)gridDim.x * blockDim.x) {
+    for (uint64_t k = row_ptr[row]; k < row_ptr[row + 1]; k++) {
+      if (cols[k] >= num_cols) continue;  // flagged by csr_count_cols_kernel
+      unsigned long long pos = atomicAdd(&cursor[cols[k]], 1ull);
+      cols_t[pos] = (uint32_t)row;
+      fr_store(vals_t, pos, fr_load_ro(vals, k));
+    }
+  }
+}
+
+__global__ void widen_kernel(const uint32_t* __restrict__ in, size_t n, unsigned long long* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+
+static int red_grid(size_t n) {
+  size_t b = (n + kRedThreads - 1) / kRedThreads;
+  return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sm_count() * 4));
+}
+static int ew_grid(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sm_count() * 32));
+}
+
+// One Spartan round on device tables; writes 3 Fr (f0, f(-1), f(inf)) to
+// d_out (device).  part: >= red_grid(q) * 3 Fr of scratch.
+int spartan_round_device(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t* eq, size_t size,
+                         const uint64_t* fold_host, uint64_t* part, uint64_t* d_out,
+                         cudaStream_t s) {
+  Tables4 tabs = {{a, b, c, eq}};
+  Fr f;
+  memset(&f, 0, sizeof f);
+  size_t q;
+  int g;
+  if (fold_host) {
+    memcpy(f.v, fold_host, 32);
+    q = size / 4;
+    g = red_grid(q);
+    spartan_round_kernel<true><<<g, kRedThreads, 0, s>>>(tabs, q, f, part);
+  } else {
+    q = size / 2;
+    g = red_grid(q);
+    spartan_round_kernel<false><<<g, kRedThreads, 0, s>>>(tabs, q, f, part);
+  }
+  PK_CHECK_LAUNCH("spartan_round_kernel");
+  sum_partials_kernel<3><<<1, kRedThreads, 0, s>>>(part, g, d_out);
+  PK_CHECK_LAUNCH("sum_partials_kernel");
+  return PKG_OK;
+}
+
+int eq_hypercube_device(const uint64_t* r_host, size_t nr, size_t num_entries, uint64_t* out,
+                        cudaStream_t s) {
+  if (num_entries == 0) return PKG_OK;
+  PK_REQUIRE(nr < 40 && num_entries <= (size_t(1) << nr), "num_entries %zu exceeds 2^%zu",
+             num_entries, nr);
+  PK_REQUIRE(out && aligned16(out), "out must be a 16-byte aligned device pointer");
+  if (nr == 0) {  // eq over no variables is the single entry 1
+    HostFr one = HostFr::one();
+    PK_CUDA(cudaMemcpyAsync(out, one.l, 32, cudaMemcpyHostToDevice, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    return PKG_OK;
+  }
+  int nhi = (int)(nr + 1) / 2, nlo = (int)nr - nhi;
+  Scratch scr;
+  size_t nh = size_t(1) << nhi, nl = size_t(1) << nlo;
+  int rc = scr.alloc(32 * (nr + nh + nl), s);
+  if (rc) return rc;
+  uint64_t* d_r = static_cast<uint64_t*>(scr.ptr);
+  uint64_t* d_hi = d_r + 4 * nr;
+  uint64_t* d_lo = d_hi + 4 * nh;
+  PK_CUDA(cudaMemcpyAsync(d_r, r_host, 32 * nr, cudaMemcpyHostToDevice, s));
+  eq_small_kernel<<<ew_grid(nh), 256, 0, s>>>(d_r, nhi, d_hi);
+  PK_CHECK_LAUNCH("eq_small_kernel");
+  eq_small_kernel<<<ew_grid(nl), 256, 0, s>>>(d_r + 4 * nhi, nlo, d_lo);
+  PK_CHECK_LAUNCH("eq_small_kernel");
+  eq_combine_kernel<<<ew_grid(num_entries), 256, 0, s>>>(d_hi, d_lo, nlo, num_entries, out);
+  PK_CHECK_LAUNCH("eq_combine_kernel");
+  // the host copy of r above must outlive the async copy
+  PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}
+
+// err: device word, zeroed by the caller before the launch.
+int spmv_device(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
+                size_t num_rows, size_t num_cols, const uint64_t* x, uint64_t* y, uint32_t* err,
+                cudaStream_t s) {
+  if (num_rows == 0) return PKG_OK;
+  PK_REQUIRE(row_ptr && y && aligned16(y) && aligned16(vals) && aligned16(x),
+             "null or unaligned device pointer");
+  spmv_csr_kernel<<<ew_grid(num_rows), 256, 0, s>>>(row_ptr, cols, vals, num_rows, num_cols, x, y,
+                                                   err);
+  PK_CHECK_LAUNCH("spmv_csr_kernel");
+  return PKG_OK;
+}
+
+static int read_err_flag(uint32_t* d_err, cudaStream_t s, const char* what) {
+  uint32_t h = 0;
+  PK_CUDA(cudaMemcpyAsync(&h, d_err, 4, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  if (h) {
+    set_last_error("%s: column index out of range", what);
+    return PKG_ERR_INVALID_ARGUMENT;
+  }
+  return PKG_OK;
+}
+
+int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* d_out, uint64_t* part,
+               cudaStream_t s) {
+  int g = red_grid(n);
+  dot_kernel<<<g, kRedThreads, 0, s>>>(a, b, n, part);
+  PK_CHECK_LAUNCH("dot_kernel");
+  sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, g, d_out);
+  PK_CHECK_LAUNCH("sum_partials_kernel");
+  return PKG_OK;
+}
+
+// ---- host transcript stand-in ------------------------------------------
+struct HostTranscript {
+  HostFr l, r;
+  void init(const uint64_t domain[4]) {
+    l = HostSky::reduce(HostFr::from_limbs(domain));
+    r = HostFr::zero();
+    HostSky::permute(l, r);
+  }
+  void absorb(const HostFr& x_mont) {
+    l = HostFr::add(l, HostFr::from_mont(x_mont));
+    HostSky::permute(l, r);
+  }
+  HostFr squeeze() {
+    HostSky::permute(l, r);
+    return HostFr::to_mont(l);
+  }
+};
+
+static HostFr eval_cubic(const HostFr* c, const HostFr& x) {
+  HostFr acc = HostFr::mul(x, c[3]);
+  acc = HostFr::mul(HostFr::add(acc, c[2]), x);
+  acc = HostFr::mul(HostFr::add(acc, c[1]), x);
+  return HostFr::add(acc, c[0]);
+}
+
+// compute_blinding_coefficients_for_round (whir_r1cs.rs:427-492)
+static void blinding_coeffs(const HostFr* g, size_t n, size_t compute_for, const HostFr* alphas,
+                            HostFr out[4]) {
+  bool all_fixed = false;
+  size_t cf = compute_for;
+  if (cf == n) {
+    all_fixed = true;
+    cf = n - 1;
+  }
+  HostFr prefix = HostFr::zero(), suffix = HostFr::zero();
+  for (size_t i = 0; i < cf; i++) prefix = HostFr::add(prefix, eval_cubic(g + 4 * i, alphas[i]));
+  for (size_t i = cf + 1; i < n; i++)
+    suffix = HostFr::add(suffix, HostFr::add(eval_cubic(g + 4 * i, HostFr::zero()),
+                                             eval_cubic(g + 4 * i, HostFr::one())));
+  HostFr pm = HostFr::one();
+  for (size_t i = 0; i < n - 1 - cf; i++) pm = HostFr::add(pm, pm);
+  HostFr sm = HostFr::mul(pm, HostFr::inv(HostFr::add(HostFr::one(), HostFr::one())));
+  HostFr cst = HostFr::add(HostFr::mul(pm, prefix), HostFr::mul(sm, suffix));
+  const HostFr* cur = g + 4 * cf;
+  HostFr res[4] = {HostFr::add(HostFr::mul(pm, cur[0]), cst), HostFr::mul(pm, cur[1]),
+                   HostFr::mul(pm, cur[2]), HostFr::mul(pm, cur[3])};
+  if (all_fixed) {
+    out[0] = eval_cubic(res, alphas[cf]);
+    out[1] = out[2] = out[3] = HostFr::zero();
+    return;
+  }
+  for (int k = 0; k < 4; k++) out[k] = res[k];
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+static_assert(sizeof(pkg_transcript) == 64, "transcript state is two field elements");
+
+extern "C" int pkg_transcript_init(pkg_transcript* t, const uint64_t domain[4]) {
+  PK_REQUIRE(t && domain, "null pointer");
+  HostTranscript ht;
+  ht.init(domain);
+  memcpy(t->l, ht.l.l, 32);
+  memcpy(t->r, ht.r.l, 32);
+  return PKG_OK;
+}
+
+extern "C" int pkg_transcript_absorb(pkg_transcript* t, const uint64_t x[4]) {
+  PK_REQUIRE(t && x, "null pointer");
+  HostTranscript ht;
+  ht.l = HostFr::from_limbs(t->l);
+  ht.r = HostFr::from_limbs(t->r);
+  ht.absorb(HostFr::from_limbs(x));
+  memcpy(t->l, ht.l.l, 32);
+  memcpy(t->r, ht.r.l, 32);
+  return PKG_OK;
+}
+
+extern "C" int pkg_transcript_squeeze(pkg_transcript* t, uint64_t out[4]) {
+  PK_REQUIRE(t && out, "null pointer");
+  HostTranscript ht;
+  ht.l = HostFr::from_limbs(t->l);
+  ht.r = HostFr::from_limbs(t->r);
+  HostFr v = ht.squeeze();
+  memcpy(out, v.l, 32);
+  memcpy(t->l, ht.l.l, 32);
+  memcpy(t->r, ht.r.l, 32);
+  return PKG_OK;
+}
+
+extern "C" int pkg_spartan_round(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t* eq, size_t size,
+                                 const uint64_t* fold, uint64_t out[12], pkg_stream_t stream) {
+  PK_REQUIRE(is_pow2(size) && size >= 2, "table size %zu must be a power of two >= 2", size);
+  PK_REQUIRE(!fold || size >= 4, "folding needs size >= 4 (got %zu)", size);
+  PK_REQUIRE(a && b && c && eq && out, "null pointer");
+  PK_REQUIRE(aligned16(a) && aligned16(b) && aligned16(c) && aligned16(eq),
+             "device buffers must be 16-byte aligned");
+  cudaStream_t s = as_stream(stream);
+  size_t q = fold ? size / 4 : size / 2;
+  Scratch scr;
+  int rc = scr.alloc(32 * (3 * (size_t)red_grid(q) + 3), s);
+  if (rc) return rc;
+  uint64_t* part = static_cast<uint64_t*>(scr.ptr);
+  uint64_t* d_out = part + 4 * 3 * (size_t)red_grid(q);
+  rc = spartan_round_device(a, b, c, eq, size, fold, part, d_out, s);
+  if (rc) return rc;
+  PK_CUDA(cudaMemcpyAsync(out, d_out, 96, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}
+
+extern "C" int pkg_eq_hypercube(const uint64_t* r, size_t nr, size_t num_entries, uint64_t* out,
+                                pkg_stream_t stream) {
+  return eq_hypercube_device(r, nr, num_entries, out, as_stream(stream));
+}
+
+extern "C" int pkg_spmv_csr(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
+                            size_t num_rows, size_t num_cols, const uint64_t* x, uint64_t* y,
+                            pkg_stream_t stream) {
+  if (num_rows == 0) return PKG_OK;
+  cudaStream_t s = as_stream(stream);
+  Scratch scr;
+  int rc = scr.alloc(256, s);
+  if (rc) return rc;
+  uint32_t* err = static_cast<uint32_t*>(scr.ptr);
+  PK_CUDA(cudaMemsetAsync(err, 0, 4, s));
+  rc = spmv_device(row_ptr, cols, vals, num_rows, num_cols, x, y, err, s);
+  if (rc) return rc;
+  return read_err_flag(err, s, "pkg_spmv_csr");
+}
+
+extern "C" int pkg_hadamard_pad(const uint64_t* a, const uint64_t* b, size_t n, size_t padded,
+                                uint64_t* c, pkg_stream_t stream) {
+  PK_REQUIRE(padded >= n, "padded length %zu < n %zu", padded, n);
+  if (padded == 0) return PKG_OK;
+  PK_REQUIRE(c && aligned16(c) && aligned16(a) && aligned16(b), "null or unaligned pointer");
+  cudaStream_t s = as_stream(stream);
+  hadamard_pad_kernel<<<ew_grid(padded), 256, 0, s>>>(a, b, n, padded, c);
+  PK_CHECK_LAUNCH("hadamard_pad_kernel");
+  return PKG_OK;
+}
+
+extern "C" int pkg_dot(const uint64_t* a, const uint64_t* b, size_t n, uint64_t out[4],
+                       pkg_stream_t stream) {
+  PK_REQUIRE(out, "null output");
+  if (n == 0) {
+    memset(out, 0, 32);
+    return PKG_OK;
+  }
+  PK_REQUIRE(a && b && aligned16(a) && aligned16(b), "null or unaligned pointer");
+  cudaStream_t s = as_stream(stream);
+  Scratch scr;
+  int g = red_grid(n);
+  int rc = scr.alloc(32 * ((size_t)g + 1), s);
+  if (rc) return rc;
+  uint64_t* part = static_cast<uint64_t*>(scr.ptr);
+  rc = dot_device(a, b, n, part + 4 * (size_t)g, part, s);
+  if (rc) return rc;
+  PK_CUDA(cudaMemcpyAsync(out, part + 4 * (size_t)g, 32, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}
+
+extern "C" int pkg_csr_transpose(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
+                                 size_t num_rows, size_t num_cols, size_t nnz,
+                                 uint64_t* row_ptr_t, uint32_t* cols_t, uint64_t* vals_t,
+                                 pkg_stream_t stream) {
+  PK_REQUIRE(row_ptr && row_ptr_t, "null row pointer array");
+  PK_REQUIRE(num_cols < (size_t(1) << 32) && num_rows < (size_t(1) << 32),
+             "matrix dimensions must fit u32 column indices");
+  cudaStream_t s = as_stream(stream);
+  Scratch scr;
+  // counts (u32, num_cols), cursor (u64, num_cols + 1), cub temp
+  size_t cub_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (unsigned long long*)nullptr,
+                                (unsigned long long*)nullptr, (int)(num_cols + 1), s);
+  size_t counts_bytes = ((4 * num_cols + 255) / 256) * 256;
+  size_t wide_bytes = ((8 * (num_cols + 1) + 255) / 256) * 256;
+  int rc = scr.alloc(counts_bytes + wide_bytes + cub_bytes + 512, s);
+  if (rc) return rc;
+  uint8_t* base = static_cast<uint8_t*>(scr.ptr);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(base);
+  unsigned long long* wide = reinterpret_cast<unsigned long long*>(base + counts_bytes);
+  void* cub_tmp = base + counts_bytes + wide_bytes;
+  uint32_t* err = reinterpret_cast<uint32_t*>(base + counts_bytes + wide_bytes + ((cub_bytes + 255) / 256) * 256);
+  PK_CUDA(cudaMemsetAsync(err, 0, 4, s));
+  PK_CUDA(cudaMemsetAsync(counts, 0, 4 * num_cols, s));
+  PK_CUDA(cudaMemsetAsync(wide, 0, 8 * (num_cols + 1), s));
+  if (nnz) {
+    csr_count_cols_kernel<<<ew_grid(nnz), 256, 0, s>>>(cols, nnz, num_cols, counts, err);
+    PK_CHECK_LAUNCH("csr_count_cols_kernel");
+  }
+  if (num_cols) {
+    widen_kernel<<<ew_grid(num_cols), 256, 0, s>>>(counts, num_cols, wide);
+    PK_CHECK_LAUNCH("widen_kernel");
+  }
+  PK_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, cub_bytes, wide,
+                                        reinterpret_cast<unsigned long long*>(row_ptr_t),
+                                        (int)(num_cols + 1), s));
+  count_launch();
+  // cursor = row_ptr_t[0..num_cols) (reuse `wide`)
+  PK_CUDA(cudaMemcpyAsync(wide, row_ptr_t, 8 * (num_cols + 1), cudaMemcpyDeviceToDevice, s));
+  if (nnz && num_rows) {
+    csr_scatter_kernel<<<ew_grid(num_rows), 256, 0, s>>>(row_ptr, cols, vals, num_rows, num_cols,
+                                                         wide, cols_t, vals_t);
+    PK_CHECK_LAUNCH("csr_scatter_kernel");
+  }
+  return read_err_flag(err, s, "pkg_csr_transpose");
+}
+
+extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_t m0,
+                                    const uint64_t* g, const uint64_t* w1_blinding,
+                                    pkg_transcript* transcript, uint64_t* r_out, uint64_t rho_out[4],
+                                    uint64_t sum_g_out[4], uint64_t* coeffs_out,
+                                    uint64_t* alpha_out, uint64_t blinding_eval[4],
+                                    pkg_stream_t stream) {
+  PK_REQUIRE(m0 >= 1 && m0 <= 30, "m0 %zu out of range [1, 30]", m0);
+  PK_REQUIRE(a && b && c && g && w1_blinding && transcript && r_out && rho_out && sum_g_out &&
+                 coeffs_out && alpha_out && blinding_eval,
+             "null pointer");
+  PK_REQUIRE(aligned16(a) && aligned16(b) && aligned16(c), "device buffers must be 16-byte aligned");
+  cudaStream_t s = as_stream(stream);
+  const size_t n = size_t(1) << m0;
+  HostTranscript t;
+  t.l = HostFr::from_limbs(transcript->l);
+  t.r = HostFr::from_limbs(transcript->r);
+  std::vector<HostFr> r(m0), alpha(m0), gv(4 * m0);
+  for (size_t i = 0; i < 4 * m0; i++) gv[i] = HostFr::from_limbs(g + 4 * i);
+  for (size_t i = 0; i < m0; i++) {  // whir_r1cs.rs:529
+    r[i] = t.squeeze();
+    memcpy(r_out + 4 * i, r[i].l, 32);
+  }
+  // scratch: eq table (n Fr), partials, one round result
+  const int gmax = red_grid(n / 2);
+  Scratch scr;
+  int rc = scr.alloc(32 * (n + 3 * (size_t)gmax + 3), s);
+  if (rc) return rc;
+  uint64_t* eq = static_cast<uint64_t*>(scr.ptr);
+  uint64_t* part = eq + 4 * n;
+  uint64_t* d_out = part + 4 * 3 * (size_t)gmax;
+  rc = eq_hypercube_device(r_out, m0, n, eq, s);  // :530
+  if (rc) return rc;
+  HostFr g0[4];
+  blinding_coeffs(gv.data(), m0, 0, nullptr, g0);  // sum_over_hypercube, :494-501
+  HostFr sum_g = HostFr::add(eval_cubic(g0, HostFr::zero()), eval_cubic(g0, HostFr::one()));
+  memcpy(sum_g_out, sum_g.l, 32);
+  t.absorb(sum_g);                  // :541
+  HostFr rho = t.squeeze();         // :543
+  memcpy(rho_out, rho.l, 32);
+  HostFr saved = HostFr::mul(rho, sum_g);
+  const HostFr half = HostFr::inv(HostFr::add(HostFr::one(), HostFr::one()));
+  size_t size = n;
+  uint64_t h[12];
+  for (size_t idx = 0; idx < m0; idx++) {  // :550-610
+    rc = spartan_round_device(a, b, c, eq, size, idx ? alpha[idx - 1].l : nullptr, part, d_out, s);
+    if (rc) return rc;
+    PK_CUDA(cudaMemcpyAsync(h, d_out, 96, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    if (idx) size /= 2;
+    HostFr gp[4];
+    blinding_coeffs(gv.data(), m0, idx, alpha.data(), gp);
+    HostFr h0 = HostFr::from_limbs(h), hem1 = HostFr::from_limbs(h + 4),
+           hinf = HostFr::from_limbs(h + 8);
+    HostFr cf[4];
+    cf[0] = HostFr::add(h0, HostFr::mul(rho, gp[0]));
+    HostFr gem1 = HostFr::sub(HostFr::add(HostFr::sub(gp[0], gp[1]), gp[2]), gp[3]);
+    HostFr cem1 = HostFr::add(hem1, HostFr::mul(rho, gem1));
+    cf[2] = HostFr::mul(half, HostFr::sub(HostFr::sub(HostFr::sub(HostFr::add(saved, cem1), cf[0]),
+                                                      cf[0]),
+                                          cf[0]));
+    cf[3] = HostFr::add(hinf, HostFr::mul(rho, gp[3]));
+    cf[1] = HostFr::sub(HostFr::sub(HostFr::sub(HostFr::sub(saved, cf[0]), cf[0]), cf[3]), cf[2]);
+    for (int k = 0; k < 4; k++) {
+      memcpy(coeffs_out + 16 * idx + 4 * k, cf[k].l, 32);
+      t.absorb(cf[k]);
+    }
+    alpha[idx] = t.squeeze();
+    memcpy(alpha_out + 4 * idx, alpha[idx].l, 32);
+    saved = eval_cubic(cf, alpha[idx]);
+  }
+  // blinding_eval = <expand_powers::<4>(alpha), w1[offset..offset + 4*m0]> (:613-618)
+  HostFr acc = HostFr::zero();
+  for (size_t i = 0; i < m0; i++) {
+    HostFr pw = HostFr::one();
+    for (int k = 0; k < 4; k++) {
+      acc = HostFr::add(acc, HostFr::mul(pw, HostFr::from_limbs(w1_blinding + 4 * (4 * i + k))));
+      pw = HostFr::mul(pw, alpha[i]);
+    }
+  }
+  memcpy(blinding_eval, acc.l, 32);
+  t.absorb(acc);  // prover_message(&blinding_eval), :618
+  memcpy(transcript->l, t.l.l, 32);
+  memcpy(transcript->r, t.r.l, 32);
+  return PKG_OK;
+}

@@ -17,6 +17,10 @@ _u8p = ctypes.POINTER(ctypes.c_uint8)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _sz = ctypes.c_size_t
 
+class Transcript(ctypes.Structure):
+    _fields_ = [("l", ctypes.c_uint64 * 4), ("r", ctypes.c_uint64 * 4)]
+
+
 _lib = None
 
 
@@ -51,6 +55,14 @@ def lib():
         L.pko_blinding_coeffs.argtypes = [_u64p, _sz, _sz, _u64p, _u64p]
         L.pko_dot.argtypes = [_u64p, _u64p, _u64p, _sz]
         L.pko_num_threads.restype = ctypes.c_int
+        tp = ctypes.POINTER(Transcript)
+        L.pko_transcript_init.argtypes = [tp, _u64p]
+        L.pko_transcript_absorb.argtypes = [tp, _u64p]
+        L.pko_transcript_squeeze.argtypes = [tp, _u64p]
+        L.pko_spartan_sumcheck.argtypes = [tp, _u64p, _u64p, _u64p, _sz, _u64p, _u64p, _sz,
+                                           _u64p, _u64p, _u64p, _u64p, _u64p, _u64p]
+        L.pko_from_mont_many.argtypes = [_u64p, _sz]
+        L.pko_to_mont_many.argtypes = [_u64p, _sz]
     return _lib
 
 

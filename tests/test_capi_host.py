@@ -93,3 +93,23 @@ def test_rs_encode_validation(L):
 def test_merkle_requires_power_of_two_leaves(L):
     assert L.pkg_merkle_tree_fr(None, 4, 6, 0, None, None) == -1
     assert L.pkg_merkle_tree_fr(None, 4, 8, 7, None, None) == -1
+
+
+def test_transcript_matches_oracle(L):
+    """The library's host transcript (pkg_transcript_*) and the oracle's agree
+    message by message; both run the KAT-pinned Skyscraper permutation."""
+    from provekit_b200.spartan import Transcript
+    for domain in (0, 42, (1 << 255) + 12345):
+        t = Transcript.new(domain)
+        o = O.Transcript()
+        d = np.array([(domain >> (64 * i)) & (2**64 - 1) for i in range(4)], np.uint64)
+        O.lib().pko_transcript_init(ctypes.byref(o), O.p64(d))
+        assert list(t.l) == list(o.l) and list(t.r) == list(o.r)
+        xs = O.sample_fr(domain % 1000 + 1, 6)
+        for x in xs:
+            t.absorb(x)
+            O.lib().pko_transcript_absorb(ctypes.byref(o), O.p64(np.ascontiguousarray(x)))
+            a = t.squeeze()
+            b = np.zeros(4, np.uint64)
+            O.lib().pko_transcript_squeeze(ctypes.byref(o), O.p64(b))
+            assert np.array_equal(a, b)
