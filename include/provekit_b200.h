@@ -225,6 +225,57 @@ int pkg_hadamard_pad(const uint64_t *a, const uint64_t *b, size_t n, size_t padd
  * 650).  a, b device; out host; synchronous. */
 int pkg_dot(const uint64_t *a, const uint64_t *b, size_t n, uint64_t out[4], pkg_stream_t stream);
 
+/* ---- Spartan prove core ---------------------------------------------------- */
+/* An R1CS instance as three CSR matrices (num_constraints x num_witnesses, one
+ * Fr per nonzero, hydrated).  Device pointers. */
+typedef struct {
+  size_t num_constraints, num_witnesses;
+  const uint64_t *row_ptr[3]; /* A, B, C; num_constraints + 1 entries each */
+  const uint32_t *cols[3];
+  const uint64_t *vals[3];
+  size_t nnz[3];
+} pkg_r1cs;
+
+/* Everything the prover produces before WHIR's own prove rounds. */
+typedef struct {
+  size_t m, m0;                  /* committed variables, sumcheck variables */
+  uint8_t root[32];              /* Merkle root of the witness commitment  */
+  uint64_t r[30][4];             /* eq challenges (m0)                     */
+  uint64_t coeffs[120][4];       /* 4 round coefficients per round (4*m0) */
+  uint64_t alpha[30][4];         /* sumcheck challenges (m0)               */
+  uint64_t rho[4], sum_g[4], blinding_eval[4], public_x[4];
+  uint64_t evals[3][4];          /* <A^T eq(alpha), w>, <B^T ...>, <C^T ...> */
+  pkg_transcript transcript;     /* state after the last message           */
+} pkg_spartan_proof;
+
+/* The prover's work up to WHIR's prove call for a single-commitment R1CS
+ * (no public inputs, no challenges): WhirR1CSScheme::new_for_r1cs sizing
+ * (provekit/r1cs-compiler/src/whir_r1cs.rs:48-92); WhirR1CSProver::commit
+ * (provekit/prover/src/whir_r1cs.rs:82-140) with the 4*m0 blinding
+ * coefficients drawn from pkg_sample_fr(blinding_seed) instead of thread_rng
+ * and the commitment = pkg_whir_commit(folding_factor, log_inv_rate,
+ * canonical leaves) of the padded witness, root absorbed; prove_noir
+ * (:143-187): witness bounds, zk sumcheck, eq(alpha), transposed SpMV;
+ * prove_from_alphas (:247-301): public-weight challenge (hash of no public
+ * inputs = 0), the three covector evaluations absorbed.  witness: device,
+ * num_witnesses Fr.  Synchronous. */
+int pkg_spartan_prove(const pkg_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
+                      uint64_t transcript_domain, unsigned folding_factor, unsigned log_inv_rate,
+                      pkg_spartan_proof *out, pkg_stream_t stream);
+
+/* Synthetic satisfiable R1CS (host memory), the workload of the 2^20-constraint
+ * prove benchmark: w[0] = 1, w[1..num_inputs] from pkg_sample_fr(seed); row
+ * i: A_i and B_i each hold 1-3 nonzeros at uniform columns in
+ * [0, num_inputs + i] with uniform Fr coefficients, C_i = e_{num_inputs+1+i},
+ * and w[num_inputs+1+i] = <A_i, w> * <B_i, w>.  Integer choices come from
+ * splitmix64(seed), coefficients from pkg_sample_fr(seed + 1).  Capacities:
+ * row_ptr[k] num_constraints+1, cols/vals of A and B 3*num_constraints, of C
+ * num_constraints; witness 1 + num_inputs + num_constraints Fr.  No
+ * reference counterpart (the reference compiles R1CS from Noir programs). */
+int pkg_synthetic_r1cs(uint64_t seed, size_t num_constraints, size_t num_inputs,
+                       uint64_t *row_ptr[3], uint32_t *cols[3], uint64_t *vals[3],
+                       size_t nnz_out[3], uint64_t *witness);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 /* Number of kernels this library has launched in this process. */
 uint64_t pkg_kernel_launches(void);

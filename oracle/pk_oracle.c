@@ -927,3 +927,90 @@ int pko_spartan_sumcheck(pko_transcript *t, uint64_t *a, uint64_t *b, uint64_t *
     pko_transcript_absorb(t, acc);
     return 0;
 }
+
+/* ======================================================================= */
+/* Spartan prove core                                                      */
+/* ======================================================================= */
+static size_t ceil_log2(size_t n) { /* utils::next_power_of_two (utils/mod.rs:71-79) */
+    size_t p = 1, k = 0;
+    while (p < n) { p <<= 1; k++; }
+    return k;
+}
+
+int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
+                      uint64_t domain, unsigned ff, unsigned lr, pko_spartan_proof *out) {
+    const size_t nc = r1cs->num_constraints, nw = r1cs->num_witnesses, w1_size = nw;
+    size_t m = ceil_log2(w1_size), m0 = ceil_log2(nc);
+    if (m < 13) m = 13;                                   /* MIN_WHIR_NUM_VARIABLES */
+    if (m0 < 1) m0 = 1;                                   /* MIN_SUMCHECK_NUM_VARIABLES */
+    if (((size_t)1 << m) - w1_size < 4 * m0) m++;
+    if (m0 > 30 || m > 28 || ff > m) return -1;
+    memset(out, 0, sizeof *out);
+    out->m = m;
+    out->m0 = m0;
+    pko_transcript *t = &out->transcript;
+    uint64_t dom[4] = {domain, 0, 0, 0};
+    pko_transcript_init(t, dom);
+    /* commit: pad, blinding coefficients at offset w1_size */
+    size_t n = (size_t)1 << m;
+    uint64_t *poly = (uint64_t *)calloc(n, 32);
+    uint64_t *g = (uint64_t *)malloc(32 * 4 * m0);
+    if (!poly || !g) return -2;
+    memcpy(poly, witness, 32 * nw);
+    pko_sample_fr(blinding_seed, 4 * m0, g, 1);
+    memcpy(poly + 4 * w1_size, g, 32 * 4 * m0);
+    size_t M = (size_t)1 << ff, L = n >> ff, cw_len = L << lr;
+    uint64_t *cw = (uint64_t *)malloc(32 * M * cw_len);
+    uint8_t *layers = (uint8_t *)malloc(32 * (2 * cw_len - 1));
+    if (!cw || !layers) return -2;
+    int rc = pko_rs_interleaved_encode(poly, M, L, poly, 0, cw_len, cw);
+    if (rc) return rc;
+    pko_from_mont_many(cw, M * cw_len);
+    rc = pko_merkle_tree((const uint8_t *)cw, 32 * M, cw_len, layers);
+    if (rc) return rc;
+    memcpy(out->root, layers + 32 * (2 * cw_len - 2), 32);
+    free(cw);
+    free(layers);
+    uint64_t root_m[4];
+    memcpy(root_m, out->root, 32);
+    pko_fr_to_mont(root_m, root_m);
+    pko_transcript_absorb(t, root_m);
+    /* witness bounds (sumcheck.rs:163-179) */
+    size_t n0 = (size_t)1 << m0;
+    uint64_t *a = (uint64_t *)calloc(n0, 32), *b = (uint64_t *)calloc(n0, 32), *cc = (uint64_t *)calloc(n0, 32);
+    if (!a || !b || !cc) return -2;
+    pko_spmv(r1cs->row_ptr[0], r1cs->cols[0], r1cs->vals[0], nc, witness, a);
+    pko_spmv(r1cs->row_ptr[1], r1cs->cols[1], r1cs->vals[1], nc, witness, b);
+    for (size_t i = 0; i < nc; i++) pko_fr_mul(cc + 4 * i, a + 4 * i, b + 4 * i);
+    /* zk sumcheck */
+    rc = pko_spartan_sumcheck(t, a, b, cc, m0, g, poly, w1_size, &out->r[0][0], out->rho,
+                              out->sum_g, &out->coeffs[0][0], &out->alpha[0][0], out->blinding_eval);
+    free(a); free(b); free(cc); free(g);
+    if (rc) return rc;
+    /* eq(alpha) truncated to num_constraints, then M^T eq for A, B, C
+     * (multiply_transposed_by_eq_alpha, sumcheck.rs:206-227): computed as
+     * the scatter sum over the rows of M, which equals the transposed SpMV */
+    uint64_t *eq = (uint64_t *)calloc(nc ? nc : 1, 32);
+    uint64_t *alph = (uint64_t *)calloc(nw ? nw : 1, 32);
+    if (!eq || !alph) return -2;
+    pko_eq_hypercube(&out->alpha[0][0], m0, nc, eq);
+    /* public weights (whir_r1cs.rs:665-676): hash of no public inputs is 0 */
+    static const uint64_t zero[4] = {0, 0, 0, 0};
+    pko_transcript_absorb(t, zero);
+    pko_transcript_squeeze(t, out->public_x);
+    for (int k = 0; k < 3; k++) {
+        memset(alph, 0, 32 * nw);
+        for (size_t row = 0; row < nc; row++)
+            for (uint64_t e = r1cs->row_ptr[k][row]; e < r1cs->row_ptr[k][row + 1]; e++) {
+                uint64_t tt[4];
+                pko_fr_mul(tt, r1cs->vals[k] + 4 * e, eq + 4 * row);
+                size_t col = r1cs->cols[k][e];
+                pko_fr_add(alph + 4 * col, alph + 4 * col, tt);
+            }
+        /* create_weights_and_evaluations (:623-642): dot over the padded prefix */
+        pko_dot(out->evals[k], alph, poly, nw);
+        pko_transcript_absorb(t, out->evals[k]);
+    }
+    free(eq); free(alph); free(poly);
+    return 0;
+}

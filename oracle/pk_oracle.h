@@ -108,6 +108,31 @@ int pko_spartan_sumcheck(pko_transcript *t, uint64_t *a, uint64_t *b, uint64_t *
                          uint64_t *r_out, uint64_t rho_out[4], uint64_t sum_g_out[4],
                          uint64_t *coeffs_out, uint64_t *alpha_out, uint64_t blinding_eval[4]);
 
+/* Spartan prove core (the prover's work before WHIR's own rounds):
+ * WhirR1CSScheme::new_for_r1cs sizing (provekit/r1cs-compiler/src/whir_r1cs.rs:48-92),
+ * commit (provekit/prover/src/whir_r1cs.rs:82-140) with the blinding
+ * polynomial drawn from the ChaCha sampler (seed) instead of thread_rng and
+ * the commitment = RS encode + Skyscraper tree of 2^ff contiguous messages,
+ * prove_noir (:143-187) up to the WHIR prove call: witness bounds, zk
+ * sumcheck, eq(alpha), transposed SpMV, public-weight challenge, the three
+ * covector evaluations (:247-301). */
+typedef struct {
+    size_t num_constraints, num_witnesses;
+    const uint64_t *row_ptr[3];   /* A, B, C: num_constraints + 1 */
+    const uint32_t *cols[3];
+    const uint64_t *vals[3];
+} pko_r1cs;
+typedef struct {
+    size_t m, m0;
+    uint8_t root[32];
+    uint64_t r[30][4], coeffs[120][4], alpha[30][4];
+    uint64_t rho[4], sum_g[4], blinding_eval[4], public_x[4], evals[3][4];
+    pko_transcript transcript;
+} pko_spartan_proof;
+int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
+                      uint64_t domain, unsigned folding_factor, unsigned log_inv_rate,
+                      pko_spartan_proof *out);
+
 int pko_num_threads(void);
 
 #ifdef __cplusplus

@@ -60,6 +60,9 @@ SIGNATURES = {
     "pkg_csr_transpose": [_c_vp, _c_vp, _c_vp, _c_sz, _c_sz, _c_sz, _c_vp, _c_vp, _c_vp, _c_vp],
     "pkg_hadamard_pad": [_c_vp, _c_vp, _c_sz, _c_sz, _c_vp, _c_vp],
     "pkg_dot": [_c_vp, _c_vp, _c_sz, _c_vp, _c_vp],
+    "pkg_spartan_prove": [_c_vp, _c_vp, ctypes.c_uint64, ctypes.c_uint64, _c_uint, _c_uint, _c_vp,
+                          _c_vp],
+    "pkg_synthetic_r1cs": [ctypes.c_uint64, _c_sz, _c_sz, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
     "pkg_measure_imad_rate": [ctypes.POINTER(ctypes.c_double)],
     "pkg_version": [],
 }

@@ -1,0 +1,145 @@
+// prove.cu -- pkg_spartan_prove: the Spartan prover's work up to WHIR's own
+// prove rounds, device-resident from the witness to the covector
+// evaluations (provekit/prover/src/whir_r1cs.rs:82-301,
+// provekit/r1cs-compiler/src/whir_r1cs.rs:48-92).
+//
+// Device data: the padded witness polynomial (2^m Fr), its RS codeword and
+// Merkle layers, the a/b/c sumcheck tables (2^m0 Fr each), eq(alpha), the
+// transposed matrices and the alpha covectors.  The host keeps the
+// transcript and reads back only the root, three Fr per sumcheck round and
+// the final scalars.
+#include <cstring>
+#include <vector>
+
+#include "fr_host.hpp"
+#include "internal.cuh"
+#include "pk_common.cuh"
+#include "rs_internal.cuh"
+
+namespace pk {
+
+static size_t ceil_log2(size_t n) {  // utils::next_power_of_two (utils/mod.rs:71-79)
+  size_t p = 1, k = 0;
+  while (p < n) {
+    p <<= 1;
+    k++;
+  }
+  return k;
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
+                                 uint64_t blinding_seed, uint64_t transcript_domain,
+                                 unsigned ff, unsigned lr, pkg_spartan_proof* out,
+                                 pkg_stream_t stream) {
+  PK_REQUIRE(r1cs && witness && out, "null pointer");
+  PK_REQUIRE(aligned16(witness), "witness must be 16-byte aligned");
+  const size_t nc = r1cs->num_constraints, nw = r1cs->num_witnesses, w1_size = nw;
+  PK_REQUIRE(nc >= 1 && nw >= 1, "empty R1CS");
+  size_t m = ceil_log2(w1_size), m0 = ceil_log2(nc);
+  if (m < 13) m = 13;  // MIN_WHIR_NUM_VARIABLES
+  if (m0 < 1) m0 = 1;  // MIN_SUMCHECK_NUM_VARIABLES
+  if ((size_t(1) << m) - w1_size < 4 * m0) m++;
+  PK_REQUIRE(m0 <= 30 && m <= 28 && ff <= m && lr <= 8, "instance too large (m=%zu, m0=%zu)", m,
+             m0);
+  memset(out, 0, sizeof *out);
+  out->m = m;
+  out->m0 = m0;
+  cudaStream_t s = as_stream(stream);
+  const uint64_t dom[4] = {transcript_domain, 0, 0, 0};
+  int rc = pkg_transcript_init(&out->transcript, dom);
+  if (rc) return rc;
+
+  // ---- commit (whir_r1cs.rs:82-140)
+  const size_t n = size_t(1) << m, M = size_t(1) << ff, L = n >> ff, cw_len = L << lr;
+  const size_t n0 = size_t(1) << m0;
+  Scratch s_poly, s_cw, s_layers, s_tab, s_misc;
+  if ((rc = s_poly.alloc(32 * n, s))) return rc;
+  if ((rc = s_cw.alloc(32 * M * cw_len, s))) return rc;
+  if ((rc = s_layers.alloc(32 * (2 * cw_len - 1), s))) return rc;
+  if ((rc = s_tab.alloc(32 * 3 * n0, s))) return rc;
+  uint64_t* poly = static_cast<uint64_t*>(s_poly.ptr);
+  uint64_t* cw = static_cast<uint64_t*>(s_cw.ptr);
+  uint8_t* layers = static_cast<uint8_t*>(s_layers.ptr);
+  uint64_t* ta = static_cast<uint64_t*>(s_tab.ptr);
+  uint64_t* tb = ta + 4 * n0;
+  uint64_t* tc = tb + 4 * n0;
+  std::vector<uint64_t> g(16 * m0);
+  pkg_sample_fr(blinding_seed, 4 * m0, g.data(), 1);  // generate_blinding_univariates, seeded
+  PK_CUDA(cudaMemcpyAsync(poly, witness, 32 * nw, cudaMemcpyDeviceToDevice, s));
+  PK_CUDA(cudaMemsetAsync(poly + 4 * nw, 0, 32 * (n - nw), s));
+  PK_CUDA(cudaMemcpyAsync(poly + 4 * w1_size, g.data(), 32 * 4 * m0, cudaMemcpyHostToDevice, s));
+  if ((rc = rs_encode_device(poly, M, L, nullptr, 0, cw_len, cw, s))) return rc;
+  if ((rc = merkle_tree_fr_device(cw, M, cw_len, PKG_LEAF_CANONICAL, layers, s))) return rc;
+  PK_CUDA(cudaMemcpyAsync(out->root, layers + 32 * (2 * cw_len - 2), 32, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  {
+    HostFr root = HostFr::to_mont(HostFr::from_limbs(reinterpret_cast<const uint64_t*>(out->root)));
+    pkg_transcript_absorb(&out->transcript, root.l);
+  }
+
+  // ---- witness bounds (sumcheck.rs:163-179)
+  // partial sums of dot_device (<= 4 * SMs CTAs) and its result slot
+  const size_t nparts = 4 * (size_t)sm_count();
+  if ((rc = s_misc.alloc(256 + 32 * (nparts + 8), s))) return rc;
+  uint32_t* err = static_cast<uint32_t*>(s_misc.ptr);
+  uint64_t* part = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(s_misc.ptr) + 256);
+  uint64_t* dot_out = part + 4 * nparts;
+  PK_CUDA(cudaMemsetAsync(err, 0, 4, s));
+  PK_CUDA(cudaMemsetAsync(ta, 0, 32 * 3 * n0, s));
+  if ((rc = spmv_device(r1cs->row_ptr[0], r1cs->cols[0], r1cs->vals[0], nc, nw, witness, ta, err, s)))
+    return rc;
+  if ((rc = spmv_device(r1cs->row_ptr[1], r1cs->cols[1], r1cs->vals[1], nc, nw, witness, tb, err, s)))
+    return rc;
+  if ((rc = pkg_hadamard_pad(ta, tb, nc, nc, tc, stream))) return rc;
+
+  // ---- zk sumcheck (whir_r1cs.rs:519-621)
+  std::vector<uint64_t> wb(16 * m0);
+  PK_CUDA(cudaMemcpyAsync(wb.data(), poly + 4 * w1_size, 32 * 4 * m0, cudaMemcpyDeviceToHost, s));
+  {
+    uint32_t h_err = 0;
+    PK_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    PK_REQUIRE(!h_err, "R1CS column index out of range");
+  }
+  rc = pkg_spartan_sumcheck(ta, tb, tc, m0, g.data(), wb.data(), &out->transcript, &out->r[0][0],
+                            out->rho, out->sum_g, &out->coeffs[0][0], &out->alpha[0][0],
+                            out->blinding_eval, stream);
+  if (rc) return rc;
+
+  // ---- eq(alpha) and the transposed products (sumcheck.rs:195-227)
+  Scratch s_eq, s_alph;
+  if ((rc = s_eq.alloc(32 * nc, s))) return rc;
+  if ((rc = s_alph.alloc(32 * nw, s))) return rc;
+  uint64_t* eq = static_cast<uint64_t*>(s_eq.ptr);
+  uint64_t* alph = static_cast<uint64_t*>(s_alph.ptr);
+  if ((rc = eq_hypercube_device(&out->alpha[0][0], m0, nc, eq, s))) return rc;
+  // public weights (whir_r1cs.rs:665-676): the hash of no public inputs is 0
+  const uint64_t zero[4] = {0, 0, 0, 0};
+  pkg_transcript_absorb(&out->transcript, zero);
+  pkg_transcript_squeeze(&out->transcript, out->public_x);
+  for (int k = 0; k < 3; k++) {
+    Scratch s_t;
+    const size_t nnz = r1cs->nnz[k];
+    const size_t rp_bytes = ((8 * (nw + 1) + 255) / 256) * 256;
+    const size_t cl_bytes = ((4 * (nnz ? nnz : 1) + 255) / 256) * 256;
+    if ((rc = s_t.alloc(rp_bytes + cl_bytes + 32 * (nnz ? nnz : 1), s))) return rc;
+    uint8_t* base = static_cast<uint8_t*>(s_t.ptr);
+    uint64_t* rp_t = reinterpret_cast<uint64_t*>(base);
+    uint32_t* cl_t = reinterpret_cast<uint32_t*>(base + rp_bytes);
+    uint64_t* vl_t = reinterpret_cast<uint64_t*>(base + rp_bytes + cl_bytes);
+    rc = pkg_csr_transpose(r1cs->row_ptr[k], r1cs->cols[k], r1cs->vals[k], nc, nw, nnz, rp_t, cl_t,
+                           vl_t, stream);
+    if (rc) return rc;
+    if ((rc = spmv_device(rp_t, cl_t, vl_t, nw, nc, eq, alph, err, s))) return rc;
+    // create_weights_and_evaluations (:623-642): the zero padding adds nothing
+    if ((rc = dot_device(alph, poly, nw, dot_out, part, s))) return rc;
+    PK_CUDA(cudaMemcpyAsync(out->evals[k], dot_out, 32, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    pkg_transcript_absorb(&out->transcript, out->evals[k]);
+  }
+  return PKG_OK;
+}

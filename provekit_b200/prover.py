@@ -1,0 +1,88 @@
+"""Prover-level entry points: the synthetic R1CS workload and the Spartan
+prove core (provekit/prover/src/whir_r1cs.rs up to WHIR's prove call)."""
+import ctypes
+
+import numpy as np
+import torch
+
+from ._lib import check, lib
+from .spartan import Transcript
+
+
+class R1csC(ctypes.Structure):
+    _fields_ = [("num_constraints", ctypes.c_size_t), ("num_witnesses", ctypes.c_size_t),
+                ("row_ptr", ctypes.c_void_p * 3), ("cols", ctypes.c_void_p * 3),
+                ("vals", ctypes.c_void_p * 3), ("nnz", ctypes.c_size_t * 3)]
+
+
+class SpartanProofC(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_size_t), ("m0", ctypes.c_size_t), ("root", ctypes.c_uint8 * 32),
+                ("r", ctypes.c_uint64 * 120), ("coeffs", ctypes.c_uint64 * 480),
+                ("alpha", ctypes.c_uint64 * 120), ("rho", ctypes.c_uint64 * 4),
+                ("sum_g", ctypes.c_uint64 * 4), ("blinding_eval", ctypes.c_uint64 * 4),
+                ("public_x", ctypes.c_uint64 * 4), ("evals", ctypes.c_uint64 * 12),
+                ("transcript", Transcript)]
+
+    def as_dict(self):
+        m0 = self.m0
+        arr = lambda x, n: np.array(x[: 4 * n], dtype=np.uint64).reshape(n, 4)  # noqa: E731
+        return {"m": self.m, "m0": m0, "root": bytes(self.root), "r": arr(self.r, m0),
+                "coeffs": arr(self.coeffs, 4 * m0), "alpha": arr(self.alpha, m0),
+                "rho": np.array(self.rho, np.uint64), "sum_g": np.array(self.sum_g, np.uint64),
+                "blinding_eval": np.array(self.blinding_eval, np.uint64),
+                "public_x": np.array(self.public_x, np.uint64), "evals": arr(self.evals, 3),
+                "transcript": (list(self.transcript.l), list(self.transcript.r))}
+
+
+class HostR1CS:
+    """Synthetic satisfiable R1CS in host memory (pkg_synthetic_r1cs)."""
+
+    def __init__(self, seed: int, num_constraints: int, num_inputs: int):
+        nc, ni = num_constraints, num_inputs
+        self.num_constraints, self.num_inputs = nc, ni
+        self.num_witnesses = 1 + ni + nc
+        self.row_ptr = [np.zeros(nc + 1, np.uint64) for _ in range(3)]
+        caps = [3 * nc, 3 * nc, nc]
+        self.cols = [np.zeros(max(c, 1), np.uint32) for c in caps]
+        self.vals = [np.zeros((max(c, 1), 4), np.uint64) for c in caps]
+        self.witness = np.zeros((self.num_witnesses, 4), np.uint64)
+        nnz = (ctypes.c_size_t * 3)()
+        rp = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.row_ptr])
+        cl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.cols])
+        vl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.vals])
+        check(lib().pkg_synthetic_r1cs(seed, nc, ni, rp, cl, vl, nnz, self.witness.ctypes.data))
+        self.nnz = list(nnz)
+        self.cols = [c[:n] for c, n in zip(self.cols, self.nnz)]
+        self.vals = [v[:n] for v, n in zip(self.vals, self.nnz)]
+
+    def to_device(self, device="cuda"):
+        return DeviceR1CS(self, device)
+
+
+class DeviceR1CS:
+    def __init__(self, h: HostR1CS, device="cuda"):
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(  # noqa: E731
+            np.int32 if a.dtype == np.uint32 else np.int64)).to(device)
+        self.num_constraints, self.num_witnesses = h.num_constraints, h.num_witnesses
+        self.row_ptr = [t(a) for a in h.row_ptr]
+        self.cols = [t(a) for a in h.cols]
+        self.vals = [t(a) for a in h.vals]
+        self.nnz = list(h.nnz)
+        self.witness = t(h.witness)
+        self.c = R1csC(h.num_constraints, h.num_witnesses,
+                       (ctypes.c_void_p * 3)(*[x.data_ptr() for x in self.row_ptr]),
+                       (ctypes.c_void_p * 3)(*[x.data_ptr() for x in self.cols]),
+                       (ctypes.c_void_p * 3)(*[x.data_ptr() for x in self.vals]),
+                       (ctypes.c_size_t * 3)(*self.nnz))
+
+
+def spartan_prove(r1cs: DeviceR1CS, witness=None, blinding_seed=1, transcript_domain=3,
+                  folding_factor=3, log_inv_rate=2, stream=None):
+    """pkg_spartan_prove: returns the proof fields as a dict of host values."""
+    w = r1cs.witness if witness is None else witness
+    out = SpartanProofC()
+    s = (stream if stream is not None else torch.cuda.current_stream()).cuda_stream
+    check(lib().pkg_spartan_prove(ctypes.byref(r1cs.c), w.data_ptr(), blinding_seed,
+                                  transcript_domain, folding_factor, log_inv_rate,
+                                  ctypes.byref(out), s))
+    return out.as_dict()

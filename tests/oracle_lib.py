@@ -21,6 +21,41 @@ class Transcript(ctypes.Structure):
     _fields_ = [("l", ctypes.c_uint64 * 4), ("r", ctypes.c_uint64 * 4)]
 
 
+class R1CS(ctypes.Structure):
+    _fields_ = [("num_constraints", ctypes.c_size_t), ("num_witnesses", ctypes.c_size_t),
+                ("row_ptr", ctypes.c_void_p * 3), ("cols", ctypes.c_void_p * 3),
+                ("vals", ctypes.c_void_p * 3)]
+
+
+class SpartanProof(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_size_t), ("m0", ctypes.c_size_t), ("root", ctypes.c_uint8 * 32),
+                ("r", ctypes.c_uint64 * 120), ("coeffs", ctypes.c_uint64 * 480),
+                ("alpha", ctypes.c_uint64 * 120), ("rho", ctypes.c_uint64 * 4),
+                ("sum_g", ctypes.c_uint64 * 4), ("blinding_eval", ctypes.c_uint64 * 4),
+                ("public_x", ctypes.c_uint64 * 4), ("evals", ctypes.c_uint64 * 12),
+                ("transcript", Transcript)]
+
+
+def spartan_prove(h, blinding_seed, domain, ff, lr):
+    """Run pko_spartan_prove on a HostR1CS-like object; returns the proof dict."""
+    r = R1CS(h.num_constraints, h.num_witnesses,
+             (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.row_ptr]),
+             (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.cols]),
+             (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.vals]))
+    out = SpartanProof()
+    rc = lib().pko_spartan_prove(ctypes.byref(r), p64(np.ascontiguousarray(h.witness)), blinding_seed,
+                                 domain, ff, lr, ctypes.byref(out))
+    assert rc == 0, rc
+    m0 = out.m0
+    arr = lambda x, n: np.array(x[: 4 * n], dtype=np.uint64).reshape(n, 4)  # noqa: E731
+    return {"m": out.m, "m0": m0, "root": bytes(out.root), "r": arr(out.r, m0),
+            "coeffs": arr(out.coeffs, 4 * m0), "alpha": arr(out.alpha, m0),
+            "rho": np.array(out.rho, np.uint64), "sum_g": np.array(out.sum_g, np.uint64),
+            "blinding_eval": np.array(out.blinding_eval, np.uint64),
+            "public_x": np.array(out.public_x, np.uint64), "evals": arr(out.evals, 3),
+            "transcript": (list(out.transcript.l), list(out.transcript.r))}
+
+
 _lib = None
 
 
@@ -63,6 +98,8 @@ def lib():
                                            _u64p, _u64p, _u64p, _u64p, _u64p, _u64p]
         L.pko_from_mont_many.argtypes = [_u64p, _sz]
         L.pko_to_mont_many.argtypes = [_u64p, _sz]
+        L.pko_spartan_prove.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_uint64,
+                                        ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]
     return _lib
 
 

@@ -53,8 +53,8 @@ def test_zk_sumcheck_satisfies_verifier_identities(m0):
     n = 1 << m0
     a = [rng.randrange(P) for _ in range(n)]
     b = [rng.randrange(P) for _ in range(n)]
-    c = [x * y % P for x, y in zip(a, b)]  # satisfied instance: sum is rho * sum_g
-    c[0] = (c[0] + 1) % P                    # ...and one that is not: identities still hold
+    c = [x * y % P for x, y in zip(a, b)]
+    c[0] = (c[0] + 1) % P  # unsatisfied: the per-round identities still hold
     g = [rng.randrange(P) for _ in range(4 * m0)]
     offset = 3
     w1 = [rng.randrange(P) for _ in range(offset + 4 * m0 + 5)]
@@ -71,20 +71,12 @@ def test_zk_sumcheck_satisfies_verifier_identities(m0):
         eqr.append(v)
     total_f = sum(e * (x * y - z) for e, x, y, z in zip(eqr, a, b, c)) % P
     claim = rho * sum_g % P
-    # first round: h(0) + h(1) == claim only if sum F == 0 (c = a*b except c[0]):
     for i in range(m0):
         cf = coeffs[4 * i: 4 * i + 4]
         assert (2 * cf[0] + cf[1] + cf[2] + cf[3]) % P == claim   # prover's own assert
         claim = cubic(cf, alpha[i])
-    eq_ra = 1
-    for ri, ai in zip(r, alpha):
-        eq_ra = eq_ra * (ri * ai + (1 - ri) * (1 - ai)) % P
-    f_alpha = eq_ra * (mle(a, alpha) * mle(b, alpha) - mle(c, alpha)) % P
-    g_alpha = sum(cubic(gi, ai) for gi, ai in zip(gs, alpha)) % P
-    # The sumcheck claim is consistent with F only when sum F == 0; here
-    # sum F = eq(r,0..0)*(-1) != 0, so check the identity with that offset
-    # propagated: final = F(alpha) + rho*G(alpha) + (error terms) is only
-    # exact for satisfied instances -- test those separately below.
+    # sum F != 0 here, so the final claim cannot match F(alpha) + rho G(alpha)
+    # (the next test checks that on satisfied instances)
     assert total_f != 0
     expected_be = 0
     for i in range(m0):
@@ -117,3 +109,26 @@ def test_zk_sumcheck_final_claim_on_satisfied_instance(m0):
     f_alpha = eq_ra * (mle(a, alpha) * mle(b, alpha) - mle(c, alpha)) % P
     g_alpha = sum(cubic(gi, ai) for gi, ai in zip(gs, alpha)) % P
     assert claim == (f_alpha + rho * g_alpha) % P
+
+
+@pytest.mark.parametrize("nc,ni", [(1, 1), (3, 2), (1 << 10, 1 << 8), (5000, 3000)])
+def test_synthetic_r1cs_is_satisfied_and_sized_like_new_for_r1cs(nc, ni):
+    """pkg_synthetic_r1cs gives A w o B w == C w, and the prove core sizes
+    m, m0 as WhirR1CSScheme::new_for_r1cs does
+    (provekit/r1cs-compiler/src/whir_r1cs.rs:48-92)."""
+    from provekit_b200.prover import HostR1CS
+    h = HostR1CS(nc + ni, nc, ni)
+    ys = []
+    for k in range(3):
+        y = np.zeros((nc, 4), np.uint64)
+        O.lib().pko_spmv(O.p64(h.row_ptr[k]), O.p32(np.ascontiguousarray(h.cols[k])),
+                         O.p64(np.ascontiguousarray(h.vals[k])), nc, O.p64(h.witness), O.p64(y))
+        ys.append(unpack(y))
+    assert all((x * y - z) % P == 0 for x, y, z in zip(*ys))
+    pr = O.spartan_prove(h, 1, 2, 3, 2)
+    nw = h.num_witnesses
+    clog = lambda n: max(n - 1, 0).bit_length()  # noqa: E731
+    m, m0 = max(clog(nw), 13), max(clog(nc), 1)
+    if (1 << m) - nw < 4 * m0:
+        m += 1
+    assert (pr["m"], pr["m0"]) == (m, m0)
