@@ -133,6 +133,16 @@ int pkg_host_skyscraper_hash_many(size_t size, const uint8_t *input, size_t coun
 int pkg_skyscraper_pow_solve(const uint64_t challenge[4], const uint64_t threshold[4],
                              uint64_t *nonce_out);
 
+/* ---- Poseidon2 (poseidon2/src), BN254, t = 4, rf = 8, rp = 56 ------------ */
+/* In-place permutation of n states of 4 Fr (Montgomery form), state i at
+ * states[16*i .. 16*i + 16).  Replaces poseidon2_permutation
+ * (poseidon2/src/permutation.rs:134-177).  Device pointer. */
+int pkg_poseidon2_permutation_many(uint64_t *states, size_t n, pkg_stream_t stream);
+/* out[i] = poseidon2_hash(inputs[i*len .. (i+1)*len)) (poseidon2/src/hash.rs:17-47:
+ * rate 3, capacity lane initialised to len * 2^64).  Device pointers. */
+int pkg_poseidon2_hash_many(const uint64_t *inputs, size_t len, size_t n, uint64_t *out,
+                            pkg_stream_t stream);
+
 /* ---- Merkle commit ------------------------------------------------------- */
 /* Binary Skyscraper Merkle tree over num_leaves (power of two) leaves of
  * leaf_size bytes: leaf digests = hash_many(leaf_size), internal nodes =
@@ -276,7 +286,57 @@ int pkg_synthetic_r1cs(uint64_t seed, size_t num_constraints, size_t num_inputs,
                        uint64_t *row_ptr[3], uint32_t *cols[3], uint64_t *vals[3],
                        size_t nnz_out[3], uint64_t *witness);
 
+/* ---- Batched form ----------------------------------------------------------- */
+/* A batch of independent jobs of uneven sizes.  Job j (size n = 2^log_n,
+ * 4 <= log_n <= 24) has n coefficients from pkg_sample_fr(seed + j) and runs
+ *   (1) ntt_nr over a copy of its coefficients (pkg_ntt_nr),
+ *   (2) the WHIR commit of its coefficients: 8 contiguous messages, rate 1/4,
+ *       canonical leaves of 8 Fr (pkg_whir_commit with folding factor 3),
+ *   (3) the Spartan zk-sumcheck (pkg_spartan_sumcheck) over a = its
+ *       coefficients, b = its NTT output, c = the first n codeword entries,
+ *       with blinding g = pkg_sample_fr(seed + 0x100000 + j), w1 blinding
+ *       values = pkg_sample_fr(seed + 0x200000 + j), transcript domain j + 1.
+ * Each phase runs as one grouped kernel over all jobs and the transcript runs
+ * on the device, so the batch is one CUDA graph; results equal the plain
+ * entry points run job by job.  No reference counterpart (the reference
+ * proves one instance at a time). */
+typedef struct pkg_batch pkg_batch;
+typedef struct {
+  uint32_t log_n;
+  size_t n;
+  uint64_t *coeffs, *ntt, *codeword; /* device: n, n, 4n Fr */
+  uint8_t *layers;                   /* device: 2*num_leaves - 1 digests */
+  size_t num_leaves;
+  uint64_t transcript_domain;
+  uint64_t g[120][4];            /* host copy: blinding polynomial, 4*m0 Fr  */
+  uint64_t w1_blinding[120][4];  /* host copy: w1 blinding values, 4*m0 Fr  */
+} pkg_batch_job;
+typedef struct {
+  size_t m0;
+  uint64_t r[30][4], coeffs[120][4], alpha[30][4];
+  uint64_t rho[4], sum_g[4], blinding_eval[4];
+  pkg_transcript transcript;
+} pkg_sumcheck_result;
+int pkg_batch_create(const uint32_t *log_sizes, size_t njobs, uint64_t seed, pkg_batch **out);
+void pkg_batch_destroy(pkg_batch *batch);
+int pkg_batch_job_info(pkg_batch *batch, size_t job, pkg_batch_job *out);
+/* NTT plan: passes of at most kmax stages (radix 2^kmax), 2^log_elems_per_cta
+ * elements staged per CTA.  Re-planning drops a captured graph. */
+int pkg_batch_set_params(pkg_batch *batch, int kmax, int log_elems_per_cta);
+/* Autotuner: times every (kmax in 4..11, elements per CTA) on this batch and
+ * keeps the fastest. */
+int pkg_batch_tune(pkg_batch *batch, pkg_stream_t stream, int *best_kmax, int *best_log_elems,
+                   double *best_ms);
+/* Run the batch on stream.  use_graph: the first call captures the batch as
+ * a CUDA graph (stream must not be the legacy default stream), later calls
+ * replay it. */
+int pkg_batch_run(pkg_batch *batch, int use_graph, pkg_stream_t stream);
+/* Host copy of job j's sumcheck outputs (synchronous). */
+int pkg_batch_sumcheck_result(pkg_batch *batch, size_t job, pkg_sumcheck_result *out);
+
 /* ---- diagnostics ---------------------------------------------------------- */
+/* Synchronous device -> host copy of library-owned memory (e.g. batch buffers). */
+int pkg_copy_to_host(void *dst, const void *src, size_t bytes);
 /* Number of kernels this library has launched in this process. */
 uint64_t pkg_kernel_launches(void);
 /* Measured 32-bit IMAD-class throughput of the current device (instructions

@@ -7,6 +7,7 @@
  * loops are parallelised with OpenMP where the reference uses rayon.
  */
 #include "pk_oracle.h"
+#include "poseidon2_t4_constants.h"
 
 #include <stdlib.h>
 #include <string.h>
@@ -1013,4 +1014,85 @@ int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t bl
     }
     free(eq); free(alph); free(poly);
     return 0;
+}
+
+/* ======================================================================= */
+/* Poseidon2, t = 4, rf = 8, rp = 56 (poseidon2/src/permutation.rs)         */
+/* ======================================================================= */
+static void p2_sbox(uint64_t x[4]) { /* x^5, :86-89 */
+    uint64_t s[4];
+    pko_fr_mul(s, x, x);
+    pko_fr_mul(s, s, s);
+    pko_fr_mul(x, s, x);
+}
+
+static void p2_ext(uint64_t st[16]) { /* matrix_multiplication_4x4, :101-120 */
+    uint64_t t0[4], t1[4], t2[4], t3[4], t4[4], t5[4], t6[4], t7[4];
+    pko_fr_add(t0, st, st + 4);
+    pko_fr_add(t1, st + 8, st + 12);
+    pko_fr_add(t2, st + 4, st + 4);
+    pko_fr_add(t2, t2, t1);
+    pko_fr_add(t3, st + 12, st + 12);
+    pko_fr_add(t3, t3, t0);
+    pko_fr_add(t4, t1, t1);
+    pko_fr_add(t4, t4, t4);
+    pko_fr_add(t4, t4, t3);
+    pko_fr_add(t5, t0, t0);
+    pko_fr_add(t5, t5, t5);
+    pko_fr_add(t5, t5, t2);
+    pko_fr_add(t6, t3, t5);
+    pko_fr_add(t7, t2, t4);
+    cpy4(st, t6);
+    cpy4(st + 4, t5);
+    cpy4(st + 8, t7);
+    cpy4(st + 12, t4);
+}
+
+static void p2_int(uint64_t st[16]) { /* internal_m_multiplication, :122-127 */
+    uint64_t sum[4] = {0, 0, 0, 0}, t[4];
+    for (int i = 0; i < 4; i++) pko_fr_add(sum, sum, st + 4 * i);
+    for (int i = 0; i < 4; i++) {
+        pko_fr_mul(t, st + 4 * i, POSEIDON2_T4_DIAG_MONT[i]);
+        pko_fr_add(st + 4 * i, t, sum);
+    }
+}
+
+void pko_poseidon2_permutation(uint64_t st[16]) { /* permutation, :134-167 */
+    p2_ext(st);
+    for (int r = 0; r < 64; r++) {
+        if (r < 4 || r >= 60) {
+            for (int i = 0; i < 4; i++) {
+                pko_fr_add(st + 4 * i, st + 4 * i, POSEIDON2_T4_RC_MONT[r][i]);
+                p2_sbox(st + 4 * i);
+            }
+            p2_ext(st);
+        } else {
+            pko_fr_add(st, st, POSEIDON2_T4_RC_MONT[r][0]);
+            p2_sbox(st);
+            p2_int(st);
+        }
+    }
+}
+
+/* poseidon2_hash (poseidon2/src/hash.rs:17-47): rate 3, IV = len * 2^64 in lane 3. */
+void pko_poseidon2_hash(uint64_t out[4], const uint64_t *inputs, size_t n) {
+    uint64_t st[16] = {0}, cache[12] = {0};
+    uint64_t two64[4] = {0, 1, 0, 0}, lenv[4] = {n, 0, 0, 0};
+    pko_fr_to_mont(two64, two64);
+    pko_fr_to_mont(lenv, lenv);
+    pko_fr_mul(st + 12, lenv, two64);
+    size_t cs = 0;
+    for (size_t k = 0; k < n; k++) {
+        if (cs == 3) {
+            for (int i = 0; i < 3; i++) pko_fr_add(st + 4 * i, st + 4 * i, cache + 4 * i);
+            memset(cache, 0, sizeof cache);
+            cs = 0;
+            pko_poseidon2_permutation(st);
+        }
+        cpy4(cache + 4 * cs, inputs + 4 * k);
+        cs++;
+    }
+    for (size_t i = 0; i < cs; i++) pko_fr_add(st + 4 * i, st + 4 * i, cache + 4 * i);
+    pko_poseidon2_permutation(st);
+    cpy4(out, st);
 }

@@ -133,6 +133,10 @@ int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t bl
                       uint64_t domain, unsigned folding_factor, unsigned log_inv_rate,
                       pko_spartan_proof *out);
 
+/* ---- Poseidon2 t = 4 (poseidon2/src) ----------------------------------- */
+void pko_poseidon2_permutation(uint64_t state[16]);                      /* mont in/out */
+void pko_poseidon2_hash(uint64_t out[4], const uint64_t *inputs, size_t n); /* mont */
+
 int pko_num_threads(void);
 
 #ifdef __cplusplus

@@ -44,6 +44,8 @@ SIGNATURES = {
     "pkg_skyscraper_hash_many": [_c_sz, _c_vp, _c_sz, _c_vp, _c_vp],
     "pkg_host_skyscraper_hash_many": [_c_sz, _c_vp, _c_sz, _c_vp],
     "pkg_skyscraper_pow_solve": [_c_vp, _c_vp, _c_u64p],
+    "pkg_poseidon2_permutation_many": [_c_vp, _c_sz, _c_vp],
+    "pkg_poseidon2_hash_many": [_c_vp, _c_sz, _c_sz, _c_vp, _c_vp],
     "pkg_merkle_tree": [_c_vp, _c_sz, _c_sz, _c_vp, _c_vp],
     "pkg_merkle_tree_fr": [_c_vp, _c_sz, _c_sz, _c_int, _c_vp, _c_vp],
     "pkg_merkle_leaves_fr": [_c_vp, _c_sz, _c_sz, _c_int, _c_vp, _c_vp],
@@ -63,6 +65,13 @@ SIGNATURES = {
     "pkg_spartan_prove": [_c_vp, _c_vp, ctypes.c_uint64, ctypes.c_uint64, _c_uint, _c_uint, _c_vp,
                           _c_vp],
     "pkg_synthetic_r1cs": [ctypes.c_uint64, _c_sz, _c_sz, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+    "pkg_batch_create": [_c_vp, _c_sz, ctypes.c_uint64, _c_vp],
+    "pkg_batch_job_info": [_c_vp, _c_sz, _c_vp],
+    "pkg_batch_set_params": [_c_vp, _c_int, _c_int],
+    "pkg_batch_tune": [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+    "pkg_batch_run": [_c_vp, _c_int, _c_vp],
+    "pkg_batch_sumcheck_result": [_c_vp, _c_sz, _c_vp],
+    "pkg_copy_to_host": [_c_vp, _c_vp, _c_sz],
     "pkg_measure_imad_rate": [ctypes.POINTER(ctypes.c_double)],
     "pkg_version": [],
 }
@@ -92,6 +101,8 @@ def lib():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = ctypes.c_int
+        L.pkg_batch_destroy.argtypes = [_c_vp]
+        L.pkg_batch_destroy.restype = None
         L.pkg_kernel_launches.argtypes = []
         L.pkg_kernel_launches.restype = ctypes.c_uint64
         _lib = L
@@ -109,4 +120,4 @@ def check(rc: int):
 
 
 def exported_symbols():
-    return sorted(SIGNATURES) + ["pkg_last_error", "pkg_kernel_launches"]
+    return sorted(SIGNATURES) + ["pkg_last_error", "pkg_kernel_launches", "pkg_batch_destroy"]

@@ -23,7 +23,8 @@ def sources():
 
 
 def deps():
-    return sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) + [
+    return sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) + \
+        glob.glob(os.path.join(CSRC, "*.h")) + [
         os.path.join(ROOT, "include", "provekit_b200.h")]
 
 

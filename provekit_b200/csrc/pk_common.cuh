@@ -33,6 +33,8 @@ inline int cuda_status(cudaError_t e, const char* what) {
   } while (0)
 
 void count_launch();
+// Subtract n launches from the counter (n may wrap to add: 0 - n).
+void count_launches_undo(uint64_t n);
 
 #define PK_CHECK_LAUNCH(name) \
   do {                        \

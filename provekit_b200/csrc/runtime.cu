@@ -25,6 +25,7 @@ void clear_last_error() { g_last_error[0] = 0; }
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches_undo(uint64_t n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 
 int sm_count() {
   static std::mutex mu;
@@ -148,5 +149,12 @@ extern "C" int pkg_measure_imad_rate(double* instr_per_second) {
   if (err != cudaSuccess) return cuda_status(err, "imad_rate_kernel");
   double instr = (double)blocks * threads * iters * 8.0 * 8.0;
   *instr_per_second = instr / (ms * 1e-3);
+  return PKG_OK;
+}
+
+extern "C" int pkg_copy_to_host(void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return PKG_OK;
+  PK_REQUIRE(dst && src, "null pointer");
+  PK_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
   return PKG_OK;
 }

@@ -98,6 +98,8 @@ def lib():
                                            _u64p, _u64p, _u64p, _u64p, _u64p, _u64p]
         L.pko_from_mont_many.argtypes = [_u64p, _sz]
         L.pko_to_mont_many.argtypes = [_u64p, _sz]
+        L.pko_poseidon2_permutation.argtypes = [_u64p]
+        L.pko_poseidon2_hash.argtypes = [_u64p, _u64p, _sz]
         L.pko_spartan_prove.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_uint64,
                                         ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]
     return _lib

@@ -320,3 +320,22 @@ def test_multiply_transposed_by_eq_alpha_kat():
         O.lib().pko_spmv(O.p64(row_ptr), O.p32(np.array(cols, np.uint32)), O.p64(pack(vals)), nw,
                          O.p64(eq), O.p64(y))
         assert unpack(y) == [v % P for v in exp["expected"][name]]
+
+
+# --------------------------------------------------------------------------
+# Poseidon2 (poseidon2/src/permutation.rs:182-195, hash.rs:53-70)
+# --------------------------------------------------------------------------
+def test_poseidon2_permutation_kat():
+    k = KATS["poseidon2"]["permutation_zero"]
+    st = np.zeros((4, 4), np.uint64)
+    O.lib().pko_poseidon2_permutation(O.p64(st))
+    assert unpack(st) == [int(x) for x in k["expected"]]
+
+
+@pytest.mark.parametrize("name", ["hash_single", "hash_two"])
+def test_poseidon2_hash_kat(name):
+    k = KATS["poseidon2"][name]
+    inp = pack([int(x) for x in k["input"]])
+    out = np.zeros(4, np.uint64)
+    O.lib().pko_poseidon2_hash(O.p64(out), O.p64(inp), inp.shape[0])
+    assert unpack(out.reshape(1, 4))[0] == int(k["expected"])
