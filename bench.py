@@ -45,6 +45,12 @@ def parse_args():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plugin-e2e", action="store_true")
+    p.add_argument("--workload", choices=["commit", "prove", "batched"], default="commit",
+                   help="commit (default, the headline line): WHIR commit of 2^20 coefficients; "
+                        "prove: Spartan prove core of a 2^20-constraint R1CS; batched: 256 uneven "
+                        "jobs as one CUDA graph vs the same jobs one at a time")
+    p.add_argument("--jobs", type=int, default=256)
+    p.add_argument("--tune", action="store_true", help="batched: run the NTT radix autotuner first")
     return p.parse_args()
 
 
@@ -429,10 +435,187 @@ def run_b200(a):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# Config 3: the Spartan prove core (everything before WHIR's own rounds) of a
+# synthetic 2^20-constraint R1CS.
+# ---------------------------------------------------------------------------
+def run_prove(a):
+    import numpy as np
+    import torch
+
+    from provekit_b200 import _lib
+    from provekit_b200.prover import HostR1CS, spartan_prove
+
+    L = _lib.lib()
+    torch.cuda.set_device(0)
+    nc, ni = 1 << 20, 1 << 18
+    t0 = time.perf_counter()
+    h = HostR1CS(a.seed, nc, ni)
+    gen_s = time.perf_counter() - t0
+    d = h.to_device()
+    stream = torch.cuda.Stream()
+    w_pinned = torch.from_numpy(h.witness.view(np.int64)).pin_memory()
+    w_dev = torch.empty_like(d.witness)
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            spartan_prove(d, stream=stream)
+    stream.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
+    clocks = ClockSampler(physical_gpu_index(0))
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = L.pkg_kernel_launches()
+    with torch.cuda.stream(stream):
+        for i in range(a.steps):
+            evs[i][0].record(stream)
+            spartan_prove(d, stream=stream)
+            evs[i][1].record(stream)
+    stream.synchronize()
+    launches = L.pkg_kernel_launches() - launches0
+    clk = clocks.stop()
+    ms = [e[0].elapsed_time(e[1]) for e in evs]
+    # e2e: witness from pinned host memory each step, proof struct read back
+    e2e = []
+    with torch.cuda.stream(stream):
+        for i in range(a.steps):
+            t0 = time.perf_counter()
+            w_dev.copy_(w_pinned, non_blocking=True)
+            spartan_prove(d, witness=w_dev, stream=stream)
+            e2e.append(time.perf_counter() - t0)
+    cpu = None
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as O
+        t0 = time.perf_counter()
+        O.spartan_prove(h, 1, 3, 3, 2)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": 1.0 / cpu_s, "unit": "proof-cores/s", "cores": O.lib().pko_num_threads(),
+               "kind": "port", "sample": "one full prove core on the host (C restatement, OpenMP)"}
+    line = {"metric": "Spartan prove core (before WHIR rounds) @2^20-constraint synthetic R1CS",
+            "value": 1e3 / statistics.mean(ms), "unit": "prove-cores/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": statistics.mean(ms),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32 (BN254 Fr, 8x32-bit limbs)", "data": "synthetic R1CS (pkg_synthetic_r1cs)",
+            "config": {"workload": "spartan_prove_core", "num_constraints": nc, "num_inputs": ni,
+                       "num_witnesses": h.num_witnesses, "folding_factor": 3, "log_inv_rate": 2,
+                       "host_generation_s": gen_s},
+            "e2e": {"value": len(e2e) / sum(e2e), "unit": "prove-cores/s",
+                    "h2d_bytes_per_step": 32 * h.num_witnesses,
+                    "d2h_bytes_per_step": 32 * 3 + 32 * 4 * 20 * 4,
+                    "note": "wall clock, witness copied from pinned host memory every step"},
+            "p50_ms": statistics.median(ms), "cpu_baseline": cpu, "gpu_launches": int(launches),
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Config 4: the batched form vs the plain path.
+# ---------------------------------------------------------------------------
+def batched_sizes(seed, jobs, lo=10, hi=22):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [int(x) for x in rng.integers(lo, hi + 1, size=jobs)]
+
+
+def run_batched(a):
+    import numpy as np
+    import torch
+
+    from provekit_b200 import _lib
+    from provekit_b200.batch import Batch
+    from provekit_b200.merkle import whir_commit
+    from provekit_b200.ntt import ntt_nr
+    from provekit_b200.spartan import Transcript, spartan_sumcheck
+
+    L = _lib.lib()
+    torch.cuda.set_device(0)
+    sizes = batched_sizes(a.seed, a.jobs)
+    total_fr = sum(1 << k for k in sizes)
+    t0 = time.perf_counter()
+    b = Batch(sizes, seed=a.seed)
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    tuned = None
+    if a.tune:
+        k, e, ms = b.tune(stream)
+        tuned = {"kmax": k, "log_elems_per_cta": e, "ms": ms}
+    b.run(use_graph=True, stream=stream)  # capture
+    for _ in range(a.warmup):
+        b.run(use_graph=True, stream=stream)
+    stream.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
+    clocks = ClockSampler(physical_gpu_index(0))
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = L.pkg_kernel_launches()
+    for i in range(a.steps):
+        evs[i][0].record(stream)
+        b.run(use_graph=True, stream=stream)
+        evs[i][1].record(stream)
+    stream.synchronize()
+    launches = L.pkg_kernel_launches() - launches0
+    clk = clocks.stop()
+    ms = [e[0].elapsed_time(e[1]) for e in evs]
+    # plain path: the same jobs one at a time (pkg_ntt_nr, pkg_whir_commit,
+    # pkg_spartan_sumcheck), device-resident inputs
+    plain_ms = 0.0
+    mismatches = 0
+    with torch.cuda.stream(stream):
+        for j in range(len(sizes)):
+            job = b.job(j)
+            n = job.n
+            coeffs = torch.from_numpy(Batch.read_fr(job.coeffs, n).view(np.int64)).cuda()
+            g = np.array(job.g[: 16 * job.log_n], np.uint64).reshape(-1, 4)
+            wb = np.array(job.w1_blinding[: 16 * job.log_n], np.uint64).reshape(-1, 4)
+            ntt = torch.empty_like(coeffs)
+            cwb = torch.empty((4 * n, 4), dtype=torch.int64, device="cuda")
+            lay = torch.empty(32 * (2 * job.num_leaves - 1), dtype=torch.uint8, device="cuda")
+            ta, tb, tc = (torch.empty_like(coeffs) for _ in range(3))
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ntt.copy_(coeffs)
+            ntt_nr(ntt, n, 1, stream=stream)
+            whir_commit(coeffs, 3, 2, codeword=cwb, layers=lay, stream=stream)
+            ta.copy_(coeffs)
+            tb.copy_(ntt)
+            tc.copy_(cwb[:n])
+            t = Transcript.new(job.transcript_domain)
+            sc = spartan_sumcheck(ta, tb, tc, job.log_n, g, wb, t, stream=stream)
+            e1.record(stream)
+            stream.synchronize()
+            plain_ms += e0.elapsed_time(e1)
+            if j % 32 == 0:  # spot parity (the full check is in tests/test_gpu_batch.py)
+                got = b.sumcheck_result(j)
+                if not (np.array_equal(got["alpha"], sc["alpha"])
+                        and Batch.read(job.layers, 32 * (2 * job.num_leaves - 1)) == lay.cpu().numpy().tobytes()):
+                    mismatches += 1
+    batch_ms = statistics.mean(ms)
+    line = {"metric": "batched form: 256 uneven jobs (NTT + WHIR commit + zk-sumcheck each) as one "
+                      "CUDA graph vs the same jobs one at a time",
+            "value": len(sizes) / (batch_ms * 1e-3), "unit": "jobs/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": batch_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32 (BN254 Fr, 8x32-bit limbs)", "data": "synthetic (ChaCha20-seeded Fr)",
+            "config": {"workload": "batched", "jobs": len(sizes), "log_sizes": sizes,
+                       "total_fr": total_fr, "log2_total_fr": float(np.log2(total_fr)),
+                       "setup_s": setup_s, "tuned": tuned},
+            "fr_per_s": total_fr / (batch_ms * 1e-3),
+            "plain": {"value": len(sizes) / (plain_ms * 1e-3), "unit": "jobs/s", "ms": plain_ms},
+            "speedup_vs_plain": plain_ms / batch_ms, "spot_parity_mismatches": mismatches,
+            "gpu_launches": int(launches), "clocks": clk}
+    print(json.dumps(line), flush=True)
+    b.close()
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "prove":
+        run_prove(a)
+    elif a.workload == "batched":
+        run_batched(a)
     else:
         run_b200(a)
 

@@ -14,7 +14,9 @@
 // Results are bit-identical to running each job alone through pkg_ntt_nr,
 // pkg_whir_commit and pkg_spartan_sumcheck.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "fr.cuh"
@@ -744,7 +746,6 @@ extern "C" int pkg_batch_create(const uint32_t* log_sizes, size_t njobs, uint64_
   }
   b->jobs.resize(njobs);
   b->init_state.resize(njobs);
-  std::vector<uint64_t> host(4 * max_order);
   for (size_t j = 0; j < njobs; j++) {
     const size_t n = size_t(1) << log_sizes[j];
     JobDev& jb = b->jobs[j];
@@ -771,13 +772,6 @@ extern "C" int pkg_batch_create(const uint32_t* log_sizes, size_t njobs, uint64_
     jb.eq_hi = reinterpret_cast<uint64_t*>(take(32 * (size_t(1) << jb.nhi)));
     jb.eq_lo = reinterpret_cast<uint64_t*>(take(32 * (size_t(1) << jb.nlo)));
     jb.part = reinterpret_cast<uint64_t*>(take(32 * 3 * kScCtaCap));
-    // inputs: coefficients from the sampler, seed + j
-    pkg_sample_fr(seed + j, n, host.data(), 1);
-    e = cudaMemcpy(jb.coeffs, host.data(), 32 * n, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-      pkg_batch_destroy(b);
-      return cuda_status(e, "pkg_batch_create upload");
-    }
     // sumcheck state: blinding g and w1 blinding values from the sampler
     ScState& st = b->init_state[j];
     memset(&st, 0, sizeof st);
@@ -789,6 +783,35 @@ extern "C" int pkg_batch_create(const uint32_t* log_sizes, size_t njobs, uint64_
     memcpy(st.wb, wb.data(), 32 * 4 * jb.m0);
     uint64_t dom[4] = {j + 1, 0, 0, 0};
     memcpy(st.domain.v, dom, 32);
+  }
+  // inputs: job j's coefficients from pkg_sample_fr(seed + j); jobs are
+  // sampled on all host threads (each job is its own ChaCha stream)
+  {
+    const unsigned nthreads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::atomic<size_t> next{0};
+    std::atomic<int> failed{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nthreads; t++)
+      pool.emplace_back([&, dev]() {
+        if (cudaSetDevice(dev) != cudaSuccess) failed = 1;
+        std::vector<uint64_t> host;
+        for (size_t j = next++; j < njobs; j = next++) {
+          const size_t n = b->jobs[j].n;
+          host.resize(4 * n);
+          pkg_sample_fr(seed + j, n, host.data(), 1);
+          if (cudaMemcpy(b->jobs[j].coeffs, host.data(), 32 * n, cudaMemcpyHostToDevice) !=
+              cudaSuccess)
+            failed = 1;
+        }
+      });
+    for (auto& th : pool) th.join();
+    if (failed) {
+      pkg_batch_destroy(b);
+      set_last_error("pkg_batch_create: input upload failed");
+      return PKG_ERR_CUDA;
+    }
   }
   e = cudaMalloc(&b->d_jobs, sizeof(JobDev) * njobs);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_state, sizeof(ScState) * njobs);
