@@ -45,12 +45,14 @@ def parse_args():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plugin-e2e", action="store_true")
-    p.add_argument("--workload", choices=["commit", "prove", "batched"], default="commit",
+    p.add_argument("--workload", choices=["commit", "prove", "batched", "served"], default="commit",
                    help="commit (default, the headline line): WHIR commit of 2^20 coefficients; "
                         "prove: Spartan prove core of a 2^20-constraint R1CS; batched: 256 uneven "
                         "jobs as one CUDA graph vs the same jobs one at a time")
     p.add_argument("--jobs", type=int, default=256)
     p.add_argument("--tune", action="store_true", help="batched: run the NTT radix autotuner first")
+    p.add_argument("--requests", type=int, default=32, help="served: requests per arrival rate")
+    p.add_argument("--clock-ms", type=int, default=200, help="nvidia-smi sampling interval")
     return p.parse_args()
 
 
@@ -169,8 +171,9 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, interval_ms=200):
         self.gpu_index = gpu_index
+        self.interval_ms = interval_ms
         self.proc = None
         self.lines = []
 
@@ -178,7 +181,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu_index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -461,7 +464,7 @@ def run_prove(a):
             spartan_prove(d, stream=stream)
     stream.synchronize()
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
-    clocks = ClockSampler(physical_gpu_index(0))
+    clocks = ClockSampler(physical_gpu_index(0), a.clock_ms)
     clocks.start()
     time.sleep(0.3)
     launches0 = L.pkg_kernel_launches()
@@ -608,6 +611,88 @@ def run_batched(a):
     b.close()
 
 
+# ---------------------------------------------------------------------------
+# Config 5: the served form under open-loop Poisson arrivals.
+# ---------------------------------------------------------------------------
+def run_served(a):
+    import concurrent.futures as cf
+
+    import numpy as np
+    import torch
+
+    from provekit_b200.prover import HostR1CS
+    from provekit_b200.server import ProofServer
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(a.seed)
+    logs = [int(x) for x in rng.integers(14, 23, size=a.requests)]
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        reqs = list(ex.map(lambda i: HostR1CS(10_000 + i, 1 << logs[i], 1 << (logs[i] - 2)),
+                           range(a.requests)))
+    gen_s = time.perf_counter() - t0
+    free_b, _ = torch.cuda.mem_get_info()
+    budget = int(min(free_b * 0.8, 120e9))
+    # sequential plain proving: one request at a time (1 slot), service times
+    srv = ProofServer(budget, max_inflight=1)
+    srv.wait(srv.submit(reqs[0], blinding_seed=0, transcript_domain=0))  # warm-up
+    service = []
+    for i, h in enumerate(reqs):
+        _, tm = srv.wait(srv.submit(h, blinding_seed=i, transcript_domain=i))
+        service.append((tm["done_ns"] - tm["submit_ns"]) * 1e-9)
+    srv.close()
+    cap = len(service) / sum(service)
+
+    def pct(v, p):
+        v = sorted(v)
+        return v[min(len(v) - 1, max(0, int(np.ceil(p * len(v))) - 1))]
+
+    sweeps = []
+    for mult in (0.5, 1.0, 1.5, 2.0, 3.0):
+        lam = cap * mult
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(reqs)))
+        # sequential plain proving under the same arrivals (FIFO, measured service times)
+        fin, seq_lat = 0.0, []
+        for t_arr, sv in zip(arrivals, service):
+            start = max(t_arr, fin)
+            fin = start + sv
+            seq_lat.append(fin - t_arr)
+        srv = ProofServer(budget, max_inflight=8)
+        ids = [None] * len(reqs)
+        t_start = time.perf_counter()
+        for i, (t_arr, h) in enumerate(zip(arrivals, reqs)):
+            delay = t_start + t_arr - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids[i] = srv.submit(h, blinding_seed=i, transcript_domain=i)
+        lat = []
+        for rid in ids:
+            _, tm = srv.wait(rid)
+            lat.append((tm["done_ns"] - tm["submit_ns"]) * 1e-9)
+        st = srv.stats()
+        srv.close()
+        served_span = max(arrivals[-1], 0) + 0  # for reference only
+        sweeps.append({
+            "rate_per_s": lam, "rate_vs_sequential_capacity": mult,
+            "served": {"proofs_per_s": st["proofs_per_s"], "p50_ms": 1e3 * pct(lat, 0.5),
+                       "p99_ms": 1e3 * pct(lat, 0.99), "p999_ms": 1e3 * pct(lat, 0.999),
+                       "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9},
+            "sequential": {"proofs_per_s": len(reqs) / fin, "p50_ms": 1e3 * pct(seq_lat, 0.5),
+                           "p99_ms": 1e3 * pct(seq_lat, 0.99), "p999_ms": 1e3 * pct(seq_lat, 0.999)},
+        })
+        del served_span
+    line = {"metric": "served form: open-loop Poisson prove requests (Spartan prove core), "
+                      "log2 constraints uniform on [14, 22]; proofs/s and p50/p99/p99.9 latency vs "
+                      "sequential plain-GPU proving",
+            "value": max(s["served"]["proofs_per_s"] for s in sweeps), "unit": "prove-cores/s",
+            "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32 (BN254 Fr, 8x32-bit limbs)", "data": "synthetic R1CS (pkg_synthetic_r1cs)",
+            "config": {"workload": "served", "requests": len(reqs), "log2_constraints": logs,
+                       "hbm_budget_gb": budget / 1e9, "max_inflight": 8, "generation_s": gen_s},
+            "sequential_capacity_per_s": cap, "sweeps": sweeps}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
@@ -616,6 +701,8 @@ def main():
         run_prove(a)
     elif a.workload == "batched":
         run_batched(a)
+    elif a.workload == "served":
+        run_served(a)
     else:
         run_b200(a)
 

@@ -72,8 +72,10 @@ int pkg_ntt_nr(uint64_t *values, size_t len, size_t codeword_size, size_t num_gr
  * Replaces `pub fn intt_rn(input: &mut [Fr])` (ntt/src/ntt.rs:326-348). */
 int pkg_intt_rn(uint64_t *values, size_t len, pkg_stream_t stream);
 /* Grow the device-resident twiddle table to `order` (power of two <= 2^28).
- * Replaces `NTTEngine::with_order` (ntt/src/ntt.rs:39-45).  Growing
- * synchronises the current device. */
+ * Replaces `NTTEngine::with_order` (ntt/src/ntt.rs:39-45).  Growing builds
+ * the new table synchronously (cudaMalloc + a private stream); superseded
+ * tables stay allocated, so concurrent callers on other streams are safe.
+ * Reserve before capturing a CUDA graph. */
 int pkg_ntt_engine_reserve(size_t order);
 /* pkg_intt_rn for callers that cannot let this library allocate device
  * memory (a service that reserves all HBM for its own admission control, or
@@ -333,6 +335,48 @@ int pkg_batch_tune(pkg_batch *batch, pkg_stream_t stream, int *best_kmax, int *b
 int pkg_batch_run(pkg_batch *batch, int use_graph, pkg_stream_t stream);
 /* Host copy of job j's sumcheck outputs (synchronous). */
 int pkg_batch_sumcheck_result(pkg_batch *batch, size_t job, pkg_sumcheck_result *out);
+
+/* ---- Served form -------------------------------------------------------------- */
+/* A proving service on the current device: requests (host R1CS + witness) are
+ * queued, admitted by their estimated HBM footprint within hbm_budget_bytes
+ * and max_inflight slots, and proved with pkg_spartan_prove by one worker
+ * thread + CUDA stream per slot, so admitted jobs overlap on the device and
+ * their R1CS, witness, codeword, tree and tables stay resident until done.
+ * Latencies are measured from submit to completion.  No reference
+ * counterpart (the reference proves one request per call,
+ * tooling/provekit-ffi/src/ffi.rs:536-595). */
+typedef struct pkg_server pkg_server;
+typedef struct {
+  size_t num_constraints, num_witnesses;
+  const uint64_t *row_ptr[3]; /* host CSR A, B, C */
+  const uint32_t *cols[3];
+  const uint64_t *vals[3];
+  size_t nnz[3];
+  const uint64_t *witness;    /* host, num_witnesses Fr */
+  uint64_t blinding_seed, transcript_domain;
+  unsigned folding_factor, log_inv_rate;
+} pkg_prove_request;
+typedef struct {
+  uint64_t submit_ns, admit_ns, done_ns; /* steady clock */
+  size_t footprint_bytes;                /* admission estimate */
+} pkg_request_times;
+typedef struct {
+  size_t completed, queued, inflight;
+  size_t reserved_bytes, peak_reserved_bytes;
+  double p50_ms, p99_ms, p999_ms, proofs_per_s;
+} pkg_server_stats;
+int pkg_server_create(size_t hbm_budget_bytes, int max_inflight, pkg_server **out);
+/* Queues the request without copying it: the caller's host buffers must stay
+ * valid and unchanged until pkg_server_wait returns for the returned id (the
+ * worker uploads them when the request is admitted).  A request whose
+ * estimate exceeds the whole budget returns PKG_ERR_OUT_OF_MEMORY. */
+int pkg_server_submit(pkg_server *server, const pkg_prove_request *req, uint64_t *request_id);
+/* Blocks until the request is done; returns its status. */
+int pkg_server_wait(pkg_server *server, uint64_t request_id, pkg_spartan_proof *proof,
+                    pkg_request_times *times);
+int pkg_server_get_stats(pkg_server *server, pkg_server_stats *out);
+/* Finishes admitted work, fails queued requests, joins the workers. */
+void pkg_server_destroy(pkg_server *server);
 
 /* ---- diagnostics ---------------------------------------------------------- */
 /* Synchronous device -> host copy of library-owned memory (e.g. batch buffers). */

@@ -72,6 +72,10 @@ SIGNATURES = {
     "pkg_batch_run": [_c_vp, _c_int, _c_vp],
     "pkg_batch_sumcheck_result": [_c_vp, _c_sz, _c_vp],
     "pkg_copy_to_host": [_c_vp, _c_vp, _c_sz],
+    "pkg_server_create": [_c_sz, _c_int, _c_vp],
+    "pkg_server_submit": [_c_vp, _c_vp, _c_vp],
+    "pkg_server_wait": [_c_vp, ctypes.c_uint64, _c_vp, _c_vp],
+    "pkg_server_get_stats": [_c_vp, _c_vp],
     "pkg_measure_imad_rate": [ctypes.POINTER(ctypes.c_double)],
     "pkg_version": [],
 }
@@ -103,6 +107,8 @@ def lib():
             fn.restype = ctypes.c_int
         L.pkg_batch_destroy.argtypes = [_c_vp]
         L.pkg_batch_destroy.restype = None
+        L.pkg_server_destroy.argtypes = [_c_vp]
+        L.pkg_server_destroy.restype = None
         L.pkg_kernel_launches.argtypes = []
         L.pkg_kernel_launches.restype = ctypes.c_uint64
         _lib = L
@@ -120,4 +126,5 @@ def check(rc: int):
 
 
 def exported_symbols():
-    return sorted(SIGNATURES) + ["pkg_last_error", "pkg_kernel_launches", "pkg_batch_destroy"]
+    return sorted(SIGNATURES) + ["pkg_last_error", "pkg_kernel_launches", "pkg_batch_destroy",
+                                  "pkg_server_destroy"]

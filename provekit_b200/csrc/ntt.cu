@@ -32,6 +32,7 @@ namespace pk {
 struct RootsTable {
   uint64_t* d = nullptr;
   size_t order = 0;
+  std::vector<uint64_t*> retired;
 };
 static std::mutex g_roots_mu;
 static std::vector<RootsTable> g_roots;
@@ -64,9 +65,10 @@ int roots_reserve(size_t order, const uint64_t** out) {
     *out = tab.d;
     return PKG_OK;
   }
-  // Grow: build the order-`order` table; in-flight users of the old table
-  // are drained first.
-  PK_CUDA(cudaDeviceSynchronize());
+  // Grow: build the order-`order` table.  Superseded tables stay allocated
+  // (kept in `retired`) so that kernels already enqueued on any stream, or
+  // pointers already handed to another thread, stay valid; by the prefix
+  // property their total size is below the new table's.
   int log_half = log2_exact(order / 2);
   int s = (log_half + 1) / 2;
   size_t nlo = size_t(1) << s, nhi = size_t(1) << (log_half - s);
@@ -89,19 +91,25 @@ int roots_reserve(size_t order, const uint64_t** out) {
   if (e == cudaSuccess) e = cudaMalloc(&d_hi, 32 * nhi);
   if (e == cudaSuccess) e = cudaMemcpy(d_lo, h_lo.data(), 32 * nlo, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(d_hi, h_hi.data(), 32 * nhi, cudaMemcpyHostToDevice);
+  // Built on a private stream and waited for, so the table is complete before
+  // any caller (on any stream) can see the new pointer.
+  cudaStream_t bs = nullptr;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking);
   if (e == cudaSuccess) {
     int blocks = (int)std::min<size_t>((order / 2 + 255) / 256, (size_t)sm_count() * 16);
-    roots_kernel<<<blocks, 256>>>(d_new, d_lo, d_hi, log_half, s);
+    roots_kernel<<<blocks, 256, 0, bs>>>(d_new, d_lo, d_hi, log_half, s);
     e = cudaGetLastError();
+    count_launch();
   }
-  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(bs);
+  if (bs) cudaStreamDestroy(bs);
   cudaFree(d_lo);
   cudaFree(d_hi);
   if (e != cudaSuccess) {
     cudaFree(d_new);
     return cuda_status(e, "twiddle table");
   }
-  if (tab.d) cudaFree(tab.d);
+  if (tab.d) tab.retired.push_back(tab.d);
   tab.d = d_new;
   tab.order = order;
   *out = tab.d;

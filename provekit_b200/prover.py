@@ -52,8 +52,8 @@ class HostR1CS:
         vl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.vals])
         check(lib().pkg_synthetic_r1cs(seed, nc, ni, rp, cl, vl, nnz, self.witness.ctypes.data))
         self.nnz = list(nnz)
-        self.cols = [c[:n] for c, n in zip(self.cols, self.nnz)]
-        self.vals = [v[:n] for v, n in zip(self.vals, self.nnz)]
+        self.cols = [np.ascontiguousarray(c[:n]) for c, n in zip(self.cols, self.nnz)]
+        self.vals = [np.ascontiguousarray(v[:n]) for v, n in zip(self.vals, self.nnz)]
 
     def to_device(self, device="cuda"):
         return DeviceR1CS(self, device)

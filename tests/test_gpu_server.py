@@ -1,0 +1,78 @@
+"""Served form: requests of different sizes submitted together to a server
+whose HBM budget and slots force queueing and overlap; every proof equals the
+same request proved alone with pkg_spartan_prove."""
+import threading
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    from provekit_b200 import build
+    build.build()
+
+
+def same(a, b):
+    for k in a:
+        if isinstance(a[k], np.ndarray):
+            assert np.array_equal(a[k], b[k]), k
+        else:
+            assert a[k] == b[k], k
+
+
+def test_served_results_equal_alone_results():
+    from provekit_b200.prover import HostR1CS, spartan_prove
+    from provekit_b200.server import ProofServer
+    sizes = [(12, 10), (10, 8), (14, 12), (11, 9), (13, 11), (10, 8), (14, 12), (12, 10)]
+    reqs = [HostR1CS(500 + i, 1 << lc, 1 << li) for i, (lc, li) in enumerate(sizes)]
+    alone = [spartan_prove(h.to_device(), blinding_seed=7 + i, transcript_domain=100 + i)
+             for i, h in enumerate(reqs)]
+    # budget: room for about two of the largest requests at once
+    srv = ProofServer(hbm_budget_bytes=2 * 96 << 20, max_inflight=3)
+    ids = [srv.submit(h, blinding_seed=7 + i, transcript_domain=100 + i) for i, h in enumerate(reqs)]
+    results = [srv.wait(rid) for rid in ids]
+    for (proof, times), ref in zip(results, alone):
+        same(proof, ref)
+        assert times["submit_ns"] <= times["admit_ns"] <= times["done_ns"]
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["p50_ms"] > 0
+    assert st["peak_reserved_bytes"] <= 2 * 96 << 20
+    srv.close()
+
+
+def test_submit_from_threads_and_overlap():
+    """Requests submitted from several host threads while others run."""
+    from provekit_b200.prover import HostR1CS, spartan_prove
+    from provekit_b200.server import ProofServer
+    reqs = [HostR1CS(900 + i, 1 << 12, 1 << 10) for i in range(6)]
+    srv = ProofServer(hbm_budget_bytes=1 << 30, max_inflight=4)
+    out = {}
+
+    def client(i):
+        rid = srv.submit(reqs[i], blinding_seed=i, transcript_domain=i)
+        out[i] = srv.wait(rid)[0]
+
+    th = [threading.Thread(target=client, args=(i,)) for i in range(len(reqs))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for i, h in enumerate(reqs):
+        same(out[i], spartan_prove(h.to_device(), blinding_seed=i, transcript_domain=i))
+    srv.close()
+
+
+def test_request_above_budget_is_rejected():
+    from provekit_b200 import PkgError
+    from provekit_b200.prover import HostR1CS
+    from provekit_b200.server import ProofServer
+    srv = ProofServer(hbm_budget_bytes=64 << 20, max_inflight=1)
+    with pytest.raises(PkgError):
+        srv.submit(HostR1CS(1, 1 << 16, 1 << 14))
+    srv.close()
