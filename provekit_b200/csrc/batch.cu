@@ -76,16 +76,17 @@ __device__ __forceinline__ uint32_t find_desc(const uint64_t* begins, uint32_t n
   return lo;
 }
 
-__device__ __forceinline__ Fr sm_get(const uint4* sm, int i) {
-  uint4 a = sm[2 * i], b = sm[2 * i + 1];
+// Shared memory as two planes of 16-byte halves (see ntt_pass_kernel).
+__device__ __forceinline__ Fr sm_get(const uint4* sm, int E, int i) {
+  uint4 a = sm[i], b = sm[E + i];
   Fr x;
   x.v[0] = a.x; x.v[1] = a.y; x.v[2] = a.z; x.v[3] = a.w;
   x.v[4] = b.x; x.v[5] = b.y; x.v[6] = b.z; x.v[7] = b.w;
   return x;
 }
-__device__ __forceinline__ void sm_put(uint4* sm, int i, const Fr& x) {
-  sm[2 * i] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
-  sm[2 * i + 1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+__device__ __forceinline__ void sm_put(uint4* sm, int E, int i, const Fr& x) {
+  sm[i] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+  sm[E + i] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
 }
 
 // ---- grouped NTT pass: the ntt_pass_kernel index scheme with run-time K ----
@@ -120,8 +121,8 @@ __global__ void __launch_bounds__(512) batch_ntt_pass_kernel(const PassDesc* __r
       sidx = j * T + (hl << log_u) + u;
     }
     const uint4* src = reinterpret_cast<const uint4*>(data + 4 * g);
-    sm[2 * sidx] = src[0];
-    sm[2 * sidx + 1] = src[1];
+    sm[sidx] = src[0];      // low 16 bytes: plane 0
+    sm[E + sidx] = src[1];  // high 16 bytes: plane 1
   }
   __syncthreads();
   for (int s = 0; s < K; s++) {
@@ -136,10 +137,10 @@ __global__ void __launch_bounds__(512) batch_ntt_pass_kernel(const PassDesc* __r
       uint64_t high = d.mode_b ? ((l0 + ll) >> log_u) : high_a;
       Fr tw = fr_load_ro(roots, (high << s) | (uint64_t)grp);
       int i0 = j0 * T + ll, i1 = j1 * T + ll;
-      Fr x0 = sm_get(sm, i0), x1 = sm_get(sm, i1);
+      Fr x0 = sm_get(sm, E, i0), x1 = sm_get(sm, E, i1);
       Fr m = fr_mul(tw, x1);
-      sm_put(sm, i0, fr_add(x0, m));
-      sm_put(sm, i1, fr_sub(x0, m));
+      sm_put(sm, E, i0, fr_add(x0, m));
+      sm_put(sm, E, i1, fr_sub(x0, m));
     }
     __syncthreads();
   }
@@ -158,8 +159,8 @@ __global__ void __launch_bounds__(512) batch_ntt_pass_kernel(const PassDesc* __r
       sidx = j * T + (hl << log_u) + u;
     }
     uint4* dst = reinterpret_cast<uint4*>(data + 4 * g);
-    dst[0] = sm[2 * sidx];
-    dst[1] = sm[2 * sidx + 1];
+    dst[0] = sm[sidx];
+    dst[1] = sm[E + sidx];
   }
 }
 

@@ -232,7 +232,64 @@ __device__ __forceinline__ Fr fr_mul(const Fr& a, const Fr& b) {
   return r;
 }
 
-__device__ __forceinline__ Fr fr_sqr(const Fr& a) { return fr_mul(a, a); }
+// Montgomery square a^2 * 2^-256 mod p for a < p, as separated operand
+// scanning (SOS): the 28 cross products a_i a_j (i < j) once, doubled, plus
+// the 8 diagonal squares -- 36 word products instead of 64 -- then the
+// word-by-word Montgomery reduction.  Accumulation uses 64-bit
+// multiply-adds; the result is fully reduced.
+__device__ __forceinline__ Fr fr_sqr(const Fr& a) {
+  const uint32_t P[8] = {PK_P0, PK_P1, PK_P2, PK_P3, PK_P4, PK_P5, PK_P6, PK_P7};
+  uint32_t t[17];
+#pragma unroll
+  for (int i = 0; i < 17; i++) t[i] = 0;
+#pragma unroll
+  for (int i = 0; i < 7; i++) {
+    uint64_t c = 0;
+#pragma unroll
+    for (int j = i + 1; j < 8; j++) {
+      uint64_t s = (uint64_t)a.v[i] * a.v[j] + t[i + j] + c;
+      t[i + j] = (uint32_t)s;
+      c = s >> 32;
+    }
+    t[i + 8] = (uint32_t)c;
+  }
+#pragma unroll
+  for (int k = 15; k > 0; k--) t[k] = (t[k] << 1) | (t[k - 1] >> 31);
+  t[0] <<= 1;
+  uint64_t c = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    uint64_t sq = (uint64_t)a.v[i] * a.v[i];
+    uint64_t s = (uint64_t)t[2 * i] + (uint32_t)sq + c;
+    t[2 * i] = (uint32_t)s;
+    c = s >> 32;
+    s = (uint64_t)t[2 * i + 1] + (uint32_t)(sq >> 32) + c;
+    t[2 * i + 1] = (uint32_t)s;
+    c = s >> 32;
+  }
+  // reduction: t += m_i * p * 2^(32 i), i = 0..7 (a^2 < p^2 keeps t < 2^512 + p 2^256)
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint32_t m = t[i] * PK_MU;
+    uint64_t c2 = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      uint64_t s = (uint64_t)m * P[j] + t[i + j] + c2;
+      t[i + j] = (uint32_t)s;
+      c2 = s >> 32;
+    }
+#pragma unroll
+    for (int k = i + 8; k < 17; k++) {
+      uint64_t s = (uint64_t)t[k] + c2;
+      t[k] = (uint32_t)s;
+      c2 = s >> 32;
+    }
+  }
+  Fr r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.v[i] = t[i + 8];
+  return fr_reduce_once(r);
+}
 
 // canonical -> Montgomery: a * R^2 * R^-1
 __device__ __forceinline__ Fr fr_to_mont(const Fr& a) {

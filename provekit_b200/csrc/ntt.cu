@@ -119,6 +119,10 @@ int roots_reserve(size_t order, const uint64_t** out) {
 // ---------------------------------------------------------------------------
 // Pass kernel.
 //
+// Shared memory holds the CTA's E elements as two planes of 16-byte halves
+// (plane 0: bytes 0-15 of every element, plane 1: bytes 16-31), so a warp
+// touching consecutive elements reads consecutive 16-byte words.
+//
 // Row r of the transform (codeword position) has log2(N) bits.  A pass over
 // global stages [t, t+K) splits r = (high : j : low) with high = top t bits,
 // j = next K bits, low = remaining B bits.  With M interleaved columns, the
@@ -160,8 +164,8 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
       sidx = j * T + (hl << log_u) + u;
     }
     const uint4* src = reinterpret_cast<const uint4*>(data + 4 * g);
-    sm[2 * sidx] = src[0];
-    sm[2 * sidx + 1] = src[1];
+    sm[sidx] = src[0];      // low 16 bytes: plane 0
+    sm[E + sidx] = src[1];  // high 16 bytes: plane 1
   }
   __syncthreads();
   // ---- K radix-2 stages in shared memory ----
@@ -179,20 +183,20 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
       Fr w = fr_load_ro(roots, (high << s) | (uint64_t)grp);
       int i0 = j0 * T + ll, i1 = j1 * T + ll;
       Fr x0, x1;
-      uint4 a = sm[2 * i0], bb = sm[2 * i0 + 1];
+      uint4 a = sm[i0], bb = sm[E + i0];
       x0.v[0] = a.x; x0.v[1] = a.y; x0.v[2] = a.z; x0.v[3] = a.w;
       x0.v[4] = bb.x; x0.v[5] = bb.y; x0.v[6] = bb.z; x0.v[7] = bb.w;
-      a = sm[2 * i1];
-      bb = sm[2 * i1 + 1];
+      a = sm[i1];
+      bb = sm[E + i1];
       x1.v[0] = a.x; x1.v[1] = a.y; x1.v[2] = a.z; x1.v[3] = a.w;
       x1.v[4] = bb.x; x1.v[5] = bb.y; x1.v[6] = bb.z; x1.v[7] = bb.w;
       Fr m = fr_mul(w, x1);
       Fr y0 = fr_add(x0, m);
       Fr y1 = fr_sub(x0, m);
-      sm[2 * i0] = make_uint4(y0.v[0], y0.v[1], y0.v[2], y0.v[3]);
-      sm[2 * i0 + 1] = make_uint4(y0.v[4], y0.v[5], y0.v[6], y0.v[7]);
-      sm[2 * i1] = make_uint4(y1.v[0], y1.v[1], y1.v[2], y1.v[3]);
-      sm[2 * i1 + 1] = make_uint4(y1.v[4], y1.v[5], y1.v[6], y1.v[7]);
+      sm[i0] = make_uint4(y0.v[0], y0.v[1], y0.v[2], y0.v[3]);
+      sm[E + i0] = make_uint4(y0.v[4], y0.v[5], y0.v[6], y0.v[7]);
+      sm[i1] = make_uint4(y1.v[0], y1.v[1], y1.v[2], y1.v[3]);
+      sm[E + i1] = make_uint4(y1.v[4], y1.v[5], y1.v[6], y1.v[7]);
     }
     __syncthreads();
   }
@@ -212,8 +216,8 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
       sidx = j * T + (hl << log_u) + u;
     }
     uint4* dst = reinterpret_cast<uint4*>(data + 4 * g);
-    dst[0] = sm[2 * sidx];
-    dst[1] = sm[2 * sidx + 1];
+    dst[0] = sm[sidx];
+    dst[1] = sm[E + sidx];
   }
 }
 
