@@ -30,7 +30,7 @@ IMAD_PER_MONT = 264  # mad.lo/madc.hi/mul.lo per 8x32 CIOS product (fr.cuh: 8 x 
 # dram__bytes_read.sum + dram__bytes_write.sum of one leaf_fold_fr_kernel launch
 # from an ncu capture of this workload (profiles/leaf_fold_fr_kernel_whir_commit_2p20.md),
 # keyed by (log2 coeffs, folding factor, log inv rate).
-LEAF_TRAFFIC_BYTES = {(20, 4, 2): 134.672896e6 + 6.241024e6}
+LEAF_TRAFFIC_BYTES = {(20, 4, 2): 134.514432e6 + 6.164480e6}
 
 
 def parse_args():
@@ -238,6 +238,7 @@ def run_b200(a):
 
     from provekit_b200 import _lib
     from provekit_b200._lib import PKG_LEAF_CANONICAL, check
+    from provekit_b200.replicas import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -316,10 +317,7 @@ def run_b200(a):
     leaf_ms = [e[1].elapsed_time(e[2]) for e in events]
     lvl_ms = [e[2].elapsed_time(e[3]) for e in events]
     total_ms = sum(step_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=d_coeffs.device)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms_max = float(t.item())
+    total_ms_max = max_over_ranks(total_ms, device=d_coeffs.device)
 
     # ---- end to end through the C ABI: pinned host coefficients in, root out
     e2e_events = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
@@ -336,10 +334,7 @@ def run_b200(a):
                 e2e_events[i - a.warmup][1].record(stream)
     stream.synchronize()
     e2e_ms = sum(e[0].elapsed_time(e[1]) for e in e2e_events)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=d_coeffs.device)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_ms_max = float(t.item())
+    e2e_ms_max = max_over_ranks(e2e_ms, device=d_coeffs.device)
 
     # ---- the trait-shaped drop-in: host slices through RSFr / HashEngine
     plugin = None
