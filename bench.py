@@ -45,7 +45,8 @@ def parse_args():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plugin-e2e", action="store_true")
-    p.add_argument("--workload", choices=["commit", "prove", "batched", "served"], default="commit",
+    p.add_argument("--workload", choices=["commit", "prove", "batched", "served", "ntt"],
+                   default="commit",
                    help="commit (default, the headline line): WHIR commit of 2^20 coefficients; "
                         "prove: Spartan prove core of a 2^20-constraint R1CS; batched: 256 uneven "
                         "jobs as one CUDA graph vs the same jobs one at a time")
@@ -688,6 +689,64 @@ def run_served(a):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# NTT: 2^24 (the north star's roofline target) and config 1 (2^16).
+# ---------------------------------------------------------------------------
+def run_ntt(a):
+    import numpy as np
+    import torch
+
+    from provekit_b200 import _lib
+    from provekit_b200._lib import check
+
+    L = _lib.lib()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    imad = ctypes.c_double(0)
+    check(L.pkg_measure_imad_rate(ctypes.byref(imad)))
+    mont_peak = imad.value / IMAD_PER_MONT
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    out = {}
+    for logn in (24, 16):
+        n = 1 << logn
+        h = np.zeros((n, 4), np.uint64)
+        check(L.pkg_sample_fr(1 if logn == 16 else 24, n, h.ctypes.data, 1))
+        src = torch.from_numpy(h.view(np.int64)).cuda()
+        d = torch.empty_like(src)
+        check(L.pkg_ntt_engine_reserve(n))
+        with torch.cuda.stream(stream):
+            for _ in range(a.warmup):
+                d.copy_(src)
+                check(L.pkg_ntt_nr(d.data_ptr(), n, n, 1, stream.cuda_stream))
+        stream.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
+        with torch.cuda.stream(stream):
+            for i in range(a.steps):
+                d.copy_(src)
+                flush.zero_()
+                evs[i][0].record(stream)
+                check(L.pkg_ntt_nr(d.data_ptr(), n, n, 1, stream.cuda_stream))
+                evs[i][1].record(stream)
+        stream.synchronize()
+        ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+        products = (n // 2) * logn
+        out[logn] = {"ms": ms, "fr_per_s": n / (ms * 1e-3), "gmont_per_s": products / (ms * 1e-3) / 1e9,
+                     "roofline_frac": products / (ms * 1e-3) / mont_peak,
+                     "hbm_gbs": 2 * 32 * n * ((logn + 8) // 9) / (ms * 1e-3) / 1e9}
+    line = {"metric": "BN254 Fr ntt_nr throughput, 2^24 (roofline target) and 2^16 (config 1)",
+            "value": out[24]["fr_per_s"], "unit": "Fr/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": out[24]["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 (BN254 Fr, 8x32-bit limbs)",
+            "data": "synthetic (ChaCha20-seeded Fr)",
+            "config": {"workload": "ntt", "log2_n": 24, "l2": "flushed between steps"},
+            "roofline": {"kernel": "ntt_pass_kernel", "bound": "int",
+                         "achieved": out[24]["gmont_per_s"], "peak": mont_peak / 1e9,
+                         "unit": "Gmont/s", "frac": out[24]["roofline_frac"],
+                         "algorithmic": "(n/2) log2 n Montgomery products per transform"},
+            "ntt_2p16": out[16]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
@@ -698,6 +757,8 @@ def main():
         run_batched(a)
     elif a.workload == "served":
         run_served(a)
+    elif a.workload == "ntt":
+        run_ntt(a)
     else:
         run_b200(a)
 
