@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(512) batch_ntt_pass_kernel(const PassDesc* __r
       Fr tw = fr_load_ro(roots, (high << s) | (uint64_t)grp);
       int i0 = j0 * T + ll, i1 = j1 * T + ll;
       Fr x0 = sm_get(sm, E, i0), x1 = sm_get(sm, E, i1);
-      Fr m = fr_mul(tw, x1);
+      Fr m = fr_mul_f64(tw, x1);
       sm_put(sm, E, i0, fr_add(x0, m));
       sm_put(sm, E, i1, fr_sub(x0, m));
     }

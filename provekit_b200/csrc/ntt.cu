@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "fr.cuh"
+#include "fr_f64.cuh"
 #include "fr_host.hpp"
 #include "ntt_internal.cuh"
 #include "pk_common.cuh"
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
       bb = sm[E + i1];
       x1.v[0] = a.x; x1.v[1] = a.y; x1.v[2] = a.z; x1.v[3] = a.w;
       x1.v[4] = bb.x; x1.v[5] = bb.y; x1.v[6] = bb.z; x1.v[7] = bb.w;
-      Fr m = fr_mul(w, x1);
+      Fr m = fr_mul_f64(w, x1);
       Fr y0 = fr_add(x0, m);
       Fr y1 = fr_sub(x0, m);
       sm[i0] = make_uint4(y0.v[0], y0.v[1], y0.v[2], y0.v[3]);

@@ -10,6 +10,7 @@
 // reference.rs:64).
 #pragma once
 #include "fr.cuh"
+#include "fr_f64.cuh"
 
 namespace pk {
 
@@ -111,7 +112,7 @@ __device__ __forceinline__ Fr sky_compress(Fr l, Fr r) {
 #pragma unroll 1
   for (int k = 0; k < 18; k++) {
     const bool is_bar = (k == 6 || k == 7 || k == 10 || k == 11);
-    Fr f = is_bar ? sky_bar(l) : fr_sqr(l);
+    Fr f = is_bar ? sky_bar(l) : fr_sqr_f64(l);
     Fr nl = fr_add(r, f);
     nl = fr_add(nl, sky_rc(k));
     r = l;
