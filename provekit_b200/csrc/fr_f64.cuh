@@ -143,4 +143,14 @@ __device__ __forceinline__ Fr fr_sqr_f64(const Fr& a) {
   return f64::tail16(T);
 }
 
+// a * 2^-256 mod p (Montgomery -> canonical) for any 256-bit a: the
+// reduction steps alone, without a product; result < p.
+__device__ __forceinline__ Fr fr_from_mont_f64(const Fr& a) {
+  double T[11];
+  f64::digits(a, T);
+#pragma unroll
+  for (int i = 0; i < 10; i++) f64::step24(T);
+  return f64::tail16(T);
+}
+
 }  // namespace pk

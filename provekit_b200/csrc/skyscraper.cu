@@ -68,17 +68,17 @@ __global__ void leaf_fold_kernel(const uint8_t* __restrict__ in, size_t size, si
 // (x*2^256 -> x) before hashing; Montgomery encoding hashes the raw limbs.
 // A one-element leaf is the element itself (hash_many(32) copies).
 template <bool kCanonical>
-__global__ void leaf_fold_fr_kernel(const uint64_t* __restrict__ cw, size_t fr_per_leaf,
+__global__ void __launch_bounds__(128, 7) leaf_fold_fr_kernel(const uint64_t* __restrict__ cw, size_t fr_per_leaf,
                                     size_t count, uint8_t* __restrict__ out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
        i += (size_t)gridDim.x * blockDim.x) {
     const size_t base = i * fr_per_leaf;
     Fr acc = fr_load_ro(cw, base);
-    if (kCanonical) acc = fr_from_mont(acc);
+    if (kCanonical) acc = fr_from_mont_f64(acc);
 #pragma unroll 1
     for (size_t k = 1; k < fr_per_leaf; k++) {
       Fr e = fr_load_ro(cw, base + k);
-      if (kCanonical) e = fr_from_mont(e);
+      if (kCanonical) e = fr_from_mont_f64(e);
       acc = sky_compress(acc, e);
     }
     store_raw(out + 32 * i, acc);
