@@ -378,6 +378,27 @@ int pkg_server_get_stats(pkg_server *server, pkg_server_stats *out);
 /* Finishes admitted work, fails queued requests, joins the workers. */
 void pkg_server_destroy(pkg_server *server);
 
+/* ---- field arithmetic (skyscraper/bn254-multiplier/src/scalar.rs:12-132,
+ *      ark-ff Montgomery conversion) ---------------------------------------- */
+/* out[i] = op(a[i], b[i]) over n Fr (4 x u64 LE each, device, 16-byte
+ * aligned), asynchronous on stream; results fully reduced (< p).
+ *   PKG_FR_MUL_F64 / PKG_FR_SQR_F64: a*b*2^-256, a^2*2^-256 mod p on the FP64
+ *     pipe (the routines of the NTT and Skyscraper kernels); inputs < 2p.
+ *   PKG_FR_FROM_MONT_F64: a*2^-256 mod p on the FP64 pipe; any 256-bit a.
+ *   PKG_FR_MUL_INT / PKG_FR_SQR_INT: the same on the integer pipe; inputs < p.
+ *   PKG_FR_FROM_MONT_INT: integer pipe; a < 2p.
+ * b is read only by the two products (may be NULL otherwise).  The reference's
+ * scalar_mul/scalar_sqr return values in [0, 2^256 - 2p) with the same
+ * residue; only the residue is part of the contract. */
+#define PKG_FR_MUL_F64 0
+#define PKG_FR_SQR_F64 1
+#define PKG_FR_FROM_MONT_F64 2
+#define PKG_FR_MUL_INT 3
+#define PKG_FR_SQR_INT 4
+#define PKG_FR_FROM_MONT_INT 5
+int pkg_fr_mul_batch(const uint64_t *a, const uint64_t *b, uint64_t *out, size_t n, int op,
+                     pkg_stream_t stream);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 /* Synchronous device -> host copy of library-owned memory (e.g. batch buffers). */
 int pkg_copy_to_host(void *dst, const void *src, size_t bytes);
@@ -387,6 +408,13 @@ uint64_t pkg_kernel_launches(void);
  * per second, from a dependent-chain-free mad.lo/madc.hi microbenchmark).
  * Synchronous. */
 int pkg_measure_imad_rate(double *instr_per_second);
+
+/* Sustained double-precision fma rate of this GPU (fma instructions per
+ * second, one thread-instruction each), from eight independent chains per
+ * thread on every SM.  Denominator of the FP64-pipe roofline: the Fr
+ * products of the NTT butterflies and Skyscraper rounds run on that pipe.
+ * Synchronous.  No counterpart in the reference (a measurement helper). */
+int pkg_measure_dfma_rate(double *instr_per_second);
 
 #ifdef __cplusplus
 }

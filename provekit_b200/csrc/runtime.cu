@@ -93,6 +93,22 @@ __global__ void imad_rate_kernel(uint32_t* sink, uint32_t seed, int iters) {
   if (s == 0x12345678u) sink[threadIdx.x] = s;
 }
 
+// Eight independent fma chains per thread; x -> x * c + d converges to
+// d / (1 - c) and never leaves the normal range.
+__global__ void dfma_rate_kernel(double* sink, double c, double d, int iters) {
+  double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5,
+         x6 = x0 + 6, x7 = x0 + 7;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      x0 = fma(x0, c, d); x1 = fma(x1, c, d); x2 = fma(x2, c, d); x3 = fma(x3, c, d);
+      x4 = fma(x4, c, d); x5 = fma(x5, c, d); x6 = fma(x6, c, d); x7 = fma(x7, c, d);
+    }
+  }
+  const double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == -1.0) sink[threadIdx.x] = s;
+}
+
 }  // namespace pk
 
 using namespace pk;
@@ -147,6 +163,30 @@ extern "C" int pkg_measure_imad_rate(double* instr_per_second) {
   cudaEventDestroy(e1);
   cudaFree(sink);
   if (err != cudaSuccess) return cuda_status(err, "imad_rate_kernel");
+  double instr = (double)blocks * threads * iters * 8.0 * 8.0;
+  *instr_per_second = instr / (ms * 1e-3);
+  return PKG_OK;
+}
+
+extern "C" int pkg_measure_dfma_rate(double* instr_per_second) {
+  if (!instr_per_second) return PKG_ERR_INVALID_ARGUMENT;
+  double* sink = nullptr;
+  PK_CUDA(cudaMalloc(&sink, 1024 * sizeof(double)));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int threads = 256, blocks = sm_count() * 8, iters = 4096;
+  dfma_rate_kernel<<<blocks, threads>>>(sink, 0.999999, 1e-7, 64);  // warm-up
+  cudaEventRecord(e0);
+  dfma_rate_kernel<<<blocks, threads>>>(sink, 0.999999, 1e-7, iters);
+  cudaEventRecord(e1);
+  cudaError_t err = cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  if (err != cudaSuccess) return cuda_status(err, "dfma_rate_kernel");
   double instr = (double)blocks * threads * iters * 8.0 * 8.0;
   *instr_per_second = instr / (ms * 1e-3);
   return PKG_OK;
