@@ -20,6 +20,7 @@
 #include "fr_f64.cuh"
 #include "fr_host.hpp"
 #include "ntt_internal.cuh"
+#include "host_stage.cuh"
 #include "pk_common.cuh"
 
 namespace pk {
@@ -387,36 +388,38 @@ extern "C" int pkg_ntt_engine_reserve(size_t order) {
   return roots_reserve(order, &r);
 }
 
+// In-place transform of a host slice through the host stager: one pipelined
+// upload, the device transform on the stager's stream, one pipelined download.
+static int host_transform(uint64_t* values, size_t len, size_t codeword_size,
+                          size_t num_groups, bool inverse) {
+  HostStager& hs = HostStager::current();
+  std::lock_guard<std::mutex> lk(hs.mutex());
+  uint8_t* ws = nullptr;
+  int rc = hs.workspace(32 * len, &ws);
+  if (rc) return rc;
+  rc = hs.h2d(ws, values, 32 * len);
+  if (rc) return rc;
+  uint64_t* d = reinterpret_cast<uint64_t*>(ws);
+  rc = inverse ? intt_rn_device(d, len, hs.stream())
+               : ntt_nr_device(d, len, codeword_size, num_groups, hs.stream());
+  if (rc) return rc;
+  rc = hs.d2h(values, ws, 32 * len);
+  if (rc) return rc;
+  PK_CUDA(cudaStreamSynchronize(hs.stream()));
+  return PKG_OK;
+}
+
 extern "C" int pkg_host_ntt_nr(uint64_t* values, size_t len, size_t codeword_size,
                                size_t num_groups) {
   int noop = 0;
   int rc = ntt_validate(len, codeword_size, num_groups, &noop);
   if (rc || noop) return rc;
   PK_REQUIRE(values != nullptr, "null values pointer");
-  uint64_t* d = nullptr;
-  PK_CUDA(cudaMalloc(&d, 32 * len));
-  cudaError_t e = cudaMemcpy(d, values, 32 * len, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) {
-    rc = ntt_nr_device(d, len, codeword_size, num_groups, 0);
-    if (!rc) e = cudaMemcpy(values, d, 32 * len, cudaMemcpyDeviceToHost);
-  }
-  cudaFree(d);
-  if (e != cudaSuccess) return cuda_status(e, "pkg_host_ntt_nr");
-  return rc;
+  return host_transform(values, len, codeword_size, num_groups, false);
 }
 
 extern "C" int pkg_host_intt_rn(uint64_t* values, size_t len) {
   PK_REQUIRE(is_pow2(len), "intt_rn length %zu is not a power of two", len);
   PK_REQUIRE(values != nullptr, "null values pointer");
-  uint64_t* d = nullptr;
-  PK_CUDA(cudaMalloc(&d, 32 * len));
-  cudaError_t e = cudaMemcpy(d, values, 32 * len, cudaMemcpyHostToDevice);
-  int rc = PKG_OK;
-  if (e == cudaSuccess) {
-    rc = intt_rn_device(d, len, 0);
-    if (!rc) e = cudaMemcpy(values, d, 32 * len, cudaMemcpyDeviceToHost);
-  }
-  cudaFree(d);
-  if (e != cudaSuccess) return cuda_status(e, "pkg_host_intt_rn");
-  return rc;
+  return host_transform(values, len, len, 1, true);
 }

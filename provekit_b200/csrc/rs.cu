@@ -14,6 +14,7 @@
 #include "fr.cuh"
 #include "fr_host.hpp"
 #include "ntt_internal.cuh"
+#include "host_stage.cuh"
 #include "pk_common.cuh"
 #include "rs_internal.cuh"
 
@@ -161,25 +162,36 @@ extern "C" int pkg_host_rs_interleaved_encode(const uint64_t* const* messages,
   size_t total = num_messages * codeword_length;
   if (total == 0) return PKG_OK;
   PK_REQUIRE(messages != nullptr && out != nullptr, "null pointer");
-  uint64_t *d_msg = nullptr, *d_mask = nullptr, *d_out = nullptr;
-  size_t msg_elems = num_messages * message_length;
-  cudaError_t e = cudaSuccess;
-  if (msg_elems) e = cudaMalloc(&d_msg, 32 * msg_elems);
-  if (e == cudaSuccess && mask_len) e = cudaMalloc(&d_mask, 32 * mask_len);
-  if (e == cudaSuccess) e = cudaMalloc(&d_out, 32 * total);
-  for (size_t j = 0; e == cudaSuccess && j < num_messages && message_length; j++)
-    e = cudaMemcpy(d_msg + 4 * j * message_length, messages[j], 32 * message_length,
-                   cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && mask_len)
-    e = cudaMemcpy(d_mask, masks, 32 * mask_len, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) {
-    rc = rs_encode_device(d_msg, num_messages, message_length, d_mask, mask_len,
-                          codeword_length, d_out, 0);
-    if (!rc) e = cudaMemcpy(out, d_out, 32 * total, cudaMemcpyDeviceToHost);
+  PK_REQUIRE(mask_len == 0 || masks != nullptr, "null masks pointer");
+  const size_t msg_bytes = 32 * num_messages * message_length, mask_bytes = 32 * mask_len;
+  const size_t msg_span = (msg_bytes + 255) & ~size_t(255);
+  const size_t mask_span = (mask_bytes + 255) & ~size_t(255);
+  HostStager& hs = HostStager::current();
+  std::lock_guard<std::mutex> lk(hs.mutex());
+  uint8_t* ws = nullptr;
+  rc = hs.workspace(msg_span + mask_span + 32 * total, &ws);
+  if (rc) return rc;
+  uint64_t* d_msg = reinterpret_cast<uint64_t*>(ws);
+  uint64_t* d_mask = reinterpret_cast<uint64_t*>(ws + msg_span);
+  uint64_t* d_out = reinterpret_cast<uint64_t*>(ws + msg_span + mask_span);
+  if (msg_bytes) {
+    std::vector<HostSegment> segs(num_messages);
+    for (size_t j = 0; j < num_messages; j++) {
+      PK_REQUIRE(messages[j] != nullptr, "null message pointer %zu", j);
+      segs[j] = HostSegment{messages[j], 32 * message_length};
+    }
+    rc = hs.h2d(ws, segs.data(), segs.size());
+    if (rc) return rc;
   }
-  cudaFree(d_msg);
-  cudaFree(d_mask);
-  cudaFree(d_out);
-  if (e != cudaSuccess) return cuda_status(e, "pkg_host_rs_interleaved_encode");
-  return rc;
+  if (mask_bytes) {
+    rc = hs.h2d(ws + msg_span, masks, mask_bytes);
+    if (rc) return rc;
+  }
+  rc = rs_encode_device(d_msg, num_messages, message_length, mask_len ? d_mask : nullptr,
+                        mask_len, codeword_length, d_out, hs.stream());
+  if (rc) return rc;
+  rc = hs.d2h(out, reinterpret_cast<uint8_t*>(d_out), 32 * total);
+  if (rc) return rc;
+  PK_CUDA(cudaStreamSynchronize(hs.stream()));
+  return PKG_OK;
 }

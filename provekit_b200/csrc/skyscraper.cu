@@ -16,6 +16,7 @@
 
 #include "fr.cuh"
 #include "ntt_internal.cuh"
+#include "host_stage.cuh"
 #include "pk_common.cuh"
 #include "rs_internal.cuh"
 #include "skyscraper.cuh"
@@ -249,19 +250,20 @@ extern "C" int pkg_host_skyscraper_hash_many(size_t size, const uint8_t* input, 
              size);
   if (count == 0) return PKG_OK;
   PK_REQUIRE(input && output, "null pointer");
-  uint8_t *d_in = nullptr, *d_out = nullptr;
-  PK_CUDA(cudaMalloc(&d_in, size * count));
-  cudaError_t e = cudaMalloc(&d_out, 32 * count);
-  int rc = PKG_OK;
-  if (e == cudaSuccess) e = cudaMemcpy(d_in, input, size * count, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) {
-    rc = hash_many_device(size, d_in, count, d_out, 0);
-    if (!rc) e = cudaMemcpy(output, d_out, 32 * count, cudaMemcpyDeviceToHost);
-  }
-  cudaFree(d_in);
-  cudaFree(d_out);
-  if (e != cudaSuccess) return cuda_status(e, "pkg_host_skyscraper_hash_many");
-  return rc;
+  const size_t in_span = (size * count + 255) & ~size_t(255);
+  HostStager& hs = HostStager::current();
+  std::lock_guard<std::mutex> lk(hs.mutex());
+  uint8_t* ws = nullptr;
+  int rc = hs.workspace(in_span + 32 * count, &ws);
+  if (rc) return rc;
+  rc = hs.h2d(ws, input, size * count);
+  if (rc) return rc;
+  rc = hash_many_device(size, ws, count, ws + in_span, hs.stream());
+  if (rc) return rc;
+  rc = hs.d2h(output, ws + in_span, 32 * count);
+  if (rc) return rc;
+  PK_CUDA(cudaStreamSynchronize(hs.stream()));
+  return PKG_OK;
 }
 
 extern "C" int pkg_merkle_tree(const uint8_t* leaves, size_t leaf_size, size_t num_leaves,
