@@ -534,6 +534,10 @@ def run_prove(a):
     launches = L.pkg_kernel_launches() - launches0
     clk = clocks.stop()
     ms = [e[0].elapsed_time(e[1]) for e in evs]
+    stages = (ctypes.c_double * 5)()
+    L.pkg_last_prove_stages(stages)
+    stage_ms = dict(zip(["commit", "witness_bounds", "zk_sumcheck", "eq_alpha",
+                         "transposed_products"], list(stages)))
     # e2e: witness from pinned host memory each step, proof struct read back
     e2e = []
     with torch.cuda.stream(stream):
@@ -563,7 +567,8 @@ def run_prove(a):
                     "h2d_bytes_per_step": 32 * h.num_witnesses,
                     "d2h_bytes_per_step": 32 * 3 + 32 * 4 * 20 * 4,
                     "note": "wall clock, witness copied from pinned host memory every step"},
-            "p50_ms": statistics.median(ms), "cpu_baseline": cpu, "gpu_launches": int(launches),
+            "p50_ms": statistics.median(ms), "stages_ms_last_step": stage_ms,
+            "cpu_baseline": cpu, "gpu_launches": int(launches),
             "clocks": clk}
     print(json.dumps(line), flush=True)
 
@@ -722,10 +727,12 @@ def run_served(a):
             if delay > 0:
                 time.sleep(delay)
             ids[i] = srv.submit(h, blinding_seed=i, transcript_domain=i)
-        lat = []
+        lat, qwait, svc = [], [], []
         for rid in ids:
             _, tm = srv.wait(rid)
             lat.append((tm["done_ns"] - tm["submit_ns"]) * 1e-9)
+            qwait.append((tm["admit_ns"] - tm["submit_ns"]) * 1e-9)
+            svc.append((tm["done_ns"] - tm["admit_ns"]) * 1e-9)
         st = srv.stats()
         srv.close()
         served_span = max(arrivals[-1], 0) + 0  # for reference only
@@ -733,7 +740,10 @@ def run_served(a):
             "rate_per_s": lam, "rate_vs_sequential_capacity": mult,
             "served": {"proofs_per_s": st["proofs_per_s"], "p50_ms": 1e3 * pct(lat, 0.5),
                        "p99_ms": 1e3 * pct(lat, 0.99), "p999_ms": 1e3 * pct(lat, 0.999),
-                       "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9},
+                       "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9,
+                       "queue_wait_ms": {"p50": 1e3 * pct(qwait, 0.5), "p99": 1e3 * pct(qwait, 0.99)},
+                       "service_ms": {"p50": 1e3 * pct(svc, 0.5), "p99": 1e3 * pct(svc, 0.99),
+                                      "max": 1e3 * max(svc)}},
             "sequential": {"proofs_per_s": len(reqs) / fin, "p50_ms": 1e3 * pct(seq_lat, 0.5),
                            "p99_ms": 1e3 * pct(seq_lat, 0.99), "p999_ms": 1e3 * pct(seq_lat, 0.999)},
         })

@@ -275,6 +275,14 @@ int pkg_spartan_prove(const pkg_r1cs *r1cs, const uint64_t *witness, uint64_t bl
                       uint64_t transcript_domain, unsigned folding_factor, unsigned log_inv_rate,
                       pkg_spartan_proof *out, pkg_stream_t stream);
 
+/* Per-stage host wall-clock (ms) of the calling thread's last
+ * pkg_spartan_prove: [0] commit (to the root), [1] witness bounds,
+ * [2] zk sumcheck, [3] eq(alpha) + public weight, [4] transposed products and
+ * evaluations.  Each stage ends with a stream synchronisation.  No
+ * counterpart in the reference (diagnostics). */
+#define PKG_PROVE_STAGES 5
+int pkg_last_prove_stages(double ms[PKG_PROVE_STAGES]);
+
 /* Synthetic satisfiable R1CS (host memory), the workload of the 2^20-constraint
  * prove benchmark: w[0] = 1, w[1..num_inputs] from pkg_sample_fr(seed); row
  * i: A_i and B_i each hold 1-3 nonzeros at uniform columns in
@@ -398,6 +406,14 @@ void pkg_server_destroy(pkg_server *server);
 #define PKG_FR_FROM_MONT_INT 5
 int pkg_fr_mul_batch(const uint64_t *a, const uint64_t *b, uint64_t *out, size_t n, int op,
                      pkg_stream_t stream);
+
+/* ---- memory ------------------------------------------------------------------ */
+/* Device scratch (prove, sumcheck, transposes, server requests) comes from a
+ * stream-ordered pool private to this library on each device, which keeps
+ * the memory it has grown to so that repeated proofs do not map it again.
+ * Returns unused pool memory on the current device to the driver, keeping at
+ * least keep_bytes.  No counterpart in the reference. */
+int pkg_trim_memory(size_t keep_bytes);
 
 /* ---- diagnostics ---------------------------------------------------------- */
 /* Synchronous device -> host copy of library-owned memory (e.g. batch buffers). */

@@ -78,6 +78,8 @@ SIGNATURES = {
     "pkg_server_get_stats": [_c_vp, _c_vp],
     "pkg_measure_imad_rate": [ctypes.POINTER(ctypes.c_double)],
     "pkg_measure_dfma_rate": [ctypes.POINTER(ctypes.c_double)],
+    "pkg_last_prove_stages": [ctypes.c_void_p],
+    "pkg_trim_memory": [ctypes.c_size_t],
     "pkg_fr_mul_batch": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                          ctypes.c_int, ctypes.c_void_p],
     "pkg_version": [],

@@ -87,7 +87,16 @@ int HostStager::init() {
       PK_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&pinned_[i]), kChunk, cudaHostAllocDefault));
     if (!done_[i]) PK_CUDA(cudaEventCreateWithFlags(&done_[i], cudaEventDisableTiming));
   }
+  if (!handoff_) PK_CUDA(cudaEventCreateWithFlags(&handoff_, cudaEventDisableTiming));
   device_ = dev;  // set last: a failed set-up is retried by the next call
+  return PKG_OK;
+}
+
+int HostStager::ensure() { return device_ < 0 ? init() : PKG_OK; }
+
+int HostStager::handoff(cudaStream_t consumer) {
+  PK_CUDA(cudaEventRecord(handoff_, stream_));
+  PK_CUDA(cudaStreamWaitEvent(consumer, handoff_, 0));
   return PKG_OK;
 }
 
@@ -101,10 +110,8 @@ HostStager& HostStager::current() {
 }
 
 int HostStager::workspace(size_t bytes, uint8_t** out) {
-  if (device_ < 0) {
-    int rc = init();
-    if (rc) return rc;
-  }
+  int rc = ensure();
+  if (rc) return rc;
   if (bytes > ws_bytes_) {
     if (ws_) {
       PK_CUDA(cudaStreamSynchronize(stream_));

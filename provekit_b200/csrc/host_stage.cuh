@@ -43,6 +43,10 @@ class HostStager {
   }
   // Device src -> host dst (after the work queued on stream()).
   int d2h(void* dst, const uint8_t* src, size_t bytes);
+  // Set up the stream, pinned chunks and events if not done yet.
+  int ensure();
+  // Make `consumer` wait for every copy queued so far on stream().
+  int handoff(cudaStream_t consumer);
 
  private:
   HostStager() = default;
@@ -54,6 +58,7 @@ class HostStager {
   static constexpr size_t kChunk = size_t(8) << 20;
   uint8_t* pinned_[kSlots] = {};
   cudaEvent_t done_[kSlots] = {};
+  cudaEvent_t handoff_ = nullptr;
   uint8_t* ws_ = nullptr;
   size_t ws_bytes_ = 0;
 };

@@ -64,6 +64,14 @@ int sm_count();
 
 // Stream-ordered scratch allocation (cudaMallocAsync), freed on scope exit
 // in stream order.
+// The library's stream-ordered memory pool on the current device (created on
+// first use).  Unlike the device's default pool (release threshold 0, which
+// hands freed memory back to the driver at every synchronisation and makes
+// the next allocation map it again), it keeps what it has grown to until
+// pkg_trim_memory.  Returns nullptr if the pool cannot be created.
+cudaMemPool_t lib_pool();
+
+// Stream-ordered scratch from lib_pool(), freed (stream-ordered) on scope exit.
 struct Scratch {
   void* ptr = nullptr;
   cudaStream_t stream = nullptr;
@@ -73,7 +81,12 @@ struct Scratch {
   int alloc(size_t bytes, cudaStream_t s) {
     stream = s;
     if (bytes == 0) return PKG_OK;
-    PK_CUDA(cudaMallocAsync(&ptr, bytes, s));
+    cudaMemPool_t pool = lib_pool();
+    if (!pool) {
+      set_last_error("could not create the library memory pool");
+      return PKG_ERR_CUDA;
+    }
+    PK_CUDA(cudaMallocFromPoolAsync(&ptr, bytes, pool, s));
     return PKG_OK;
   }
   ~Scratch() {

@@ -8,6 +8,7 @@
 // transposed matrices and the alpha covectors.  The host keeps the
 // transcript and reads back only the root, three Fr per sumcheck round and
 // the final scalars.
+#include <chrono>
 #include <cstring>
 #include <vector>
 
@@ -27,9 +28,29 @@ static size_t ceil_log2(size_t n) {  // utils::next_power_of_two (utils/mod.rs:7
   return k;
 }
 
+// Host wall-clock of the calling thread's last pkg_spartan_prove, per stage;
+// every stage ends with a stream synchronisation, so these are the stages'
+// device time plus their host work.
+thread_local double g_stage_ms[PKG_PROVE_STAGES];
+
+struct StageClock {
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void mark(int k) {
+    const auto now = std::chrono::steady_clock::now();
+    g_stage_ms[k] = std::chrono::duration<double, std::milli>(now - t).count();
+    t = now;
+  }
+};
+
 }  // namespace pk
 
 using namespace pk;
+
+extern "C" int pkg_last_prove_stages(double ms[PKG_PROVE_STAGES]) {
+  PK_REQUIRE(ms, "null output");
+  memcpy(ms, g_stage_ms, sizeof g_stage_ms);
+  return PKG_OK;
+}
 
 extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
                                  uint64_t blinding_seed, uint64_t transcript_domain,
@@ -46,6 +67,8 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
   PK_REQUIRE(m0 <= 30 && m <= 28 && ff <= m && lr <= 8, "instance too large (m=%zu, m0=%zu)", m,
              m0);
   memset(out, 0, sizeof *out);
+  memset(g_stage_ms, 0, sizeof g_stage_ms);
+  StageClock clk;
   out->m = m;
   out->m0 = m0;
   cudaStream_t s = as_stream(stream);
@@ -80,6 +103,7 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
     HostFr root = HostFr::to_mont(HostFr::from_limbs(reinterpret_cast<const uint64_t*>(out->root)));
     pkg_transcript_absorb(&out->transcript, root.l);
   }
+  clk.mark(0);
 
   // ---- witness bounds (sumcheck.rs:163-179)
   // partial sums of dot_device (<= 4 * SMs CTAs) and its result slot
@@ -105,10 +129,12 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
     PK_CUDA(cudaStreamSynchronize(s));
     PK_REQUIRE(!h_err, "R1CS column index out of range");
   }
+  clk.mark(1);
   rc = pkg_spartan_sumcheck(ta, tb, tc, m0, g.data(), wb.data(), &out->transcript, &out->r[0][0],
                             out->rho, out->sum_g, &out->coeffs[0][0], &out->alpha[0][0],
                             out->blinding_eval, stream);
   if (rc) return rc;
+  clk.mark(2);
 
   // ---- eq(alpha) and the transposed products (sumcheck.rs:195-227)
   Scratch s_eq, s_alph;
@@ -121,6 +147,7 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
   const uint64_t zero[4] = {0, 0, 0, 0};
   pkg_transcript_absorb(&out->transcript, zero);
   pkg_transcript_squeeze(&out->transcript, out->public_x);
+  clk.mark(3);
   for (int k = 0; k < 3; k++) {
     Scratch s_t;
     const size_t nnz = r1cs->nnz[k];
@@ -141,5 +168,6 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
     PK_CUDA(cudaStreamSynchronize(s));
     pkg_transcript_absorb(&out->transcript, out->evals[k]);
   }
+  clk.mark(4);
   return PKG_OK;
 }

@@ -109,9 +109,43 @@ __global__ void dfma_rate_kernel(double* sink, double c, double d, int iters) {
   if (s == -1.0) sink[threadIdx.x] = s;
 }
 
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+}  // namespace
+
+cudaMemPool_t lib_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pools[dev] = p;
+  }
+  return g_pools[dev];
+}
+
 }  // namespace pk
 
 using namespace pk;
+
+extern "C" int pkg_trim_memory(size_t keep_bytes) {
+  cudaMemPool_t p = lib_pool();
+  if (!p) {
+    set_last_error("could not create the library memory pool");
+    return PKG_ERR_CUDA;
+  }
+  PK_CUDA(cudaMemPoolTrimTo(p, keep_bytes));
+  return PKG_OK;
+}
 
 extern "C" const char* pkg_last_error(void) { return g_last_error; }
 

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "ntt_internal.cuh"
+#include "host_stage.cuh"
 #include "pk_common.cuh"
 
 namespace pk {
@@ -123,9 +124,12 @@ static void admit_locked(pkg_server* s) {
 
 static int run_request(HostRequest& r, cudaStream_t st) {
   std::vector<void*> bufs;
+  cudaMemPool_t pool = lib_pool();
+  if (!pool) return PKG_ERR_CUDA;
   auto alloc = [&](size_t bytes) -> void* {
     void* p = nullptr;
-    if (cudaMallocAsync(&p, std::max<size_t>(bytes, 256), st) != cudaSuccess) return nullptr;
+    if (cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 256), pool, st) != cudaSuccess)
+      return nullptr;
     bufs.push_back(p);
     return p;
   };
@@ -134,6 +138,13 @@ static int run_request(HostRequest& r, cudaStream_t st) {
   rc1.num_constraints = r.nc;
   rc1.num_witnesses = r.nw;
   int rc = PKG_OK;
+  // (destination, host source, bytes) of every upload
+  struct Up {
+    void* dst;
+    const void* src;
+    size_t bytes;
+  };
+  std::vector<Up> ups;
   for (int k = 0; k < 3 && !rc; k++) {
     void* rp = alloc(8 * (r.nc + 1));
     void* cl = alloc(4 * r.nnz[k]);
@@ -142,10 +153,10 @@ static int run_request(HostRequest& r, cudaStream_t st) {
       rc = PKG_ERR_OUT_OF_MEMORY;
       break;
     }
-    cudaMemcpyAsync(rp, r.row_ptr[k], 8 * (r.nc + 1), cudaMemcpyHostToDevice, st);
+    ups.push_back({rp, r.row_ptr[k], 8 * (r.nc + 1)});
     if (r.nnz[k]) {
-      cudaMemcpyAsync(cl, r.cols[k], 4 * r.nnz[k], cudaMemcpyHostToDevice, st);
-      cudaMemcpyAsync(vl, r.vals[k], 32 * r.nnz[k], cudaMemcpyHostToDevice, st);
+      ups.push_back({cl, r.cols[k], 4 * r.nnz[k]});
+      ups.push_back({vl, r.vals[k], 32 * r.nnz[k]});
     }
     rc1.row_ptr[k] = static_cast<uint64_t*>(rp);
     rc1.cols[k] = static_cast<uint32_t*>(cl);
@@ -155,10 +166,31 @@ static int run_request(HostRequest& r, cudaStream_t st) {
   void* w = rc ? nullptr : alloc(32 * r.nw);
   if (!rc && !w) rc = PKG_ERR_OUT_OF_MEMORY;
   if (!rc) {
-    cudaMemcpyAsync(w, r.witness, 32 * r.nw, cudaMemcpyHostToDevice, st);
+    ups.push_back({w, r.witness, 32 * r.nw});
+    // Uploads go through the host stager (pinned chunks, threaded host copies)
+    // rather than pageable copies from several workers at once; the worker's
+    // stream waits for them.  The buffers were allocated on `st`, so the
+    // stager's stream first waits for `st`.
+    HostStager& hs = HostStager::current();
+    std::lock_guard<std::mutex> lk(hs.mutex());
+    rc = hs.ensure();
+    cudaEvent_t allocated = nullptr;
+    if (!rc && cudaEventCreateWithFlags(&allocated, cudaEventDisableTiming) != cudaSuccess)
+      rc = PKG_ERR_CUDA;
+    if (!rc && (cudaEventRecord(allocated, st) != cudaSuccess ||
+                cudaStreamWaitEvent(hs.stream(), allocated, 0) != cudaSuccess))
+      rc = PKG_ERR_CUDA;
+    for (size_t i = 0; !rc && i < ups.size(); i++)
+      rc = hs.h2d(static_cast<uint8_t*>(ups[i].dst), ups[i].src, ups[i].bytes);
+    if (!rc) rc = hs.handoff(st);
+    if (allocated) cudaEventDestroy(allocated);
+  }
+  if (!rc) {
     rc = pkg_spartan_prove(&rc1, static_cast<uint64_t*>(w), r.blinding_seed, r.domain, r.ff, r.lr,
                            &r.proof, st);
     if (rc) r.error = pkg_last_error();
+  } else if (r.error.empty()) {
+    r.error = pkg_last_error();
   }
   for (void* p : bufs) cudaFreeAsync(p, st);
   cudaStreamSynchronize(st);
@@ -216,13 +248,9 @@ extern "C" int pkg_server_create(size_t hbm_budget_bytes, int max_inflight, pkg_
   if (rc) return rc;
   pkg_server* s = new pkg_server();
   PK_CUDA(cudaGetDevice(&s->device));
-  // Keep freed blocks in the stream-ordered pool up to the budget, so
-  // back-to-back proves reuse memory instead of returning it to the driver.
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
-    uint64_t thr = hbm_budget_bytes;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-  }
+  // Request buffers come from the library's pool, which keeps freed memory,
+  // so back-to-back proves reuse it instead of mapping it again.
+  PK_REQUIRE(lib_pool() != nullptr, "could not create the library memory pool");
   s->budget = hbm_budget_bytes;
   s->slots = max_inflight;
   for (int i = 0; i < max_inflight; i++) s->workers.emplace_back(worker_main, s);
