@@ -1096,3 +1096,185 @@ void pko_poseidon2_hash(uint64_t out[4], const uint64_t *inputs, size_t n) {
     pko_poseidon2_permutation(st);
     cpy4(out, st);
 }
+
+
+/* ======================================================================= */
+/* WHIR prove-round building blocks (conventions of the reference's Go      */
+/* WHIR verifier: recursive-verifier/app/utilities/utilities.go,            */
+/* recursive-verifier/app/circuit/whir_utilities.go)                        */
+/* ======================================================================= */
+/* MultivarPoly (utilities.go:16-23) splits the coefficients in halves on the
+ * last variable, so row entry j carries prod_t alpha[t]^(bit t of j). */
+void pko_multilinear_weights(uint64_t *w, const uint64_t *alpha, unsigned k) {
+    size_t m = (size_t)1 << k;
+    cpy4(w, ONE_MONT);
+    for (unsigned t = 0; t < k; t++) {
+        size_t half = (size_t)1 << t;
+        for (size_t j = 0; j < half; j++) pko_fr_mul(w + 4 * (j + half), w + 4 * j, alpha + 4 * t);
+    }
+    (void)m;
+}
+
+int pko_whir_fold_coeffs(const uint64_t *coeffs, size_t n, unsigned k, const uint64_t *alpha,
+                         uint64_t *out) {
+    if (k > 16 || !is_pow2(n) || n < ((size_t)1 << k)) return -1;
+    size_t m = (size_t)1 << k, L = n >> k;
+    uint64_t *w = (uint64_t *)malloc(32 * m);
+    if (!w) return -2;
+    pko_multilinear_weights(w, alpha, k);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < L; i++) {
+        uint64_t acc[4] = {0, 0, 0, 0}, t[4];
+        for (size_t j = 0; j < m; j++) {
+            pko_fr_mul(t, w + 4 * j, coeffs + 4 * (j * L + i));
+            pko_fr_add(acc, acc, t);
+        }
+        cpy4(out + 4 * i, acc);
+    }
+    free(w);
+    return 0;
+}
+
+/* computeFold (whir_utilities.go:176-182): MultivarPoly of each row. */
+int pko_whir_fold_rows(const uint64_t *rows, size_t nrows, unsigned k, const uint64_t *alpha,
+                       uint64_t *out) {
+    if (k > 16) return -1;
+    size_t m = (size_t)1 << k;
+    uint64_t *w = (uint64_t *)malloc(32 * m);
+    if (!w) return -2;
+    pko_multilinear_weights(w, alpha, k);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < nrows; i++) {
+        uint64_t acc[4] = {0, 0, 0, 0}, t[4];
+        for (size_t j = 0; j < m; j++) {
+            pko_fr_mul(t, w + 4 * j, rows + 4 * (i * m + j));
+            pko_fr_add(acc, acc, t);
+        }
+        cpy4(out + 4 * i, acc);
+    }
+    free(w);
+    return 0;
+}
+
+/* UnivarPoly (utilities.go:25-39): Horner from the top coefficient. */
+void pko_poly_eval(uint64_t out[4], const uint64_t *coeffs, size_t n, const uint64_t z[4]) {
+    uint64_t acc[4] = {0, 0, 0, 0};
+    for (size_t i = 0; i < n; i++) {
+        pko_fr_mul(acc, acc, z);
+        pko_fr_add(acc, acc, coeffs + 4 * (n - 1 - i));
+    }
+    cpy4(out, acc);
+}
+
+/* ExpandFromUnivariate (utilities.go:183-191). */
+void pko_expand_from_univariate(uint64_t *out, const uint64_t z[4], size_t n) {
+    uint64_t acc[4];
+    cpy4(acc, z);
+    for (size_t i = 0; i < n; i++) {
+        cpy4(out + 4 * (n - 1 - i), acc);
+        pko_fr_mul(acc, acc, acc);
+    }
+}
+
+int pko_merkle_open(const uint8_t *layers, size_t num_leaves, uint64_t idx, uint8_t *path) {
+    if (!is_pow2(num_leaves) || idx >= num_leaves) return -1;
+    int depth = log2_exact(num_leaves);
+    size_t off = 0, width = num_leaves;
+    for (int l = 0; l < depth; l++) {
+        memcpy(path + 32 * l, layers + 32 * (off + ((idx >> l) ^ 1)), 32);
+        off += width;
+        width >>= 1;
+    }
+    return 0;
+}
+
+/* verifyMerkleTreeProofs (whir_utilities.go:14-47) for one leaf; the
+ * sibling of the leaf hash is path[0], the auth path the rest. */
+int pko_merkle_verify(const uint64_t *leaf_canonical, size_t fr_per_leaf, uint64_t idx,
+                      const uint8_t *path, size_t depth, const uint8_t root[32]) {
+    uint64_t h[4], l[4], r[4], s[4];
+    if (fr_per_leaf == 0) return 0;
+    cpy4(h, leaf_canonical);
+    for (size_t x = 1; x < fr_per_leaf; x++) {
+        pko_sky_compress(l, h, leaf_canonical + 4 * x);
+        cpy4(h, l);
+    }
+    for (size_t lev = 0; lev < depth; lev++) {
+        memcpy(s, path + 32 * lev, 32);
+        if ((idx >> lev) & 1) { cpy4(l, s); cpy4(r, h); }
+        else { cpy4(l, h); cpy4(r, s); }
+        pko_sky_compress(h, l, r);
+    }
+    return memcmp(h, root, 32) == 0;
+}
+
+/* getStirChallenges (whir_utilities.go:49-79) for a power-of-two folded
+ * domain. */
+void pko_stir_indices(const uint8_t *bytes, size_t folded_domain_size, size_t nq, uint64_t *out) {
+    int bits = log2_exact(folded_domain_size);
+    size_t nbytes = (size_t)(bits + 7) / 8;
+    for (size_t i = 0; i < nq; i++) {
+        uint64_t v = 0;
+        for (size_t j = 0; j < nbytes; j++) v = (v << 8) | bytes[i * nbytes + j];
+        out[i] = bits >= 64 ? v : (v & (((uint64_t)1 << bits) - 1));
+    }
+}
+
+int pko_whir_sumcheck_round(uint64_t *f, uint64_t *w, size_t size, const uint64_t *fold,
+                            uint64_t out[12]) {
+    if (!is_pow2(size) || size < 2 || (fold && size < 4)) return -1;
+    if (fold) {
+        size_t h = size / 2;
+        uint64_t *tabs[2] = {f, w};
+        for (int k = 0; k < 2; k++) {
+            uint64_t *t = tabs[k];
+#pragma omp parallel for schedule(static)
+            for (size_t i = 0; i < h; i++) {
+                uint64_t d[4];
+                pko_fr_sub(d, t + 4 * (i + h), t + 4 * i);
+                pko_fr_mul(d, fold, d);
+                pko_fr_add(t + 4 * i, t + 4 * i, d);
+            }
+        }
+        size = h;
+    }
+    size_t half = size / 2;
+    uint64_t h0[4] = {0, 0, 0, 0}, h1[4] = {0, 0, 0, 0}, h2[4] = {0, 0, 0, 0};
+    for (size_t i = 0; i < half; i++) {
+        uint64_t t[4], a[4], b[4];
+        pko_fr_mul(t, f + 4 * i, w + 4 * i);
+        pko_fr_add(h0, h0, t);
+        pko_fr_mul(t, f + 4 * (i + half), w + 4 * (i + half));
+        pko_fr_add(h1, h1, t);
+        /* value at X = 2: 2*hi - lo */
+        pko_fr_add(a, f + 4 * (i + half), f + 4 * (i + half));
+        pko_fr_sub(a, a, f + 4 * i);
+        pko_fr_add(b, w + 4 * (i + half), w + 4 * (i + half));
+        pko_fr_sub(b, b, w + 4 * i);
+        pko_fr_mul(t, a, b);
+        pko_fr_add(h2, h2, t);
+    }
+    cpy4(out, h0);
+    cpy4(out + 4, h1);
+    cpy4(out + 8, h2);
+    return 0;
+}
+
+int pko_eq_accumulate(uint64_t *w, size_t nv, const uint64_t *points, const uint64_t *coeffs,
+                      size_t npts) {
+    if (nv >= 40) return -1;
+    size_t n = (size_t)1 << nv;
+    uint64_t *eq = (uint64_t *)malloc(32 * n);
+    if (!eq) return -2;
+    for (size_t j = 0; j < npts; j++) {
+        pko_eq_hypercube(points + 4 * nv * j, nv, n, eq);
+#pragma omp parallel for schedule(static)
+        for (size_t b = 0; b < n; b++) {
+            uint64_t t[4];
+            pko_fr_mul(t, coeffs + 4 * j, eq + 4 * b);
+            pko_fr_add(w + 4 * b, w + 4 * b, t);
+        }
+    }
+    free(eq);
+    return 0;
+}

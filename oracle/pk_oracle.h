@@ -137,6 +137,49 @@ int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t bl
 void pko_poseidon2_permutation(uint64_t state[16]);                      /* mont in/out */
 void pko_poseidon2_hash(uint64_t out[4], const uint64_t *inputs, size_t n); /* mont */
 
+/* ---- WHIR prove-round building blocks ----------------------------------
+ * Arithmetic conventions follow the reference's WHIR verifier restated in Go
+ * (recursive-verifier/app/...): MultivarPoly (utilities/utilities.go:16-23),
+ * UnivarPoly (:25-39), ExpandFromUnivariate (:183-191),
+ * EvaluateQuadraticPolynomialFromEvaluationList (:149-155),
+ * verifyMerkleTreeProofs and getStirChallenges (circuit/whir_utilities.go:14-79).
+ * Field values are Montgomery form unless stated. */
+/* w_j = prod_t alpha[t]^(bit t of j), j < 2^k: the coefficient of row entry j
+ * in MultivarPoly(row, alpha). */
+void pko_multilinear_weights(uint64_t *w, const uint64_t *alpha, unsigned k);
+/* out[i] = sum_j w_j * coeffs[j*(n>>k) + i], i < n >> k: the folded polynomial
+ * whose RS codeword is the fold of the interleaved codeword's rows. */
+int  pko_whir_fold_coeffs(const uint64_t *coeffs, size_t n, unsigned k, const uint64_t *alpha,
+                          uint64_t *out);
+/* out[i] = MultivarPoly(rows[i*2^k .. (i+1)*2^k), alpha) (computeFold). */
+int  pko_whir_fold_rows(const uint64_t *rows, size_t nrows, unsigned k, const uint64_t *alpha,
+                        uint64_t *out);
+/* sum_i coeffs[i] * z^i (UnivarPoly, Horner). */
+void pko_poly_eval(uint64_t out[4], const uint64_t *coeffs, size_t n, const uint64_t z[4]);
+/* out[n-1-i] = z^(2^i) (ExpandFromUnivariate). */
+void pko_expand_from_univariate(uint64_t *out, const uint64_t z[4], size_t n);
+/* Authentication path of leaf idx in a layers array (leaves first, root
+ * last): path[l] = node (idx >> l) ^ 1 of level l, l < log2(num_leaves). */
+int  pko_merkle_open(const uint8_t *layers, size_t num_leaves, uint64_t idx, uint8_t *path);
+/* verifyMerkleTreeProofs for one leaf: leaf hash = left fold of compress over
+ * the leaf's field elements (canonical limbs), then up the path with the
+ * index bits choosing sides.  Returns 1 when the root matches. */
+int  pko_merkle_verify(const uint64_t *leaf_canonical, size_t fr_per_leaf, uint64_t idx,
+                       const uint8_t *path, size_t depth, const uint8_t root[32]);
+/* getStirChallenges: ceil(log2(folded)/8) big-endian challenge bytes per
+ * query, reduced to the low log2(folded) bits. */
+void pko_stir_indices(const uint8_t *bytes, size_t folded_domain_size, size_t nq, uint64_t *out);
+/* WHIR sumcheck round over tables f, w (size entries, top variable first):
+ * with fold, first t[i] += fold*(t[i+size/2]-t[i]) for i < size/2 and the
+ * live size halves; then out = (h(0), h(1), h(2)) of
+ * h(X) = sum_b f(X, b) w(X, b) over the live tables' top variable. */
+int  pko_whir_sumcheck_round(uint64_t *f, uint64_t *w, size_t size, const uint64_t *fold,
+                             uint64_t out[12]);
+/* w[b] += sum_j coeffs[j] * eq(points[j], b) for b < 2^nv, point
+ * coordinate 0 on the top bit of b (as pko_eq_hypercube). */
+int  pko_eq_accumulate(uint64_t *w, size_t nv, const uint64_t *points, const uint64_t *coeffs,
+                       size_t npts);
+
 int pko_num_threads(void);
 
 #ifdef __cplusplus

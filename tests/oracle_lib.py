@@ -102,7 +102,56 @@ def lib():
         L.pko_poseidon2_hash.argtypes = [_u64p, _u64p, _sz]
         L.pko_spartan_prove.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_uint64,
                                         ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]
+        L.pko_multilinear_weights.argtypes = [_u64p, _u64p, ctypes.c_uint]
+        L.pko_whir_fold_coeffs.argtypes = [_u64p, _sz, ctypes.c_uint, _u64p, _u64p]
+        L.pko_whir_fold_rows.argtypes = [_u64p, _sz, ctypes.c_uint, _u64p, _u64p]
+        L.pko_poly_eval.argtypes = [_u64p, _u64p, _sz, _u64p]
+        L.pko_expand_from_univariate.argtypes = [_u64p, _u64p, _sz]
+        L.pko_merkle_open.argtypes = [_u8p, _sz, ctypes.c_uint64, _u8p]
+        L.pko_merkle_verify.argtypes = [_u64p, _sz, ctypes.c_uint64, _u8p, _sz, _u8p]
+        L.pko_stir_indices.argtypes = [_u8p, _sz, _sz, _u64p]
+        L.pko_whir_sumcheck_round.argtypes = [_u64p, _u64p, _sz, _u64p, _u64p]
+        L.pko_eq_accumulate.argtypes = [_u64p, _sz, _u64p, _u64p, _sz]
     return _lib
+
+
+# ---- WHIR prove-round building blocks ------------------------------------
+def whir_fold_coeffs(coeffs: np.ndarray, k: int, alpha: np.ndarray) -> np.ndarray:
+    c = np.ascontiguousarray(coeffs, dtype=np.uint64).reshape(-1, 4)
+    out = np.zeros((max(c.shape[0] >> k, 1), 4), np.uint64)
+    assert lib().pko_whir_fold_coeffs(p64(c), c.shape[0], k, p64(np.ascontiguousarray(alpha)),
+                                      p64(out)) == 0
+    return out
+
+
+def whir_fold_rows(rows: np.ndarray, k: int, alpha: np.ndarray) -> np.ndarray:
+    r = np.ascontiguousarray(rows, dtype=np.uint64).reshape(-1, 4)
+    n = r.shape[0] >> k
+    out = np.zeros((max(n, 1), 4), np.uint64)
+    assert lib().pko_whir_fold_rows(p64(r), n, k, p64(np.ascontiguousarray(alpha)), p64(out)) == 0
+    return out[:n]
+
+
+def poly_eval(coeffs: np.ndarray, z: np.ndarray) -> np.ndarray:
+    c = np.ascontiguousarray(coeffs, dtype=np.uint64).reshape(-1, 4)
+    out = np.zeros(4, np.uint64)
+    lib().pko_poly_eval(p64(out), p64(c), c.shape[0], p64(np.ascontiguousarray(z, dtype=np.uint64)))
+    return out
+
+
+def merkle_open(layers: bytes, num_leaves: int, idx: int) -> bytes:
+    lay = np.frombuffer(layers, dtype=np.uint8).copy()
+    depth = num_leaves.bit_length() - 1
+    out = np.zeros(max(32 * depth, 1), np.uint8)
+    assert lib().pko_merkle_open(p8(lay), num_leaves, idx, p8(out)) == 0
+    return out[: 32 * depth].tobytes()
+
+
+def whir_sumcheck_round(f: np.ndarray, w: np.ndarray, size: int, fold=None) -> np.ndarray:
+    out = np.zeros(12, np.uint64)
+    fd = None if fold is None else p64(np.ascontiguousarray(fold, dtype=np.uint64))
+    assert lib().pko_whir_sumcheck_round(p64(f), p64(w), size, fd, p64(out)) == 0
+    return out.reshape(3, 4)
 
 
 def p64(a: np.ndarray):
