@@ -386,6 +386,61 @@ int pkg_server_get_stats(pkg_server *server, pkg_server_stats *out);
 /* Finishes admitted work, fails queued requests, joins the workers. */
 void pkg_server_destroy(pkg_server *server);
 
+/* ---- WHIR prove rounds: the data-parallel operations ---------------------
+ * The WHIR prover is inside the un-vendored `whir` crate (called at
+ * provekit/prover/src/whir_r1cs.rs:295-301, 378-414); these are the device
+ * operations its rounds are made of.  Their arithmetic follows the
+ * reference's WHIR verifier restated in Go (recursive-verifier/app/...), cited
+ * per function.  Fr values are Montgomery form; "host" arrays are read or
+ * written synchronously, device arrays are 16-byte aligned. */
+/* out[i] = sum_j w_j coeffs[j (n >> k) + i], w_j = prod_t alpha[t]^(bit t of j)
+ * (MultivarPoly's weights, recursive-verifier/app/utilities/utilities.go:16-23):
+ * the polynomial whose RS codeword is the fold of the 2^k-message interleaved
+ * codeword.  k <= 6; n a power of two >= 2^k; alpha: host, k Fr.  Async. */
+int pkg_whir_fold_coeffs(const uint64_t *coeffs, size_t n, unsigned k, const uint64_t *alpha,
+                         uint64_t *out, pkg_stream_t stream);
+/* out[i] = MultivarPoly(rows[i 2^k .. (i+1) 2^k), alpha): computeFold
+ * (recursive-verifier/app/circuit/whir_utilities.go:182-188) over nrows rows
+ * of a codeword.  k <= 6; alpha: host.  Async. */
+int pkg_whir_fold_rows(const uint64_t *rows, size_t nrows, unsigned k, const uint64_t *alpha,
+                       uint64_t *out, pkg_stream_t stream);
+/* out[j] = sum_i coeffs[i] points[j]^i (UnivarPoly, utilities.go:25-39): the
+ * out-of-domain answers.  coeffs: device, n Fr; points, out: host, npts Fr.
+ * Synchronous. */
+int pkg_poly_eval_many(const uint64_t *coeffs, size_t n, const uint64_t *points, size_t npts,
+                       uint64_t *out, pkg_stream_t stream);
+/* Authentication paths in a layers array (leaves first, root last, as
+ * pkg_merkle_tree writes it): paths[q][l] = node (indices[q] >> l) ^ 1 of
+ * level l, l < log2(num_leaves) -- path[0] is the leaf's sibling, the rest
+ * the auth path that verifyMerkleTreeProofs walks
+ * (recursive-verifier/app/circuit/whir_utilities.go:14-47).  indices, paths:
+ * host (nq x log2(num_leaves) x 32 bytes).  Synchronous. */
+int pkg_merkle_open(const uint8_t *layers, size_t num_leaves, const uint64_t *indices, size_t nq,
+                    uint8_t *paths, pkg_stream_t stream);
+/* rows[q] = codeword row indices[q] (fr_per_row Fr each): the opened leaves'
+ * values.  indices, rows: host.  Synchronous. */
+int pkg_gather_rows(const uint64_t *codeword, size_t fr_per_row, size_t num_rows,
+                    const uint64_t *indices, size_t nq, uint64_t *rows, pkg_stream_t stream);
+/* getStirChallenges (whir_utilities.go:49-79) for a power-of-two folded
+ * domain: per query ceil(log2(size) / 8) big-endian challenge bytes, reduced
+ * to the low log2(size) bits.  Host. */
+int pkg_stir_indices(const uint8_t *bytes, size_t folded_domain_size, size_t nq, uint64_t *out);
+/* One round of WHIR's weighted sumcheck over device tables f, w of size
+ * entries (top variable first).  fold (host, or NULL): first fold the top
+ * variable, t[i] += fold (t[i + size/2] - t[i]) (quarter layout, as
+ * pkg_spartan_round); then out = (h(0), h(1), h(2)) of
+ * h(X) = sum_b f(X, b) w(X, b), the evaluation form that
+ * EvaluateQuadraticPolynomialFromEvaluationList and CheckSumOverBool read
+ * (utilities.go:149-171).  Synchronous. */
+int pkg_whir_sumcheck_round(uint64_t *f, uint64_t *w, size_t size, const uint64_t *fold,
+                            uint64_t out[12], pkg_stream_t stream);
+/* w[b] += sum_j coeffs[j] eq(points[j], b) for b < 2^nv (coordinate 0 on the
+ * top bit of b, as pkg_eq_hypercube): the weight update for new OOD and STIR
+ * constraints (computeWPoly's terms, whir_utilities.go:128-161).  w: device;
+ * points (npts x nv Fr), coeffs (npts Fr): host.  Synchronous. */
+int pkg_eq_accumulate(uint64_t *w, size_t nv, const uint64_t *points, const uint64_t *coeffs,
+                      size_t npts, pkg_stream_t stream);
+
 /* ---- field arithmetic (skyscraper/bn254-multiplier/src/scalar.rs:12-132,
  *      ark-ff Montgomery conversion) ---------------------------------------- */
 /* out[i] = op(a[i], b[i]) over n Fr (4 x u64 LE each, device, 16-byte

@@ -80,6 +80,14 @@ SIGNATURES = {
     "pkg_measure_dfma_rate": [ctypes.POINTER(ctypes.c_double)],
     "pkg_last_prove_stages": [ctypes.c_void_p],
     "pkg_trim_memory": [ctypes.c_size_t],
+    "pkg_whir_fold_coeffs": [_c_vp, _c_sz, _c_uint, _c_vp, _c_vp, _c_vp],
+    "pkg_whir_fold_rows": [_c_vp, _c_sz, _c_uint, _c_vp, _c_vp, _c_vp],
+    "pkg_poly_eval_many": [_c_vp, _c_sz, _c_vp, _c_sz, _c_vp, _c_vp],
+    "pkg_merkle_open": [_c_vp, _c_sz, _c_vp, _c_sz, _c_vp, _c_vp],
+    "pkg_gather_rows": [_c_vp, _c_sz, _c_sz, _c_vp, _c_sz, _c_vp, _c_vp],
+    "pkg_stir_indices": [_c_vp, _c_sz, _c_sz, _c_vp],
+    "pkg_whir_sumcheck_round": [_c_vp, _c_vp, _c_sz, _c_vp, _c_vp, _c_vp],
+    "pkg_eq_accumulate": [_c_vp, _c_sz, _c_vp, _c_vp, _c_sz, _c_vp],
     "pkg_fr_mul_batch": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                          ctypes.c_int, ctypes.c_void_p],
     "pkg_version": [],

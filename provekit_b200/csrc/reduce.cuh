@@ -1,0 +1,77 @@
+// reduce.cuh -- block-wide sums of field elements and the grid-size helpers
+// shared by the reduction kernels (sumcheck, dot products, WHIR rounds).
+//
+// Each thread accumulates a grid-stride slice; warps combine with
+// __shfl_down_sync (8 limbs per element, field additions), warps combine
+// through shared memory, and one partial per CTA goes to a small scratch
+// array that a single-CTA kernel sums.  Field addition is exact, so the
+// result does not depend on the reduction order.
+#pragma once
+#include <algorithm>
+
+#include "fr.cuh"
+#include "pk_common.cuh"
+
+namespace pk {
+
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ Fr shfl_down(const Fr& x, int off) {
+  Fr r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.v[i] = __shfl_down_sync(0xffffffffu, x.v[i], off);
+  return r;
+}
+
+// Block-wide sum of K field elements per thread; thread 0 gets the result.
+template <int K>
+__device__ __forceinline__ void block_sum(Fr (&v)[K]) {
+  __shared__ Fr warp_sums[kRedThreads / 32][K];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = fr_add(v[k], shfl_down(v[k], off));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) warp_sums[warp][k] = v[k];
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = lane < nw ? warp_sums[lane][k] : fr_zero();
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = fr_add(v[k], shfl_down(v[k], off));
+  }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kRedThreads) sum_partials_kernel(const uint64_t* __restrict__ part,
+                                                                 int nparts,
+                                                                 uint64_t* __restrict__ out) {
+  Fr v[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) v[k] = fr_zero();
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = fr_add(v[k], fr_load(part, (size_t)i * K + k));
+  block_sum<K>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) fr_store(out, k, v[k]);
+}
+
+// CTAs for a reduction over n items (at most 4 per SM).
+inline int red_grid(size_t n) {
+  size_t b = (n + kRedThreads - 1) / kRedThreads;
+  return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sm_count() * 4));
+}
+// CTAs of 256 threads for an element-wise kernel over n items (grid-stride).
+inline int ew_grid(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sm_count() * 32));
+}
+
+}  // namespace pk

@@ -12,11 +12,7 @@
 //   pkg_dot                whir::algebra::dot (whir_r1cs.rs:614-617, 637, 650)
 //   pkg_transcript_*       host Fiat-Shamir transcript stand-in (see the header)
 //
-// Reductions: each thread accumulates a grid-stride slice; warps combine
-// with __shfl_down_sync (8 limbs per element, field additions), warps
-// combine through shared memory, and one partial per CTA goes to a small
-// scratch array that a single-CTA kernel sums.  Field addition is exact, so
-// the result does not depend on the reduction order.
+// Reductions use the block-wide sums of reduce.cuh.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -26,58 +22,11 @@
 #include "fr.cuh"
 #include "fr_host.hpp"
 #include "pk_common.cuh"
+#include "reduce.cuh"
 #include "sky_host.hpp"
 
 namespace pk {
 
-constexpr int kRedThreads = 256;
-
-__device__ __forceinline__ Fr shfl_down(const Fr& x, int off) {
-  Fr r;
-#pragma unroll
-  for (int i = 0; i < 8; i++) r.v[i] = __shfl_down_sync(0xffffffffu, x.v[i], off);
-  return r;
-}
-
-// Block-wide sum of K field elements per thread; thread 0 gets the result.
-template <int K>
-__device__ __forceinline__ void block_sum(Fr (&v)[K]) {
-  __shared__ Fr warp_sums[kRedThreads / 32][K];
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1)
-#pragma unroll
-    for (int k = 0; k < K; k++) v[k] = fr_add(v[k], shfl_down(v[k], off));
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < K; k++) warp_sums[warp][k] = v[k];
-  __syncthreads();
-  if (warp == 0) {
-    const int nw = blockDim.x >> 5;
-#pragma unroll
-    for (int k = 0; k < K; k++) v[k] = lane < nw ? warp_sums[lane][k] : fr_zero();
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-#pragma unroll
-      for (int k = 0; k < K; k++) v[k] = fr_add(v[k], shfl_down(v[k], off));
-  }
-}
-
-template <int K>
-__global__ void __launch_bounds__(kRedThreads) sum_partials_kernel(const uint64_t* __restrict__ part,
-                                                                 int nparts,
-                                                                 uint64_t* __restrict__ out) {
-  Fr v[K];
-#pragma unroll
-  for (int k = 0; k < K; k++) v[k] = fr_zero();
-  for (int i = threadIdx.x; i < nparts; i += blockDim.x)
-#pragma unroll
-    for (int k = 0; k < K; k++) v[k] = fr_add(v[k], fr_load(part, (size_t)i * K + k));
-  block_sum<K>(v);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int k = 0; k < K; k++) fr_store(out, k, v[k]);
-}
 
 struct Tables4 {
   uint64_t* t[4];  // a, b, c, eq
@@ -230,14 +179,6 @@ __global__ void widen_kernel(const uint32_t* __restrict__ in, size_t n, unsigned
     out[i] = in[i];
 }
 
-static int red_grid(size_t n) {
-  size_t b = (n + kRedThreads - 1) / kRedThreads;
-  return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sm_count() * 4));
-}
-static int ew_grid(size_t n) {
-  size_t b = (n + 255) / 256;
-  return (int)std::max<size_t>(1, std::min<size_t>(b, (size_t)sm_count() * 32));
-}
 
 // One Spartan round on device tables; writes 3 Fr (f0, f(-1), f(inf)) to
 // d_out (device).  part: >= red_grid(q) * 3 Fr of scratch.

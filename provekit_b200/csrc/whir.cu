@@ -1,0 +1,394 @@
+// whir.cu -- the data-parallel pieces of WHIR's prove rounds on the device.
+//
+// The WHIR prover itself lives in the un-vendored `whir` crate (called from
+// provekit/prover/src/whir_r1cs.rs:295-301, 378-414).  Its rounds are built
+// from the operations below; their arithmetic follows the reference's WHIR
+// verifier restated in Go (recursive-verifier/app/utilities/utilities.go,
+// recursive-verifier/app/circuit/whir_utilities.go):
+//   pkg_whir_fold_coeffs     fold 2^k interleaved messages with the folding
+//                            randomness (MultivarPoly weights, utilities.go:16-23)
+//   pkg_whir_fold_rows       computeFold over codeword rows (whir_utilities.go:182-188)
+//   pkg_poly_eval_many       UnivarPoly at OOD points (utilities.go:25-39)
+//   pkg_merkle_open          authentication paths as verifyMerkleTreeProofs
+//   pkg_gather_rows          reads them (whir_utilities.go:14-47)
+//   pkg_whir_sumcheck_round  one round of the weighted sumcheck, sent as
+//                            evaluations at 0, 1, 2 (utilities.go:149-171)
+//   pkg_eq_accumulate        w += sum_j c_j eq(p_j, .) for new constraints
+//   pkg_stir_indices         getStirChallenges (whir_utilities.go:49-79), host
+#include <cstring>
+#include <vector>
+
+#include "fr.cuh"
+#include "fr_f64.cuh"
+#include "fr_host.hpp"
+#include "pk_common.cuh"
+#include "reduce.cuh"
+
+namespace pk {
+
+constexpr int kMaxFoldK = 6;
+
+// Montgomery field elements passed by value as kernel parameters.
+template <int N>
+struct FrParams {
+  uint32_t v[N][8];
+};
+
+template <int N>
+__device__ __forceinline__ Fr param_fr(const FrParams<N>& p, int j) {
+  Fr r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.v[i] = p.v[j][i];
+  return r;
+}
+
+template <int N>
+static void put_param(FrParams<N>& p, int j, const HostFr& x) {
+  memcpy(p.v[j], x.l, 32);
+}
+
+// w_j = prod_t alpha[t]^(bit t of j): MultivarPoly's coefficient of row entry j.
+static void fold_weights(const uint64_t* alpha, unsigned k, FrParams<1 << kMaxFoldK>& W) {
+  std::vector<HostFr> w((size_t)1 << k);
+  w[0] = HostFr::one();
+  for (unsigned t = 0; t < k; t++) {
+    const HostFr a = HostFr::from_limbs(alpha + 4 * t);
+    const size_t half = size_t(1) << t;
+    for (size_t j = 0; j < half; j++) w[j + half] = HostFr::mul(w[j], a);
+  }
+  for (size_t j = 0; j < w.size(); j++) put_param(W, (int)j, w[j]);
+}
+
+// out[i] = sum_j w_j c[j L + i]  (w_0 = 1)
+__global__ void whir_fold_coeffs_kernel(const uint64_t* __restrict__ c, size_t L, int m,
+                                        const __grid_constant__ FrParams<1 << kMaxFoldK> W,
+                                        uint64_t* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < L;
+       i += (size_t)gridDim.x * blockDim.x) {
+    Fr acc = fr_load_ro(c, i);
+    for (int j = 1; j < m; j++) acc = fr_add(acc, fr_mul_f64(param_fr(W, j), fr_load_ro(c, j * L + i)));
+    fr_store(out, i, acc);
+  }
+}
+
+// out[i] = sum_j w_j rows[i m + j]
+__global__ void whir_fold_rows_kernel(const uint64_t* __restrict__ rows, size_t nrows, int m,
+                                      const __grid_constant__ FrParams<1 << kMaxFoldK> W,
+                                      uint64_t* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nrows;
+       i += (size_t)gridDim.x * blockDim.x) {
+    Fr acc = fr_load_ro(rows, i * m);
+    for (int j = 1; j < m; j++)
+      acc = fr_add(acc, fr_mul_f64(param_fr(W, j), fr_load_ro(rows, i * m + j)));
+    fr_store(out, i, acc);
+  }
+}
+
+// Thread t of G owns coefficients t, t + G, t + 2G, ...: Horner in y = z^G
+// from the top, times z^t (from the squares z^(2^b)); CTA sums to part.
+// P.v[0] = y, P.v[1 + b] = z^(2^b).
+__global__ void __launch_bounds__(kRedThreads) poly_eval_kernel(
+    const uint64_t* __restrict__ c, size_t n, const __grid_constant__ FrParams<33> P,
+    uint64_t* __restrict__ part) {
+  const size_t G = (size_t)gridDim.x * blockDim.x;
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  Fr v[1] = {fr_zero()};
+  if (t < n) {
+    const Fr y = param_fr(P, 0);
+    Fr acc = fr_zero();
+    for (size_t k = (n - 1 - t) / G + 1; k-- > 0;) acc = fr_add(fr_mul_f64(acc, y), fr_load_ro(c, t + k * G));
+    for (int b = 0; b < 32; b++)
+      if ((t >> b) & 1) acc = fr_mul_f64(acc, param_fr(P, 1 + b));
+    v[0] = acc;
+  }
+  block_sum<1>(v);
+  if (threadIdx.x == 0) fr_store(part, blockIdx.x, v[0]);
+}
+
+// path[q depth + l] = node (idx[q] >> l) ^ 1 of level l
+__global__ void merkle_open_kernel(const uint8_t* __restrict__ layers, size_t num_leaves,
+                                   int depth, const uint64_t* __restrict__ idx, size_t nq,
+                                   uint8_t* __restrict__ out) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nq * (size_t)depth;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t q = t / depth;
+    const int l = (int)(t % depth);
+    size_t off = 0, width = num_leaves;
+    for (int j = 0; j < l; j++) {
+      off += width;
+      width >>= 1;
+    }
+    const uint4* src = reinterpret_cast<const uint4*>(layers + 32 * (off + ((idx[q] >> l) ^ 1)));
+    uint4* dst = reinterpret_cast<uint4*>(out + 32 * t);
+    dst[0] = src[0];
+    dst[1] = src[1];
+  }
+}
+
+// rows_out[q][e] = codeword[idx[q]][e]
+__global__ void gather_rows_kernel(const uint64_t* __restrict__ cw, size_t row_fr,
+                                   const uint64_t* __restrict__ idx, size_t nq,
+                                   uint64_t* __restrict__ out) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nq * row_fr;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t q = t / row_fr, e = t % row_fr;
+    fr_store(out, t, fr_load_ro(cw, idx[q] * row_fr + e));
+  }
+}
+
+// One WHIR sumcheck round over f, w (quarter layout when folding, as the
+// Spartan rounds): pairs (i, i + q); sums f0 w0, f1 w1, (2f1-f0)(2w1-w0).
+template <bool kFold>
+__global__ void __launch_bounds__(kRedThreads) whir_round_kernel(
+    uint64_t* __restrict__ f, uint64_t* __restrict__ w, size_t q,
+    const __grid_constant__ FrParams<1> A, uint64_t* __restrict__ part) {
+  Fr acc[3] = {fr_zero(), fr_zero(), fr_zero()};
+  const Fr alpha = param_fr(A, 0);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < q;
+       i += (size_t)gridDim.x * blockDim.x) {
+    Fr f0 = fr_load(f, i), f1 = fr_load(f, i + q), w0 = fr_load(w, i), w1 = fr_load(w, i + q);
+    if (kFold) {
+      f0 = fr_add(f0, fr_mul_f64(alpha, fr_sub(fr_load(f, i + 2 * q), f0)));
+      f1 = fr_add(f1, fr_mul_f64(alpha, fr_sub(fr_load(f, i + 3 * q), f1)));
+      w0 = fr_add(w0, fr_mul_f64(alpha, fr_sub(fr_load(w, i + 2 * q), w0)));
+      w1 = fr_add(w1, fr_mul_f64(alpha, fr_sub(fr_load(w, i + 3 * q), w1)));
+      fr_store(f, i, f0);
+      fr_store(f, i + q, f1);
+      fr_store(w, i, w0);
+      fr_store(w, i + q, w1);
+    }
+    acc[0] = fr_add(acc[0], fr_mul_f64(f0, w0));
+    acc[1] = fr_add(acc[1], fr_mul_f64(f1, w1));
+    const Fr f2 = fr_sub(fr_add(f1, f1), f0), w2 = fr_sub(fr_add(w1, w1), w0);
+    acc[2] = fr_add(acc[2], fr_mul_f64(f2, w2));
+  }
+  block_sum<3>(acc);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 3; k++) fr_store(part, (size_t)blockIdx.x * 3 + k, acc[k]);
+}
+
+// tables[j][x] = scale_j * prod_i (bit i of x, top first ? p_j[i] : 1 - p_j[i])
+// over k variables; p_j = pts + 4 (j * stride + first).
+__global__ void eq_tables_kernel(const uint64_t* __restrict__ pts, size_t stride, size_t first,
+                                 int k, const uint64_t* __restrict__ scale, size_t npts,
+                                 uint64_t* __restrict__ tables) {
+  const size_t per = size_t(1) << k;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < npts * per;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t j = t / per, x = t % per;
+    Fr acc = scale ? fr_load_ro(scale, j) : fr_one_mont();
+    for (int i = 0; i < k; i++) {
+      const Fr p = fr_load_ro(pts, j * stride + first + i);
+      const bool bit = (x >> (k - 1 - i)) & 1;
+      acc = fr_mul_f64(acc, bit ? p : fr_sub(fr_one_mont(), p));
+    }
+    fr_store(tables, t, acc);
+  }
+}
+
+// w[b] += sum_j hi_j[b >> nlo] lo_j[b & (2^nlo - 1)]
+__global__ void eq_accumulate_kernel(uint64_t* __restrict__ w, size_t n, int nlo,
+                                     const uint64_t* __restrict__ hi, size_t nhi_entries,
+                                     const uint64_t* __restrict__ lo, size_t npts) {
+  const size_t nlo_entries = size_t(1) << nlo;
+  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < n;
+       b += (size_t)gridDim.x * blockDim.x) {
+    Fr acc = fr_load(w, b);
+    for (size_t j = 0; j < npts; j++)
+      acc = fr_add(acc, fr_mul_f64(fr_load_ro(hi, j * nhi_entries + (b >> nlo)),
+                                   fr_load_ro(lo, j * nlo_entries + (b & (nlo_entries - 1)))));
+    fr_store(w, b, acc);
+  }
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+extern "C" int pkg_whir_fold_coeffs(const uint64_t* coeffs, size_t n, unsigned k,
+                                    const uint64_t* alpha, uint64_t* out, pkg_stream_t stream) {
+  PK_REQUIRE(k <= (unsigned)kMaxFoldK, "folding factor %u above %d", k, kMaxFoldK);
+  PK_REQUIRE(is_pow2(n) && n >= (size_t(1) << k), "length %zu is not a power of two >= 2^%u", n, k);
+  PK_REQUIRE(coeffs && out && (k == 0 || alpha), "null pointer");
+  PK_REQUIRE(aligned16(coeffs) && aligned16(out), "device buffers must be 16-byte aligned");
+  FrParams<1 << kMaxFoldK> W;
+  memset(&W, 0, sizeof W);
+  fold_weights(alpha, k, W);
+  const size_t L = n >> k;
+  whir_fold_coeffs_kernel<<<ew_grid(L), 256, 0, as_stream(stream)>>>(coeffs, L, 1 << k, W, out);
+  PK_CHECK_LAUNCH("whir_fold_coeffs_kernel");
+  return PKG_OK;
+}
+
+extern "C" int pkg_whir_fold_rows(const uint64_t* rows, size_t nrows, unsigned k,
+                                  const uint64_t* alpha, uint64_t* out, pkg_stream_t stream) {
+  PK_REQUIRE(k <= (unsigned)kMaxFoldK, "folding factor %u above %d", k, kMaxFoldK);
+  if (nrows == 0) return PKG_OK;
+  PK_REQUIRE(rows && out && (k == 0 || alpha), "null pointer");
+  PK_REQUIRE(aligned16(rows) && aligned16(out), "device buffers must be 16-byte aligned");
+  FrParams<1 << kMaxFoldK> W;
+  memset(&W, 0, sizeof W);
+  fold_weights(alpha, k, W);
+  whir_fold_rows_kernel<<<ew_grid(nrows), 256, 0, as_stream(stream)>>>(rows, nrows, 1 << k, W, out);
+  PK_CHECK_LAUNCH("whir_fold_rows_kernel");
+  return PKG_OK;
+}
+
+extern "C" int pkg_poly_eval_many(const uint64_t* coeffs, size_t n, const uint64_t* points,
+                                  size_t npts, uint64_t* out, pkg_stream_t stream) {
+  if (npts == 0) return PKG_OK;
+  PK_REQUIRE(points && out, "null pointer");
+  if (n == 0) {
+    memset(out, 0, 32 * npts);
+    return PKG_OK;
+  }
+  PK_REQUIRE(coeffs && aligned16(coeffs), "null or unaligned coefficients");
+  PK_REQUIRE(n < (size_t(1) << 40), "too many coefficients");
+  cudaStream_t s = as_stream(stream);
+  const int g = red_grid(n);
+  const size_t G = (size_t)g * kRedThreads;
+  Scratch scr;
+  int rc = scr.alloc(32 * ((size_t)g + npts), s);
+  if (rc) return rc;
+  uint64_t* part = static_cast<uint64_t*>(scr.ptr);
+  uint64_t* d_out = part + 4 * (size_t)g;
+  for (size_t j = 0; j < npts; j++) {
+    const HostFr z = HostFr::from_limbs(points + 4 * j);
+    FrParams<33> P;
+    put_param(P, 0, HostFr::pow_u64(z, G));
+    HostFr sq = z;
+    for (int b = 0; b < 32; b++) {
+      put_param(P, 1 + b, sq);
+      sq = HostFr::mul(sq, sq);
+    }
+    poly_eval_kernel<<<g, kRedThreads, 0, s>>>(coeffs, n, P, part);
+    PK_CHECK_LAUNCH("poly_eval_kernel");
+    sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, g, d_out + 4 * j);
+    PK_CHECK_LAUNCH("sum_partials_kernel");
+  }
+  PK_CUDA(cudaMemcpyAsync(out, d_out, 32 * npts, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}
+
+extern "C" int pkg_merkle_open(const uint8_t* layers, size_t num_leaves, const uint64_t* indices,
+                               size_t nq, uint8_t* paths, pkg_stream_t stream) {
+  PK_REQUIRE(is_pow2(num_leaves), "num_leaves %zu is not a power of two", num_leaves);
+  const int depth = log2_exact(num_leaves);
+  if (nq == 0 || depth == 0) return PKG_OK;
+  PK_REQUIRE(layers && indices && paths && aligned16(layers), "null or unaligned pointer");
+  for (size_t q = 0; q < nq; q++)
+    PK_REQUIRE(indices[q] < num_leaves, "index %llu out of range (%zu leaves)",
+               (unsigned long long)indices[q], num_leaves);
+  cudaStream_t s = as_stream(stream);
+  Scratch scr;
+  const size_t idx_bytes = (8 * nq + 255) & ~size_t(255);
+  int rc = scr.alloc(idx_bytes + 32 * nq * depth, s);
+  if (rc) return rc;
+  uint64_t* d_idx = static_cast<uint64_t*>(scr.ptr);
+  uint8_t* d_out = static_cast<uint8_t*>(scr.ptr) + idx_bytes;
+  PK_CUDA(cudaMemcpyAsync(d_idx, indices, 8 * nq, cudaMemcpyHostToDevice, s));
+  merkle_open_kernel<<<ew_grid(nq * depth), 256, 0, s>>>(layers, num_leaves, depth, d_idx, nq, d_out);
+  PK_CHECK_LAUNCH("merkle_open_kernel");
+  PK_CUDA(cudaMemcpyAsync(paths, d_out, 32 * nq * depth, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}
+
+extern "C" int pkg_gather_rows(const uint64_t* codeword, size_t fr_per_row, size_t num_rows,
+                               const uint64_t* indices, size_t nq, uint64_t* rows,
+                               pkg_stream_t stream) {
+  if (nq == 0 || fr_per_row == 0) return PKG_OK;
+  PK_REQUIRE(codeword && indices && rows && aligned16(codeword), "null or unaligned pointer");
+  for (size_t q = 0; q < nq; q++)
+    PK_REQUIRE(indices[q] < num_rows, "index %llu out of range (%zu rows)",
+               (unsigned long long)indices[q], num_rows);
+  cudaStream_t s = as_stream(stream);
+  Scratch scr;
+  const size_t idx_bytes = (8 * nq + 255) & ~size_t(255);
+  int rc = scr.alloc(idx_bytes + 32 * nq * fr_per_row, s);
+  if (rc) return rc;
+  uint64_t* d_idx = static_cast<uint64_t*>(scr.ptr);
+  uint64_t* d_out = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(scr.ptr) + idx_bytes);
+  PK_CUDA(cudaMemcpyAsync(d_idx, indices, 8 * nq, cudaMemcpyHostToDevice, s));
+  gather_rows_kernel<<<ew_grid(nq * fr_per_row), 256, 0, s>>>(codeword, fr_per_row, d_idx, nq, d_out);
+  PK_CHECK_LAUNCH("gather_rows_kernel");
+  PK_CUDA(cudaMemcpyAsync(rows, d_out, 32 * nq * fr_per_row, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}
+
+extern "C" int pkg_stir_indices(const uint8_t* bytes, size_t folded_domain_size, size_t nq,
+                                uint64_t* out) {
+  PK_REQUIRE(is_pow2(folded_domain_size), "folded domain size %zu is not a power of two",
+             folded_domain_size);
+  if (nq == 0) return PKG_OK;
+  PK_REQUIRE(bytes && out, "null pointer");
+  const int bits = log2_exact(folded_domain_size);
+  const size_t nbytes = (size_t)(bits + 7) / 8;
+  for (size_t i = 0; i < nq; i++) {
+    uint64_t v = 0;
+    for (size_t j = 0; j < nbytes; j++) v = (v << 8) | bytes[i * nbytes + j];
+    out[i] = bits >= 64 ? v : (v & ((uint64_t(1) << bits) - 1));
+  }
+  return PKG_OK;
+}
+
+extern "C" int pkg_whir_sumcheck_round(uint64_t* f, uint64_t* w, size_t size, const uint64_t* fold,
+                                       uint64_t out[12], pkg_stream_t stream) {
+  PK_REQUIRE(is_pow2(size) && size >= 2, "table size %zu must be a power of two >= 2", size);
+  PK_REQUIRE(!fold || size >= 4, "folding needs size >= 4 (got %zu)", size);
+  PK_REQUIRE(f && w && out && aligned16(f) && aligned16(w), "null or unaligned pointer");
+  cudaStream_t s = as_stream(stream);
+  const size_t q = fold ? size / 4 : size / 2;
+  const int g = red_grid(q);
+  Scratch scr;
+  int rc = scr.alloc(32 * (3 * (size_t)g + 3), s);
+  if (rc) return rc;
+  uint64_t* part = static_cast<uint64_t*>(scr.ptr);
+  uint64_t* d_out = part + 12 * (size_t)g;
+  FrParams<1> A;
+  memset(&A, 0, sizeof A);
+  if (fold) memcpy(A.v[0], fold, 32);
+  if (fold)
+    whir_round_kernel<true><<<g, kRedThreads, 0, s>>>(f, w, q, A, part);
+  else
+    whir_round_kernel<false><<<g, kRedThreads, 0, s>>>(f, w, q, A, part);
+  PK_CHECK_LAUNCH("whir_round_kernel");
+  sum_partials_kernel<3><<<1, kRedThreads, 0, s>>>(part, g, d_out);
+  PK_CHECK_LAUNCH("sum_partials_kernel");
+  PK_CUDA(cudaMemcpyAsync(out, d_out, 96, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}
+
+extern "C" int pkg_eq_accumulate(uint64_t* w, size_t nv, const uint64_t* points,
+                                 const uint64_t* coeffs, size_t npts, pkg_stream_t stream) {
+  PK_REQUIRE(nv < 40, "too many variables (%zu)", nv);
+  if (npts == 0) return PKG_OK;
+  PK_REQUIRE(w && points && coeffs && aligned16(w), "null or unaligned pointer");
+  cudaStream_t s = as_stream(stream);
+  const int nhi = (int)(nv + 1) / 2, nlo = (int)nv - nhi;
+  const size_t nh = size_t(1) << nhi, nl = size_t(1) << nlo, n = size_t(1) << nv;
+  Scratch scr;
+  const size_t pts_fr = npts * (nv ? nv : 1);
+  int rc = scr.alloc(32 * (pts_fr + npts + npts * (nh + nl)), s);
+  if (rc) return rc;
+  uint64_t* d_pts = static_cast<uint64_t*>(scr.ptr);
+  uint64_t* d_cf = d_pts + 4 * pts_fr;
+  uint64_t* d_hi = d_cf + 4 * npts;
+  uint64_t* d_lo = d_hi + 4 * npts * nh;
+  if (nv) PK_CUDA(cudaMemcpyAsync(d_pts, points, 32 * npts * nv, cudaMemcpyHostToDevice, s));
+  PK_CUDA(cudaMemcpyAsync(d_cf, coeffs, 32 * npts, cudaMemcpyHostToDevice, s));
+  // hi tables carry the coefficient, lo tables are plain eq tables
+  eq_tables_kernel<<<ew_grid(npts * nh), 256, 0, s>>>(d_pts, nv, 0, nhi, d_cf, npts, d_hi);
+  PK_CHECK_LAUNCH("eq_tables_kernel");
+  eq_tables_kernel<<<ew_grid(npts * nl), 256, 0, s>>>(d_pts, nv, nhi, nlo, nullptr, npts, d_lo);
+  PK_CHECK_LAUNCH("eq_tables_kernel");
+  eq_accumulate_kernel<<<ew_grid(n), 256, 0, s>>>(w, n, nlo, d_hi, nh, d_lo, npts);
+  PK_CHECK_LAUNCH("eq_accumulate_kernel");
+  // the host points and coefficients must outlive their async copies
+  PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}

@@ -4,7 +4,7 @@ Python big-int restatements of the reference's Go WHIR verifier
 UnivarPoly :25-39, EvaluateQuadraticPolynomialFromEvaluationList :149-155,
 CheckSumOverBool :168-171, ExpandFromUnivariate :183-191;
 recursive-verifier/app/circuit/whir_utilities.go: verifyMerkleTreeProofs
-:14-47, getStirChallenges :49-79, computeFold :176-182), plus the
+:14-47, getStirChallenges :49-79, computeFold :182-188), plus the
 protocol identities a WHIR prover relies on: folding the interleaved
 codeword's rows equals encoding the folded coefficients, and each sumcheck
 round polynomial sums to the previous claim evaluated at the challenge."""
