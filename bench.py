@@ -52,7 +52,7 @@ def parse_args():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plugin-e2e", action="store_true")
-    p.add_argument("--workload", choices=["commit", "prove", "batched", "served", "ntt"],
+    p.add_argument("--workload", choices=["commit", "prove", "batched", "served", "ntt", "whir_ops"],
                    default="commit",
                    help="commit (default, the headline line): WHIR commit of 2^20 coefficients; "
                         "prove: Spartan prove core of a 2^20-constraint R1CS; batched: 256 uneven "
@@ -827,6 +827,93 @@ def run_ntt(a):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# WHIR prove-round operations at the prove core's first-round sizes
+# (m = 21 variables, folding factor 3, rate 1/4).
+# ---------------------------------------------------------------------------
+def run_whir_ops(a):
+    import numpy as np
+    import torch
+
+    from provekit_b200 import _lib, whir
+    from provekit_b200._lib import check
+    from provekit_b200.merkle import whir_commit
+
+    L = _lib.lib()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    dfma = ctypes.c_double(0)
+    check(L.pkg_measure_dfma_rate(ctypes.byref(dfma)))
+    m, k, lr = 21, 3, 2
+    n = 1 << m
+
+    def sample(seed, cnt):
+        h = np.zeros((cnt, 4), np.uint64)
+        check(L.pkg_sample_fr(seed, cnt, h.ctypes.data, 1))
+        return h
+
+    coeffs = torch.from_numpy(sample(1, n).view(np.int64)).cuda()
+    alpha = sample(2, k)
+    cw, layers = whir_commit(coeffs, k, lr)
+    nl = (n >> k) << lr
+    f = torch.from_numpy(sample(3, n).view(np.int64)).cuda()
+    w = torch.from_numpy(sample(4, n).view(np.int64)).cuda()
+    pts = sample(5, 2)
+    eq_pts = sample(6, 40 * 18)
+    eq_cf = sample(7, 40)
+    w18 = torch.from_numpy(sample(8, 1 << 18).view(np.int64)).cuda()
+    idx = np.arange(0, nl, nl // 64, dtype=np.uint64)[:64]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    out_fold = torch.empty((n >> k, 4), dtype=torch.int64, device="cuda")
+    out_rows = torch.empty((nl, 4), dtype=torch.int64, device="cuda")
+    ops = {
+        "fold_coeffs_2p21_k3": (lambda: whir.fold_coeffs(coeffs, k, alpha, out=out_fold, stream=stream),
+                                n, 32 * (n + (n >> k))),
+        "fold_rows_2p21_rows": (lambda: whir.fold_rows(cw, k, alpha, out=out_rows, stream=stream),
+                                cw.shape[0], 32 * (cw.shape[0] + nl)),
+        "sumcheck_round_2p21": (lambda: whir.sumcheck_round(f, w, n, None, stream=stream),
+                                3 * (n // 2), 32 * 2 * n),
+        "poly_eval_2p21_x2": (lambda: whir.poly_eval_many(coeffs, pts, stream=stream),
+                              2 * n, 32 * 2 * n),
+        "eq_accumulate_2p18_x40": (lambda: whir.eq_accumulate(w18, 18, eq_pts, eq_cf, stream=stream),
+                                   40 << 18, 64 << 18),
+        "merkle_open_64_of_2p20": (lambda: whir.merkle_open(layers, nl, idx, stream=stream),
+                                   0, 64 * 20 * 32),
+    }
+    res = {}
+    for name, (fn, products, nbytes) in ops.items():
+        with torch.cuda.stream(stream):
+            for _ in range(a.warmup):
+                fn()
+            stream.synchronize()
+            evs = []
+            for _ in range(a.steps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                evs.append((e0, e1))
+        stream.synchronize()
+        ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs)
+        res[name] = {"ms": ms, "gmont_per_s": products / (ms * 1e-3) / 1e9,
+                     "fp64_frac": products * F64_PER_MUL / (ms * 1e-3) / dfma.value,
+                     "hbm_gbs": nbytes / (ms * 1e-3) / 1e9}
+    line = {"metric": "WHIR prove-round operations (device), first-round sizes of the 2^20-"
+                      "constraint prove core: m = 21, folding factor 3, rate 1/4",
+            "value": 1e3 / sum(r["ms"] for r in res.values()), "unit": "op-sets/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": sum(r["ms"] for r in res.values()), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 (BN254 Fr, 8x32-bit limbs)",
+            "data": "synthetic (ChaCha20-seeded Fr)",
+            "config": {"workload": "whir_ops", "m": m, "folding_factor": k, "log_inv_rate": lr,
+                       "l2": "flushed between steps"},
+            "ops": res, "dfma_rate_tops": dfma.value / 1e12,
+            "note": "synchronous ops (poly_eval, sumcheck_round, eq_accumulate, merkle_open) "
+                    "include their host read-back"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
@@ -839,6 +926,8 @@ def main():
         run_served(a)
     elif a.workload == "ntt":
         run_ntt(a)
+    elif a.workload == "whir_ops":
+        run_whir_ops(a)
     else:
         run_b200(a)
 
