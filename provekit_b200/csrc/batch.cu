@@ -235,7 +235,7 @@ __global__ void batch_sc_start_kernel(ScState* __restrict__ st, const JobDev* __
   s.sum_g = fr_add(dev_cubic(g0, fr_zero()), dev_cubic(g0, fr_one_mont()));
   t.absorb(s.sum_g);   // :541
   s.rho = t.squeeze();  // :543
-  s.saved = fr_mul(s.rho, s.sum_g);
+  s.saved = fr_mul_f64(s.rho, s.sum_g);
   s.tl = t.l;
   s.tr = t.r;
 }
@@ -258,7 +258,7 @@ __global__ void batch_eq_half_kernel(const RangeDesc* __restrict__ rd,
     Fr acc = fr_one_mont();
     for (int i = 0; i < nr; i++) {
       const Fr ri = st[d.job].r[r0 + i];
-      acc = fr_mul(acc, ((x >> (nr - 1 - i)) & 1) ? ri : fr_sub(fr_one_mont(), ri));
+      acc = fr_mul_f64(acc, ((x >> (nr - 1 - i)) & 1) ? ri : fr_sub(fr_one_mont(), ri));
     }
     fr_store(is_hi ? jb.eq_hi : jb.eq_lo, x, acc);
   }
@@ -272,7 +272,7 @@ __global__ void batch_eq_combine_kernel(const RangeDesc* __restrict__ rd,
     const RangeDesc d = rd[find_desc(begins, nd, o)];
     const JobDev& jb = jobs[d.job];
     const uint64_t x = o - d.begin;
-    fr_store(jb.eq, x, fr_mul(fr_load_ro(jb.eq_hi, x >> jb.nlo),
+    fr_store(jb.eq, x, fr_mul_f64(fr_load_ro(jb.eq_hi, x >> jb.nlo),
                               fr_load_ro(jb.eq_lo, x & ((uint64_t(1) << jb.nlo) - 1))));
   }
 }
@@ -310,23 +310,23 @@ __global__ void __launch_bounds__(kScThreads) batch_sc_round_kernel(
       Fr x0 = fr_load(t, j), x1 = fr_load(t, j + q);
       if (kFold) {
         Fr x2 = fr_load(t, j + 2 * q), x3 = fr_load(t, j + 3 * q);
-        x0 = fr_add(x0, fr_mul(fold, fr_sub(x2, x0)));
-        x1 = fr_add(x1, fr_mul(fold, fr_sub(x3, x1)));
+        x0 = fr_add(x0, fr_mul_f64(fold, fr_sub(x2, x0)));
+        x1 = fr_add(x1, fr_mul_f64(fold, fr_sub(x3, x1)));
         fr_store(t, j, x0);
         fr_store(t, j + q, x1);
       }
       lo[k] = x0;
       hi[k] = x1;
     }
-    Fr ab = fr_mul(lo[0], lo[1]);
-    acc[0] = fr_add(acc[0], fr_mul(lo[3], fr_sub(ab, lo[2])));
+    Fr ab = fr_mul_f64(lo[0], lo[1]);
+    acc[0] = fr_add(acc[0], fr_mul_f64(lo[3], fr_sub(ab, lo[2])));
     Fr x = fr_sub(fr_add(lo[0], lo[0]), hi[0]);
     Fr y = fr_sub(fr_add(lo[1], lo[1]), hi[1]);
     Fr z = fr_sub(fr_add(lo[2], lo[2]), hi[2]);
     Fr e = fr_sub(fr_add(lo[3], lo[3]), hi[3]);
-    acc[1] = fr_add(acc[1], fr_mul(e, fr_sub(fr_mul(x, y), z)));
-    Fr dd = fr_mul(fr_sub(hi[3], lo[3]), fr_sub(hi[0], lo[0]));
-    acc[2] = fr_add(acc[2], fr_mul(dd, fr_sub(hi[1], lo[1])));
+    acc[1] = fr_add(acc[1], fr_mul_f64(e, fr_sub(fr_mul_f64(x, y), z)));
+    Fr dd = fr_mul_f64(fr_sub(hi[3], lo[3]), fr_sub(hi[0], lo[0]));
+    acc[2] = fr_add(acc[2], fr_mul_f64(dd, fr_sub(hi[1], lo[1])));
   }
   __shared__ Fr wsum[kScThreads / 32][3];
 #pragma unroll
@@ -366,11 +366,11 @@ __global__ void batch_sc_finish_round_kernel(ScState* __restrict__ st,
   Fr gp[4];
   dev_blinding_coeffs(&s.g[0][0], (int)s.m0, (int)round, s.alpha, gp);
   Fr cf[4];
-  cf[0] = fr_add(h[0], fr_mul(s.rho, gp[0]));
+  cf[0] = fr_add(h[0], fr_mul_f64(s.rho, gp[0]));
   Fr gem1 = fr_sub(fr_add(fr_sub(gp[0], gp[1]), gp[2]), gp[3]);
-  Fr cem1 = fr_add(h[1], fr_mul(s.rho, gem1));
-  cf[2] = fr_mul(fr_half_mont(), fr_sub(fr_sub(fr_sub(fr_add(s.saved, cem1), cf[0]), cf[0]), cf[0]));
-  cf[3] = fr_add(h[2], fr_mul(s.rho, gp[3]));
+  Fr cem1 = fr_add(h[1], fr_mul_f64(s.rho, gem1));
+  cf[2] = fr_mul_f64(fr_half_mont(), fr_sub(fr_sub(fr_sub(fr_add(s.saved, cem1), cf[0]), cf[0]), cf[0]));
+  cf[3] = fr_add(h[2], fr_mul_f64(s.rho, gp[3]));
   cf[1] = fr_sub(fr_sub(fr_sub(fr_sub(s.saved, cf[0]), cf[0]), cf[3]), cf[2]);
   DevTranscript t;
   t.l = s.tl;
@@ -395,8 +395,8 @@ __global__ void batch_sc_end_kernel(ScState* __restrict__ st, uint32_t njobs) {
   for (uint32_t i = 0; i < s.m0; i++) {
     Fr pw = fr_one_mont();
     for (int k = 0; k < 4; k++) {
-      acc = fr_add(acc, fr_mul(pw, s.wb[i][k]));
-      pw = fr_mul(pw, s.alpha[i]);
+      acc = fr_add(acc, fr_mul_f64(pw, s.wb[i][k]));
+      pw = fr_mul_f64(pw, s.alpha[i]);
     }
   }
   s.blinding_eval = acc;

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "fr.cuh"
+#include "fr_f64.cuh"
 #include "fr_host.hpp"
 #include "pk_common.cuh"
 #include "poseidon2_t4_constants.h"
@@ -46,9 +47,9 @@ __device__ __forceinline__ Fr p2_const(const uint64_t* c) {
 }
 
 __device__ __forceinline__ Fr p2_sbox(const Fr& x) {  // x^5
-  Fr s = fr_sqr(x);
-  s = fr_sqr(s);
-  return fr_mul(s, x);
+  Fr s = fr_sqr_f64(x);
+  s = fr_sqr_f64(s);
+  return fr_mul_f64(s, x);
 }
 
 // matrix_multiplication_4x4 (permutation.rs:101-120)
@@ -73,7 +74,7 @@ __device__ __forceinline__ void p2_ext(Fr (&s)[4]) {
 __device__ __forceinline__ void p2_int(Fr (&s)[4]) {
   Fr sum = fr_add(fr_add(s[0], s[1]), fr_add(s[2], s[3]));
 #pragma unroll
-  for (int i = 0; i < 4; i++) s[i] = fr_add(fr_mul(s[i], p2_const(kP2Diag[i])), sum);
+  for (int i = 0; i < 4; i++) s[i] = fr_add(fr_mul_f64(s[i], p2_const(kP2Diag[i])), sum);
 }
 
 __device__ __forceinline__ void p2_permute(Fr (&s)[4]) {

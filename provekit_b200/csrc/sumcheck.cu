@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "fr.cuh"
+#include "fr_f64.cuh"
 #include "fr_host.hpp"
 #include "pk_common.cuh"
 #include "reduce.cuh"
@@ -35,17 +36,17 @@ struct Tables4 {
 // The Spartan closure (whir_r1cs.rs:552-558) on one pair of each table.
 __device__ __forceinline__ void spartan_map(const Fr (&lo)[4], const Fr (&hi)[4], Fr (&acc)[3]) {
   // f(0) = eq0 * (a0*b0 - c0)
-  Fr ab = fr_mul(lo[0], lo[1]);
-  acc[0] = fr_add(acc[0], fr_mul(lo[3], fr_sub(ab, lo[2])));
+  Fr ab = fr_mul_f64(lo[0], lo[1]);
+  acc[0] = fr_add(acc[0], fr_mul_f64(lo[3], fr_sub(ab, lo[2])));
   // f(-1) = (2eq0 - eq1) * ((2a0 - a1)(2b0 - b1) - (2c0 - c1))
   Fr x = fr_sub(fr_add(lo[0], lo[0]), hi[0]);
   Fr y = fr_sub(fr_add(lo[1], lo[1]), hi[1]);
   Fr z = fr_sub(fr_add(lo[2], lo[2]), hi[2]);
   Fr e = fr_sub(fr_add(lo[3], lo[3]), hi[3]);
-  acc[1] = fr_add(acc[1], fr_mul(e, fr_sub(fr_mul(x, y), z)));
+  acc[1] = fr_add(acc[1], fr_mul_f64(e, fr_sub(fr_mul_f64(x, y), z)));
   // f(inf) = (eq1 - eq0)(a1 - a0)(b1 - b0)
-  Fr d = fr_mul(fr_sub(hi[3], lo[3]), fr_sub(hi[0], lo[0]));
-  acc[2] = fr_add(acc[2], fr_mul(d, fr_sub(hi[1], lo[1])));
+  Fr d = fr_mul_f64(fr_sub(hi[3], lo[3]), fr_sub(hi[0], lo[0]));
+  acc[2] = fr_add(acc[2], fr_mul_f64(d, fr_sub(hi[1], lo[1])));
 }
 
 // kFold: current size s = 4q; fold t[j] += f*(t[j+2q]-t[j]),
@@ -64,8 +65,8 @@ __global__ void __launch_bounds__(kRedThreads) spartan_round_kernel(Tables4 tabs
       Fr x0 = fr_load(t, j), x1 = fr_load(t, j + q);
       if (kFold) {
         Fr x2 = fr_load(t, j + 2 * q), x3 = fr_load(t, j + 3 * q);
-        x0 = fr_add(x0, fr_mul(fold, fr_sub(x2, x0)));
-        x1 = fr_add(x1, fr_mul(fold, fr_sub(x3, x1)));
+        x0 = fr_add(x0, fr_mul_f64(fold, fr_sub(x2, x0)));
+        x1 = fr_add(x1, fr_mul_f64(fold, fr_sub(x3, x1)));
         fr_store(t, j, x0);
         fr_store(t, j + q, x1);
       }
@@ -90,7 +91,7 @@ __global__ void eq_small_kernel(const uint64_t* __restrict__ r, int nr, uint64_t
     for (int i = 0; i < nr; i++) {
       Fr ri = fr_load_ro(r, i);
       Fr f = ((x >> (nr - 1 - i)) & 1) ? ri : fr_sub(fr_one_mont(), ri);
-      acc = fr_mul(acc, f);
+      acc = fr_mul_f64(acc, f);
     }
     fr_store(out, x, acc);
   }
@@ -101,7 +102,7 @@ __global__ void eq_combine_kernel(const uint64_t* __restrict__ hi, const uint64_
                                   int nlo, size_t num_entries, uint64_t* __restrict__ out) {
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < num_entries;
        x += (size_t)gridDim.x * blockDim.x) {
-    fr_store(out, x, fr_mul(fr_load_ro(hi, x >> nlo), fr_load_ro(lo, x & ((size_t(1) << nlo) - 1))));
+    fr_store(out, x, fr_mul_f64(fr_load_ro(hi, x >> nlo), fr_load_ro(lo, x & ((size_t(1) << nlo) - 1))));
   }
 }
 
@@ -120,7 +121,7 @@ __global__ void spmv_csr_kernel(const uint64_t* __restrict__ row_ptr, const uint
         atomicOr(err, 1u);
         continue;
       }
-      acc = fr_add(acc, fr_mul(fr_load_ro(vals, k), fr_load_ro(x, col)));
+      acc = fr_add(acc, fr_mul_f64(fr_load_ro(vals, k), fr_load_ro(x, col)));
     }
     fr_store(y, row, acc);
   }
@@ -130,7 +131,7 @@ __global__ void hadamard_pad_kernel(const uint64_t* __restrict__ a, const uint64
                                     size_t n, size_t padded, uint64_t* __restrict__ c) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < padded;
        i += (size_t)gridDim.x * blockDim.x)
-    fr_store(c, i, i < n ? fr_mul(fr_load_ro(a, i), fr_load_ro(b, i)) : fr_zero());
+    fr_store(c, i, i < n ? fr_mul_f64(fr_load_ro(a, i), fr_load_ro(b, i)) : fr_zero());
 }
 
 __global__ void __launch_bounds__(kRedThreads) dot_kernel(const uint64_t* __restrict__ a,
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kRedThreads) dot_kernel(const uint64_t* __rest
   Fr acc[1] = {fr_zero()};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    acc[0] = fr_add(acc[0], fr_mul(fr_load_ro(a, i), fr_load_ro(b, i)));
+    acc[0] = fr_add(acc[0], fr_mul_f64(fr_load_ro(a, i), fr_load_ro(b, i)));
   block_sum<1>(acc);
   if (threadIdx.x == 0) fr_store(part, blockIdx.x, acc[0]);
 }

@@ -16,7 +16,7 @@ __device__ __forceinline__ void sky_permute(Fr& l, Fr& r) {
 #pragma unroll 1
   for (int k = 0; k < 18; k++) {
     const bool is_bar = (k == 6 || k == 7 || k == 10 || k == 11);
-    Fr f = is_bar ? sky_bar(l) : fr_sqr(l);
+    Fr f = is_bar ? sky_bar(l) : fr_sqr_f64(l);
     Fr nl = fr_add(fr_add(r, f), sky_rc(k));
     r = l;
     l = nl;
@@ -41,9 +41,9 @@ struct DevTranscript {
 };
 
 __device__ __forceinline__ Fr dev_cubic(const Fr* c, const Fr& x) {
-  Fr acc = fr_mul(x, c[3]);
-  acc = fr_mul(fr_add(acc, c[2]), x);
-  acc = fr_mul(fr_add(acc, c[1]), x);
+  Fr acc = fr_mul_f64(x, c[3]);
+  acc = fr_mul_f64(fr_add(acc, c[2]), x);
+  acc = fr_mul_f64(fr_add(acc, c[1]), x);
   return fr_add(acc, c[0]);
 }
 
@@ -92,11 +92,11 @@ __device__ __forceinline__ void dev_blinding_coeffs(const Fr* g, int n, int comp
     suffix = fr_add(suffix, fr_add(dev_cubic(g + 4 * i, fr_zero()), dev_cubic(g + 4 * i, fr_one_mont())));
   Fr pm = fr_one_mont();
   for (int i = 0; i < n - 1 - cf; i++) pm = fr_add(pm, pm);
-  Fr sm = fr_mul(pm, fr_half_mont());
-  Fr cst = fr_add(fr_mul(pm, prefix), fr_mul(sm, suffix));
+  Fr sm = fr_mul_f64(pm, fr_half_mont());
+  Fr cst = fr_add(fr_mul_f64(pm, prefix), fr_mul_f64(sm, suffix));
   const Fr* cur = g + 4 * cf;
-  Fr res[4] = {fr_add(fr_mul(pm, cur[0]), cst), fr_mul(pm, cur[1]), fr_mul(pm, cur[2]),
-               fr_mul(pm, cur[3])};
+  Fr res[4] = {fr_add(fr_mul_f64(pm, cur[0]), cst), fr_mul_f64(pm, cur[1]), fr_mul_f64(pm, cur[2]),
+               fr_mul_f64(pm, cur[3])};
   if (all_fixed) {
     out[0] = dev_cubic(res, alphas[cf]);
     out[1] = out[2] = out[3] = fr_zero();
