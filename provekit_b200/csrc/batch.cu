@@ -299,35 +299,11 @@ __global__ void __launch_bounds__(kScThreads) batch_sc_round_kernel(
   const uint32_t nctas = (uint32_t)d.count;
   Fr fold = fr_zero();
   if (kFold) fold = st[d.job].alpha[round - 1];
-  uint64_t* tabs[4] = {jb.a, jb.b, jb.c, jb.eq};
+  uint64_t* const tabs[4] = {jb.a, jb.b, jb.c, jb.eq};
   Fr acc[3] = {fr_zero(), fr_zero(), fr_zero()};
   for (uint64_t j = (uint64_t)cta * blockDim.x + threadIdx.x; j < q;
-       j += (uint64_t)nctas * blockDim.x) {
-    Fr lo[4], hi[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      uint64_t* t = tabs[k];
-      Fr x0 = fr_load(t, j), x1 = fr_load(t, j + q);
-      if (kFold) {
-        Fr x2 = fr_load(t, j + 2 * q), x3 = fr_load(t, j + 3 * q);
-        x0 = fr_add(x0, fr_mul_f64(fold, fr_sub(x2, x0)));
-        x1 = fr_add(x1, fr_mul_f64(fold, fr_sub(x3, x1)));
-        fr_store(t, j, x0);
-        fr_store(t, j + q, x1);
-      }
-      lo[k] = x0;
-      hi[k] = x1;
-    }
-    Fr ab = fr_mul_f64(lo[0], lo[1]);
-    acc[0] = fr_add(acc[0], fr_mul_f64(lo[3], fr_sub(ab, lo[2])));
-    Fr x = fr_sub(fr_add(lo[0], lo[0]), hi[0]);
-    Fr y = fr_sub(fr_add(lo[1], lo[1]), hi[1]);
-    Fr z = fr_sub(fr_add(lo[2], lo[2]), hi[2]);
-    Fr e = fr_sub(fr_add(lo[3], lo[3]), hi[3]);
-    acc[1] = fr_add(acc[1], fr_mul_f64(e, fr_sub(fr_mul_f64(x, y), z)));
-    Fr dd = fr_mul_f64(fr_sub(hi[3], lo[3]), fr_sub(hi[0], lo[0]));
-    acc[2] = fr_add(acc[2], fr_mul_f64(dd, fr_sub(hi[1], lo[1])));
-  }
+       j += (uint64_t)nctas * blockDim.x)
+    spartan_pair<kFold>(tabs, j, q, fold, acc);
   __shared__ Fr wsum[kScThreads / 32][3];
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1)

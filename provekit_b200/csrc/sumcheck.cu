@@ -25,6 +25,7 @@
 #include "pk_common.cuh"
 #include "reduce.cuh"
 #include "sky_host.hpp"
+#include "sumcheck_device.cuh"
 
 namespace pk {
 
@@ -33,48 +34,16 @@ struct Tables4 {
   uint64_t* t[4];  // a, b, c, eq
 };
 
-// The Spartan closure (whir_r1cs.rs:552-558) on one pair of each table.
-__device__ __forceinline__ void spartan_map(const Fr (&lo)[4], const Fr (&hi)[4], Fr (&acc)[3]) {
-  // f(0) = eq0 * (a0*b0 - c0)
-  Fr ab = fr_mul_f64(lo[0], lo[1]);
-  acc[0] = fr_add(acc[0], fr_mul_f64(lo[3], fr_sub(ab, lo[2])));
-  // f(-1) = (2eq0 - eq1) * ((2a0 - a1)(2b0 - b1) - (2c0 - c1))
-  Fr x = fr_sub(fr_add(lo[0], lo[0]), hi[0]);
-  Fr y = fr_sub(fr_add(lo[1], lo[1]), hi[1]);
-  Fr z = fr_sub(fr_add(lo[2], lo[2]), hi[2]);
-  Fr e = fr_sub(fr_add(lo[3], lo[3]), hi[3]);
-  acc[1] = fr_add(acc[1], fr_mul_f64(e, fr_sub(fr_mul_f64(x, y), z)));
-  // f(inf) = (eq1 - eq0)(a1 - a0)(b1 - b0)
-  Fr d = fr_mul_f64(fr_sub(hi[3], lo[3]), fr_sub(hi[0], lo[0]));
-  acc[2] = fr_add(acc[2], fr_mul_f64(d, fr_sub(hi[1], lo[1])));
-}
-
-// kFold: current size s = 4q; fold t[j] += f*(t[j+2q]-t[j]),
-// t[j+q] += f*(t[j+3q]-t[j+q]) in place and map (t[j], t[j+q]).
-// !kFold: size s = 2q; map (t[j], t[j+q]).
+// kFold: current size s = 4q, folded in place, then pairs (t[j], t[j+q]);
+// !kFold: size s = 2q, pairs (t[j], t[j+q]).
 template <bool kFold>
-__global__ void __launch_bounds__(kRedThreads) spartan_round_kernel(Tables4 tabs, size_t q, Fr fold,
-                                                                  uint64_t* __restrict__ part) {
+__global__ void __launch_bounds__(kRedThreads) spartan_round_kernel(Tables4 tabs, size_t q,
+                                                                     Fr fold,
+                                                                     uint64_t* __restrict__ part) {
   Fr acc[3] = {fr_zero(), fr_zero(), fr_zero()};
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < q;
-       j += (size_t)gridDim.x * blockDim.x) {
-    Fr lo[4], hi[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      uint64_t* t = tabs.t[k];
-      Fr x0 = fr_load(t, j), x1 = fr_load(t, j + q);
-      if (kFold) {
-        Fr x2 = fr_load(t, j + 2 * q), x3 = fr_load(t, j + 3 * q);
-        x0 = fr_add(x0, fr_mul_f64(fold, fr_sub(x2, x0)));
-        x1 = fr_add(x1, fr_mul_f64(fold, fr_sub(x3, x1)));
-        fr_store(t, j, x0);
-        fr_store(t, j + q, x1);
-      }
-      lo[k] = x0;
-      hi[k] = x1;
-    }
-    spartan_map(lo, hi, acc);
-  }
+       j += (size_t)gridDim.x * blockDim.x)
+    spartan_pair<kFold>(tabs.t, j, q, fold, acc);
   block_sum<3>(acc);
   if (threadIdx.x == 0)
 #pragma unroll

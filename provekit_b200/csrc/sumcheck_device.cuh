@@ -106,4 +106,50 @@ __device__ __forceinline__ void dev_blinding_coeffs(const Fr* g, int n, int comp
   for (int k = 0; k < 4; k++) out[k] = res[k];
 }
 
+// The Spartan round code below multiplies 14 times per pair; inlining every
+// FP64 product makes a ~100 KB kernel that runs from cold instruction cache
+// (small rounds took ~40 us whatever their size).  One out-of-line product
+// keeps the kernel small.
+static __device__ __noinline__ Fr fr_mul_call(const Fr a, const Fr b) { return fr_mul_f64(a, b); }
+
+// One pair (t[j], t[j + q]) of a table; with kFold the live size is 4q and
+// the top variable is folded first, t[j] += f (t[j+2q] - t[j]) and
+// t[j+q] += f (t[j+3q] - t[j+q]), in place.
+template <bool kFold>
+__device__ __forceinline__ void round_pair(uint64_t* t, size_t j, size_t q, const Fr& fold, Fr& x0,
+                                           Fr& x1) {
+  x0 = fr_load(t, j);
+  x1 = fr_load(t, j + q);
+  if (kFold) {
+    x0 = fr_add(x0, fr_mul_call(fold, fr_sub(fr_load(t, j + 2 * q), x0)));
+    x1 = fr_add(x1, fr_mul_call(fold, fr_sub(fr_load(t, j + 3 * q), x1)));
+    fr_store(t, j, x0);
+    fr_store(t, j + q, x1);
+  }
+}
+
+// The Spartan closure (whir_r1cs.rs:552-558) on one pair of each table,
+// streaming the tables a, b, c, eq in turn so that only partial products
+// stay live:
+//   f(0)   = eq0 (a0 b0 - c0)
+//   f(-1)  = (2eq0 - eq1) ((2a0 - a1)(2b0 - b1) - (2c0 - c1))
+//   f(inf) = (eq1 - eq0)(a1 - a0)(b1 - b0)
+template <bool kFold>
+__device__ __forceinline__ void spartan_pair(uint64_t* const (&tabs)[4], size_t j, size_t q,
+                                             const Fr& fold, Fr (&acc)[3]) {
+  Fr x0, x1;
+  round_pair<kFold>(tabs[0], j, q, fold, x0, x1);
+  const Fr a0 = x0, a2 = fr_sub(fr_add(x0, x0), x1), da = fr_sub(x1, x0);
+  round_pair<kFold>(tabs[1], j, q, fold, x0, x1);
+  const Fr ab = fr_mul_call(a0, x0);
+  const Fr ab2 = fr_mul_call(a2, fr_sub(fr_add(x0, x0), x1));
+  const Fr dab = fr_mul_call(da, fr_sub(x1, x0));
+  round_pair<kFold>(tabs[2], j, q, fold, x0, x1);
+  const Fr t0 = fr_sub(ab, x0), t1 = fr_sub(ab2, fr_sub(fr_add(x0, x0), x1));
+  round_pair<kFold>(tabs[3], j, q, fold, x0, x1);
+  acc[0] = fr_add(acc[0], fr_mul_call(x0, t0));
+  acc[1] = fr_add(acc[1], fr_mul_call(fr_sub(fr_add(x0, x0), x1), t1));
+  acc[2] = fr_add(acc[2], fr_mul_call(fr_sub(x1, x0), dab));
+}
+
 }  // namespace pk
