@@ -136,11 +136,22 @@ int roots_reserve(size_t order, const uint64_t** out) {
 // Stage s of the pass (global stage t+s) pairs j0 = grp*2h + pos with
 // j0 + h (h = 2^(K-1-s)) and uses twiddle roots[(high << s) | grp].
 // ---------------------------------------------------------------------------
-template <int K>
+// Element g of the RS-encode layout (see NttSource).
+__device__ __forceinline__ Fr source_load(const NttSource& s, uint64_t g) {
+  const uint64_t x = g % s.chunk;
+  if (x < s.L * s.M) {
+    const uint64_t row = x / s.M, col = x - row * s.M;
+    return fr_load_ro(s.messages, col * s.L + row);
+  }
+  if (x - s.L * s.M < s.mask_len) return fr_load_ro(s.masks, x - s.L * s.M);
+  return fr_zero();
+}
+
+template <int K, bool kSrc>
 __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ data,
                                                       const uint64_t* __restrict__ roots,
                                                       uint64_t U, int log_u, int T, int log_t,
-                                                      int mode_b) {
+                                                      int mode_b, const NttSource src) {
   extern __shared__ uint4 sm[];
   constexpr int R = 1 << K;
   const int E = R * T;
@@ -165,9 +176,15 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
       g = (l0 >> log_u) * R * U + e;
       sidx = j * T + (hl << log_u) + u;
     }
-    const uint4* src = reinterpret_cast<const uint4*>(data + 4 * g);
-    sm[sidx] = src[0];      // low 16 bytes: plane 0
-    sm[E + sidx] = src[1];  // high 16 bytes: plane 1
+    if (kSrc) {
+      const Fr v = source_load(src, g);
+      sm[sidx] = make_uint4(v.v[0], v.v[1], v.v[2], v.v[3]);
+      sm[E + sidx] = make_uint4(v.v[4], v.v[5], v.v[6], v.v[7]);
+    } else {
+      const uint4* in = reinterpret_cast<const uint4*>(data + 4 * g);
+      sm[sidx] = in[0];      // low 16 bytes: plane 0
+      sm[E + sidx] = in[1];  // high 16 bytes: plane 1
+    }
   }
   __syncthreads();
   // ---- K radix-2 stages in shared memory ----
@@ -223,27 +240,29 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
   }
 }
 
-typedef void (*PassFn)(uint64_t*, const uint64_t*, uint64_t, int, int, int, int);
-static PassFn pass_fn(int k) {
+typedef void (*PassFn)(uint64_t*, const uint64_t*, uint64_t, int, int, int, int, const NttSource);
+template <bool kSrc>
+static PassFn pass_fn_t(int k) {
   switch (k) {
-    case 1: return ntt_pass_kernel<1>;
-    case 2: return ntt_pass_kernel<2>;
-    case 3: return ntt_pass_kernel<3>;
-    case 4: return ntt_pass_kernel<4>;
-    case 5: return ntt_pass_kernel<5>;
-    case 6: return ntt_pass_kernel<6>;
-    case 7: return ntt_pass_kernel<7>;
-    case 8: return ntt_pass_kernel<8>;
-    case 9: return ntt_pass_kernel<9>;
-    default: return ntt_pass_kernel<10>;
+    case 1: return ntt_pass_kernel<1, kSrc>;
+    case 2: return ntt_pass_kernel<2, kSrc>;
+    case 3: return ntt_pass_kernel<3, kSrc>;
+    case 4: return ntt_pass_kernel<4, kSrc>;
+    case 5: return ntt_pass_kernel<5, kSrc>;
+    case 6: return ntt_pass_kernel<6, kSrc>;
+    case 7: return ntt_pass_kernel<7, kSrc>;
+    case 8: return ntt_pass_kernel<8, kSrc>;
+    case 9: return ntt_pass_kernel<9, kSrc>;
+    default: return ntt_pass_kernel<10, kSrc>;
   }
 }
+static PassFn pass_fn(int k, bool src) { return src ? pass_fn_t<true>(k) : pass_fn_t<false>(k); }
 
 static inline uint64_t pow2_part(uint64_t x) { return x & (~x + 1); }
 
 // Run global stages [t_begin, t_end) of an N-point transform over M columns.
 int ntt_stages(uint64_t* data, size_t N, size_t M, int t_begin, int t_end, const uint64_t* roots,
-               cudaStream_t stream) {
+               cudaStream_t stream, const NttSource* src) {
   const int S = log2_exact(N);
   (void)S;
   const int kmax = 9;
@@ -275,11 +294,15 @@ int ntt_stages(uint64_t* data, size_t N, size_t M, int t_begin, int t_end, const
     if (threads < 32) threads = 32;
     size_t smem = 32 * E;
     uint64_t grid = num_lines / T;
-    PassFn fn = pass_fn(K);
+    const bool from_src = src != nullptr && pi == 0;
+    PassFn fn = pass_fn(K, from_src);
     if (smem > 48 * 1024) {
       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
-    fn<<<(unsigned)grid, threads, smem, stream>>>(data, roots, U, log_u, (int)T, log_t, mode_b);
+    NttSource s;
+    memset(&s, 0, sizeof s);
+    if (from_src) s = *src;
+    fn<<<(unsigned)grid, threads, smem, stream>>>(data, roots, U, log_u, (int)T, log_t, mode_b, s);
     PK_CHECK_LAUNCH("ntt_pass_kernel");
     t += K;
   }
@@ -319,6 +342,20 @@ int ntt_nr_device(uint64_t* values, size_t len, size_t codeword_size, size_t num
   size_t M = len / codeword_size;
   return ntt_stages(values, codeword_size, M, log2_exact(num_groups), log2_exact(codeword_size),
                     roots, stream);
+}
+
+int ntt_nr_from_source(uint64_t* out, size_t len, size_t codeword_size, size_t num_groups,
+                       const NttSource& src, cudaStream_t stream) {
+  int noop = 0;
+  int rc = ntt_validate(len, codeword_size, num_groups, &noop);
+  if (rc) return rc;
+  PK_REQUIRE(!noop, "no transform stage to read the source");
+  PK_REQUIRE(out != nullptr && aligned16(out), "null or unaligned output");
+  const uint64_t* roots = nullptr;
+  rc = roots_reserve(codeword_size, &roots);
+  if (rc) return rc;
+  return ntt_stages(out, codeword_size, len / codeword_size, log2_exact(num_groups),
+                    log2_exact(codeword_size), roots, stream, &src);
 }
 
 // ---------------------------------------------------------------------------

@@ -88,12 +88,22 @@ int rs_encode_device(const uint64_t* messages, size_t num_messages, size_t messa
   PK_REQUIRE(mask_len == 0 || masks != nullptr, "null masks pointer");
   PK_REQUIRE(aligned16(out) && aligned16(messages) && aligned16(masks),
              "device buffers must be 16-byte aligned");
+  if (codeword_length > 1 && num_cosets < codeword_length) {
+    // the transpose and coset replication are the first NTT pass's loads
+    NttSource src;
+    src.messages = messages;
+    src.masks = masks;
+    src.M = num_messages;
+    src.L = message_length;
+    src.mask_len = mask_len;
+    src.chunk = coset_size * num_messages;
+    return ntt_nr_from_source(out, total, codeword_length, num_cosets, src, stream);
+  }
   int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)sm_count() * 32);
   rs_gather_kernel<<<blocks, 256, 0, stream>>>(messages, num_messages, message_length, masks,
                                                mask_len, coset_size * num_messages, total, out);
   PK_CHECK_LAUNCH("rs_gather_kernel");
-  if (codeword_length <= 1) return PKG_OK;
-  return ntt_nr_device(out, total, codeword_length, num_cosets, stream);
+  return PKG_OK;
 }
 
 }  // namespace pk
