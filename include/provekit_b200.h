@@ -449,7 +449,7 @@ int pkg_eq_accumulate(uint64_t *w, size_t nv, const uint64_t *points, const uint
  *     pipe (the routines of the NTT and Skyscraper kernels); inputs < 2p.
  *   PKG_FR_FROM_MONT_F64: a*2^-256 mod p on the FP64 pipe; any 256-bit a.
  *   PKG_FR_MUL_INT / PKG_FR_SQR_INT: the same on the integer pipe; inputs < p.
- *   PKG_FR_FROM_MONT_INT: integer pipe; a < 2p.
+ *   PKG_FR_FROM_MONT_INT: the same on the integer pipe (REDC alone); any 256-bit a.
  * b is read only by the two products (may be NULL otherwise).  The reference's
  * scalar_mul/scalar_sqr return values in [0, 2^256 - 2p) with the same
  * residue; only the residue is part of the contract. */

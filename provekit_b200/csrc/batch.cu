@@ -201,9 +201,9 @@ __global__ void batch_leaves_kernel(const RangeDesc* __restrict__ rd,
        o += (uint64_t)gridDim.x * blockDim.x) {
     const RangeDesc d = rd[find_desc(begins, nd, o)];
     const uint64_t i = o - d.begin;
-    Fr acc = fr_from_mont_f64(fr_load_ro(d.in, i * kMsgs));
+    Fr acc = fr_from_mont(fr_load_ro(d.in, i * kMsgs));
 #pragma unroll 1
-    for (int k = 1; k < kMsgs; k++) acc = sky_compress(acc, fr_from_mont_f64(fr_load_ro(d.in, i * kMsgs + k)));
+    for (int k = 1; k < kMsgs; k++) acc = sky_compress(acc, fr_from_mont(fr_load_ro(d.in, i * kMsgs + k)));
     fr_store(reinterpret_cast<uint64_t*>(d.out), i, acc);
   }
 }

@@ -300,10 +300,27 @@ __device__ __forceinline__ Fr fr_to_mont(const Fr& a) {
 }
 
 // Montgomery -> canonical: a * 1 * R^-1
+// Montgomery -> canonical, a * 2^-256 mod p, for any 256-bit a: the
+// word-by-word Montgomery reduction alone (REDC, 8 x (1 + 16) multiply-adds
+// on the integer pipe, no product); t < 2^256 + p 2^256 keeps 9 words, the
+// result is < p + 1 before the one conditional subtraction.
 __device__ __forceinline__ Fr fr_from_mont(const Fr& a) {
-  Fr one = fr_zero();
-  one.v[0] = 1;
-  return fr_mul(a, one);
+  uint32_t t[9];
+#pragma unroll
+  for (int i = 0; i < 8; i++) t[i] = a.v[i];
+  t[8] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint32_t m = t[0] * PK_MU;
+    PK_ROW_P(t, m);
+#pragma unroll
+    for (int j = 0; j < 8; j++) t[j] = t[j + 1];
+    t[8] = 0;
+  }
+  Fr r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.v[i] = t[i];
+  return fr_reduce_once(r);
 }
 
 __device__ __forceinline__ bool fr_eq(const Fr& a, const Fr& b) {

@@ -75,11 +75,11 @@ __global__ void __launch_bounds__(128, 7) leaf_fold_fr_kernel(const uint64_t* __
        i += (size_t)gridDim.x * blockDim.x) {
     const size_t base = i * fr_per_leaf;
     Fr acc = fr_load_ro(cw, base);
-    if (kCanonical) acc = fr_from_mont_f64(acc);
+    if (kCanonical) acc = fr_from_mont(acc);
 #pragma unroll 1
     for (size_t k = 1; k < fr_per_leaf; k++) {
       Fr e = fr_load_ro(cw, base + k);
-      if (kCanonical) e = fr_from_mont_f64(e);
+      if (kCanonical) e = fr_from_mont(e);
       acc = sky_compress(acc, e);
     }
     store_raw(out + 32 * i, acc);

@@ -69,7 +69,7 @@ def test_sqr(pipe, bound):
     assert got == [x * x * RINV % P for x in a]
 
 
-@pytest.mark.parametrize("pipe,bound", [("fp64", 1 << 256), ("int", 2 * P)])
+@pytest.mark.parametrize("pipe,bound", [("fp64", 1 << 256), ("int", 1 << 256)])
 def test_from_mont(pipe, bound):
     from provekit_b200.field import fr_op
     a, _ = operands(bound, 20000, 13)
