@@ -52,7 +52,8 @@ def parse_args():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plugin-e2e", action="store_true")
-    p.add_argument("--workload", choices=["commit", "prove", "batched", "served", "ntt", "whir_ops"],
+    p.add_argument("--workload", choices=["commit", "prove", "batched", "served", "ntt", "whir_ops",
+                                          "poseidon2"],
                    default="commit",
                    help="commit (default, the headline line): WHIR commit of 2^20 coefficients; "
                         "prove: Spartan prove core of a 2^20-constraint R1CS; batched: 256 uneven "
@@ -805,11 +806,27 @@ def run_ntt(a):
                 evs[i][1].record(stream)
         stream.synchronize()
         ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+        # intt_rn round trip on the transform's output (ntt/src/ntt.rs:326-348)
+        evi = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
+        ok = True
+        with torch.cuda.stream(stream):
+            for i in range(a.steps):
+                d.copy_(src)
+                check(L.pkg_ntt_nr(d.data_ptr(), n, n, 1, stream.cuda_stream))
+                flush.zero_()
+                evi[i][0].record(stream)
+                check(L.pkg_intt_rn(d.data_ptr(), n, stream.cuda_stream))
+                evi[i][1].record(stream)
+            ok = bool(torch.equal(d, src))
+        stream.synchronize()
+        ms_inv = statistics.mean(e[0].elapsed_time(e[1]) for e in evi)
         products = (n // 2) * logn
         out[logn] = {"ms": ms, "fr_per_s": n / (ms * 1e-3), "gmont_per_s": products / (ms * 1e-3) / 1e9,
                      "roofline_frac": products / (ms * 1e-3) / f64_peak,
                      "int_pipe_frac": products / (ms * 1e-3) / mont_peak,
-                     "hbm_gbs": 2 * 32 * n * ((logn + 8) // 9) / (ms * 1e-3) / 1e9}
+                     "hbm_gbs": 2 * 32 * n * ((logn + 8) // 9) / (ms * 1e-3) / 1e9,
+                     "intt_rn_ms": ms_inv, "intt_fr_per_s": n / (ms_inv * 1e-3),
+                     "round_trip_ok": ok}
     line = {"metric": "BN254 Fr ntt_nr throughput, 2^24 (roofline target) and 2^16 (config 1)",
             "value": out[24]["fr_per_s"], "unit": "Fr/s", "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": out[24]["ms"], "higher_is_better": True,
@@ -825,7 +842,7 @@ def run_ntt(a):
                                         f"(pkg_measure_dfma_rate) / {F64_PER_MUL}",
                          "int_pipe_alt": {"peak_gmont_per_s": mont_peak / 1e9,
                                           "frac": out[24]["int_pipe_frac"]}},
-            "ntt_2p16": out[16]}
+            "ntt_2p24": out[24], "ntt_2p16": out[16]}
     print(json.dumps(line), flush=True)
 
 
@@ -916,6 +933,71 @@ def run_whir_ops(a):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Poseidon2 (t = 4, rf = 8, rp = 56) permutations and hashes over 2^22 states.
+# ---------------------------------------------------------------------------
+def run_poseidon2(a):
+    import numpy as np
+    import torch
+
+    from provekit_b200 import _lib
+    from provekit_b200._lib import check
+    from provekit_b200.poseidon2 import poseidon2_hash_many, poseidon2_permutation_many
+
+    L = _lib.lib()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    dfma = ctypes.c_double(0)
+    check(L.pkg_measure_dfma_rate(ctypes.byref(dfma)))
+    n = 1 << 22
+    h = np.zeros((4 * n, 4), np.uint64)
+    check(L.pkg_sample_fr(17, 4 * n, h.ctypes.data, 1))
+    src = torch.from_numpy(h.view(np.int64)).cuda()
+    st = torch.empty_like(src)
+    out = torch.empty(((4 * n) // 3, 4), dtype=torch.int64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            for _ in range(a.warmup):
+                fn()
+            evs = []
+            for _ in range(a.steps):
+                st.copy_(src)
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                evs.append((e0, e1))
+        stream.synchronize()
+        return statistics.mean(x.elapsed_time(y) for x, y in evs)
+
+    ms_perm = timed(lambda: poseidon2_permutation_many(st, stream=stream))
+    ms_hash = timed(lambda: poseidon2_hash_many(src[: 3 * ((4 * n) // 3)], 3, out=out, stream=stream))
+    # products per permutation: full rounds 8 x 4 s-boxes (x^5: 2 squares + 1
+    # product), partial rounds 56 x 1 s-box, plus the internal layer's 4
+    # diagonal products in each of the 56 partial rounds
+    prod_perm = 8 * 4 * 3 + 56 * 3 + 56 * 4
+    fp64 = prod_perm * F64_PER_MUL
+    line = {"metric": "Poseidon2 (BN254, t = 4) permutations/s over 2^22 states",
+            "value": n / (ms_perm * 1e-3), "unit": "permutations/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_perm,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32 (BN254 Fr, 8x32-bit limbs)", "data": "synthetic (ChaCha20-seeded Fr)",
+            "config": {"workload": "poseidon2", "states": n, "l2": "flushed between steps"},
+            "roofline": {"kernel": "poseidon2 permutation kernel", "bound": "fp64",
+                         "achieved": n * fp64 / (ms_perm * 1e-3) / 1e12,
+                         "peak": dfma.value / 1e12, "unit": "T fp64-op/s",
+                         "frac": n * fp64 / (ms_perm * 1e-3) / dfma.value,
+                         "algorithmic": f"{prod_perm} Fr products per permutation at "
+                                        f"{F64_PER_MUL} binary64 instructions (squares counted as "
+                                        "products: an upper bound on the work)"},
+            "hash_rate_per_s": ((4 * n) // 3) / (ms_hash * 1e-3),
+            "hash_note": "poseidon2_hash of 3-element inputs (one permutation each)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse_args()
     if a.impl == "reference":
@@ -930,6 +1012,8 @@ def main():
         run_ntt(a)
     elif a.workload == "whir_ops":
         run_whir_ops(a)
+    elif a.workload == "poseidon2":
+        run_poseidon2(a)
     else:
         run_b200(a)
 
