@@ -1135,7 +1135,7 @@ int pko_whir_fold_coeffs(const uint64_t *coeffs, size_t n, unsigned k, const uin
     return 0;
 }
 
-/* computeFold (whir_utilities.go:176-182): MultivarPoly of each row. */
+/* computeFold (whir_utilities.go:182-188): MultivarPoly of each row. */
 int pko_whir_fold_rows(const uint64_t *rows, size_t nrows, unsigned k, const uint64_t *alpha,
                        uint64_t *out) {
     if (k > 16) return -1;
