@@ -37,7 +37,7 @@ F64_PER_FROM_MONT = 11 + 140 + 69      # 220
 # dram__bytes_read.sum + dram__bytes_write.sum of one leaf_fold_fr_kernel launch
 # from an ncu capture of this workload (profiles/leaf_fold_fr_kernel_whir_commit_2p20.md),
 # keyed by (log2 coeffs, folding factor, log inv rate).
-LEAF_TRAFFIC_BYTES = {(20, 4, 2): 134.846720e6 + 6.334208e6}
+LEAF_TRAFFIC_BYTES = {(20, 4, 2): 134.264064e6 + 6.855168e6}
 
 
 def parse_args():
