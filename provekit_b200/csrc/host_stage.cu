@@ -7,6 +7,8 @@
 #include <thread>
 #include <vector>
 
+#include <unistd.h>
+
 #include "pk_common.cuh"
 
 namespace pk {
@@ -17,13 +19,14 @@ namespace {
 // purpose: its threads park on a condition variable and end with the process.
 class CopyPool {
  public:
-  CopyPool() {
+  CopyPool() : owner_(getpid()) {
     unsigned hw = std::thread::hardware_concurrency();
     nthreads_ = (int)std::min(8u, hw > 2 ? hw / 2 : 1u);
     for (int i = 0; i < nthreads_; i++) std::thread([this, i] { worker(i); }).detach();
   }
   void run(void* dst, const void* src, size_t bytes) {
-    if (bytes < (size_t(1) << 20) || nthreads_ < 2) {
+    // A forked child has none of the parent's threads: copy on the caller.
+    if (bytes < (size_t(1) << 20) || nthreads_ < 2 || getpid() != owner_) {
       std::memcpy(dst, src, bytes);
       return;
     }
@@ -56,6 +59,7 @@ class CopyPool {
       if (--pending_ == 0) done_cv_.notify_one();
     }
   }
+  const pid_t owner_;
   int nthreads_ = 0;
   std::mutex run_mu_, mu_;
   std::condition_variable cv_, done_cv_;

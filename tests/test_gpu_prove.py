@@ -35,3 +35,21 @@ def test_spartan_prove_matches_oracle(log_nc, log_ni, ff):
     got = spartan_prove(h.to_device(), blinding_seed=5, transcript_domain=9, folding_factor=ff,
                         log_inv_rate=2)
     assert_same(got, exp)
+
+
+def test_stage_timers_and_memory_trim_keep_results():
+    """pkg_last_prove_stages reports the calling thread's last prove; returning
+    the library pool's memory (pkg_trim_memory) between proves changes no
+    output."""
+    import ctypes
+    from provekit_b200._lib import check, lib
+    from provekit_b200.prover import HostR1CS, spartan_prove
+    h = HostR1CS(77, 1 << 14, 1 << 12)
+    d = h.to_device()
+    first = spartan_prove(d, blinding_seed=3, transcript_domain=4)
+    stages = (ctypes.c_double * 5)()
+    check(lib().pkg_last_prove_stages(stages))
+    assert all(v > 0 for v in stages), list(stages)
+    check(lib().pkg_trim_memory(0))
+    again = spartan_prove(d, blinding_seed=3, transcript_domain=4)
+    assert_same(again, first)
