@@ -13,6 +13,10 @@ The vectors are read as text from the reference's Rust test modules:
   vectors).
 * Poseidon2: ``poseidon2/src/permutation.rs`` ``smoke_test`` and
   ``poseidon2/src/hash.rs`` single/two-element hashes.
+* The field's two-adic root of unity: the square-root constants of
+  ``noir-examples/babyjubjub/src/hash_to_curve.nr`` (Z = 5, C1 = 28 = the
+  two-adicity, C5 = Z^((p-1)/2^28)), i.e. the 2^28-th root of unity that
+  ark-bn254's ``Fr::get_root_of_unity`` raises to the NTT's order.
 
 Run from the repository root:  python tests/golden/extract_reference_kats.py
 (the reference checkout is only needed to regenerate the JSON; the tests read
@@ -116,10 +120,22 @@ def poseidon2_kats():
     return out
 
 
+def root_of_unity_kats():
+    path = "noir-examples/babyjubjub/src/hash_to_curve.nr"
+    src = open(os.path.join(REF, path)).read()
+    consts = {}
+    for name in ("Z", "C1", "C5"):
+        m = re.search(r"global\s+" + name + r"\s*:\s*\w+\s*=\s*(\d+)\s*;", src)
+        consts[name] = m.group(1)
+    return {"source": path, "generator": consts["Z"], "two_adicity": consts["C1"],
+            "two_adic_root": consts["C5"]}
+
+
 def main():
     if not os.path.isdir(REF):
         sys.exit(f"reference checkout not found at {REF}")
-    kats = {"skyscraper": skyscraper_kats(), "sumcheck": sumcheck_kats(), "poseidon2": poseidon2_kats()}
+    kats = {"skyscraper": skyscraper_kats(), "sumcheck": sumcheck_kats(), "poseidon2": poseidon2_kats(),
+            "root_of_unity": root_of_unity_kats()}
     with open(OUT, "w") as f:
         json.dump(kats, f, indent=1, sort_keys=True)
         f.write("\n")

@@ -52,7 +52,7 @@ def test_rs_host_helpers_match_oracle(L):
     rs = RSFr()
     assert rs.next_order(0) == 1 and rs.next_order(5) == 8 and rs.next_order(1 << 28) == 1 << 28
     assert rs.next_order((1 << 28) + 1) is None
-    for n in (1, 2, 1024, 1 << 20):
+    for n in (1, 2, 1024, 1 << 20, 1 << 28):
         g = rs.generator(n)
         assert unpack(g.reshape(1, 4))[0] == root_of_unity(n)
     for cw in (1, 2, 16, 64):

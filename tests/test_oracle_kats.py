@@ -2,6 +2,7 @@
 (tests/golden/reference_kats.json, extracted from the reference test modules by
 tests/golden/extract_reference_kats.py) and against independent plain-Python
 big-int restatements.  CPU only."""
+import ctypes
 import json
 import os
 import random
@@ -339,3 +340,23 @@ def test_poseidon2_hash_kat(name):
     out = np.zeros(4, np.uint64)
     O.lib().pko_poseidon2_hash(O.p64(out), O.p64(inp), inp.shape[0])
     assert unpack(out.reshape(1, 4))[0] == int(k["expected"])
+
+
+# --------------------------------------------------------------------------
+# The NTT's root of unity, pinned to the reference's own constant
+# (noir-examples/babyjubjub/src/hash_to_curve.nr: Z = 5, C1 = 28, C5 =
+# Z^((p-1)/2^28), the 2^28-th root of unity that ark-bn254's
+# Fr::get_root_of_unity squares down to each NTT order).
+# --------------------------------------------------------------------------
+def test_two_adic_root_matches_the_reference_constant():
+    k = KATS["root_of_unity"]
+    c5, z, c1 = int(k["two_adic_root"]), int(k["generator"]), int(k["two_adicity"])
+    assert c1 == 28 and (P - 1) % (1 << c1) == 0 and ((P - 1) >> c1) % 2 == 1
+    assert c5 == pow(z, (P - 1) >> c1, P)
+    assert pow(c5, 1 << 27, P) == P - 1          # order exactly 2^28
+    assert root_of_unity(1 << 28) == c5            # the tests' helper
+    out = np.zeros(4, np.uint64)
+    O.lib().pko_fr_root_of_unity.argtypes = [O._u64p, ctypes.c_uint64]
+    for logn in (28, 24, 16, 1):
+        O.lib().pko_fr_root_of_unity(O.p64(out), 1 << logn)
+        assert unpack(out.reshape(1, 4))[0] == pow(c5, 1 << (28 - logn), P)
