@@ -33,7 +33,6 @@ IMAD_PER_MONT = 264  # mad.lo/madc.hi/mul.lo per 8x32 CIOS product (fr.cuh: 8 x 
 # step plus normalisation (69).
 F64_PER_MUL = 22 + 121 + 140 + 69      # 352
 F64_PER_SQR = 11 + 66 + 10 + 140 + 69  # 296
-F64_PER_FROM_MONT = 11 + 140 + 69      # 220
 # dram__bytes_read.sum + dram__bytes_write.sum of one leaf_fold_fr_kernel launch
 # from an ncu capture of this workload (profiles/leaf_fold_fr_kernel_whir_commit_2p20.md),
 # keyed by (log2 coeffs, folding factor, log inv rate).

@@ -2,7 +2,6 @@
 device execution (pkg_server_* in the C header)."""
 import ctypes
 
-import numpy as np
 
 from ._lib import check, lib
 from .prover import SpartanProofC

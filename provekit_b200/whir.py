@@ -3,8 +3,6 @@ vendored with the reference; its arithmetic here follows the reference's Go
 WHIR verifier, recursive-verifier/app/).  Tensors are (n, 4) int64 CUDA
 tensors of Montgomery-form Fr limbs; small per-round values are (k, 4)
 uint64 host arrays."""
-import ctypes
-
 import numpy as np
 import torch
 
@@ -95,5 +93,3 @@ def eq_accumulate(w, nv: int, points, coeffs, stream=None):
                                   stream_handle(stream)))
     return w
 
-
-_ = ctypes

@@ -8,7 +8,7 @@ import re
 import numpy as np
 import pytest
 
-from fieldutil import P, R, from_limbs, root_of_unity, unpack
+from fieldutil import root_of_unity, unpack
 import oracle_lib as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

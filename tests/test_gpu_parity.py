@@ -6,7 +6,7 @@ import pytest
 import torch
 
 import oracle_lib as O
-from fieldutil import P, R, from_limbs, pack, to_limbs, unpack
+from fieldutil import P, to_limbs
 
 pytestmark = pytest.mark.gpu
 

@@ -10,7 +10,6 @@ import pytest
 import torch
 
 import oracle_lib as O
-from fieldutil import P, pack, unpack
 
 pytestmark = pytest.mark.gpu
 

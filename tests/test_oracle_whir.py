@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import oracle_lib as O
-from fieldutil import P, from_limbs, pack, to_limbs, unpack
+from fieldutil import P, pack, to_limbs, unpack
 
 INV2 = pow(2, P - 2, P)
 
