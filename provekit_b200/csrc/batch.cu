@@ -39,6 +39,12 @@ struct PassDesc {  // one job's share of one grouped NTT pass
   uint64_t U;
   uint64_t cta_begin;
   uint32_t log_u, K, T, log_t, mode_b, pad;
+  // Where a job's first pass reads its input: 0 = data itself, 1 = src (the
+  // coefficients, same indices), 2 = src through the RS-encode layout of
+  // kMsgs messages of src_n / kMsgs (the transpose and 4-coset replication).
+  const uint64_t* src;
+  uint64_t src_n;
+  uint32_t src_kind, pad2;
 };
 
 struct RangeDesc {  // job j owns [begin, begin + count) of a grouped launch
@@ -120,9 +126,17 @@ __global__ void __launch_bounds__(512) batch_ntt_pass_kernel(const PassDesc* __r
       g = (l0 >> log_u) * R * U + e;
       sidx = j * T + (hl << log_u) + u;
     }
-    const uint4* src = reinterpret_cast<const uint4*>(data + 4 * g);
-    sm[sidx] = src[0];      // low 16 bytes: plane 0
-    sm[E + sidx] = src[1];  // high 16 bytes: plane 1
+    const uint4* in;
+    if (d.src_kind == 0) {
+      in = reinterpret_cast<const uint4*>(data + 4 * g);
+    } else if (d.src_kind == 1) {
+      in = reinterpret_cast<const uint4*>(d.src + 4 * g);
+    } else {  // row x of each n-element coset block holds messages[x % 8][x / 8]
+      const uint64_t x = g & (d.src_n - 1);
+      in = reinterpret_cast<const uint4*>(d.src + 4 * ((x % kMsgs) * (d.src_n / kMsgs) + x / kMsgs));
+    }
+    sm[sidx] = in[0];      // low 16 bytes: plane 0
+    sm[E + sidx] = in[1];  // high 16 bytes: plane 1
   }
   __syncthreads();
   for (int s = 0; s < K; s++) {
@@ -173,23 +187,6 @@ __global__ void batch_copy_kernel(const RangeDesc* __restrict__ rd, const uint64
     const RangeDesc d = rd[find_desc(begins, nd, o)];
     const uint64_t i = o - d.begin;
     fr_store(reinterpret_cast<uint64_t*>(d.out), i, fr_load_ro(d.in, i));
-  }
-}
-
-// RS gather (rs_gather_kernel for 8 messages of L = n/8, no masks, coset
-// size L, 4 cosets): cw[o] = coeffs[(x % 8) * L + x / 8], x = o mod n.
-__global__ void batch_rs_gather_kernel(const RangeDesc* __restrict__ rd,
-                                       const uint64_t* __restrict__ begins, uint32_t nd,
-                                       uint64_t total) {
-  for (uint64_t o = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; o < total;
-       o += (uint64_t)gridDim.x * blockDim.x) {
-    const RangeDesc d = rd[find_desc(begins, nd, o)];
-    const uint64_t i = o - d.begin;
-    const uint64_t n = d.count / 4;  // codeword = 4n Fr
-    const uint64_t L = n / kMsgs;
-    const uint64_t x = i & (n - 1);
-    const uint64_t row = x / kMsgs, col = x % kMsgs;
-    fr_store(reinterpret_cast<uint64_t*>(d.out), i, fr_load_ro(d.in, col * L + row));
   }
 }
 
@@ -421,7 +418,7 @@ struct pkg_batch {
   int kmax = 9, log_elems = 9;
   // plan
   std::vector<pk::PassLaunch> passes;
-  pk::Grouped copy_in, gather, leaves, eq_half, eq_comb, copy_sc;
+  pk::Grouped leaves, eq_half, eq_comb, copy_sc;
   std::vector<pk::Grouped> levels, rounds;
   std::vector<uint64_t> round_ctas;
   uint32_t max_m0 = 0;
@@ -434,7 +431,8 @@ namespace pk {
 static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 static void plan_passes(size_t N, size_t M, int t_begin, int t_end, int kmax, int log_elems,
-                        uint64_t* data, std::vector<std::vector<PassDesc>>& out) {
+                        uint64_t* data, const uint64_t* src, uint64_t src_n, uint32_t src_kind,
+                        std::vector<std::vector<PassDesc>>& out) {
   int total = t_end - t_begin;
   if (total <= 0) return;
   int np = (total + kmax - 1) / kmax;
@@ -465,6 +463,10 @@ static void plan_passes(size_t N, size_t M, int t_begin, int t_end, int kmax, in
     d.log_t = (uint32_t)log2_exact(T);
     d.mode_b = mode_b;
     d.pad = 0;
+    d.src = pi == 0 ? src : nullptr;
+    d.src_n = src_n;
+    d.src_kind = pi == 0 ? src_kind : 0;
+    d.pad2 = 0;
     if ((int)out.size() <= pi) out.resize(pi + 1);
     out[pi].push_back(d);
     t += K;
@@ -499,18 +501,19 @@ static int batch_plan(pkg_batch* b) {
   std::vector<std::vector<PassDesc>> pass_descs;
   for (size_t j = 0; j < nj; j++) {
     const JobDev& jb = b->jobs[j];
-    plan_passes(jb.n, 1, 0, (int)jb.log_n, b->kmax, b->log_elems, jb.ntt, pass_descs);
+    // first passes read the coefficients directly: the plain NTT's copy and
+    // the RS transpose + coset replication are their loads
+    plan_passes(jb.n, 1, 0, (int)jb.log_n, b->kmax, b->log_elems, jb.ntt, jb.coeffs, jb.n, 1,
+                pass_descs);
     plan_passes(jb.cw_rows, kMsgs, kLogInvRate, log2_exact(jb.cw_rows), b->kmax, b->log_elems,
-                jb.cw, pass_descs);
+                jb.cw, jb.coeffs, jb.n, 2, pass_descs);
   }
   std::vector<std::vector<RangeDesc>> lv, rd_rounds;
-  std::vector<RangeDesc> cp, ga, lf, eh, ec, csc;
+  std::vector<RangeDesc> lf, eh, ec, csc;
   uint32_t max_m0 = 0;
   for (size_t j = 0; j < nj; j++) {
     const JobDev& jb = b->jobs[j];
     const uint32_t jj = (uint32_t)j;
-    cp.push_back({0, jb.n, jb.coeffs, reinterpret_cast<uint8_t*>(jb.ntt), jj, 0});
-    ga.push_back({0, 4 * jb.n, jb.coeffs, reinterpret_cast<uint8_t*>(jb.cw), jj, 0});
     lf.push_back({0, jb.cw_rows, jb.cw, jb.layers, jj, 0});
     size_t nodes = jb.cw_rows, off = 0;
     for (int l = 0; nodes > 1; l++) {
@@ -547,7 +550,7 @@ static int batch_plan(pkg_batch* b) {
   size_t bytes = 0;
   auto grp = [](size_t n) { return align256(sizeof(RangeDesc) * std::max<size_t>(n, 1)) + align256(8 * std::max<size_t>(n, 1)); };
   for (auto& p : pass_descs) bytes += align256(sizeof(PassDesc) * p.size()) + align256(8 * p.size());
-  bytes += grp(cp.size()) + grp(ga.size()) + grp(lf.size()) + grp(eh.size()) + grp(ec.size()) + grp(csc.size());
+  bytes += grp(lf.size()) + grp(eh.size()) + grp(ec.size()) + grp(csc.size());
   for (auto& l : lv) bytes += grp(l.size());
   for (auto& r : rd_rounds) bytes += grp(r.size());
   if (b->tables) cudaFree(b->tables);
@@ -581,8 +584,6 @@ static int batch_plan(pkg_batch* b) {
     b->passes.push_back(pl);
   }
   int rc;
-  if ((rc = upload_grouped(b, cp, b->copy_in, cur))) return rc;
-  if ((rc = upload_grouped(b, ga, b->gather, cur))) return rc;
   if ((rc = upload_grouped(b, lf, b->leaves, cur))) return rc;
   if ((rc = upload_grouped(b, eh, b->eq_half, cur))) return rc;
   if ((rc = upload_grouped(b, ec, b->eq_comb, cur))) return rc;
@@ -606,12 +607,6 @@ static int batch_enqueue(pkg_batch* b, cudaStream_t s) {
   const uint32_t nj = (uint32_t)b->jobs.size();
   PK_CUDA(cudaMemcpyAsync(b->d_state, b->d_state_init, sizeof(ScState) * nj,
                           cudaMemcpyDeviceToDevice, s));
-  batch_copy_kernel<<<ew_blocks(b->copy_in.total), 256, 0, s>>>(b->copy_in.d_desc, b->copy_in.d_begin,
-                                                                b->copy_in.n, b->copy_in.total);
-  PK_CHECK_LAUNCH("batch_copy_kernel");
-  batch_rs_gather_kernel<<<ew_blocks(b->gather.total), 256, 0, s>>>(
-      b->gather.d_desc, b->gather.d_begin, b->gather.n, b->gather.total);
-  PK_CHECK_LAUNCH("batch_rs_gather_kernel");
   for (auto& p : b->passes) {
     if (p.smem > 48 * 1024)
       PK_CUDA(cudaFuncSetAttribute(batch_ntt_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
