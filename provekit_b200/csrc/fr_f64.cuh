@@ -124,6 +124,23 @@ __device__ __forceinline__ Fr fr_mul_f64(const Fr& a, const Fr& b) {
   return f64::tail16(T);
 }
 
+// fr_mul_f64 with the first operand already in digit form (A: the 11 digits
+// f64::digits produced, e.g. a twiddle converted once and shared).
+__device__ __forceinline__ Fr fr_mul_f64_digits(const double* A, const Fr& b) {
+  double B[11], T[11];
+  f64::digits(b, B);
+#pragma unroll
+  for (int j = 0; j < 11; j++) T[j] = 0.0;
+#pragma unroll
+  for (int i = 0; i < 11; i++) {
+    const double ai = A[i];
+#pragma unroll
+    for (int j = 0; j < 11; j++) T[j] = fma(ai, B[j], T[j]);
+    if (i < 10) f64::step24(T);
+  }
+  return f64::tail16(T);
+}
+
 // a^2 * 2^-256 mod p for a < 2p; result < p (same value as fr_sqr).  The 55
 // cross products are taken once with a doubled operand (2 a_i < 2^25, so a
 // product stays below 2^49 and a column below 2^53 as above).

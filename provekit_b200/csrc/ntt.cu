@@ -147,14 +147,22 @@ __device__ __forceinline__ Fr source_load(const NttSource& s, uint64_t g) {
   return fr_zero();
 }
 
-template <int K, bool kSrc>
+// kModeB selects mode B at compile time.  In mode A every line of the CTA
+// shares `high`, so stage s needs only the 2^s twiddles roots[(high << s) |
+// grp]; they are converted to FP64 digits once per CTA into shared memory
+// after the data tile (double-buffered across stages, 2 x 2^(K-1) x 11
+// doubles) instead of once per butterfly.
+template <int K, bool kSrc, bool kModeB>
 __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ data,
                                                       const uint64_t* __restrict__ roots,
                                                       uint64_t U, int log_u, int T, int log_t,
-                                                      int mode_b, const NttSource src) {
+                                                      int mode_b_unused, const NttSource src) {
   extern __shared__ uint4 sm[];
   constexpr int R = 1 << K;
+  constexpr bool mode_b = kModeB;
   const int E = R * T;
+  double* tw = reinterpret_cast<double*>(sm + 2 * E);
+  constexpr int kTw = (R / 2) * 11;
   const uint64_t l0 = (uint64_t)blockIdx.x * T;
   uint64_t high_a = 0, u0 = 0;
   if (!mode_b) {
@@ -186,6 +194,7 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
       sm[E + sidx] = in[1];  // high 16 bytes: plane 1
     }
   }
+  if (!kModeB && threadIdx.x == 0) f64::digits(fr_load_ro(roots, high_a), tw);  // stage 0
   __syncthreads();
   // ---- K radix-2 stages in shared memory ----
 #pragma unroll 1
@@ -198,8 +207,6 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
       int pos = p & ((1 << log_h) - 1);
       int j0 = (grp << (log_h + 1)) + pos;
       int j1 = j0 + (1 << log_h);
-      uint64_t high = mode_b ? ((l0 + ll) >> log_u) : high_a;
-      Fr w = fr_load_ro(roots, (high << s) | (uint64_t)grp);
       int i0 = j0 * T + ll, i1 = j1 * T + ll;
       Fr x0, x1;
       uint4 a = sm[i0], bb = sm[E + i0];
@@ -209,13 +216,27 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
       bb = sm[E + i1];
       x1.v[0] = a.x; x1.v[1] = a.y; x1.v[2] = a.z; x1.v[3] = a.w;
       x1.v[4] = bb.x; x1.v[5] = bb.y; x1.v[6] = bb.z; x1.v[7] = bb.w;
-      Fr m = fr_mul_f64(w, x1);
+      Fr m;
+      if (kModeB) {
+        const uint64_t high = (l0 + ll) >> log_u;
+        m = fr_mul_f64(fr_load_ro(roots, (high << s) | (uint64_t)grp), x1);
+      } else {
+        m = fr_mul_f64_digits(tw + (s & 1) * kTw + 11 * grp, x1);
+      }
       Fr y0 = fr_add(x0, m);
       Fr y1 = fr_sub(x0, m);
       sm[i0] = make_uint4(y0.v[0], y0.v[1], y0.v[2], y0.v[3]);
       sm[E + i0] = make_uint4(y0.v[4], y0.v[5], y0.v[6], y0.v[7]);
       sm[i1] = make_uint4(y1.v[0], y1.v[1], y1.v[2], y1.v[3]);
       sm[E + i1] = make_uint4(y1.v[4], y1.v[5], y1.v[6], y1.v[7]);
+    }
+    // next stage's twiddles into the other buffer: no thread reads it before
+    // the barrier below, and its previous readers finished before the last one
+    if (!kModeB && s + 1 < K) {
+#pragma unroll 1
+      for (int g = threadIdx.x; g < (2 << s); g += blockDim.x)
+        f64::digits(fr_load_ro(roots, (high_a << (s + 1)) | (uint64_t)g),
+                    tw + ((s + 1) & 1) * kTw + 11 * g);
     }
     __syncthreads();
   }
@@ -241,22 +262,24 @@ __global__ void __launch_bounds__(512) ntt_pass_kernel(uint64_t* __restrict__ da
 }
 
 typedef void (*PassFn)(uint64_t*, const uint64_t*, uint64_t, int, int, int, int, const NttSource);
-template <bool kSrc>
+template <bool kSrc, bool kModeB>
 static PassFn pass_fn_t(int k) {
   switch (k) {
-    case 1: return ntt_pass_kernel<1, kSrc>;
-    case 2: return ntt_pass_kernel<2, kSrc>;
-    case 3: return ntt_pass_kernel<3, kSrc>;
-    case 4: return ntt_pass_kernel<4, kSrc>;
-    case 5: return ntt_pass_kernel<5, kSrc>;
-    case 6: return ntt_pass_kernel<6, kSrc>;
-    case 7: return ntt_pass_kernel<7, kSrc>;
-    case 8: return ntt_pass_kernel<8, kSrc>;
-    case 9: return ntt_pass_kernel<9, kSrc>;
-    default: return ntt_pass_kernel<10, kSrc>;
+    case 1: return ntt_pass_kernel<1, kSrc, kModeB>;
+    case 2: return ntt_pass_kernel<2, kSrc, kModeB>;
+    case 3: return ntt_pass_kernel<3, kSrc, kModeB>;
+    case 4: return ntt_pass_kernel<4, kSrc, kModeB>;
+    case 5: return ntt_pass_kernel<5, kSrc, kModeB>;
+    case 6: return ntt_pass_kernel<6, kSrc, kModeB>;
+    case 7: return ntt_pass_kernel<7, kSrc, kModeB>;
+    case 8: return ntt_pass_kernel<8, kSrc, kModeB>;
+    default: return ntt_pass_kernel<9, kSrc, kModeB>;
   }
 }
-static PassFn pass_fn(int k, bool src) { return src ? pass_fn_t<true>(k) : pass_fn_t<false>(k); }
+static PassFn pass_fn(int k, bool src, bool mode_b) {
+  if (src) return mode_b ? pass_fn_t<true, true>(k) : pass_fn_t<true, false>(k);
+  return mode_b ? pass_fn_t<false, true>(k) : pass_fn_t<false, false>(k);
+}
 
 static inline uint64_t pow2_part(uint64_t x) { return x & (~x + 1); }
 
@@ -292,10 +315,10 @@ int ntt_stages(uint64_t* data, size_t N, size_t M, int t_begin, int t_end, const
     uint64_t E = (uint64_t(1) << K) * T;
     int threads = (int)std::min<uint64_t>(E / 2, 512);
     if (threads < 32) threads = 32;
-    size_t smem = 32 * E;
+    size_t smem = 32 * E + (mode_b ? 0 : sizeof(double) * 2 * 11 * (size_t(1) << (K - 1)));
     uint64_t grid = num_lines / T;
     const bool from_src = src != nullptr && pi == 0;
-    PassFn fn = pass_fn(K, from_src);
+    PassFn fn = pass_fn(K, from_src, mode_b != 0);
     if (smem > 48 * 1024) {
       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
