@@ -83,3 +83,36 @@ def test_host_commit_through_the_trait_calls():
         level = eng.host_hash_many(64, level)
     _, layers = whir_commit(dev(coeffs), ff, lr, leaf_encoding=PKG_LEAF_MONTGOMERY)
     assert level == layers[-32:].cpu().numpy().tobytes()
+
+
+def test_concurrent_host_calls_match_sequential():
+    """Host-slice calls from several threads at once (the stager serialises
+    them per device and shares its pinned chunks) return exactly what the
+    same calls return one at a time."""
+    import threading
+    from provekit_b200.ntt import host_ntt_nr
+    from provekit_b200.skyscraper import SkyscraperHashEngine
+    eng = SkyscraperHashEngine()
+    rng = np.random.default_rng(42)
+    blobs = [rng.integers(0, 256, size=512 * (1 << 14), dtype=np.uint8).tobytes() for _ in range(4)]
+    polys = [O.sample_fr(500 + i, 1 << 18) for i in range(4)]
+    exp_h = [eng.host_hash_many(512, b) for b in blobs]
+    exp_n = [host_ntt_nr(p.copy(), 1 << 18, 1) for p in polys]
+    got_h, got_n, errors = [None] * 4, [None] * 4, []
+
+    def work(i):
+        try:
+            for _ in range(3):
+                got_h[i] = eng.host_hash_many(512, blobs[i])
+                got_n[i] = host_ntt_nr(polys[i].copy(), 1 << 18, 1)
+        except Exception as e:  # surfaced below
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(i,)) for i in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    assert got_h == exp_h
+    assert all(np.array_equal(g, e) for g, e in zip(got_n, exp_n))
