@@ -10,16 +10,16 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.path.join(HERE, "pk_oracle.c")
+SRCS = [os.path.join(HERE, "pk_oracle.c"), os.path.join(HERE, "pk_oracle_whir.c")]
 LIB = os.path.join(HERE, "libpk_oracle.so")
 
 
 def build(force: bool = False) -> str:
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(
-        os.path.getmtime(SRC), os.path.getmtime(os.path.join(HERE, "pk_oracle.h"))
+        [os.path.getmtime(s) for s in SRCS] + [os.path.getmtime(os.path.join(HERE, "pk_oracle.h"))]
     ):
         return LIB
-    cmd = ["gcc", "-O3", "-fopenmp", "-Wall", "-Wextra", "-shared", "-fPIC", "-o", LIB, SRC]
+    cmd = ["gcc", "-O3", "-fopenmp", "-Wall", "-Wextra", "-shared", "-fPIC", "-o", LIB] + SRCS
     subprocess.run(cmd, check=True)
     return LIB
 

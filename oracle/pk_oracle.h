@@ -180,6 +180,71 @@ int  pko_whir_sumcheck_round(uint64_t *f, uint64_t *w, size_t size, const uint64
 int  pko_eq_accumulate(uint64_t *w, size_t nv, const uint64_t *points, const uint64_t *coeffs,
                        size_t npts);
 
+/* ---- WHIR round orchestration (pk_oracle_whir.c) --------------------------
+ * A whole WHIR proof of linear statements <a_k, c> = v_k about a committed
+ * coefficient vector c (2^n Fr), in the round order of the reference's Go
+ * verifier runWhir (recursive-verifier/app/circuit/whir.go:587-724), with
+ *  - query points from RSFr::evaluation_points (provekit/common/src/ntt.rs:22-42:
+ *    row i of a codeword of L rows sits at w_L^bitrev(i));
+ *  - 2^k contiguous messages per codeword row (pko_whir_fold_coeffs), so a
+ *    sumcheck binds the top bit of the coefficient index first and the
+ *    round's fold randomness is the reverse of its sumcheck challenges;
+ *  - the sumcheck over f^(b) * w(b) on the hypercube, f^ = zeta(c) (subset
+ *    sums), linear statements as w = mobius^T(a) (superset differences);
+ *  - the transcript stand-in above; PoW = pko_sky_pow_solve with threshold
+ *    floor(p / 2^bits) (CheckPoW, utilities/utilities.go:104-139).
+ * whir's own byte layout and schedule are un-vendored; this is the protocol
+ * the device prover must reproduce word for word. */
+#define PKO_WHIR_MAX_ROUNDS 16
+typedef struct {
+    uint32_t num_variables;   /* n: the committed vector has 2^n entries      */
+    uint32_t folding_factor;  /* k, 1..6 (constant over the rounds)            */
+    uint32_t log_inv_rate;    /* starting rate 2^-log_inv_rate                */
+    uint32_t num_rounds;      /* R: rounds with a new commitment              */
+    uint32_t final_vars;      /* n - (R+1) k: variables sent in the clear     */
+    uint32_t ood_samples;     /* out-of-domain samples per commitment         */
+    uint32_t pow_bits;        /* grinding per round (0: none)                 */
+    uint32_t final_pow_bits;
+    uint32_t queries[PKO_WHIR_MAX_ROUNDS + 1]; /* STIR queries of rounds 0..R-1, final at R */
+} pko_whir_params;
+/* The schedule: R + 1 = max(1, ceil((n - 6) / k)) folds of k variables,
+ * queries[r] = ceil((security - pow) / (rate_r / 2)) with rate_r =
+ * log_inv_rate + r (k - 1) the log inverse rate of codeword r. */
+int pko_whir_params_init(pko_whir_params *p, unsigned n, unsigned k, unsigned log_inv_rate,
+                         unsigned security_bits, unsigned pow_bits);
+size_t pko_whir_commit_words(const pko_whir_params *p);
+size_t pko_whir_proof_words(const pko_whir_params *p, size_t ncov);
+/* n bytes: 31 low bytes of the canonical form of each squeezed element. */
+void pko_transcript_squeeze_bytes(pko_transcript *t, uint8_t *out, size_t n);
+/* In place over 2^n entries: zeta: v[b | 2^i] += v[b]; mobius_t: v[b] -= v[b | 2^i]. */
+void pko_subset_zeta(uint64_t *v, unsigned n);
+void pko_subset_mobius_t(uint64_t *v, unsigned n);
+/* The commitment: codeword (2^(n + log_inv_rate) Fr) of 2^k contiguous
+ * messages and its tree over canonical leaves (2 L - 1 digests). */
+int pko_whir_commit(const uint64_t *coeffs, size_t num_coeffs, unsigned k, unsigned log_inv_rate,
+                    uint64_t *codeword, uint8_t *layers);
+/* Absorb the root, draw the commitment's OOD points, absorb f(z).  words:
+ * root (4) + answers (4 ood); ood_points: 4 ood. */
+int pko_whir_commit_ood(const pko_whir_params *p, pko_transcript *t, const uint64_t *coeffs,
+                        const uint8_t root[32], uint64_t *commit_words, uint64_t *ood_points);
+/* The proof (pko_whir_proof_words words) of the ncov covectors (ncov x 2^n,
+ * coefficient space) against the commitment. */
+int pko_whir_prove(const pko_whir_params *p, pko_transcript *t, const uint64_t *coeffs,
+                   const uint64_t *codeword, const uint8_t *layers, const uint64_t *commit_words,
+                   const uint64_t *ood_points, const uint64_t *covectors, size_t ncov,
+                   uint64_t *proof);
+/* 0 when the proof is accepted, else a PKO_WHIR_REJECT_* code. */
+#define PKO_WHIR_BAD_PARAMS -1
+#define PKO_WHIR_REJECT_FORMAT -2
+#define PKO_WHIR_REJECT_SUMCHECK -3
+#define PKO_WHIR_REJECT_POW -4
+#define PKO_WHIR_REJECT_MERKLE -5
+#define PKO_WHIR_REJECT_FINAL_POLY -6
+#define PKO_WHIR_REJECT_FINAL_CLAIM -7
+int pko_whir_verify(const pko_whir_params *p, pko_transcript *t, const uint64_t *covectors,
+                    size_t ncov, const uint64_t *commit_words, const uint64_t *proof,
+                    size_t proof_words);
+
 int pko_num_threads(void);
 
 #ifdef __cplusplus

@@ -112,7 +112,92 @@ def lib():
         L.pko_stir_indices.argtypes = [_u8p, _sz, _sz, _u64p]
         L.pko_whir_sumcheck_round.argtypes = [_u64p, _u64p, _sz, _u64p, _u64p]
         L.pko_eq_accumulate.argtypes = [_u64p, _sz, _u64p, _u64p, _sz]
+        wp = ctypes.POINTER(WhirParams)
+        L.pko_whir_params_init.argtypes = [wp] + [ctypes.c_uint] * 5
+        L.pko_whir_commit_words.argtypes = [wp]
+        L.pko_whir_commit_words.restype = _sz
+        L.pko_whir_proof_words.argtypes = [wp, _sz]
+        L.pko_whir_proof_words.restype = _sz
+        L.pko_transcript_squeeze_bytes.argtypes = [tp, _u8p, _sz]
+        L.pko_subset_zeta.argtypes = [_u64p, ctypes.c_uint]
+        L.pko_subset_mobius_t.argtypes = [_u64p, ctypes.c_uint]
+        L.pko_whir_commit.argtypes = [_u64p, _sz, ctypes.c_uint, ctypes.c_uint, _u64p, _u8p]
+        L.pko_whir_commit_ood.argtypes = [wp, tp, _u64p, _u8p, _u64p, _u64p]
+        L.pko_whir_prove.argtypes = [wp, tp, _u64p, _u64p, _u8p, _u64p, _u64p, _u64p, _sz, _u64p]
+        L.pko_whir_verify.argtypes = [wp, tp, _u64p, _sz, _u64p, _u64p, _sz]
     return _lib
+
+
+# ---- WHIR round orchestration ---------------------------------------------
+WHIR_MAX_ROUNDS = 16
+WHIR_REJECT = {-1: "bad params", -2: "format", -3: "sumcheck", -4: "pow", -5: "merkle",
+               -6: "final poly", -7: "final claim"}
+
+
+class WhirParams(ctypes.Structure):
+    _fields_ = [("num_variables", ctypes.c_uint32), ("folding_factor", ctypes.c_uint32),
+                ("log_inv_rate", ctypes.c_uint32), ("num_rounds", ctypes.c_uint32),
+                ("final_vars", ctypes.c_uint32), ("ood_samples", ctypes.c_uint32),
+                ("pow_bits", ctypes.c_uint32), ("final_pow_bits", ctypes.c_uint32),
+                ("queries", ctypes.c_uint32 * (WHIR_MAX_ROUNDS + 1))]
+
+
+def whir_params(n: int, k: int, log_inv_rate: int, security: int, pow_bits: int, **over) -> WhirParams:
+    p = WhirParams()
+    assert lib().pko_whir_params_init(ctypes.byref(p), n, k, log_inv_rate, security, pow_bits) == 0
+    for key, v in over.items():
+        if key == "queries":
+            for i, q in enumerate(v):
+                p.queries[i] = q
+        else:
+            setattr(p, key, v)
+    return p
+
+
+def transcript(domain: int) -> Transcript:
+    t = Transcript()
+    d = np.array([domain, 0, 0, 0], np.uint64)
+    lib().pko_transcript_init(ctypes.byref(t), p64(d))
+    return t
+
+
+def whir_commit(coeffs: np.ndarray, k: int, log_inv_rate: int):
+    c = np.ascontiguousarray(coeffs, dtype=np.uint64).reshape(-1, 4)
+    L = (c.shape[0] >> k) << log_inv_rate
+    cw = np.zeros(((c.shape[0] << log_inv_rate), 4), np.uint64)
+    layers = np.zeros((2 * L - 1) * 32, np.uint8)
+    assert lib().pko_whir_commit(p64(c), c.shape[0], k, log_inv_rate, p64(cw), p8(layers)) == 0
+    return cw, layers
+
+
+def whir_prove(p: WhirParams, domain: int, coeffs: np.ndarray, covectors: np.ndarray):
+    """Commit + prove with a fresh transcript; returns (commit_words, proof)."""
+    c = np.ascontiguousarray(coeffs, dtype=np.uint64).reshape(-1, 4)
+    cov = np.ascontiguousarray(covectors, dtype=np.uint64).reshape(-1, 4)
+    ncov = cov.shape[0] // max(c.shape[0], 1)
+    cw, layers = whir_commit(c, p.folding_factor, p.log_inv_rate)
+    root = np.ascontiguousarray(layers[-32:])
+    t = transcript(domain)
+    cwords = np.zeros(lib().pko_whir_commit_words(ctypes.byref(p)), np.uint64)
+    ood = np.zeros((max(p.ood_samples, 1), 4), np.uint64)
+    assert lib().pko_whir_commit_ood(ctypes.byref(p), ctypes.byref(t), p64(c), p8(root),
+                                     p64(cwords), p64(ood)) == 0
+    proof = np.zeros(lib().pko_whir_proof_words(ctypes.byref(p), ncov), np.uint64)
+    cov_arg = p64(cov) if ncov else None
+    rc = lib().pko_whir_prove(ctypes.byref(p), ctypes.byref(t), p64(c), p64(cw), p8(layers),
+                              p64(cwords), p64(ood), cov_arg, ncov, p64(proof))
+    assert rc == 0, rc
+    return cwords, proof
+
+
+def whir_verify(p: WhirParams, domain: int, covectors: np.ndarray, ncov: int,
+                commit_words: np.ndarray, proof: np.ndarray) -> int:
+    cov = np.ascontiguousarray(covectors, dtype=np.uint64).reshape(-1, 4)
+    t = transcript(domain)
+    cw = np.ascontiguousarray(commit_words, dtype=np.uint64)
+    pr = np.ascontiguousarray(proof, dtype=np.uint64)
+    return lib().pko_whir_verify(ctypes.byref(p), ctypes.byref(t), p64(cov) if ncov else None, ncov,
+                                 p64(cw), p64(pr), pr.shape[0])
 
 
 # ---- WHIR prove-round building blocks ------------------------------------

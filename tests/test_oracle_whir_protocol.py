@@ -1,0 +1,263 @@
+"""CPU tests of the oracle's whole WHIR proof (pk_oracle_whir.c).
+
+The prover and the verifier are both restatements: the round order is the
+reference's Go verifier runWhir (recursive-verifier/app/circuit/whir.go:587-724),
+its checks CheckSumOverBool, the Merkle path walk, CheckPoW, the final
+UnivarPoly == computeFold comparison and lastEval == W(r) f(r).  These tests
+pin the pair against each other: honest proofs are accepted for many shapes,
+and a mistake planted in any section of a proof, in the statement or in the
+transcript is rejected by the check that guards it.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+
+def layout(p, ncov):
+    """Word offsets of every section of a proof (the order pko_whir_prove writes)."""
+    k, K, o = p.folding_factor, 1 << p.folding_factor, p.ood_samples
+    n, lr = p.num_variables, p.log_inv_rate
+    pos = 0
+    out = {"values": pos}
+    pos += 4 * ncov
+    out["sc0"] = pos
+    pos += 12 * k
+    rounds = []
+    for r in range(p.num_rounds):
+        d = {"root": pos}
+        pos += 4
+        d["ood"] = pos
+        pos += 4 * o
+        if p.pow_bits:
+            d["pow"] = pos
+            pos += 1
+        depth = n + lr - k - r
+        d["open"] = pos
+        d["row_words"], d["path_words"] = 4 * K, 4 * depth
+        pos += p.queries[r] * (4 * K + 4 * depth)
+        d["sc"] = pos
+        pos += 12 * k
+        rounds.append(d)
+    out["rounds"] = rounds
+    R = p.num_rounds
+    fin = {"coeffs": pos}
+    pos += 4 << p.final_vars
+    if p.final_pow_bits:
+        fin["pow"] = pos
+        pos += 1
+    depth = n + lr - k - R
+    fin["open"] = pos
+    fin["row_words"], fin["path_words"] = 4 * K, 4 * depth
+    pos += p.queries[R] * (4 * K + 4 * depth)
+    fin["sc"] = pos
+    pos += 12 * p.final_vars
+    out["final"] = fin
+    out["total"] = pos
+    return out
+
+
+CASES = [
+    # n, k, log_inv_rate, security, pow, overrides
+    (6, 2, 1, 24, 0, {}),
+    (8, 2, 1, 32, 2, {}),
+    (10, 3, 2, 40, 3, {}),
+    (12, 3, 2, 60, 4, {"ood_samples": 2}),
+    (13, 4, 1, 40, 0, {}),
+    (14, 2, 2, 30, 2, {}),
+    (15, 5, 1, 30, 1, {}),
+    (16, 6, 2, 24, 0, {"ood_samples": 3}),
+    (12, 1, 3, 20, 1, {}),
+]
+
+
+def _problem(n, ncov, seed):
+    N = 1 << n
+    return O.sample_fr(seed, N), O.sample_fr(seed + 1, max(ncov, 1) * N)[: ncov * N]
+
+
+@pytest.mark.parametrize("n,k,lr,sec,pw,over", CASES)
+def test_honest_proofs_are_accepted(n, k, lr, sec, pw, over):
+    p = O.whir_params(n, k, lr, sec, pw, **over)
+    assert (p.num_rounds + 1) * k + p.final_vars == n
+    for ncov in (0, 1, 3):
+        c, cov = _problem(n, ncov, 1000 * n + 10 * k + ncov)
+        cw, proof = O.whir_prove(p, 0x5eed + n, c, cov)
+        lay = layout(p, ncov)
+        assert proof.shape[0] == lay["total"] == O.lib().pko_whir_proof_words(
+            O.ctypes.byref(p), ncov)
+        assert O.whir_verify(p, 0x5eed + n, cov, ncov, cw, proof) == 0
+        # the statement values are the covectors' dot products with c
+        for a in range(ncov):
+            exp = np.zeros(4, np.uint64)
+            O.lib().pko_dot(O.p64(exp), O.p64(np.ascontiguousarray(cov[a << n:(a + 1) << n])),
+                            O.p64(c), 1 << n)
+            assert np.array_equal(proof[4 * a:4 * a + 4], exp)
+
+
+def test_params_schedule_of_the_r1cs_config():
+    """n = 21 with the reference's whir config (ff 3, rate 1/4, 128 bits,
+    10 PoW bits): five folds of three variables, six sent in the clear."""
+    p = O.whir_params(21, 3, 2, 128, 10)
+    assert (p.num_rounds, p.final_vars, p.ood_samples) == (4, 6, 1)
+    assert list(p.queries[:5]) == [118, 59, 40, 30, 24]
+
+
+@pytest.fixture(scope="module")
+def honest():
+    p = O.whir_params(12, 3, 2, 40, 4, ood_samples=2)
+    ncov = 2
+    c, cov = _problem(12, ncov, 4242)
+    cw, proof = O.whir_prove(p, 99, c, cov)
+    assert O.whir_verify(p, 99, cov, ncov, cw, proof) == 0
+    return p, ncov, c, cov, cw, proof, layout(p, ncov)
+
+
+def _bump(words, at):
+    """Add one to the field element at word offset `at` (stays canonical)."""
+    w = words.copy()
+    x = O.sample_fr(1, 1)[0] * 0  # zero
+    one = np.array([1, 0, 0, 0], np.uint64)
+    m = np.zeros(4, np.uint64)
+    O.lib().pko_fr_to_mont(O.p64(m), O.p64(one))
+    O.lib().pko_fr_add(O.p64(x), O.p64(np.ascontiguousarray(w[at:at + 4])), O.p64(m))
+    w[at:at + 4] = x
+    return w
+
+
+def _verify(h, proof=None, cw=None, cov=None, domain=99):
+    p, ncov, _, cov0, cw0, proof0, _ = h
+    return O.whir_verify(p, domain, cov0 if cov is None else cov, ncov,
+                         cw0 if cw is None else cw, proof0 if proof is None else proof)
+
+
+def test_tampered_statement_value_is_rejected(honest):
+    lay = honest[6]
+    assert _verify(honest, proof=_bump(honest[5], lay["values"] + 4)) == -3
+
+
+def test_tampered_commitment_answer_is_rejected(honest):
+    assert _verify(honest, cw=_bump(honest[4], 4)) == -3
+
+
+def test_other_statement_is_rejected(honest):
+    cov = honest[3].copy()
+    cov[5] = O.sample_fr(77, 1)[0]
+    assert _verify(honest, cov=cov) == -7
+
+
+def test_other_transcript_domain_is_rejected(honest):
+    assert _verify(honest, domain=100) != 0
+
+
+def test_tampered_sumcheck_message_is_rejected(honest):
+    lay = honest[6]
+    for at in (lay["sc0"], lay["rounds"][0]["sc"] + 12, lay["final"]["sc"] + 4):
+        assert _verify(honest, proof=_bump(honest[5], at)) == -3
+
+
+def test_tampered_round_ood_answer_is_rejected(honest):
+    """The answer is absorbed before the round's PoW challenge is drawn, so
+    the grinding check sees it first; without PoW the sum check does."""
+    lay = honest[6]
+    assert _verify(honest, proof=_bump(honest[5], lay["rounds"][0]["ood"] + 4)) in (-3, -4)
+
+
+def test_tampered_opening_is_rejected(honest):
+    lay = honest[6]
+    for sec in (lay["rounds"][0], lay["final"]):
+        row_at = sec["open"] + 3 * (sec["row_words"] + sec["path_words"]) + 4
+        assert _verify(honest, proof=_bump(honest[5], row_at)) == -5
+        path_at = sec["open"] + sec["row_words"]
+        assert _verify(honest, proof=_bump(honest[5], path_at)) == -5
+
+
+def test_tampered_root_is_rejected(honest):
+    lay = honest[6]
+    assert _verify(honest, proof=_bump(honest[5], lay["rounds"][0]["root"])) != 0
+
+
+def test_tampered_pow_nonce_is_rejected(honest):
+    lay = honest[6]
+    for at in (lay["rounds"][0]["pow"], lay["final"]["pow"]):
+        bad = None
+        for d in range(1, 64):  # the first nonce above the honest one that fails
+            w = honest[5].copy()
+            w[at] = w[at] + np.uint64(d)
+            rc = _verify(honest, proof=w)
+            if rc == -4:
+                bad = d
+                break
+        assert bad is not None
+
+
+def test_tampered_final_coefficient_is_rejected(honest):
+    """The coefficients are absorbed before the final PoW challenge and the
+    final query indices are drawn, so a changed coefficient fails the PoW,
+    or opens other leaves than the proof carries (Merkle), or -- should the
+    indices survive -- UnivarPoly != computeFold."""
+    lay = honest[6]
+    assert _verify(honest, proof=_bump(honest[5], lay["final"]["coeffs"])) in (-4, -6)
+    p = O.whir_params(11, 3, 2, 40, 0)
+    c, cov = _problem(11, 1, 515)
+    cw, proof = O.whir_prove(p, 8, c, cov)
+    at = layout(p, 1)["final"]["coeffs"] + 4
+    assert O.whir_verify(p, 8, cov, 1, cw, proof) == 0
+    assert O.whir_verify(p, 8, cov, 1, cw, _bump(proof, at)) in (-5, -6)
+
+
+def test_non_canonical_and_truncated_proofs_are_rejected(honest):
+    p, ncov, _, cov, cw, proof, lay = honest
+    w = proof.copy()
+    w[lay["sc0"]:lay["sc0"] + 4] = np.array([~np.uint64(0)] * 4, np.uint64)
+    assert _verify(honest, proof=w) == -2
+    assert O.whir_verify(p, 99, cov, ncov, cw, proof[:-1]) == -2
+
+
+def test_wrong_witness_cannot_be_proven_for_the_claimed_values():
+    """A proof for another vector carries other statement values."""
+    p = O.whir_params(10, 2, 2, 30, 0)
+    c, cov = _problem(10, 1, 31)
+    cw1, pr1 = O.whir_prove(p, 5, c, cov)
+    c2 = c.copy()
+    c2[3] = O.sample_fr(32, 1)[0]
+    cw2, pr2 = O.whir_prove(p, 5, c2, cov)
+    assert not np.array_equal(pr1[:4], pr2[:4])
+    assert not np.array_equal(cw1, cw2)
+    # each proof verifies only against its own commitment
+    assert O.whir_verify(p, 5, cov, 1, cw1, pr1) == 0
+    assert O.whir_verify(p, 5, cov, 1, cw2, pr1) != 0
+
+
+def test_subset_transforms_are_inverse_pairs():
+    """mobius^T is the adjoint inverse of zeta: <mobius^T(a), zeta(c)> = <a, c>."""
+    n = 9
+    a, c = O.sample_fr(61, 1 << n), O.sample_fr(62, 1 << n)
+    za, mc = c.copy(), a.copy()
+    O.lib().pko_subset_zeta(O.p64(za), n)
+    O.lib().pko_subset_mobius_t(O.p64(mc), n)
+    d1, d2 = np.zeros(4, np.uint64), np.zeros(4, np.uint64)
+    O.lib().pko_dot(O.p64(d1), O.p64(a), O.p64(c), 1 << n)
+    O.lib().pko_dot(O.p64(d2), O.p64(mc), O.p64(za), 1 << n)
+    assert np.array_equal(d1, d2)
+    # zeta of a one-hot vector at index i is the indicator of supersets of i
+    e = np.zeros((1 << n, 4), np.uint64)
+    one = np.zeros(4, np.uint64)
+    O.lib().pko_fr_to_mont(O.p64(one), O.p64(np.array([1, 0, 0, 0], np.uint64)))
+    e[5] = one
+    O.lib().pko_subset_zeta(O.p64(e), n)
+    for b in range(1 << n):
+        assert np.array_equal(e[b], one if (b & 5) == 5 else np.zeros(4, np.uint64))
+
+
+def test_squeeze_bytes_takes_31_bytes_per_element():
+    t1, t2 = O.transcript(3), O.transcript(3)
+    out = np.zeros(70, np.uint8)
+    O.lib().pko_transcript_squeeze_bytes(O.ctypes.byref(t1), O.p8(out), 70)
+    exp = b""
+    for _ in range(3):
+        m, c = np.zeros(4, np.uint64), np.zeros(4, np.uint64)
+        O.lib().pko_transcript_squeeze(O.ctypes.byref(t2), O.p64(m))
+        O.lib().pko_fr_from_mont(O.p64(c), O.p64(m))
+        exp += c.tobytes()[:31]
+    assert out.tobytes() == exp[:70]
