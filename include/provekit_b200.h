@@ -441,6 +441,69 @@ int pkg_whir_sumcheck_round(uint64_t *f, uint64_t *w, size_t size, const uint64_
 int pkg_eq_accumulate(uint64_t *w, size_t nv, const uint64_t *points, const uint64_t *coeffs,
                       size_t npts, pkg_stream_t stream);
 
+/* ---- WHIR prover: the round loop -----------------------------------------
+ * Replaces the un-vendored whir crate's prove (called at
+ * provekit/prover/src/whir_r1cs.rs:295-301, 378-414) for linear statements
+ * <a_k, c> = v_k about a committed coefficient vector c of 2^n Fr.  The
+ * proof is what the reference's Go verifier walks (runWhir,
+ * recursive-verifier/app/circuit/whir.go:587-724): statement values, the
+ * initial sumcheck, per round a root, OOD answers, PoW nonce, STIR openings
+ * of the previous codeword (rows then authentication paths) and k sumcheck
+ * messages, then the final coefficients, PoW, openings and sumcheck -- a
+ * flat array of u64 words (Fr as 4 Montgomery limbs, digests as 4 LE words,
+ * nonces as one word), pkg_whir_proof_words long.  Conventions the crate
+ * would fix and that are chosen here: query points
+ * RSFr::evaluation_points (provekit/common/src/ntt.rs:22-42); 2^k contiguous
+ * messages per codeword row, so a sumcheck binds the top coefficient bit
+ * first; the sumcheck runs over zeta(c) (subset sums) against
+ * mobius^T(sum gamma^j a_j) (superset differences); the transcript stand-in
+ * above, with bytes taken 31 per squeezed element; PoW threshold
+ * floor(p / 2^bits) (CheckPoW, recursive-verifier/app/utilities/utilities.go:104-139). */
+#define PKG_WHIR_MAX_ROUNDS 16
+typedef struct {
+  uint32_t num_variables;   /* n: the committed vector has 2^n entries     */
+  uint32_t folding_factor;  /* k, 1..6                                      */
+  uint32_t log_inv_rate;    /* starting rate 2^-log_inv_rate (1..8)         */
+  uint32_t num_rounds;      /* R: rounds that commit a folded polynomial    */
+  uint32_t final_vars;      /* n - (R+1) k, sent as 2^final_vars coeffs     */
+  uint32_t ood_samples;     /* OOD samples per commitment (0..4)            */
+  uint32_t pow_bits;        /* grinding per round (0..27, 0 = none)         */
+  uint32_t final_pow_bits;
+  uint32_t queries[PKG_WHIR_MAX_ROUNDS + 1]; /* rounds 0..R-1, final at R   */
+} pkg_whir_params;
+/* Schedule: R + 1 = max(1, ceil((n - 6) / k)) folds; queries[r] =
+ * ceil(2 (security - pow) / rate_r), rate_r = log_inv_rate + r (k - 1). */
+int pkg_whir_params_init(pkg_whir_params *p, unsigned num_variables, unsigned folding_factor,
+                         unsigned log_inv_rate, unsigned security_bits, unsigned pow_bits);
+size_t pkg_whir_commit_words(const pkg_whir_params *p);
+/* 0 for invalid parameters. */
+size_t pkg_whir_proof_words(const pkg_whir_params *p, size_t num_covectors);
+/* n challenge bytes: the 31 low bytes of each squeezed element's canonical
+ * little-endian form. */
+int pkg_transcript_squeeze_bytes(pkg_transcript *t, uint8_t *out, size_t n);
+/* In place over 2^n device entries: ZETA v[b | 2^i] += v[b] (coefficients ->
+ * hypercube evaluations); MOBIUS_T v[b] -= v[b | 2^i] (its adjoint inverse:
+ * a covector on coefficients -> a weight on the hypercube).  Async. */
+#define PKG_SUBSET_ZETA 0
+#define PKG_SUBSET_MOBIUS_T 1
+int pkg_subset_transform(uint64_t *v, unsigned n, int mode, pkg_stream_t stream);
+/* The commitment's transcript part, after pkg_whir_commit(coeffs, 2^n,
+ * folding_factor, log_inv_rate, no masks, PKG_LEAF_CANONICAL): absorb the root,
+ * draw ood_samples points, absorb f(z).  coeffs, layers: device;
+ * commit_words (4 + 4 ood_samples: root, answers), ood_points: host.
+ * Synchronous. */
+int pkg_whir_commit_ood(const pkg_whir_params *p, pkg_transcript *t, const uint64_t *coeffs,
+                        const uint8_t *layers, uint64_t *commit_words, uint64_t *ood_points,
+                        pkg_stream_t stream);
+/* The proof of num_covectors (<= 16) statements: covectors device
+ * (num_covectors x 2^n Fr, coefficient space); coeffs, codeword, layers the
+ * commitment (device); ood_points from pkg_whir_commit_ood; proof: host,
+ * pkg_whir_proof_words words.  Synchronous; t advances past the proof. */
+int pkg_whir_prove(const pkg_whir_params *p, pkg_transcript *t, const uint64_t *coeffs,
+                   const uint64_t *codeword, const uint8_t *layers, const uint64_t *ood_points,
+                   const uint64_t *covectors, size_t num_covectors, uint64_t *proof,
+                   pkg_stream_t stream);
+
 /* ---- field arithmetic (skyscraper/bn254-multiplier/src/scalar.rs:12-132,
  *      ark-ff Montgomery conversion) ---------------------------------------- */
 /* out[i] = op(a[i], b[i]) over n Fr (4 x u64 LE each, device, 16-byte

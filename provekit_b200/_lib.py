@@ -90,6 +90,11 @@ SIGNATURES = {
     "pkg_eq_accumulate": [_c_vp, _c_sz, _c_vp, _c_vp, _c_sz, _c_vp],
     "pkg_fr_mul_batch": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                          ctypes.c_int, ctypes.c_void_p],
+    "pkg_whir_params_init": [_c_vp, _c_uint, _c_uint, _c_uint, _c_uint, _c_uint],
+    "pkg_transcript_squeeze_bytes": [_c_vp, _c_vp, _c_sz],
+    "pkg_subset_transform": [_c_vp, _c_uint, _c_int, _c_vp],
+    "pkg_whir_commit_ood": [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+    "pkg_whir_prove": [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_sz, _c_vp, _c_vp],
     "pkg_version": [],
 }
 
@@ -122,6 +127,10 @@ def lib():
         L.pkg_batch_destroy.restype = None
         L.pkg_server_destroy.argtypes = [_c_vp]
         L.pkg_server_destroy.restype = None
+        for name in ("pkg_whir_commit_words", "pkg_whir_proof_words"):
+            fn = getattr(L, name)
+            fn.argtypes = [_c_vp] if name == "pkg_whir_commit_words" else [_c_vp, _c_sz]
+            fn.restype = ctypes.c_size_t
         L.pkg_kernel_launches.argtypes = []
         L.pkg_kernel_launches.restype = ctypes.c_uint64
         _lib = L
@@ -140,4 +149,5 @@ def check(rc: int):
 
 def exported_symbols():
     return sorted(SIGNATURES) + ["pkg_last_error", "pkg_kernel_launches", "pkg_batch_destroy",
-                                  "pkg_server_destroy"]
+                                  "pkg_server_destroy", "pkg_whir_commit_words",
+                                  "pkg_whir_proof_words"]

@@ -14,6 +14,9 @@ int spmv_device(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* v
                 cudaStream_t s);
 int eq_hypercube_device(const uint64_t* r_host, size_t nr, size_t num_entries, uint64_t* out,
                         cudaStream_t s);
+// Skyscraper PoW on stream s (synchronous): generic::solve's answer.
+int pow_solve_device(const uint64_t challenge[4], const uint64_t threshold[4], cudaStream_t s,
+                     uint64_t* nonce_out);
 int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* d_out, uint64_t* part,
                cudaStream_t s);
 

@@ -17,6 +17,7 @@
 #include "fr.cuh"
 #include "ntt_internal.cuh"
 #include "host_stage.cuh"
+#include "internal.cuh"
 #include "pk_common.cuh"
 #include "rs_internal.cuh"
 #include "skyscraper.cuh"
@@ -229,6 +230,43 @@ __global__ void pow_kernel(Fr challenge, Fr threshold, uint64_t base, uint64_t n
   }
 }
 
+// The smallest nonce with compress(challenge, [nonce,0,0,0]) < threshold:
+// batches of candidates in increasing order, starting small (a PoW of b
+// bits needs about 2^b candidates) and growing four-fold, so the first
+// batch that holds a solution holds the smallest one.
+int pow_solve_device(const uint64_t challenge[4], const uint64_t threshold[4], cudaStream_t s,
+                     uint64_t* nonce_out) {
+  Fr c, t;
+  memcpy(c.v, challenge, 32);
+  memcpy(t.v, threshold, 32);
+  bool thr_zero = true;
+  for (int i = 0; i < 8; i++) thr_zero &= (t.v[i] == 0);
+  PK_REQUIRE(!thr_zero, "threshold 0 admits no nonce");
+  Scratch scr;
+  int rc = scr.alloc(sizeof(unsigned long long), s);
+  if (rc) return rc;
+  unsigned long long* d_best = static_cast<unsigned long long*>(scr.ptr);
+  PK_CUDA(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long), s));
+  const unsigned long long none = ~0ULL;
+  unsigned long long best = none;
+  const uint64_t max_batch = uint64_t(1) << 22;
+  uint64_t batch = uint64_t(1) << 13;
+  for (uint64_t base = 0; best == none; base += batch, batch = std::min(batch * 4, max_batch)) {
+    if (base > (uint64_t(1) << 62)) break;
+    const int grid = (int)std::min<uint64_t>((uint64_t)sm_count() * 8, (batch + 255) / 256);
+    pow_kernel<<<grid, 256, 0, s>>>(c, t, base, batch, d_best);
+    PK_CHECK_LAUNCH("pow_kernel");
+    PK_CUDA(cudaMemcpyAsync(&best, d_best, sizeof best, cudaMemcpyDeviceToHost, s));
+    PK_CUDA(cudaStreamSynchronize(s));
+  }
+  if (best == none) {
+    set_last_error("no nonce found");
+    return PKG_ERR_UNSUPPORTED;
+  }
+  *nonce_out = best;
+  return PKG_OK;
+}
+
 }  // namespace pk
 
 using namespace pk;
@@ -300,11 +338,13 @@ extern "C" int pkg_whir_commit(const uint64_t* coeffs, size_t num_coeffs,
                                const uint64_t* masks, size_t mask_len, int leaf_encoding,
                                uint64_t* codeword_out, uint8_t* layers_out,
                                pkg_stream_t stream) {
-  PK_REQUIRE(folding_factor <= 12 && log_inv_rate <= 8, "unsupported folding factor / rate");
+  PK_REQUIRE(folding_factor <= 12 && log_inv_rate <= 28, "unsupported folding factor / rate");
   size_t M = size_t(1) << folding_factor;
   PK_REQUIRE(is_pow2(num_coeffs) && num_coeffs >= M,
              "num_coeffs %zu must be a power of two >= 2^folding_factor", num_coeffs);
   size_t L = num_coeffs / M;
+  PK_REQUIRE((L << log_inv_rate) <= (size_t(1) << 28),
+             "codeword of %zu << %u rows exceeds the largest NTT order 2^28", L, log_inv_rate);
   size_t cw_len = L << log_inv_rate;
   cudaStream_t s = as_stream(stream);
   int rc = rs_encode_device(coeffs, M, L, masks, mask_len, cw_len, codeword_out, s);
@@ -315,30 +355,9 @@ extern "C" int pkg_whir_commit(const uint64_t* coeffs, size_t num_coeffs,
 extern "C" int pkg_skyscraper_pow_solve(const uint64_t challenge[4], const uint64_t threshold[4],
                                         uint64_t* nonce_out) {
   PK_REQUIRE(challenge && threshold && nonce_out, "null pointer");
-  Fr c, t;
-  memcpy(c.v, challenge, 32);
-  memcpy(t.v, threshold, 32);
-  bool thr_zero = true;
-  for (int i = 0; i < 8; i++) thr_zero &= (t.v[i] == 0);
-  PK_REQUIRE(!thr_zero, "threshold 0 admits no nonce");
-  unsigned long long* d_best = nullptr;
-  PK_CUDA(cudaMalloc(&d_best, sizeof(unsigned long long)));
-  const unsigned long long none = ~0ULL;
-  cudaError_t e = cudaMemcpy(d_best, &none, sizeof none, cudaMemcpyHostToDevice);
-  unsigned long long best = none;
-  const uint64_t batch = uint64_t(1) << 22;
-  for (uint64_t base = 0; e == cudaSuccess && best == none; base += batch) {
-    pow_kernel<<<sm_count() * 8, 256>>>(c, t, base, batch, d_best);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpy(&best, d_best, sizeof best, cudaMemcpyDeviceToHost);
-    if (base > (uint64_t(1) << 62)) break;
-  }
-  cudaFree(d_best);
-  if (e != cudaSuccess) return cuda_status(e, "pkg_skyscraper_pow_solve");
-  if (best == none) {
-    set_last_error("no nonce found");
-    return PKG_ERR_UNSUPPORTED;
-  }
-  *nonce_out = best;
-  return PKG_OK;
+  cudaStream_t s = nullptr;
+  PK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  const int rc = pow_solve_device(challenge, threshold, s, nonce_out);
+  cudaStreamDestroy(s);
+  return rc;
 }

@@ -322,6 +322,22 @@ extern "C" int pkg_transcript_absorb(pkg_transcript* t, const uint64_t x[4]) {
   return PKG_OK;
 }
 
+extern "C" int pkg_transcript_squeeze_bytes(pkg_transcript* t, uint8_t* out, size_t n) {
+  PK_REQUIRE(t && (out || n == 0), "null pointer");
+  HostTranscript ht;
+  ht.l = HostFr::from_limbs(t->l);
+  ht.r = HostFr::from_limbs(t->r);
+  for (size_t done = 0; done < n;) {
+    const HostFr c = HostFr::from_mont(ht.squeeze());
+    const size_t take = std::min<size_t>(31, n - done);
+    for (size_t i = 0; i < take; i++) out[done + i] = (uint8_t)(c.l[i / 8] >> (8 * (i % 8)));
+    done += take;
+  }
+  memcpy(t->l, ht.l.l, 32);
+  memcpy(t->r, ht.r.l, 32);
+  return PKG_OK;
+}
+
 extern "C" int pkg_transcript_squeeze(pkg_transcript* t, uint64_t out[4]) {
   PK_REQUIRE(t && out, "null pointer");
   HostTranscript ht;

@@ -1,0 +1,548 @@
+// whir_prove.cu -- the WHIR prover's round loop, resident in HBM.
+//
+// The whir crate's prover (called from provekit/prover/src/whir_r1cs.rs:295-301,
+// 378-414) is not vendored with the reference.  This loop produces the proof
+// that the reference's Go verifier walks (runWhir,
+// recursive-verifier/app/circuit/whir.go:587-724), for linear statements
+// <a_k, c> = v_k about a committed coefficient vector c:
+//
+//   values v_k; combination randomness; k sumcheck rounds over
+//   f^ = zeta(c) (subset sums: the hypercube evaluations of the multilinear
+//   polynomial with coefficients c) and w = mobius^T(sum gamma^j a_j) plus
+//   gamma^j eq(expand(z_j), .) for the commitment's OOD points;
+//   per round: fold the coefficients, commit them (RS encode + Skyscraper
+//   tree), OOD answers, PoW, STIR queries opened in the previous codeword,
+//   their eq constraints added to w, k sumcheck rounds;
+//   final: the remaining coefficients, PoW, STIR openings, sumcheck.
+//
+// Every table, codeword and tree stays on the device.  The host holds only the
+// transcript: it reads back the three sums of each sumcheck round, the roots,
+// the OOD answers, the PoW nonce and the opened rows and paths, which are the
+// proof, and sends back the challenges as kernel parameters.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "fr.cuh"
+#include "fr_f64.cuh"
+#include "fr_host.hpp"
+#include "internal.cuh"
+#include "pk_common.cuh"
+#include "reduce.cuh"
+
+namespace pk {
+
+static_assert(sizeof(HostFr) == 32, "vectors of HostFr are arrays of 4 x u64 limbs");
+
+// ---- subset transforms ----------------------------------------------------
+// NB bits [lo, lo + NB) of the index per pass: each thread loads the 2^NB
+// entries of one group (stride 2^lo), runs NB butterfly stages in registers
+// and stores them.  Zeta: v[b | 2^i] += v[b]; mobius^T: v[b] -= v[b | 2^i].
+template <bool kZeta, int NB>
+__global__ void __launch_bounds__(256) subset_pass_kernel(uint64_t* __restrict__ v, size_t groups,
+                                                         int lo) {
+  constexpr int G = 1 << NB;
+  const size_t low_mask = (size_t(1) << lo) - 1;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < groups;
+       g += (size_t)gridDim.x * blockDim.x) {
+    const size_t base = ((g >> lo) << (lo + NB)) | (g & low_mask);
+    Fr x[G];
+#pragma unroll
+    for (int j = 0; j < G; j++) x[j] = fr_load(v, base + ((size_t)j << lo));
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+#pragma unroll
+      for (int j = 0; j < G; j++) {
+        if (kZeta && (j >> b & 1)) x[j] = fr_add(x[j], x[j ^ (1 << b)]);
+        if (!kZeta && !(j >> b & 1)) x[j] = fr_sub(x[j], x[j | (1 << b)]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < G; j++) fr_store(v, base + ((size_t)j << lo), x[j]);
+  }
+}
+
+template <bool kZeta>
+static int subset_transform_device(uint64_t* v, unsigned n, cudaStream_t s) {
+  const size_t N = size_t(1) << n;
+  for (unsigned lo = 0; lo < n;) {
+    const int nb = (int)std::min(4u, n - lo);
+    const size_t groups = N >> nb;
+    const int grid = ew_grid(groups);
+    switch (nb) {
+      case 4: subset_pass_kernel<kZeta, 4><<<grid, 256, 0, s>>>(v, groups, (int)lo); break;
+      case 3: subset_pass_kernel<kZeta, 3><<<grid, 256, 0, s>>>(v, groups, (int)lo); break;
+      case 2: subset_pass_kernel<kZeta, 2><<<grid, 256, 0, s>>>(v, groups, (int)lo); break;
+      default: subset_pass_kernel<kZeta, 1><<<grid, 256, 0, s>>>(v, groups, (int)lo); break;
+    }
+    PK_CHECK_LAUNCH("subset_pass_kernel");
+    lo += nb;
+  }
+  return PKG_OK;
+}
+
+// ---- covector combination and table folds ----------------------------------
+constexpr int kMaxCovectors = 16;
+struct CovParams {
+  const uint64_t* cov;
+  size_t stride;  // Fr between covectors
+  int ncov;
+  uint32_t coef[kMaxCovectors][8];
+};
+
+// w[b] = sum_a coef_a cov[a][b]
+__global__ void combine_covectors_kernel(uint64_t* __restrict__ w, size_t n,
+                                         const __grid_constant__ CovParams P) {
+  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < n;
+       b += (size_t)gridDim.x * blockDim.x) {
+    Fr acc = fr_zero();
+    for (int a = 0; a < P.ncov; a++) {
+      Fr c;
+#pragma unroll
+      for (int i = 0; i < 8; i++) c.v[i] = P.coef[a][i];
+      acc = fr_add(acc, fr_mul_f64(c, fr_load_ro(P.cov, (size_t)a * P.stride + b)));
+    }
+    fr_store(w, b, acc);
+  }
+}
+
+// t[i] += r (t[i + h] - t[i]) for both tables: bind the top variable.
+__global__ void fold_tables_kernel(uint64_t* __restrict__ f, uint64_t* __restrict__ w, size_t h,
+                                   Fr r) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < h;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const Fr f0 = fr_load(f, i), w0 = fr_load(w, i);
+    fr_store(f, i, fr_add(f0, fr_mul_f64(r, fr_sub(fr_load(f, i + h), f0))));
+    fr_store(w, i, fr_add(w0, fr_mul_f64(r, fr_sub(fr_load(w, i + h), w0))));
+  }
+}
+
+// ---- parameters -------------------------------------------------------------
+static unsigned rows_log(const pkg_whir_params* p, unsigned r) {
+  return p->num_variables + p->log_inv_rate - p->folding_factor - r;
+}
+
+static bool params_ok(const pkg_whir_params* p) {
+  if (!p) return false;
+  const unsigned n = p->num_variables, k = p->folding_factor, R = p->num_rounds;
+  if (k < 1 || k > 6 || n > 30 || R > PKG_WHIR_MAX_ROUNDS) return false;
+  if (p->log_inv_rate < 1 || p->log_inv_rate > 8) return false;
+  if ((R + 1) * k + p->final_vars != n) return false;
+  if (p->ood_samples > 4 || p->pow_bits > 27 || p->final_pow_bits > 27) return false;
+  if (n + p->log_inv_rate < k + R + 1) return false;
+  for (unsigned r = 0; r <= R; r++)
+    if (p->queries[r] < 1 || p->queries[r] > 4096) return false;
+  return true;
+}
+
+// ---- host-side protocol pieces -----------------------------------------------
+static HostFr absorb_squeeze(pkg_transcript* t, const HostFr* msgs, size_t n) {
+  for (size_t i = 0; i < n; i++) pkg_transcript_absorb(t, msgs[i].l);
+  HostFr r;
+  pkg_transcript_squeeze(t, r.l);
+  return r;
+}
+
+static std::vector<HostFr> powers_of(const HostFr& g, size_t n) {
+  std::vector<HostFr> out(n);
+  if (n) out[0] = HostFr::one();
+  for (size_t i = 1; i < n; i++) out[i] = HostFr::mul(out[i - 1], g);
+  return out;
+}
+
+// ExpandFromUnivariate (recursive-verifier/app/utilities/utilities.go:183-191)
+static void expand_into(std::vector<HostFr>& out, const HostFr& z, unsigned m) {
+  HostFr acc = z;
+  const size_t base = out.size();
+  out.resize(base + m);
+  for (unsigned i = 0; i < m; i++) {
+    out[base + m - 1 - i] = acc;
+    acc = HostFr::mul(acc, acc);
+  }
+}
+
+static void pow_threshold(unsigned bits, uint64_t thr[4]) {
+  memcpy(thr, HostFr::P, 32);
+  for (unsigned s = 0; s < bits; s++) {
+    thr[0] = (thr[0] >> 1) | (thr[1] << 63);
+    thr[1] = (thr[1] >> 1) | (thr[2] << 63);
+    thr[2] = (thr[2] >> 1) | (thr[3] << 63);
+    thr[3] >>= 1;
+  }
+}
+
+// A stream-ordered allocation from the library pool that can be handed on.
+struct PoolBuf {
+  void* ptr = nullptr;
+  cudaStream_t s = nullptr;
+  PoolBuf() = default;
+  PoolBuf(const PoolBuf&) = delete;
+  PoolBuf& operator=(const PoolBuf&) = delete;
+  int alloc(size_t bytes, cudaStream_t stream) {
+    reset();
+    s = stream;
+    cudaMemPool_t pool = lib_pool();
+    if (!pool) {
+      set_last_error("could not create the library memory pool");
+      return PKG_ERR_CUDA;
+    }
+    PK_CUDA(cudaMallocFromPoolAsync(&ptr, bytes, pool, s));
+    return PKG_OK;
+  }
+  void reset() {
+    if (ptr) cudaFreeAsync(ptr, s);
+    ptr = nullptr;
+  }
+  void swap(PoolBuf& o) {
+    std::swap(ptr, o.ptr);
+    std::swap(s, o.s);
+  }
+  ~PoolBuf() { reset(); }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+#define PK_TRY(call)          \
+  do {                        \
+    const int _rc = (call);   \
+    if (_rc) return _rc;      \
+  } while (0)
+
+class WhirProver {
+ public:
+  WhirProver(const pkg_whir_params* p, pkg_transcript* t, cudaStream_t s, uint64_t* proof)
+      : p_(p), t_(t), s_(s), out_(proof) {}
+
+  int run(const uint64_t* coeffs, const uint64_t* codeword, const uint8_t* layers,
+          const uint64_t* ood_points, const uint64_t* covectors, size_t ncov);
+
+ private:
+  void put(const HostFr& x) {
+    memcpy(out_ + pos_, x.l, 32);
+    pos_ += 4;
+  }
+  int sumcheck_phase(unsigned rounds, std::vector<HostFr>& rands);
+  int pow_step(unsigned bits);
+  int stir_step(size_t q, size_t L, const uint64_t* cw, const uint8_t* layers,
+                std::vector<uint64_t>& idx);
+  int add_constraints(const std::vector<HostFr>& points, unsigned nv,
+                      const std::vector<HostFr>& coefs);
+
+  const pkg_whir_params* p_;
+  pkg_transcript* t_;
+  cudaStream_t s_;
+  uint64_t* out_;
+  size_t pos_ = 0;
+  uint64_t* E_ = nullptr;  // f^ table (live size size_)
+  uint64_t* w_ = nullptr;  // weight table
+  size_t size_ = 0;
+};
+
+// k rounds of the weighted sumcheck (runWhirSumcheckRounds,
+// circuit/whir_utilities.go:103-126): send h(0), h(1), h(2), draw r.  The fold
+// by r rides on the next round's kernel; the last one is done here.
+int WhirProver::sumcheck_phase(unsigned rounds, std::vector<HostFr>& rands) {
+  rands.clear();
+  rands.reserve(rounds);
+  const uint64_t* pending = nullptr;
+  HostFr r;
+  for (unsigned i = 0; i < rounds; i++) {
+    uint64_t h[12];
+    PK_TRY(pkg_whir_sumcheck_round(E_, w_, size_, pending, h, reinterpret_cast<pkg_stream_t>(s_)));
+    if (pending) size_ /= 2;
+    memcpy(out_ + pos_, h, 96);
+    pos_ += 12;
+    HostFr hs[3] = {HostFr::from_limbs(h), HostFr::from_limbs(h + 4), HostFr::from_limbs(h + 8)};
+    r = absorb_squeeze(t_, hs, 3);
+    rands.push_back(r);
+    pending = rands.back().l;
+  }
+  if (pending) {
+    Fr rf;
+    memcpy(rf.v, rands.back().l, 32);
+    fold_tables_kernel<<<ew_grid(size_ / 2), 256, 0, s_>>>(E_, w_, size_ / 2, rf);
+    PK_CHECK_LAUNCH("fold_tables_kernel");
+    size_ /= 2;
+  }
+  return PKG_OK;
+}
+
+// RunPoW (circuit/whir.go:726-735): a challenge from the transcript, the
+// smallest nonce below the threshold, the nonce back into the transcript.
+int WhirProver::pow_step(unsigned bits) {
+  HostFr cm;
+  pkg_transcript_squeeze(t_, cm.l);
+  const HostFr c = HostFr::from_mont(cm);
+  uint64_t thr[4], nonce = 0;
+  pow_threshold(bits, thr);
+  PK_TRY(pow_solve_device(c.l, thr, s_, &nonce));
+  out_[pos_++] = nonce;
+  const HostFr nm = HostFr::from_u64(nonce);
+  pkg_transcript_absorb(t_, nm.l);
+  return PKG_OK;
+}
+
+// getStirChallenges (circuit/whir_utilities.go:49-78) on a codeword of L
+// rows, then each queried row and its authentication path into the proof.
+int WhirProver::stir_step(size_t q, size_t L, const uint64_t* cw, const uint8_t* layers,
+                          std::vector<uint64_t>& idx) {
+  const int depth = log2_exact(L);
+  const size_t K = size_t(1) << p_->folding_factor;
+  const size_t nb = (size_t)(depth + 7) / 8;
+  std::vector<uint8_t> bytes(q * nb + 1);
+  PK_TRY(pkg_transcript_squeeze_bytes(t_, bytes.data(), q * nb));
+  idx.assign(q, 0);
+  PK_TRY(pkg_stir_indices(bytes.data(), L, q, idx.data()));
+  std::vector<uint64_t> rows(q * K * 4);
+  std::vector<uint8_t> paths(q * (size_t)depth * 32 + 1);
+  const pkg_stream_t ps = reinterpret_cast<pkg_stream_t>(s_);
+  PK_TRY(pkg_gather_rows(cw, K, L, idx.data(), q, rows.data(), ps));
+  PK_TRY(pkg_merkle_open(layers, L, idx.data(), q, paths.data(), ps));
+  for (size_t i = 0; i < q; i++) {
+    memcpy(out_ + pos_, rows.data() + i * K * 4, 32 * K);
+    pos_ += 4 * K;
+    memcpy(out_ + pos_, paths.data() + i * (size_t)depth * 32, 32 * (size_t)depth);
+    pos_ += 4 * (size_t)depth;
+  }
+  return PKG_OK;
+}
+
+// w += sum_j coefs_j eq(expand(points_j), .) on the live nv-variable table.
+int WhirProver::add_constraints(const std::vector<HostFr>& points, unsigned nv,
+                                const std::vector<HostFr>& coefs) {
+  std::vector<HostFr> pts;
+  pts.reserve(points.size() * nv);
+  for (const HostFr& z : points) expand_into(pts, z, nv);
+  return pkg_eq_accumulate(w_, nv, pts.empty() ? nullptr : pts[0].l, coefs[0].l, points.size(),
+                           reinterpret_cast<pkg_stream_t>(s_));
+}
+
+int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint8_t* layers,
+                    const uint64_t* ood_points, const uint64_t* covectors, size_t ncov) {
+  const unsigned n = p_->num_variables, k = p_->folding_factor, R = p_->num_rounds;
+  const unsigned o = p_->ood_samples;
+  const size_t N = size_t(1) << n, K = size_t(1) << k;
+  const pkg_stream_t ps = reinterpret_cast<pkg_stream_t>(s_);
+
+  PoolBuf E, W, A, B, cw_own, lay_own, cw_next, lay_next;
+  PK_TRY(E.alloc(32 * N, s_));
+  PK_TRY(W.alloc(32 * N, s_));
+  PK_TRY(A.alloc(32 * (N >> k), s_));
+  PK_TRY(B.alloc(32 * (N >> k), s_));
+  E_ = E.as<uint64_t>();
+  w_ = W.as<uint64_t>();
+  size_ = N;
+  PK_CUDA(cudaMemcpyAsync(E_, coeffs, 32 * N, cudaMemcpyDeviceToDevice, s_));
+  PK_TRY(subset_transform_device<true>(E_, n, s_));
+
+  // the statement values, then the combination randomness over
+  // (commitment OOD answers, values)
+  std::vector<HostFr> vals(ncov);
+  for (size_t a = 0; a < ncov; a++) {
+    PK_TRY(pkg_dot(covectors + 4 * N * a, coeffs, N, vals[a].l, ps));
+    put(vals[a]);
+  }
+  const HostFr gamma = absorb_squeeze(t_, vals.data(), ncov);
+  std::vector<HostFr> pw = powers_of(gamma, o + ncov);
+  if (ncov) {
+    CovParams P;
+    memset(&P, 0, sizeof P);
+    P.cov = covectors;
+    P.stride = N;
+    P.ncov = (int)ncov;
+    for (size_t a = 0; a < ncov; a++) memcpy(P.coef[a], pw[o + a].l, 32);
+    combine_covectors_kernel<<<ew_grid(N), 256, 0, s_>>>(w_, N, P);
+    PK_CHECK_LAUNCH("combine_covectors_kernel");
+    PK_TRY(subset_transform_device<false>(w_, n, s_));
+  } else {
+    PK_CUDA(cudaMemsetAsync(w_, 0, 32 * N, s_));
+  }
+  if (o) {
+    std::vector<HostFr> z(o), c(pw.begin(), pw.begin() + o);
+    for (unsigned j = 0; j < o; j++) z[j] = HostFr::from_limbs(ood_points + 4 * j);
+    PK_TRY(add_constraints(z, n, c));
+  }
+
+  std::vector<HostFr> alpha;
+  PK_TRY(sumcheck_phase(k, alpha));
+
+  const uint64_t* f = coeffs;  // current polynomial's coefficients
+  unsigned nv = n;
+  const uint64_t* cw_r = codeword;
+  const uint8_t* lay_r = layers;
+  std::vector<uint64_t> idx;
+  auto fold_into = [&](uint64_t* g) -> int {
+    std::vector<HostFr> ra(alpha.rbegin(), alpha.rend());
+    PK_TRY(pkg_whir_fold_coeffs(f, size_t(1) << nv, k, ra[0].l, g, ps));
+    nv -= k;
+    return PKG_OK;
+  };
+  for (unsigned r = 0; r < R; r++) {
+    uint64_t* g = (r & 1) ? B.as<uint64_t>() : A.as<uint64_t>();
+    PK_TRY(fold_into(g));
+    // commit the folded polynomial at the next rate
+    const size_t Ln = size_t(1) << rows_log(p_, r + 1);
+    PK_TRY(cw_next.alloc(32 * K * Ln, s_));
+    PK_TRY(lay_next.alloc(32 * (2 * Ln - 1), s_));
+    PK_TRY(pkg_whir_commit(g, size_t(1) << nv, k, p_->log_inv_rate + (r + 1) * (k - 1), nullptr, 0,
+                           PKG_LEAF_CANONICAL, cw_next.as<uint64_t>(), lay_next.as<uint8_t>(), ps));
+    HostFr root;
+    PK_CUDA(cudaMemcpyAsync(root.l, lay_next.as<uint8_t>() + 32 * (2 * Ln - 2), 32,
+                            cudaMemcpyDeviceToHost, s_));
+    PK_CUDA(cudaStreamSynchronize(s_));
+    put(root);
+    const HostFr root_m = HostFr::to_mont(root);
+    pkg_transcript_absorb(t_, root_m.l);
+    // OOD samples of the folded polynomial
+    std::vector<HostFr> points(o);
+    for (unsigned j = 0; j < o; j++) pkg_transcript_squeeze(t_, points[j].l);
+    if (o) {
+      std::vector<HostFr> ans(o);
+      PK_TRY(pkg_poly_eval_many(g, size_t(1) << nv, points[0].l, o, ans[0].l, ps));
+      for (unsigned j = 0; j < o; j++) {
+        put(ans[j]);
+        pkg_transcript_absorb(t_, ans[j].l);
+      }
+    }
+    if (p_->pow_bits) PK_TRY(pow_step(p_->pow_bits));
+    // STIR queries on the previous codeword
+    const size_t Lr = size_t(1) << rows_log(p_, r), q = p_->queries[r];
+    PK_TRY(stir_step(q, Lr, cw_r, lay_r, idx));
+    std::vector<size_t> sidx(idx.begin(), idx.end());
+    points.resize(o + q);
+    PK_TRY(pkg_rs_evaluation_points(Lr, sidx.data(), q, points[o].l));
+    HostFr gr;
+    pkg_transcript_squeeze(t_, gr.l);
+    PK_TRY(add_constraints(points, nv, powers_of(gr, o + q)));
+    PK_TRY(sumcheck_phase(k, alpha));
+    // the new codeword becomes the one the next queries open
+    f = g;
+    cw_own.swap(cw_next);
+    lay_own.swap(lay_next);
+    cw_next.reset();
+    lay_next.reset();
+    cw_r = cw_own.as<uint64_t>();
+    lay_r = lay_own.as<uint8_t>();
+  }
+  // the final polynomial in the clear
+  uint64_t* g = (R & 1) ? B.as<uint64_t>() : A.as<uint64_t>();
+  PK_TRY(fold_into(g));
+  const size_t nfin = size_t(1) << nv;
+  std::vector<HostFr> fin(nfin);
+  PK_CUDA(cudaMemcpyAsync(fin[0].l, g, 32 * nfin, cudaMemcpyDeviceToHost, s_));
+  PK_CUDA(cudaStreamSynchronize(s_));
+  for (size_t i = 0; i < nfin; i++) {
+    put(fin[i]);
+    pkg_transcript_absorb(t_, fin[i].l);
+  }
+  if (p_->final_pow_bits) PK_TRY(pow_step(p_->final_pow_bits));
+  PK_TRY(stir_step(p_->queries[R], size_t(1) << rows_log(p_, R), cw_r, lay_r, idx));
+  std::vector<HostFr> rfin;
+  PK_TRY(sumcheck_phase(nv, rfin));
+  PK_CUDA(cudaStreamSynchronize(s_));
+  return PKG_OK;
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+extern "C" int pkg_whir_params_init(pkg_whir_params* p, unsigned n, unsigned k,
+                                    unsigned log_inv_rate, unsigned security_bits,
+                                    unsigned pow_bits) {
+  PK_REQUIRE(p, "null params");
+  PK_REQUIRE(k >= 1 && k <= 6 && n >= k && n <= 30, "unsupported n = %u, k = %u", n, k);
+  PK_REQUIRE(log_inv_rate >= 1 && log_inv_rate <= 8, "log_inv_rate %u outside 1..8", log_inv_rate);
+  PK_REQUIRE(pow_bits <= 27 && security_bits > pow_bits && security_bits <= 512,
+             "unsupported security %u / pow %u", security_bits, pow_bits);
+  memset(p, 0, sizeof *p);
+  unsigned folds = n > 6 ? (n - 6 + k - 1) / k : 1;
+  if (folds * k > n) folds = n / k;
+  PK_REQUIRE(folds >= 1 && folds - 1 <= PKG_WHIR_MAX_ROUNDS, "too many rounds");
+  p->num_variables = n;
+  p->folding_factor = k;
+  p->log_inv_rate = log_inv_rate;
+  p->num_rounds = folds - 1;
+  p->final_vars = n - folds * k;
+  p->ood_samples = 1;
+  p->pow_bits = pow_bits;
+  p->final_pow_bits = pow_bits;
+  for (unsigned r = 0; r <= p->num_rounds; r++) {
+    const unsigned rate = log_inv_rate + r * (k - 1);
+    const unsigned q = (2 * (security_bits - pow_bits) + rate - 1) / rate;
+    p->queries[r] = std::min(q, 4096u);
+  }
+  PK_REQUIRE(params_ok(p), "parameters give a codeword of one row");
+  return PKG_OK;
+}
+
+extern "C" size_t pkg_whir_commit_words(const pkg_whir_params* p) {
+  return p ? 4 + 4 * (size_t)p->ood_samples : 0;
+}
+
+extern "C" size_t pkg_whir_proof_words(const pkg_whir_params* p, size_t ncov) {
+  if (!params_ok(p)) return 0;
+  const size_t K = size_t(1) << p->folding_factor, k = p->folding_factor;
+  size_t w = 4 * ncov + 12 * k;
+  for (unsigned r = 0; r < p->num_rounds; r++)
+    w += 4 + 4 * (size_t)p->ood_samples + (p->pow_bits ? 1 : 0) +
+         (size_t)p->queries[r] * (4 * K + 4 * rows_log(p, r)) + 12 * k;
+  const unsigned R = p->num_rounds;
+  w += 4 * (size_t(1) << p->final_vars) + (p->final_pow_bits ? 1 : 0) +
+       (size_t)p->queries[R] * (4 * K + 4 * rows_log(p, R)) + 12 * (size_t)p->final_vars;
+  return w;
+}
+
+extern "C" int pkg_subset_transform(uint64_t* v, unsigned n, int mode, pkg_stream_t stream) {
+  PK_REQUIRE(n <= 34, "too many variables (%u)", n);
+  PK_REQUIRE(mode == PKG_SUBSET_ZETA || mode == PKG_SUBSET_MOBIUS_T, "unknown mode %d", mode);
+  PK_REQUIRE(v && aligned16(v), "null or unaligned table");
+  return mode == PKG_SUBSET_ZETA ? subset_transform_device<true>(v, n, as_stream(stream))
+                                 : subset_transform_device<false>(v, n, as_stream(stream));
+}
+
+extern "C" int pkg_whir_commit_ood(const pkg_whir_params* p, pkg_transcript* t,
+                                   const uint64_t* coeffs, const uint8_t* layers,
+                                   uint64_t* commit_words, uint64_t* ood_points,
+                                   pkg_stream_t stream) {
+  PK_REQUIRE(params_ok(p), "invalid WHIR parameters");
+  PK_REQUIRE(t && coeffs && layers && commit_words && (ood_points || !p->ood_samples),
+             "null pointer");
+  PK_REQUIRE(aligned16(coeffs) && aligned16(layers), "device buffers must be 16-byte aligned");
+  cudaStream_t s = as_stream(stream);
+  const size_t L = size_t(1) << rows_log(p, 0);
+  HostFr root;
+  PK_CUDA(cudaMemcpyAsync(root.l, layers + 32 * (2 * L - 2), 32, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  PK_REQUIRE(root.is_canonical(), "root digest is not a canonical field element");
+  const HostFr rm = HostFr::to_mont(root);
+  pkg_transcript_absorb(t, rm.l);
+  memcpy(commit_words, root.l, 32);
+  const unsigned o = p->ood_samples;
+  for (unsigned j = 0; j < o; j++) pkg_transcript_squeeze(t, ood_points + 4 * j);
+  if (o) {
+    int rc = pkg_poly_eval_many(coeffs, size_t(1) << p->num_variables, ood_points, o,
+                                commit_words + 4, stream);
+    if (rc) return rc;
+  }
+  for (unsigned j = 0; j < o; j++) pkg_transcript_absorb(t, commit_words + 4 + 4 * j);
+  return PKG_OK;
+}
+
+extern "C" int pkg_whir_prove(const pkg_whir_params* p, pkg_transcript* t, const uint64_t* coeffs,
+                              const uint64_t* codeword, const uint8_t* layers,
+                              const uint64_t* ood_points, const uint64_t* covectors, size_t ncov,
+                              uint64_t* proof, pkg_stream_t stream) {
+  PK_REQUIRE(params_ok(p), "invalid WHIR parameters");
+  PK_REQUIRE(ncov <= (size_t)kMaxCovectors, "at most %d covectors", kMaxCovectors);
+  PK_REQUIRE(t && coeffs && codeword && layers && proof && (covectors || !ncov) &&
+                 (ood_points || !p->ood_samples),
+             "null pointer");
+  PK_REQUIRE(aligned16(coeffs) && aligned16(codeword) && aligned16(layers) &&
+                 (!ncov || aligned16(covectors)),
+             "device buffers must be 16-byte aligned");
+  WhirProver prover(p, t, as_stream(stream), proof);
+  return prover.run(coeffs, codeword, layers, ood_points, covectors, ncov);
+}

@@ -113,3 +113,61 @@ def test_transcript_matches_oracle(L):
             b = np.zeros(4, np.uint64)
             O.lib().pko_transcript_squeeze(ctypes.byref(o), O.p64(b))
             assert np.array_equal(a, b)
+
+
+def test_whir_schedule_and_sizes_match_oracle(L):
+    """pkg_whir_params_init / pkg_whir_proof_words (host only) agree with the
+    oracle for every shape, and bad shapes are refused."""
+    from provekit_b200.whir import WhirParams
+    from provekit_b200._lib import PkgError
+    for n in range(1, 25):
+        for k in range(1, 7):
+            if k > n:
+                continue
+            for lr, sec, pw in ((1, 40, 0), (2, 128, 10), (3, 100, 20)):
+                try:
+                    p = WhirParams.new(n, k, lr, sec, pw)
+                except PkgError:
+                    po = O.WhirParams()
+                    assert O.lib().pko_whir_params_init(ctypes.byref(po), n, k, lr, sec, pw) != 0
+                    continue
+                po = O.whir_params(n, k, lr, sec, pw)
+                assert bytes(p) == bytes(po)
+                for ncov in (0, 3):
+                    assert p.proof_words(ncov) == O.lib().pko_whir_proof_words(
+                        ctypes.byref(po), ncov)
+                assert p.commit_words() == O.lib().pko_whir_commit_words(ctypes.byref(po))
+    bad = WhirParams.new(12, 3, 2, 64, 4)
+    bad.final_vars += 1
+    assert L.pkg_whir_proof_words(ctypes.byref(bad), 1) == 0
+    with pytest.raises(PkgError):
+        WhirParams.new(8, 7, 2, 64, 4)
+
+
+def test_transcript_bytes_match_oracle(L):
+    from provekit_b200.spartan import Transcript
+    from provekit_b200.whir import squeeze_bytes
+    for n in (0, 1, 30, 31, 32, 62, 100):
+        t = Transcript.new(9)
+        o = O.transcript(9)
+        out = np.zeros(max(n, 1), np.uint8)
+        O.lib().pko_transcript_squeeze_bytes(ctypes.byref(o), O.p8(out), n)
+        assert squeeze_bytes(t, n) == out[:n].tobytes()
+        assert list(t.l) == list(o.l) and list(t.r) == list(o.r)
+
+
+def test_whir_prove_validation_needs_no_device(L):
+    """Invalid parameters and null pointers are refused before any device work."""
+    from provekit_b200.whir import WhirParams
+    from provekit_b200._lib import PKG_ERR_INVALID_ARGUMENT
+    from provekit_b200.spartan import Transcript
+    p = WhirParams.new(10, 3, 2, 64, 4)
+    t = Transcript.new(1)
+    proof = np.zeros(p.proof_words(0), np.uint64)
+    assert L.pkg_whir_prove(ctypes.byref(p), ctypes.byref(t), None, None, None, None, None, 0,
+                            proof.ctypes.data, None) == PKG_ERR_INVALID_ARGUMENT
+    p.queries[0] = 0
+    assert L.pkg_whir_prove(ctypes.byref(p), ctypes.byref(t), 16, 16, 16, None, None, 0,
+                            proof.ctypes.data, None) == PKG_ERR_INVALID_ARGUMENT
+    assert L.pkg_subset_transform(None, 4, 0, None) == PKG_ERR_INVALID_ARGUMENT
+    assert L.pkg_subset_transform(16, 4, 7, None) == PKG_ERR_INVALID_ARGUMENT
