@@ -569,10 +569,10 @@ def run_prove(a):
     launches = L.pkg_kernel_launches() - launches0
     clk = clocks.stop()
     ms = [e[0].elapsed_time(e[1]) for e in evs]
-    stages = (ctypes.c_double * 5)()
+    stages = (ctypes.c_double * 6)()
     L.pkg_last_prove_stages(stages)
     stage_ms = dict(zip(["commit", "witness_bounds", "zk_sumcheck", "eq_alpha",
-                         "transposed_products"], list(stages)))
+                         "transposed_products", "whir_rounds"], list(stages)))
     # e2e: witness from pinned host memory each step, proof struct read back
     e2e = []
     with torch.cuda.stream(stream):

@@ -276,12 +276,19 @@ int pkg_spartan_prove(const pkg_r1cs *r1cs, const uint64_t *witness, uint64_t bl
                       pkg_spartan_proof *out, pkg_stream_t stream);
 
 /* Per-stage host wall-clock (ms) of the calling thread's last
- * pkg_spartan_prove: [0] commit (to the root), [1] witness bounds,
- * [2] zk sumcheck, [3] eq(alpha) + public weight, [4] transposed products and
- * evaluations.  Each stage ends with a stream synchronisation.  No
- * counterpart in the reference (diagnostics). */
-#define PKG_PROVE_STAGES 5
+ * pkg_spartan_prove or pkg_prove_r1cs: [0] commit (to the root, and the
+ * OOD answers), [1] witness bounds, [2] zk sumcheck, [3] eq(alpha) + public
+ * weight, [4] transposed products and evaluations, [5] the WHIR proof (0
+ * for pkg_spartan_prove).  Each stage ends with a stream synchronisation.
+ * No counterpart in the reference (diagnostics). */
+#define PKG_PROVE_STAGES 6
 int pkg_last_prove_stages(double ms[PKG_PROVE_STAGES]);
+
+/* WhirR1CSScheme::new_for_r1cs sizing (provekit/r1cs-compiler/src/whir_r1cs.rs:48-92):
+ * m = max(ceil log2 num_witnesses, 13), plus one when fewer than 4 m0 slots
+ * are free for the blinding coefficients; m0 = max(ceil log2
+ * num_constraints, 1).  Host only. */
+int pkg_r1cs_sizing(size_t num_constraints, size_t num_witnesses, size_t *m, size_t *m0);
 
 /* Synthetic satisfiable R1CS (host memory), the workload of the 2^20-constraint
  * prove benchmark: w[0] = 1, w[1..num_inputs] from pkg_sample_fr(seed); row
@@ -502,6 +509,20 @@ int pkg_whir_commit_ood(const pkg_whir_params *p, pkg_transcript *t, const uint6
 int pkg_whir_prove(const pkg_whir_params *p, pkg_transcript *t, const uint64_t *coeffs,
                    const uint64_t *codeword, const uint8_t *layers, const uint64_t *ood_points,
                    const uint64_t *covectors, size_t num_covectors, uint64_t *proof,
+                   pkg_stream_t stream);
+
+/* A whole proof (WhirR1CSProver::prove_noir with whir's prove,
+ * provekit/prover/src/whir_r1cs.rs:143-301): pkg_spartan_prove's work with
+ * whir's commitment OOD samples drawn right after the root
+ * (pkg_whir_commit_ood: whir_commit_words), then pkg_whir_prove of the three
+ * covectors A^T eq(alpha), B^T eq(alpha), C^T eq(alpha) (zero-padded to 2^m)
+ * against out->evals (whir_proof: pkg_whir_proof_words(whir, 3) words).
+ * whir: pkg_whir_params for pkg_r1cs_sizing's m (folding factor and rate
+ * are taken from it).  out->transcript is the state the WHIR prover starts
+ * from.  Synchronous. */
+int pkg_prove_r1cs(const pkg_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
+                   uint64_t transcript_domain, const pkg_whir_params *whir,
+                   pkg_spartan_proof *out, uint64_t *whir_commit_words, uint64_t *whir_proof,
                    pkg_stream_t stream);
 
 /* ---- field arithmetic (skyscraper/bn254-multiplier/src/scalar.rs:12-132,

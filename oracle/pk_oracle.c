@@ -938,14 +938,53 @@ static size_t ceil_log2(size_t n) { /* utils::next_power_of_two (utils/mod.rs:71
     return k;
 }
 
-int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
-                      uint64_t domain, unsigned ff, unsigned lr, pko_spartan_proof *out) {
-    const size_t nc = r1cs->num_constraints, nw = r1cs->num_witnesses, w1_size = nw;
-    size_t m = ceil_log2(w1_size), m0 = ceil_log2(nc);
+void pko_r1cs_sizing(size_t num_constraints, size_t num_witnesses, size_t *m_out, size_t *m0_out) {
+    size_t m = ceil_log2(num_witnesses), m0 = ceil_log2(num_constraints);
     if (m < 13) m = 13;                                   /* MIN_WHIR_NUM_VARIABLES */
     if (m0 < 1) m0 = 1;                                   /* MIN_SUMCHECK_NUM_VARIABLES */
-    if (((size_t)1 << m) - w1_size < 4 * m0) m++;
+    if (((size_t)1 << m) - num_witnesses < 4 * m0) m++;
+    *m_out = m;
+    *m0_out = m0;
+}
+
+int pko_r1cs_covectors(const pko_r1cs *r1cs, const uint64_t *alpha, size_t m0, size_t len,
+                       uint64_t *out) {
+    const size_t nc = r1cs->num_constraints, nw = r1cs->num_witnesses;
+    if (len < nw) return -1;
+    uint64_t *eq = (uint64_t *)calloc(nc ? nc : 1, 32);
+    if (!eq) return -2;
+    memset(out, 0, 32 * 3 * len);
+    pko_eq_hypercube(alpha, m0, nc, eq);
+    for (int k = 0; k < 3; k++) {
+        uint64_t *alph = out + 4 * len * (size_t)k;
+        for (size_t row = 0; row < nc; row++)
+            for (uint64_t e = r1cs->row_ptr[k][row]; e < r1cs->row_ptr[k][row + 1]; e++) {
+                uint64_t tt[4];
+                pko_fr_mul(tt, r1cs->vals[k] + 4 * e, eq + 4 * row);
+                size_t col = r1cs->cols[k][e];
+                pko_fr_add(alph + 4 * col, alph + 4 * col, tt);
+            }
+    }
+    free(eq);
+    return 0;
+}
+
+/* With whir == NULL the commitment's root alone enters the transcript and
+ * the proof ends at the covector evaluations; with whir, the commitment's
+ * OOD samples follow the root (pko_whir_commit_ood) and pko_whir_prove of
+ * the three zero-padded covectors M^T eq(alpha) ends it, on a copy of the
+ * transcript (out->transcript is the state the WHIR prover starts from). */
+static int spartan_prove_impl(const pko_r1cs *r1cs, const uint64_t *witness,
+                              uint64_t blinding_seed, uint64_t domain, unsigned ff, unsigned lr,
+                              pko_spartan_proof *out, const pko_whir_params *whir,
+                              uint64_t *whir_commit_words, uint64_t *whir_proof) {
+    const size_t nc = r1cs->num_constraints, nw = r1cs->num_witnesses, w1_size = nw;
+    size_t m, m0;
+    pko_r1cs_sizing(nc, nw, &m, &m0);
     if (m0 > 30 || m > 28 || ff > m) return -1;
+    if (whir && (whir->num_variables != m || whir->folding_factor != ff ||
+                 whir->log_inv_rate != lr || whir->ood_samples > 4))
+        return -1;
     memset(out, 0, sizeof *out);
     out->m = m;
     out->m0 = m0;
@@ -964,18 +1003,19 @@ int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t bl
     uint64_t *cw = (uint64_t *)malloc(32 * M * cw_len);
     uint8_t *layers = (uint8_t *)malloc(32 * (2 * cw_len - 1));
     if (!cw || !layers) return -2;
-    int rc = pko_rs_interleaved_encode(poly, M, L, poly, 0, cw_len, cw);
-    if (rc) return rc;
-    pko_from_mont_many(cw, M * cw_len);
-    rc = pko_merkle_tree((const uint8_t *)cw, 32 * M, cw_len, layers);
+    int rc = pko_whir_commit(poly, n, ff, lr, cw, layers);
     if (rc) return rc;
     memcpy(out->root, layers + 32 * (2 * cw_len - 2), 32);
-    free(cw);
-    free(layers);
-    uint64_t root_m[4];
-    memcpy(root_m, out->root, 32);
-    pko_fr_to_mont(root_m, root_m);
-    pko_transcript_absorb(t, root_m);
+    uint64_t ood_points[4 * 4];
+    if (whir) {
+        rc = pko_whir_commit_ood(whir, t, poly, out->root, whir_commit_words, ood_points);
+        if (rc) return rc;
+    } else {
+        uint64_t root_m[4];
+        memcpy(root_m, out->root, 32);
+        pko_fr_to_mont(root_m, root_m);
+        pko_transcript_absorb(t, root_m);
+    }
     /* witness bounds (sumcheck.rs:163-179) */
     size_t n0 = (size_t)1 << m0;
     uint64_t *a = (uint64_t *)calloc(n0, 32), *b = (uint64_t *)calloc(n0, 32), *cc = (uint64_t *)calloc(n0, 32);
@@ -991,29 +1031,38 @@ int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t bl
     /* eq(alpha) truncated to num_constraints, then M^T eq for A, B, C
      * (multiply_transposed_by_eq_alpha, sumcheck.rs:206-227): computed as
      * the scatter sum over the rows of M, which equals the transposed SpMV */
-    uint64_t *eq = (uint64_t *)calloc(nc ? nc : 1, 32);
-    uint64_t *alph = (uint64_t *)calloc(nw ? nw : 1, 32);
-    if (!eq || !alph) return -2;
-    pko_eq_hypercube(&out->alpha[0][0], m0, nc, eq);
+    uint64_t *cov = (uint64_t *)malloc(32 * 3 * n);
+    if (!cov) return -2;
     /* public weights (whir_r1cs.rs:665-676): hash of no public inputs is 0 */
     static const uint64_t zero[4] = {0, 0, 0, 0};
     pko_transcript_absorb(t, zero);
     pko_transcript_squeeze(t, out->public_x);
+    if ((rc = pko_r1cs_covectors(r1cs, &out->alpha[0][0], m0, n, cov))) return rc;
     for (int k = 0; k < 3; k++) {
-        memset(alph, 0, 32 * nw);
-        for (size_t row = 0; row < nc; row++)
-            for (uint64_t e = r1cs->row_ptr[k][row]; e < r1cs->row_ptr[k][row + 1]; e++) {
-                uint64_t tt[4];
-                pko_fr_mul(tt, r1cs->vals[k] + 4 * e, eq + 4 * row);
-                size_t col = r1cs->cols[k][e];
-                pko_fr_add(alph + 4 * col, alph + 4 * col, tt);
-            }
         /* create_weights_and_evaluations (:623-642): dot over the padded prefix */
-        pko_dot(out->evals[k], alph, poly, nw);
+        pko_dot(out->evals[k], cov + 4 * n * (size_t)k, poly, nw);
         pko_transcript_absorb(t, out->evals[k]);
     }
-    free(eq); free(alph); free(poly);
-    return 0;
+    if (whir) {
+        pko_transcript tw = *t;
+        rc = pko_whir_prove(whir, &tw, poly, cw, layers, whir_commit_words, ood_points, cov, 3,
+                            whir_proof);
+    }
+    free(cov); free(poly); free(cw); free(layers);
+    return rc;
+}
+
+int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
+                      uint64_t domain, unsigned ff, unsigned lr, pko_spartan_proof *out) {
+    return spartan_prove_impl(r1cs, witness, blinding_seed, domain, ff, lr, out, NULL, NULL, NULL);
+}
+
+int pko_prove_r1cs(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
+                   uint64_t domain, const pko_whir_params *whir, pko_spartan_proof *out,
+                   uint64_t *whir_commit_words, uint64_t *whir_proof) {
+    if (!whir || !whir_commit_words || !whir_proof) return -1;
+    return spartan_prove_impl(r1cs, witness, blinding_seed, domain, whir->folding_factor,
+                              whir->log_inv_rate, out, whir, whir_commit_words, whir_proof);
 }
 
 /* ======================================================================= */

@@ -244,6 +244,30 @@ int pko_whir_prove(const pko_whir_params *p, pko_transcript *t, const uint64_t *
 int pko_whir_verify(const pko_whir_params *p, pko_transcript *t, const uint64_t *covectors,
                     size_t ncov, const uint64_t *commit_words, const uint64_t *proof,
                     size_t proof_words);
+/* The two halves of pko_whir_verify, for a transcript that carries other
+ * messages between the commitment and the proof: the commitment's part
+ * (root, OOD points into ood_points, answers), then the proof's. */
+int pko_whir_verify_commit(const pko_whir_params *p, pko_transcript *t,
+                           const uint64_t *commit_words, uint64_t *ood_points);
+int pko_whir_verify_proof(const pko_whir_params *p, pko_transcript *t, const uint64_t *covectors,
+                          size_t ncov, const uint64_t *commit_words, const uint64_t *ood_points,
+                          const uint64_t *proof, size_t proof_words);
+
+/* The three covectors A^T eq(alpha), B^T eq(alpha), C^T eq(alpha)
+ * (multiply_transposed_by_eq_alpha, provekit/common/src/utils/sumcheck.rs:206-227),
+ * eq truncated to num_constraints, each zero-padded to len entries: out is
+ * 3 x len Fr.  Computed as the scatter sum over the rows of M. */
+int pko_r1cs_covectors(const pko_r1cs *r1cs, const uint64_t *alpha, size_t m0, size_t len,
+                       uint64_t *out);
+/* WhirR1CSScheme::new_for_r1cs sizing (provekit/r1cs-compiler/src/whir_r1cs.rs:48-92). */
+void pko_r1cs_sizing(size_t num_constraints, size_t num_witnesses, size_t *m, size_t *m0);
+/* A whole proof: pko_spartan_prove with the commitment's OOD samples drawn
+ * after its root and the WHIR proof of the three zero-padded covectors
+ * M^T eq(alpha) against their evaluations; whir->num_variables must be the
+ * sizing's m.  out->transcript is the state the WHIR prover starts from. */
+int pko_prove_r1cs(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
+                   uint64_t domain, const pko_whir_params *whir, pko_spartan_proof *out,
+                   uint64_t *whir_commit_words, uint64_t *whir_proof);
 
 int pko_num_threads(void);
 

@@ -562,9 +562,33 @@ typedef struct {
     uint64_t *pts, *coef;
 } round_claims;
 
+int pko_whir_verify_commit(const pko_whir_params *p, pko_transcript *t,
+                           const uint64_t *commit_words, uint64_t *ood_points) {
+    if (!params_ok(p)) return PKO_WHIR_BAD_PARAMS;
+    uint64_t rm[4];
+    if (!is_canon(commit_words)) return PKO_WHIR_REJECT_FORMAT;
+    pko_fr_to_mont(rm, commit_words);
+    pko_transcript_absorb(t, rm);
+    for (unsigned j = 0; j < p->ood_samples; j++) pko_transcript_squeeze(t, ood_points + 4 * j);
+    for (unsigned j = 0; j < p->ood_samples; j++) {
+        if (!is_canon(commit_words + 4 + 4 * j)) return PKO_WHIR_REJECT_FORMAT;
+        pko_transcript_absorb(t, commit_words + 4 + 4 * j);
+    }
+    return 0;
+}
+
 int pko_whir_verify(const pko_whir_params *p, pko_transcript *t, const uint64_t *covectors,
                     size_t ncov, const uint64_t *commit_words, const uint64_t *proof,
                     size_t proof_words) {
+    uint64_t z[4 * 4];
+    int rc = pko_whir_verify_commit(p, t, commit_words, z);
+    if (rc) return rc;
+    return pko_whir_verify_proof(p, t, covectors, ncov, commit_words, z, proof, proof_words);
+}
+
+int pko_whir_verify_proof(const pko_whir_params *p, pko_transcript *t, const uint64_t *covectors,
+                          size_t ncov, const uint64_t *commit_words, const uint64_t *ood_points,
+                          const uint64_t *proof, size_t proof_words) {
     if (!params_ok(p) || ncov > 16) return PKO_WHIR_BAD_PARAMS;
     if (proof_words != pko_whir_proof_words(p, ncov)) return PKO_WHIR_REJECT_FORMAT;
     const unsigned n = p->num_variables, k = p->folding_factor, R = p->num_rounds;
@@ -586,22 +610,9 @@ int pko_whir_verify(const pko_whir_params *p, pko_transcript *t, const uint64_t 
         rc = -2;
         goto done;
     }
-    /* commitment: root, OOD */
+    /* the commitment's root and OOD points (pko_whir_verify_commit) */
     cp4(root, commit_words);
-    if (!is_canon(root)) {
-        rc = PKO_WHIR_REJECT_FORMAT;
-        goto done;
-    }
-    pko_fr_to_mont(rm, root);
-    pko_transcript_absorb(t, rm);
-    for (unsigned j = 0; j < o; j++) pko_transcript_squeeze(t, z0 + 4 * j);
-    for (unsigned j = 0; j < o; j++) {
-        if (!is_canon(commit_words + 4 + 4 * j)) {
-            rc = PKO_WHIR_REJECT_FORMAT;
-            goto done;
-        }
-        pko_transcript_absorb(t, commit_words + 4 + 4 * j);
-    }
+    if (o) memcpy(z0, ood_points, 32 * o);
     /* statement values and the initial claimed sum */
     uint64_t vals[16 * 4];
     for (size_t a = 0; a < ncov; a++) {

@@ -1,7 +1,9 @@
 // prove.cu -- pkg_spartan_prove: the Spartan prover's work up to WHIR's own
 // prove rounds, device-resident from the witness to the covector
 // evaluations (provekit/prover/src/whir_r1cs.rs:82-301,
-// provekit/r1cs-compiler/src/whir_r1cs.rs:48-92).
+// provekit/r1cs-compiler/src/whir_r1cs.rs:48-92); pkg_prove_r1cs: the same
+// with whir's commitment OOD samples and the WHIR proof (pkg_whir_prove) of
+// the covector evaluations, a whole proof.
 //
 // Device data: the padded witness polynomial (2^m Fr), its RS codeword and
 // Merkle layers, the a/b/c sumcheck tables (2^m0 Fr each), eq(alpha), the
@@ -52,20 +54,42 @@ extern "C" int pkg_last_prove_stages(double ms[PKG_PROVE_STAGES]) {
   return PKG_OK;
 }
 
-extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
-                                 uint64_t blinding_seed, uint64_t transcript_domain,
-                                 unsigned ff, unsigned lr, pkg_spartan_proof* out,
-                                 pkg_stream_t stream) {
+extern "C" int pkg_r1cs_sizing(size_t num_constraints, size_t num_witnesses, size_t* m_out,
+                               size_t* m0_out) {
+  PK_REQUIRE(m_out && m0_out, "null output");
+  PK_REQUIRE(num_constraints >= 1 && num_witnesses >= 1, "empty R1CS");
+  size_t m = ceil_log2(num_witnesses), m0 = ceil_log2(num_constraints);
+  if (m < 13) m = 13;  // MIN_WHIR_NUM_VARIABLES
+  if (m0 < 1) m0 = 1;  // MIN_SUMCHECK_NUM_VARIABLES
+  if ((size_t(1) << m) - num_witnesses < 4 * m0) m++;
+  *m_out = m;
+  *m0_out = m0;
+  return PKG_OK;
+}
+
+// With whir == nullptr the commitment's root alone enters the transcript and
+// the proof ends at the covector evaluations (pkg_spartan_prove); with whir,
+// the commitment's OOD samples follow the root and the WHIR proof of the
+// three zero-padded covectors ends it (pkg_prove_r1cs).
+static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
+                              uint64_t blinding_seed, uint64_t transcript_domain, unsigned ff,
+                              unsigned lr, pkg_spartan_proof* out, const pkg_whir_params* whir,
+                              uint64_t* whir_commit_words, uint64_t* whir_proof,
+                              pkg_stream_t stream) {
   PK_REQUIRE(r1cs && witness && out, "null pointer");
   PK_REQUIRE(aligned16(witness), "witness must be 16-byte aligned");
   const size_t nc = r1cs->num_constraints, nw = r1cs->num_witnesses, w1_size = nw;
-  PK_REQUIRE(nc >= 1 && nw >= 1, "empty R1CS");
-  size_t m = ceil_log2(w1_size), m0 = ceil_log2(nc);
-  if (m < 13) m = 13;  // MIN_WHIR_NUM_VARIABLES
-  if (m0 < 1) m0 = 1;  // MIN_SUMCHECK_NUM_VARIABLES
-  if ((size_t(1) << m) - w1_size < 4 * m0) m++;
+  size_t m = 0, m0 = 0;
+  int rc = pkg_r1cs_sizing(nc, nw, &m, &m0);
+  if (rc) return rc;
   PK_REQUIRE(m0 <= 30 && m <= 28 && ff <= m && lr <= 8, "instance too large (m=%zu, m0=%zu)", m,
              m0);
+  if (whir) {
+    PK_REQUIRE(whir_commit_words && whir_proof, "null WHIR output");
+    PK_REQUIRE(pkg_whir_proof_words(whir, 3) != 0, "invalid WHIR parameters");
+    PK_REQUIRE(whir->num_variables == m, "WHIR parameters for %u variables, the R1CS needs %zu",
+               whir->num_variables, m);
+  }
   memset(out, 0, sizeof *out);
   memset(g_stage_ms, 0, sizeof g_stage_ms);
   StageClock clk;
@@ -73,7 +97,7 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
   out->m0 = m0;
   cudaStream_t s = as_stream(stream);
   const uint64_t dom[4] = {transcript_domain, 0, 0, 0};
-  int rc = pkg_transcript_init(&out->transcript, dom);
+  rc = pkg_transcript_init(&out->transcript, dom);
   if (rc) return rc;
 
   // ---- commit (whir_r1cs.rs:82-140)
@@ -99,7 +123,13 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
   if ((rc = merkle_tree_fr_device(cw, M, cw_len, PKG_LEAF_CANONICAL, layers, s))) return rc;
   PK_CUDA(cudaMemcpyAsync(out->root, layers + 32 * (2 * cw_len - 2), 32, cudaMemcpyDeviceToHost, s));
   PK_CUDA(cudaStreamSynchronize(s));
-  {
+  uint64_t ood_points[4 * 4];
+  if (whir) {
+    // whir's commit: the root, then the OOD samples of the committed polynomial
+    if ((rc = pkg_whir_commit_ood(whir, &out->transcript, poly, layers, whir_commit_words,
+                                  ood_points, stream)))
+      return rc;
+  } else {
     HostFr root = HostFr::to_mont(HostFr::from_limbs(reinterpret_cast<const uint64_t*>(out->root)));
     pkg_transcript_absorb(&out->transcript, root.l);
   }
@@ -137,11 +167,14 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
   clk.mark(2);
 
   // ---- eq(alpha) and the transposed products (sumcheck.rs:195-227)
+  // the covectors: one nw-entry buffer, or (for the WHIR proof) three
+  // zero-padded 2^m-entry ones
   Scratch s_eq, s_alph;
   if ((rc = s_eq.alloc(32 * nc, s))) return rc;
-  if ((rc = s_alph.alloc(32 * nw, s))) return rc;
+  if ((rc = s_alph.alloc(32 * (whir ? 3 * n : nw), s))) return rc;
   uint64_t* eq = static_cast<uint64_t*>(s_eq.ptr);
-  uint64_t* alph = static_cast<uint64_t*>(s_alph.ptr);
+  uint64_t* cov = static_cast<uint64_t*>(s_alph.ptr);
+  if (whir) PK_CUDA(cudaMemsetAsync(cov, 0, 32 * 3 * n, s));
   if ((rc = eq_hypercube_device(&out->alpha[0][0], m0, nc, eq, s))) return rc;
   // public weights (whir_r1cs.rs:665-676): the hash of no public inputs is 0
   const uint64_t zero[4] = {0, 0, 0, 0};
@@ -149,6 +182,7 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
   pkg_transcript_squeeze(&out->transcript, out->public_x);
   clk.mark(3);
   for (int k = 0; k < 3; k++) {
+    uint64_t* alph = whir ? cov + 4 * n * (size_t)k : cov;
     Scratch s_t;
     const size_t nnz = r1cs->nnz[k];
     const size_t rp_bytes = ((8 * (nw + 1) + 255) / 256) * 256;
@@ -169,5 +203,31 @@ extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
     pkg_transcript_absorb(&out->transcript, out->evals[k]);
   }
   clk.mark(4);
+  if (whir) {
+    // whir's prove of <alpha_k, w> = evals[k]; out->transcript keeps the
+    // state the WHIR prover starts from
+    pkg_transcript tw = out->transcript;
+    if ((rc = pkg_whir_prove(whir, &tw, poly, cw, layers, ood_points, cov, 3, whir_proof, stream)))
+      return rc;
+    clk.mark(5);
+  }
   return PKG_OK;
+}
+
+extern "C" int pkg_spartan_prove(const pkg_r1cs* r1cs, const uint64_t* witness,
+                                 uint64_t blinding_seed, uint64_t transcript_domain,
+                                 unsigned ff, unsigned lr, pkg_spartan_proof* out,
+                                 pkg_stream_t stream) {
+  return spartan_prove_impl(r1cs, witness, blinding_seed, transcript_domain, ff, lr, out, nullptr,
+                            nullptr, nullptr, stream);
+}
+
+extern "C" int pkg_prove_r1cs(const pkg_r1cs* r1cs, const uint64_t* witness,
+                              uint64_t blinding_seed, uint64_t transcript_domain,
+                              const pkg_whir_params* whir, pkg_spartan_proof* out,
+                              uint64_t* whir_commit_words, uint64_t* whir_proof,
+                              pkg_stream_t stream) {
+  PK_REQUIRE(whir, "null WHIR parameters");
+  return spartan_prove_impl(r1cs, witness, blinding_seed, transcript_domain, whir->folding_factor,
+                            whir->log_inv_rate, out, whir, whir_commit_words, whir_proof, stream);
 }

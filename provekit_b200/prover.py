@@ -1,5 +1,6 @@
-"""Prover-level entry points: the synthetic R1CS workload and the Spartan
-prove core (provekit/prover/src/whir_r1cs.rs up to WHIR's prove call)."""
+"""Prover-level entry points: the synthetic R1CS workload, the Spartan
+prove core (provekit/prover/src/whir_r1cs.rs up to WHIR's prove call) and
+the whole proof with WHIR's rounds (pkg_prove_r1cs)."""
 import ctypes
 
 import numpy as np
@@ -86,3 +87,35 @@ def spartan_prove(r1cs: DeviceR1CS, witness=None, blinding_seed=1, transcript_do
                                   transcript_domain, folding_factor, log_inv_rate,
                                   ctypes.byref(out), s))
     return out.as_dict()
+
+
+def r1cs_sizing(num_constraints: int, num_witnesses: int):
+    """(m, m0) of WhirR1CSScheme::new_for_r1cs."""
+    m, m0 = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    check(lib().pkg_r1cs_sizing(num_constraints, num_witnesses, ctypes.byref(m), ctypes.byref(m0)))
+    return m.value, m0.value
+
+
+def whir_params_for(r1cs, folding_factor=3, log_inv_rate=2, security_bits=128, pow_bits=10,
+                    **overrides):
+    """The WHIR parameters of the R1CS's witness commitment (by default the
+    reference's: provekit/r1cs-compiler/src/whir_r1cs.rs:103-118)."""
+    from .whir import WhirParams
+    m, _ = r1cs_sizing(r1cs.num_constraints, r1cs.num_witnesses)
+    return WhirParams.new(m, folding_factor, log_inv_rate, security_bits, pow_bits, **overrides)
+
+
+def prove_r1cs(r1cs: DeviceR1CS, whir=None, witness=None, blinding_seed=1, transcript_domain=3,
+               stream=None):
+    """pkg_prove_r1cs: a whole proof.  Returns (spartan fields dict,
+    WHIR commitment words, WHIR proof words)."""
+    p = whir_params_for(r1cs) if whir is None else whir
+    w = r1cs.witness if witness is None else witness
+    out = SpartanProofC()
+    cwords = np.zeros(p.commit_words(), np.uint64)
+    proof = np.zeros(p.proof_words(3), np.uint64)
+    s = (stream if stream is not None else torch.cuda.current_stream()).cuda_stream
+    check(lib().pkg_prove_r1cs(ctypes.byref(r1cs.c), w.data_ptr(), blinding_seed,
+                               transcript_domain, ctypes.byref(p), ctypes.byref(out),
+                               cwords.ctypes.data, proof.ctypes.data, s))
+    return out.as_dict(), cwords, proof

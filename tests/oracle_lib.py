@@ -36,16 +36,67 @@ class SpartanProof(ctypes.Structure):
                 ("transcript", Transcript)]
 
 
+def _r1cs_c(h):
+    return R1CS(h.num_constraints, h.num_witnesses,
+                (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.row_ptr]),
+                (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.cols]),
+                (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.vals]))
+
+
 def spartan_prove(h, blinding_seed, domain, ff, lr):
     """Run pko_spartan_prove on a HostR1CS-like object; returns the proof dict."""
-    r = R1CS(h.num_constraints, h.num_witnesses,
-             (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.row_ptr]),
-             (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.cols]),
-             (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.vals]))
+    r = _r1cs_c(h)
     out = SpartanProof()
     rc = lib().pko_spartan_prove(ctypes.byref(r), p64(np.ascontiguousarray(h.witness)), blinding_seed,
                                  domain, ff, lr, ctypes.byref(out))
     assert rc == 0, rc
+    return _spartan_dict(out)
+
+
+def r1cs_sizing(nc, nw):
+    m, m0 = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    lib().pko_r1cs_sizing(nc, nw, ctypes.byref(m), ctypes.byref(m0))
+    return m.value, m0.value
+
+
+def prove_r1cs(h, blinding_seed, domain, wp):
+    """pko_prove_r1cs: (spartan dict, WHIR commitment words, WHIR proof)."""
+    r = _r1cs_c(h)
+    out = SpartanProof()
+    cwords = np.zeros(lib().pko_whir_commit_words(ctypes.byref(wp)), np.uint64)
+    proof = np.zeros(lib().pko_whir_proof_words(ctypes.byref(wp), 3), np.uint64)
+    rc = lib().pko_prove_r1cs(ctypes.byref(r), p64(np.ascontiguousarray(h.witness)), blinding_seed,
+                              domain, ctypes.byref(wp), ctypes.byref(out), p64(cwords), p64(proof))
+    assert rc == 0, rc
+    return _spartan_dict(out), cwords, proof
+
+
+def r1cs_covectors(h, alpha, m0, length):
+    out = np.zeros((3 * length, 4), np.uint64)
+    rc = lib().pko_r1cs_covectors(ctypes.byref(_r1cs_c(h)), p64(np.ascontiguousarray(alpha)), m0,
+                                  length, p64(out))
+    assert rc == 0
+    return out
+
+
+def verify_r1cs_whir(h, wp, domain, spartan, cwords, proof):
+    """The WHIR part of a whole proof: the commitment half on a fresh
+    transcript, the proof half from the state the WHIR prover started from."""
+    t0 = transcript(domain)
+    z = np.zeros((4, 4), np.uint64)
+    rc = lib().pko_whir_verify_commit(ctypes.byref(wp), ctypes.byref(t0), p64(cwords), p64(z))
+    if rc:
+        return rc
+    t = Transcript()
+    l, r = spartan["transcript"]
+    t.l[:] = l
+    t.r[:] = r
+    cov = r1cs_covectors(h, spartan["alpha"], spartan["m0"], 1 << spartan["m"])
+    return lib().pko_whir_verify_proof(ctypes.byref(wp), ctypes.byref(t), p64(cov), 3, p64(cwords),
+                                       p64(z), p64(np.ascontiguousarray(proof)), proof.shape[0])
+
+
+def _spartan_dict(out):
     m0 = out.m0
     arr = lambda x, n: np.array(x[: 4 * n], dtype=np.uint64).reshape(n, 4)  # noqa: E731
     return {"m": out.m, "m0": m0, "root": bytes(out.root), "r": arr(out.r, m0),
@@ -125,6 +176,12 @@ def lib():
         L.pko_whir_commit_ood.argtypes = [wp, tp, _u64p, _u8p, _u64p, _u64p]
         L.pko_whir_prove.argtypes = [wp, tp, _u64p, _u64p, _u8p, _u64p, _u64p, _u64p, _sz, _u64p]
         L.pko_whir_verify.argtypes = [wp, tp, _u64p, _sz, _u64p, _u64p, _sz]
+        L.pko_whir_verify_commit.argtypes = [wp, tp, _u64p, _u64p]
+        L.pko_whir_verify_proof.argtypes = [wp, tp, _u64p, _sz, _u64p, _u64p, _u64p, _sz]
+        L.pko_r1cs_sizing.argtypes = [_sz, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]
+        L.pko_r1cs_covectors.argtypes = [ctypes.c_void_p, _u64p, _sz, _sz, _u64p]
+        L.pko_prove_r1cs.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_uint64, wp,
+                                     ctypes.c_void_p, _u64p, _u64p]
     return _lib
 
 

@@ -1,7 +1,9 @@
 """GPU parity of the Spartan prove core (pkg_spartan_prove) against the
 oracle's pko_spartan_prove on synthetic satisfiable R1CS instances, up to the
 2^20-constraint prove workload: root, every sumcheck message and challenge,
-covector evaluations and the final transcript state must be identical."""
+covector evaluations and the final transcript state must be identical.  The
+whole proof (pkg_prove_r1cs, with the WHIR rounds) must equal the oracle's
+word for word and its WHIR part verify."""
 import numpy as np
 import pytest
 import torch
@@ -47,9 +49,44 @@ def test_stage_timers_and_memory_trim_keep_results():
     h = HostR1CS(77, 1 << 14, 1 << 12)
     d = h.to_device()
     first = spartan_prove(d, blinding_seed=3, transcript_domain=4)
-    stages = (ctypes.c_double * 5)()
+    stages = (ctypes.c_double * 6)()
     check(lib().pkg_last_prove_stages(stages))
-    assert all(v > 0 for v in stages), list(stages)
+    assert all(v > 0 for v in stages[:5]) and stages[5] == 0, list(stages)
     check(lib().pkg_trim_memory(0))
     again = spartan_prove(d, blinding_seed=3, transcript_domain=4)
     assert_same(again, first)
+
+
+@pytest.mark.parametrize("log_nc,log_ni,sec,pw", [(10, 8, 40, 3), (12, 11, 64, 5), (14, 12, 128, 10)])
+def test_whole_proof_matches_oracle_and_verifies(log_nc, log_ni, sec, pw):
+    import ctypes
+    from provekit_b200._lib import check, lib
+    from provekit_b200.prover import HostR1CS, prove_r1cs, whir_params_for
+    h = HostR1CS(300 + log_nc, 1 << log_nc, 1 << log_ni)
+    d = h.to_device()
+    p = whir_params_for(d, 3, 2, sec, pw)
+    sp, cw, proof = prove_r1cs(d, p, blinding_seed=6, transcript_domain=12)
+    stages = (ctypes.c_double * 6)()
+    check(lib().pkg_last_prove_stages(stages))
+    assert all(v > 0 for v in stages), list(stages)
+    wp = O.whir_params(sp["m"], 3, 2, sec, pw)
+    assert bytes(wp) == bytes(p)
+    esp, ecw, eproof = O.prove_r1cs(h, 6, 12, wp)
+    assert_same(sp, esp)
+    assert np.array_equal(cw, ecw)
+    assert np.array_equal(proof, eproof)
+    assert O.verify_r1cs_whir(h, wp, 12, sp, cw, proof) == 0
+
+
+def test_whole_proof_at_2p20_constraints_verifies():
+    """The prove workload's instance (2^20 constraints, 2^18 inputs, m = 21)
+    with the reference's WHIR configuration: the oracle verifier accepts the
+    device proof (the oracle prover is not run at this size)."""
+    from provekit_b200.prover import HostR1CS, prove_r1cs, whir_params_for
+    h = HostR1CS(3, 1 << 20, 1 << 18)
+    d = h.to_device()
+    p = whir_params_for(d)
+    assert (p.num_variables, p.folding_factor, p.log_inv_rate, p.pow_bits) == (21, 3, 2, 10)
+    sp, cw, proof = prove_r1cs(d, p, blinding_seed=1, transcript_domain=3)
+    wp = O.whir_params(21, 3, 2, 128, 10)
+    assert O.verify_r1cs_whir(h, wp, 3, sp, cw, proof) == 0

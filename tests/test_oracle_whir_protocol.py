@@ -261,3 +261,29 @@ def test_squeeze_bytes_takes_31_bytes_per_element():
         O.lib().pko_fr_from_mont(O.p64(c), O.p64(m))
         exp += c.tobytes()[:31]
     assert out.tobytes() == exp[:70]
+
+
+@pytest.mark.parametrize("nc,ni", [(1 << 10, 1 << 8), (3000, 500), (1 << 12, 1 << 12)])
+def test_whole_r1cs_proof_verifies(nc, ni):
+    """pko_prove_r1cs: the Spartan part, then the WHIR proof of the three
+    covectors M^T eq(alpha) against the evaluations; the WHIR part verifies
+    from the transcript state the prover started it from, and the
+    evaluations are the covectors' dot products with the padded witness."""
+    from provekit_b200.prover import HostR1CS
+    h = HostR1CS(nc + ni, nc, ni)
+    m, m0 = O.r1cs_sizing(h.num_constraints, h.num_witnesses)
+    wp = O.whir_params(m, 3, 2, 40, 3)
+    sp, cw, proof = O.prove_r1cs(h, 5, 11, wp)
+    assert (sp["m"], sp["m0"]) == (m, m0)
+    assert O.verify_r1cs_whir(h, wp, 11, sp, cw, proof) == 0
+    cov = O.r1cs_covectors(h, sp["alpha"], m0, 1 << m)
+    for k in range(3):
+        assert np.array_equal(proof[4 * k:4 * k + 4], sp["evals"][k])
+        d = np.zeros(4, np.uint64)
+        O.lib().pko_dot(O.p64(d), O.p64(np.ascontiguousarray(cov[k << m:(k << m) + h.num_witnesses])),
+                        O.p64(np.ascontiguousarray(h.witness)), h.num_witnesses)
+        assert np.array_equal(d, sp["evals"][k])
+    # the WHIR part is bound to the Spartan transcript
+    bad = dict(sp)
+    bad["transcript"] = (list(sp["transcript"][1]), list(sp["transcript"][0]))
+    assert O.verify_r1cs_whir(h, wp, 11, bad, cw, proof) != 0
