@@ -574,6 +574,10 @@ def run_prove(a):
     L.pkg_last_prove_stages(stages)
     stage_ms = dict(zip(["commit", "witness_bounds", "zk_sumcheck", "eq_alpha",
                          "transposed_products", "whir_rounds"], list(stages)))
+    wst = (ctypes.c_double * 8)()
+    L.pkg_last_whir_stages(wst)
+    whir_ms = dict(zip(["setup", "sumcheck", "fold_commit", "ood", "pow", "stir_openings",
+                        "weight_updates", "final_poly"], list(wst)))
     # the Spartan part alone (the work before whir's prove call)
     core = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
     with torch.cuda.stream(stream):
@@ -620,7 +624,7 @@ def run_prove(a):
                     "d2h_bytes_per_step": proof_bytes + 32 * (3 + 4 * 20 + 2 * 20 + 8),
                     "note": "wall clock, witness copied from pinned host memory every step"},
             "p50_ms": statistics.median(ms), "stages_ms_last_step": stage_ms,
-            "spartan_core_ms": core_ms,
+            "whir_phases_ms_last_step": whir_ms, "spartan_core_ms": core_ms,
             "cpu_baseline": cpu, "gpu_launches": int(launches),
             "clocks": clk}
     print(json.dumps(line), flush=True)

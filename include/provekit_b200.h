@@ -510,6 +510,14 @@ int pkg_whir_prove(const pkg_whir_params *p, pkg_transcript *t, const uint64_t *
                    const uint64_t *codeword, const uint8_t *layers, const uint64_t *ood_points,
                    const uint64_t *covectors, size_t num_covectors, uint64_t *proof,
                    pkg_stream_t stream);
+/* Per-phase host wall-clock (ms) of the calling thread's last WHIR prove:
+ * [0] set-up (subset transforms, statement values, weight table), [1]
+ * sumcheck rounds, [2] folds + commitments + roots, [3] OOD answers, [4] PoW,
+ * [5] STIR openings, [6] weight updates, [7] the final polynomial.  A phase
+ * that ends without a synchronisation leaves its device time to the next
+ * one that synchronises.  Diagnostics; no reference counterpart. */
+#define PKG_WHIR_STAGES 8
+int pkg_last_whir_stages(double ms[PKG_WHIR_STAGES]);
 
 /* A whole proof (WhirR1CSProver::prove_noir with whir's prove,
  * provekit/prover/src/whir_r1cs.rs:143-301): pkg_spartan_prove's work with

@@ -93,6 +93,7 @@ SIGNATURES = {
     "pkg_r1cs_sizing": [_c_sz, _c_sz, _c_vp, _c_vp],
     "pkg_prove_r1cs": [_c_vp, _c_vp, ctypes.c_uint64, ctypes.c_uint64, _c_vp, _c_vp, _c_vp, _c_vp,
                        _c_vp],
+    "pkg_last_whir_stages": [_c_vp],
     "pkg_whir_params_init": [_c_vp, _c_uint, _c_uint, _c_uint, _c_uint, _c_uint],
     "pkg_transcript_squeeze_bytes": [_c_vp, _c_vp, _c_sz],
     "pkg_subset_transform": [_c_vp, _c_uint, _c_int, _c_vp],

@@ -142,8 +142,12 @@ struct HostFr {
     return acc;
   }
   static HostFr pow_u64(const HostFr& base, uint64_t e) {
-    const uint64_t ee[4] = {e, 0, 0, 0};
-    return pow(base, ee);
+    HostFr acc = one(), b = base;
+    for (; e; e >>= 1) {
+      if (e & 1) acc = mul(acc, b);
+      b = mul(b, b);
+    }
+    return acc;
   }
   static HostFr inv(const HostFr& a) {
     uint64_t e[4] = {P[0] - 2, P[1], P[2], P[3]};

@@ -5,6 +5,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "../../include/provekit_b200.h"
+
 namespace pk {
 
 int merkle_tree_fr_device(const uint64_t* cw, size_t fr_per_leaf, size_t num_leaves, int encoding,
@@ -17,7 +19,22 @@ int eq_hypercube_device(const uint64_t* r_host, size_t nr, size_t num_entries, u
 // Skyscraper PoW on stream s (synchronous): generic::solve's answer.
 int pow_solve_device(const uint64_t challenge[4], const uint64_t threshold[4], cudaStream_t s,
                      uint64_t* nonce_out);
+// w += sum_j coeffs_j eq(points_j, .) (pkg_eq_accumulate); sync = false only
+// when points and coeffs are pageable host memory.
+int eq_accumulate_device(uint64_t* w, size_t nv, const uint64_t* points, const uint64_t* coeffs,
+                         size_t npts, cudaStream_t s, bool sync);
+// Codeword rows and their Merkle paths for nq indices (host in/out), one sync.
+int open_rows_device(const uint64_t* codeword, size_t fr_per_row, size_t num_rows,
+                     const uint8_t* layers, const uint64_t* indices, size_t nq, uint64_t* rows,
+                     uint8_t* paths, cudaStream_t s);
 int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* d_out, uint64_t* part,
                cudaStream_t s);
+
+// The WHIR prover's round loop (pkg_whir_prove); values (host, ncov Fr) are
+// the statements' values when the caller already has them, else nullptr.
+int whir_prove_device(const pkg_whir_params* p, pkg_transcript* t, const uint64_t* coeffs,
+                      const uint64_t* codeword, const uint8_t* layers, const uint64_t* ood_points,
+                      const uint64_t* covectors, size_t ncov, const uint64_t* values,
+                      uint64_t* proof, cudaStream_t s);
 
 }  // namespace pk

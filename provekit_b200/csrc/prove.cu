@@ -207,7 +207,8 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     // whir's prove of <alpha_k, w> = evals[k]; out->transcript keeps the
     // state the WHIR prover starts from
     pkg_transcript tw = out->transcript;
-    if ((rc = pkg_whir_prove(whir, &tw, poly, cw, layers, ood_points, cov, 3, whir_proof, stream)))
+    if ((rc = whir_prove_device(whir, &tw, poly, cw, layers, ood_points, cov, 3, &out->evals[0][0],
+                                whir_proof, s)))
       return rc;
     clk.mark(5);
   }

@@ -138,6 +138,10 @@ extern "C" int pkg_rs_evaluation_points(size_t codeword_length, const size_t* in
              "no root of unity of order %zu", codeword_length);
   int bits = log2_exact(codeword_length);
   HostFr g = HostFr::root_of_unity(codeword_length);
+  // g^(2^b) for b < bits: a point is then at most `bits` products
+  HostFr sq[64];
+  sq[0] = g;
+  for (int b = 1; b < bits; b++) sq[b] = HostFr::mul(sq[b - 1], sq[b - 1]);
   for (size_t x = 0; x < n; x++) {
     size_t i = indices[x];
     size_t k = i;
@@ -145,8 +149,12 @@ extern "C" int pkg_rs_evaluation_points(size_t codeword_length, const size_t* in
       size_t r = 0;
       for (int b = 0; b < 64; b++) r |= ((i >> b) & 1) << (63 - b);
       k = r >> (64 - bits);
+    } else {
+      k = 0;  // g = 1: every power is 1
     }
-    HostFr v = HostFr::pow_u64(g, k);
+    HostFr v = HostFr::one();
+    for (int b = 0; b < bits; b++)
+      if ((k >> b) & 1) v = HostFr::mul(v, sq[b]);
     memcpy(out + 4 * x, v.l, 32);
   }
   return PKG_OK;

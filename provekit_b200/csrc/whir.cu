@@ -21,6 +21,7 @@
 #include "fr.cuh"
 #include "fr_f64.cuh"
 #include "fr_host.hpp"
+#include "internal.cuh"
 #include "pk_common.cuh"
 #include "reduce.cuh"
 
@@ -319,6 +320,42 @@ extern "C" int pkg_gather_rows(const uint64_t* codeword, size_t fr_per_row, size
   return PKG_OK;
 }
 
+namespace pk {
+// pkg_gather_rows + pkg_merkle_open of the same indices with one upload and
+// one synchronisation.
+int open_rows_device(const uint64_t* codeword, size_t fr_per_row, size_t num_rows,
+                     const uint8_t* layers, const uint64_t* indices, size_t nq, uint64_t* rows,
+                     uint8_t* paths, cudaStream_t s) {
+  if (nq == 0) return PKG_OK;
+  const int depth = log2_exact(num_rows);
+  for (size_t q = 0; q < nq; q++)
+    PK_REQUIRE(indices[q] < num_rows, "index %llu out of range (%zu rows)",
+               (unsigned long long)indices[q], num_rows);
+  Scratch scr;
+  const size_t idx_bytes = (8 * nq + 255) & ~size_t(255);
+  const size_t row_bytes = (32 * nq * fr_per_row + 255) & ~size_t(255);
+  int rc = scr.alloc(idx_bytes + row_bytes + 32 * nq * (size_t)depth + 32, s);
+  if (rc) return rc;
+  uint64_t* d_idx = static_cast<uint64_t*>(scr.ptr);
+  uint64_t* d_rows = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(scr.ptr) + idx_bytes);
+  uint8_t* d_paths = static_cast<uint8_t*>(scr.ptr) + idx_bytes + row_bytes;
+  PK_CUDA(cudaMemcpyAsync(d_idx, indices, 8 * nq, cudaMemcpyHostToDevice, s));
+  gather_rows_kernel<<<ew_grid(nq * fr_per_row), 256, 0, s>>>(codeword, fr_per_row, d_idx, nq,
+                                                              d_rows);
+  PK_CHECK_LAUNCH("gather_rows_kernel");
+  if (depth) {
+    merkle_open_kernel<<<ew_grid(nq * depth), 256, 0, s>>>(layers, num_rows, depth, d_idx, nq,
+                                                           d_paths);
+    PK_CHECK_LAUNCH("merkle_open_kernel");
+  }
+  PK_CUDA(cudaMemcpyAsync(rows, d_rows, 32 * nq * fr_per_row, cudaMemcpyDeviceToHost, s));
+  if (depth)
+    PK_CUDA(cudaMemcpyAsync(paths, d_paths, 32 * nq * (size_t)depth, cudaMemcpyDeviceToHost, s));
+  PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}
+}  // namespace pk
+
 extern "C" int pkg_stir_indices(const uint8_t* bytes, size_t folded_domain_size, size_t nq,
                                 uint64_t* out) {
   PK_REQUIRE(is_pow2(folded_domain_size), "folded domain size %zu is not a power of two",
@@ -363,12 +400,10 @@ extern "C" int pkg_whir_sumcheck_round(uint64_t* f, uint64_t* w, size_t size, co
   return PKG_OK;
 }
 
-extern "C" int pkg_eq_accumulate(uint64_t* w, size_t nv, const uint64_t* points,
-                                 const uint64_t* coeffs, size_t npts, pkg_stream_t stream) {
-  PK_REQUIRE(nv < 40, "too many variables (%zu)", nv);
+namespace pk {
+int eq_accumulate_device(uint64_t* w, size_t nv, const uint64_t* points, const uint64_t* coeffs,
+                         size_t npts, cudaStream_t s, bool sync) {
   if (npts == 0) return PKG_OK;
-  PK_REQUIRE(w && points && coeffs && aligned16(w), "null or unaligned pointer");
-  cudaStream_t s = as_stream(stream);
   const int nhi = (int)(nv + 1) / 2, nlo = (int)nv - nhi;
   const size_t nh = size_t(1) << nhi, nl = size_t(1) << nlo, n = size_t(1) << nv;
   Scratch scr;
@@ -388,7 +423,17 @@ extern "C" int pkg_eq_accumulate(uint64_t* w, size_t nv, const uint64_t* points,
   PK_CHECK_LAUNCH("eq_tables_kernel");
   eq_accumulate_kernel<<<ew_grid(n), 256, 0, s>>>(w, n, nlo, d_hi, nh, d_lo, npts);
   PK_CHECK_LAUNCH("eq_accumulate_kernel");
-  // the host points and coefficients must outlive their async copies
-  PK_CUDA(cudaStreamSynchronize(s));
+  // host sources in pinned memory must outlive their async copies; pageable
+  // ones are staged before cudaMemcpyAsync returns
+  if (sync) PK_CUDA(cudaStreamSynchronize(s));
   return PKG_OK;
+}
+}  // namespace pk
+
+extern "C" int pkg_eq_accumulate(uint64_t* w, size_t nv, const uint64_t* points,
+                                 const uint64_t* coeffs, size_t npts, pkg_stream_t stream) {
+  PK_REQUIRE(nv < 40, "too many variables (%zu)", nv);
+  if (npts == 0) return PKG_OK;
+  PK_REQUIRE(w && points && coeffs && aligned16(w), "null or unaligned pointer");
+  return eq_accumulate_device(w, nv, points, coeffs, npts, as_stream(stream), true);
 }

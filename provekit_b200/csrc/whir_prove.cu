@@ -20,6 +20,7 @@
 // the OOD answers, the PoW nonce and the opened rows and paths, which are the
 // proof, and sends back the challenges as kernel parameters.
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <vector>
 
@@ -204,6 +205,21 @@ struct PoolBuf {
   }
 };
 
+// Host wall-clock of the calling thread's last WHIR prove, per phase
+// (pkg_last_whir_stages).  Phases that end without a synchronisation leave
+// their device time to the next one that synchronises.
+thread_local double g_whir_ms[PKG_WHIR_STAGES];
+
+struct PhaseTimer {
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  int k;
+  explicit PhaseTimer(int stage) : k(stage) {}
+  ~PhaseTimer() {
+    g_whir_ms[k] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                        .count();
+  }
+};
+
 #define PK_TRY(call)          \
   do {                        \
     const int _rc = (call);   \
@@ -216,7 +232,8 @@ class WhirProver {
       : p_(p), t_(t), s_(s), out_(proof) {}
 
   int run(const uint64_t* coeffs, const uint64_t* codeword, const uint8_t* layers,
-          const uint64_t* ood_points, const uint64_t* covectors, size_t ncov);
+          const uint64_t* ood_points, const uint64_t* covectors, size_t ncov,
+          const uint64_t* values);
 
  private:
   void put(const HostFr& x) {
@@ -297,9 +314,7 @@ int WhirProver::stir_step(size_t q, size_t L, const uint64_t* cw, const uint8_t*
   PK_TRY(pkg_stir_indices(bytes.data(), L, q, idx.data()));
   std::vector<uint64_t> rows(q * K * 4);
   std::vector<uint8_t> paths(q * (size_t)depth * 32 + 1);
-  const pkg_stream_t ps = reinterpret_cast<pkg_stream_t>(s_);
-  PK_TRY(pkg_gather_rows(cw, K, L, idx.data(), q, rows.data(), ps));
-  PK_TRY(pkg_merkle_open(layers, L, idx.data(), q, paths.data(), ps));
+  PK_TRY(open_rows_device(cw, K, L, layers, idx.data(), q, rows.data(), paths.data(), s_));
   for (size_t i = 0; i < q; i++) {
     memcpy(out_ + pos_, rows.data() + i * K * 4, 32 * K);
     pos_ += 4 * K;
@@ -315,18 +330,26 @@ int WhirProver::add_constraints(const std::vector<HostFr>& points, unsigned nv,
   std::vector<HostFr> pts;
   pts.reserve(points.size() * nv);
   for (const HostFr& z : points) expand_into(pts, z, nv);
-  return pkg_eq_accumulate(w_, nv, pts.empty() ? nullptr : pts[0].l, coefs[0].l, points.size(),
-                           reinterpret_cast<pkg_stream_t>(s_));
+  // pts and coefs are pageable: staged before the copies return, no sync
+  return eq_accumulate_device(w_, nv, pts.empty() ? nullptr : pts[0].l, coefs[0].l, points.size(),
+                              s_, false);
 }
 
 int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint8_t* layers,
-                    const uint64_t* ood_points, const uint64_t* covectors, size_t ncov) {
+                    const uint64_t* ood_points, const uint64_t* covectors, size_t ncov,
+                    const uint64_t* values) {
+  memset(g_whir_ms, 0, sizeof g_whir_ms);
   const unsigned n = p_->num_variables, k = p_->folding_factor, R = p_->num_rounds;
   const unsigned o = p_->ood_samples;
   const size_t N = size_t(1) << n, K = size_t(1) << k;
   const pkg_stream_t ps = reinterpret_cast<pkg_stream_t>(s_);
 
   PoolBuf E, W, A, B, cw_own, lay_own, cw_next, lay_next;
+  std::vector<HostFr> vals(ncov);
+  HostFr gamma;
+  std::vector<HostFr> pw;
+  {
+  PhaseTimer pt(0);
   PK_TRY(E.alloc(32 * N, s_));
   PK_TRY(W.alloc(32 * N, s_));
   PK_TRY(A.alloc(32 * (N >> k), s_));
@@ -339,13 +362,15 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
 
   // the statement values, then the combination randomness over
   // (commitment OOD answers, values)
-  std::vector<HostFr> vals(ncov);
   for (size_t a = 0; a < ncov; a++) {
-    PK_TRY(pkg_dot(covectors + 4 * N * a, coeffs, N, vals[a].l, ps));
+    if (values)
+      memcpy(vals[a].l, values + 4 * a, 32);
+    else
+      PK_TRY(pkg_dot(covectors + 4 * N * a, coeffs, N, vals[a].l, ps));
     put(vals[a]);
   }
-  const HostFr gamma = absorb_squeeze(t_, vals.data(), ncov);
-  std::vector<HostFr> pw = powers_of(gamma, o + ncov);
+  gamma = absorb_squeeze(t_, vals.data(), ncov);
+  pw = powers_of(gamma, o + ncov);
   if (ncov) {
     CovParams P;
     memset(&P, 0, sizeof P);
@@ -364,9 +389,13 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
     for (unsigned j = 0; j < o; j++) z[j] = HostFr::from_limbs(ood_points + 4 * j);
     PK_TRY(add_constraints(z, n, c));
   }
+  }
 
   std::vector<HostFr> alpha;
-  PK_TRY(sumcheck_phase(k, alpha));
+  {
+    PhaseTimer pt(1);
+    PK_TRY(sumcheck_phase(k, alpha));
+  }
 
   const uint64_t* f = coeffs;  // current polynomial's coefficients
   unsigned nv = n;
@@ -381,42 +410,61 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
   };
   for (unsigned r = 0; r < R; r++) {
     uint64_t* g = (r & 1) ? B.as<uint64_t>() : A.as<uint64_t>();
-    PK_TRY(fold_into(g));
-    // commit the folded polynomial at the next rate
     const size_t Ln = size_t(1) << rows_log(p_, r + 1);
-    PK_TRY(cw_next.alloc(32 * K * Ln, s_));
-    PK_TRY(lay_next.alloc(32 * (2 * Ln - 1), s_));
-    PK_TRY(pkg_whir_commit(g, size_t(1) << nv, k, p_->log_inv_rate + (r + 1) * (k - 1), nullptr, 0,
-                           PKG_LEAF_CANONICAL, cw_next.as<uint64_t>(), lay_next.as<uint8_t>(), ps));
-    HostFr root;
-    PK_CUDA(cudaMemcpyAsync(root.l, lay_next.as<uint8_t>() + 32 * (2 * Ln - 2), 32,
-                            cudaMemcpyDeviceToHost, s_));
-    PK_CUDA(cudaStreamSynchronize(s_));
-    put(root);
-    const HostFr root_m = HostFr::to_mont(root);
-    pkg_transcript_absorb(t_, root_m.l);
+    {
+      PhaseTimer pt(2);
+      PK_TRY(fold_into(g));
+      // commit the folded polynomial at the next rate
+      PK_TRY(cw_next.alloc(32 * K * Ln, s_));
+      PK_TRY(lay_next.alloc(32 * (2 * Ln - 1), s_));
+      PK_TRY(pkg_whir_commit(g, size_t(1) << nv, k, p_->log_inv_rate + (r + 1) * (k - 1), nullptr,
+                             0, PKG_LEAF_CANONICAL, cw_next.as<uint64_t>(), lay_next.as<uint8_t>(),
+                             ps));
+      HostFr root;
+      PK_CUDA(cudaMemcpyAsync(root.l, lay_next.as<uint8_t>() + 32 * (2 * Ln - 2), 32,
+                              cudaMemcpyDeviceToHost, s_));
+      PK_CUDA(cudaStreamSynchronize(s_));
+      put(root);
+      const HostFr root_m = HostFr::to_mont(root);
+      pkg_transcript_absorb(t_, root_m.l);
+    }
     // OOD samples of the folded polynomial
     std::vector<HostFr> points(o);
-    for (unsigned j = 0; j < o; j++) pkg_transcript_squeeze(t_, points[j].l);
-    if (o) {
-      std::vector<HostFr> ans(o);
-      PK_TRY(pkg_poly_eval_many(g, size_t(1) << nv, points[0].l, o, ans[0].l, ps));
-      for (unsigned j = 0; j < o; j++) {
-        put(ans[j]);
-        pkg_transcript_absorb(t_, ans[j].l);
+    {
+      PhaseTimer pt(3);
+      for (unsigned j = 0; j < o; j++) pkg_transcript_squeeze(t_, points[j].l);
+      if (o) {
+        std::vector<HostFr> ans(o);
+        PK_TRY(pkg_poly_eval_many(g, size_t(1) << nv, points[0].l, o, ans[0].l, ps));
+        for (unsigned j = 0; j < o; j++) {
+          put(ans[j]);
+          pkg_transcript_absorb(t_, ans[j].l);
+        }
       }
     }
-    if (p_->pow_bits) PK_TRY(pow_step(p_->pow_bits));
+    if (p_->pow_bits) {
+      PhaseTimer pt(4);
+      PK_TRY(pow_step(p_->pow_bits));
+    }
     // STIR queries on the previous codeword
     const size_t Lr = size_t(1) << rows_log(p_, r), q = p_->queries[r];
-    PK_TRY(stir_step(q, Lr, cw_r, lay_r, idx));
-    std::vector<size_t> sidx(idx.begin(), idx.end());
-    points.resize(o + q);
-    PK_TRY(pkg_rs_evaluation_points(Lr, sidx.data(), q, points[o].l));
-    HostFr gr;
-    pkg_transcript_squeeze(t_, gr.l);
-    PK_TRY(add_constraints(points, nv, powers_of(gr, o + q)));
-    PK_TRY(sumcheck_phase(k, alpha));
+    {
+      PhaseTimer pt(5);
+      PK_TRY(stir_step(q, Lr, cw_r, lay_r, idx));
+      std::vector<size_t> sidx(idx.begin(), idx.end());
+      points.resize(o + q);
+      PK_TRY(pkg_rs_evaluation_points(Lr, sidx.data(), q, points[o].l));
+    }
+    {
+      PhaseTimer pt(6);
+      HostFr gr;
+      pkg_transcript_squeeze(t_, gr.l);
+      PK_TRY(add_constraints(points, nv, powers_of(gr, o + q)));
+    }
+    {
+      PhaseTimer pt(1);
+      PK_TRY(sumcheck_phase(k, alpha));
+    }
     // the new codeword becomes the one the next queries open
     f = g;
     cw_own.swap(cw_next);
@@ -427,22 +475,42 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
     lay_r = lay_own.as<uint8_t>();
   }
   // the final polynomial in the clear
-  uint64_t* g = (R & 1) ? B.as<uint64_t>() : A.as<uint64_t>();
-  PK_TRY(fold_into(g));
-  const size_t nfin = size_t(1) << nv;
-  std::vector<HostFr> fin(nfin);
-  PK_CUDA(cudaMemcpyAsync(fin[0].l, g, 32 * nfin, cudaMemcpyDeviceToHost, s_));
-  PK_CUDA(cudaStreamSynchronize(s_));
-  for (size_t i = 0; i < nfin; i++) {
-    put(fin[i]);
-    pkg_transcript_absorb(t_, fin[i].l);
+  {
+    PhaseTimer pt(7);
+    uint64_t* g = (R & 1) ? B.as<uint64_t>() : A.as<uint64_t>();
+    PK_TRY(fold_into(g));
+    const size_t nfin = size_t(1) << nv;
+    std::vector<HostFr> fin(nfin);
+    PK_CUDA(cudaMemcpyAsync(fin[0].l, g, 32 * nfin, cudaMemcpyDeviceToHost, s_));
+    PK_CUDA(cudaStreamSynchronize(s_));
+    for (size_t i = 0; i < nfin; i++) {
+      put(fin[i]);
+      pkg_transcript_absorb(t_, fin[i].l);
+    }
   }
-  if (p_->final_pow_bits) PK_TRY(pow_step(p_->final_pow_bits));
-  PK_TRY(stir_step(p_->queries[R], size_t(1) << rows_log(p_, R), cw_r, lay_r, idx));
-  std::vector<HostFr> rfin;
-  PK_TRY(sumcheck_phase(nv, rfin));
-  PK_CUDA(cudaStreamSynchronize(s_));
+  if (p_->final_pow_bits) {
+    PhaseTimer pt(4);
+    PK_TRY(pow_step(p_->final_pow_bits));
+  }
+  {
+    PhaseTimer pt(5);
+    PK_TRY(stir_step(p_->queries[R], size_t(1) << rows_log(p_, R), cw_r, lay_r, idx));
+  }
+  {
+    PhaseTimer pt(1);
+    std::vector<HostFr> rfin;
+    PK_TRY(sumcheck_phase(nv, rfin));
+    PK_CUDA(cudaStreamSynchronize(s_));
+  }
   return PKG_OK;
+}
+
+int whir_prove_device(const pkg_whir_params* p, pkg_transcript* t, const uint64_t* coeffs,
+                      const uint64_t* codeword, const uint8_t* layers, const uint64_t* ood_points,
+                      const uint64_t* covectors, size_t ncov, const uint64_t* values,
+                      uint64_t* proof, cudaStream_t s) {
+  WhirProver prover(p, t, s, proof);
+  return prover.run(coeffs, codeword, layers, ood_points, covectors, ncov, values);
 }
 
 }  // namespace pk
@@ -543,6 +611,12 @@ extern "C" int pkg_whir_prove(const pkg_whir_params* p, pkg_transcript* t, const
   PK_REQUIRE(aligned16(coeffs) && aligned16(codeword) && aligned16(layers) &&
                  (!ncov || aligned16(covectors)),
              "device buffers must be 16-byte aligned");
-  WhirProver prover(p, t, as_stream(stream), proof);
-  return prover.run(coeffs, codeword, layers, ood_points, covectors, ncov);
+  return whir_prove_device(p, t, coeffs, codeword, layers, ood_points, covectors, ncov, nullptr,
+                           proof, as_stream(stream));
+}
+
+extern "C" int pkg_last_whir_stages(double ms[PKG_WHIR_STAGES]) {
+  PK_REQUIRE(ms, "null output");
+  memcpy(ms, g_whir_ms, sizeof g_whir_ms);
+  return PKG_OK;
 }
