@@ -754,10 +754,10 @@ def run_served(a):
     budget = int(min(free_b * 0.8, 120e9))
     # sequential plain proving: one request at a time (1 slot), service times
     srv = ProofServer(budget, max_inflight=1)
-    srv.wait(srv.submit(reqs[0], blinding_seed=0, transcript_domain=0))  # warm-up
+    srv.wait(srv.submit(reqs[0], whole_proof=True, blinding_seed=0, transcript_domain=0))  # warm-up
     service = []
     for i, h in enumerate(reqs):
-        _, tm = srv.wait(srv.submit(h, blinding_seed=i, transcript_domain=i))
+        _, tm = srv.wait(srv.submit(h, whole_proof=True, blinding_seed=i, transcript_domain=i))
         service.append((tm["done_ns"] - tm["submit_ns"]) * 1e-9)
     srv.close()
     cap = len(service) / sum(service)
@@ -783,7 +783,7 @@ def run_served(a):
             delay = t_start + t_arr - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            ids[i] = srv.submit(h, blinding_seed=i, transcript_domain=i)
+            ids[i] = srv.submit(h, whole_proof=True, blinding_seed=i, transcript_domain=i)
         lat, qwait, svc = [], [], []
         for rid in ids:
             _, tm = srv.wait(rid)
@@ -805,13 +805,14 @@ def run_served(a):
                            "p99_ms": 1e3 * pct(seq_lat, 0.99), "p999_ms": 1e3 * pct(seq_lat, 0.999)},
         })
         del served_span
-    line = {"metric": "served form: open-loop Poisson prove requests (Spartan prove core), "
+    line = {"metric": "served form: open-loop Poisson prove requests (whole proofs: Spartan + WHIR), "
                       "log2 constraints uniform on [14, 22]; proofs/s and p50/p99/p99.9 latency vs "
                       "sequential plain-GPU proving",
-            "value": max(s["served"]["proofs_per_s"] for s in sweeps), "unit": "prove-cores/s",
+            "value": max(s["served"]["proofs_per_s"] for s in sweeps), "unit": "proofs/s",
             "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32 (BN254 Fr, 8x32-bit limbs)", "data": "synthetic R1CS (pkg_synthetic_r1cs)",
-            "config": {"workload": "served", "requests": len(reqs), "log2_constraints": logs,
+            "dtype": "u32/f64 (BN254 Fr: 8x32-bit limbs, products on the FP64 pipe)",
+            "data": "synthetic R1CS (pkg_synthetic_r1cs)",
+            "config": {"workload": "served", "whir": "ff 3, rate 1/4, 128 bits, 10 PoW bits", "requests": len(reqs), "log2_constraints": logs,
                        "hbm_budget_gb": budget / 1e9, "max_inflight": 8, "generation_s": gen_s},
             "sequential_capacity_per_s": cap, "sweeps": sweeps}
     print(json.dumps(line), flush=True)

@@ -354,7 +354,8 @@ int pkg_batch_sumcheck_result(pkg_batch *batch, size_t job, pkg_sumcheck_result 
 /* ---- Served form -------------------------------------------------------------- */
 /* A proving service on the current device: requests (host R1CS + witness) are
  * queued, admitted by their estimated HBM footprint within hbm_budget_bytes
- * and max_inflight slots, and proved with pkg_spartan_prove by one worker
+ * and max_inflight slots, and proved with pkg_spartan_prove (or, with WHIR
+ * parameters, pkg_prove_r1cs) by one worker
  * thread + CUDA stream per slot, so admitted jobs overlap on the device and
  * their R1CS, witness, codeword, tree and tables stay resident until done.
  * Latencies are measured from submit to completion.  No reference
@@ -370,6 +371,13 @@ typedef struct {
   const uint64_t *witness;    /* host, num_witnesses Fr */
   uint64_t blinding_seed, transcript_domain;
   unsigned folding_factor, log_inv_rate;
+  /* Optional whole proof (pkg_prove_r1cs): WHIR parameters for the R1CS's
+   * m (their folding factor and rate replace the two above) and host
+   * buffers of pkg_whir_commit_words / pkg_whir_proof_words(whir, 3) words,
+   * written before pkg_server_wait returns.  NULL: the Spartan part only
+   * (pkg_spartan_prove). */
+  const struct pkg_whir_params_s *whir;
+  uint64_t *whir_commit_words, *whir_proof;
 } pkg_prove_request;
 typedef struct {
   uint64_t submit_ns, admit_ns, done_ns; /* steady clock */
@@ -467,7 +475,7 @@ int pkg_eq_accumulate(uint64_t *w, size_t nv, const uint64_t *points, const uint
  * above, with bytes taken 31 per squeezed element; PoW threshold
  * floor(p / 2^bits) (CheckPoW, recursive-verifier/app/utilities/utilities.go:104-139). */
 #define PKG_WHIR_MAX_ROUNDS 16
-typedef struct {
+typedef struct pkg_whir_params_s {
   uint32_t num_variables;   /* n: the committed vector has 2^n entries     */
   uint32_t folding_factor;  /* k, 1..6                                      */
   uint32_t log_inv_rate;    /* starting rate 2^-log_inv_rate (1..8)         */

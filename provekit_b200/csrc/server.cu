@@ -44,6 +44,11 @@ struct HostRequest {
   const uint64_t* witness = nullptr;
   uint64_t blinding_seed = 0, domain = 0;
   unsigned ff = 3, lr = 2;
+  // whole proof: WHIR parameters and the caller's output buffers
+  bool whole = false;
+  pkg_whir_params whir{};
+  uint64_t* whir_commit_words = nullptr;
+  uint64_t* whir_proof = nullptr;
   size_t footprint = 0;
   int passed_over = 0;
   // results
@@ -62,8 +67,10 @@ static size_t ceil_log2_sz(size_t n) {
   return k;
 }
 
-// Device bytes pkg_spartan_prove plus the resident request use (upper bound).
-size_t prove_footprint(size_t nc, size_t nw, const size_t nnz[3], unsigned ff, unsigned lr) {
+// Device bytes pkg_spartan_prove (with whole, pkg_prove_r1cs) plus the
+// resident request use (upper bound).
+size_t prove_footprint(size_t nc, size_t nw, const size_t nnz[3], unsigned ff, unsigned lr,
+                       bool whole) {
   size_t m = ceil_log2_sz(nw), m0 = ceil_log2_sz(nc);
   if (m < 13) m = 13;
   if (m0 < 1) m0 = 1;
@@ -80,6 +87,14 @@ size_t prove_footprint(size_t nc, size_t nw, const size_t nnz[3], unsigned ff, u
   b += 8 * (nw + 1) + 36 * maxnnz + (4 << 20);  // one transposed matrix + scan temp
   for (int k = 0; k < 3; k++) b += 8 * (nc + 1) + 36 * nnz[k];  // resident R1CS
   b += 32 * nw;                                                   // resident witness
+  if (whole) {
+    // the WHIR rounds: three padded covectors, f^ and w tables, two folded
+    // polynomials, and two round codewords with their trees at a time
+    // (round 1's, the largest, holds n << (lr - 1) Fr)
+    const size_t cw1 = lr >= 1 ? n << (lr - 1) : n;
+    b += 32 * 3 * n + 32 * 2 * n + 32 * 2 * (n >> ff);
+    b += 2 * (32 * cw1 + 32 * 2 * (cw1 >> ff));
+  }
   return b + b / 8 + (16 << 20);                                  // pool slack
 }
 
@@ -186,8 +201,10 @@ static int run_request(HostRequest& r, cudaStream_t st) {
     if (allocated) cudaEventDestroy(allocated);
   }
   if (!rc) {
-    rc = pkg_spartan_prove(&rc1, static_cast<uint64_t*>(w), r.blinding_seed, r.domain, r.ff, r.lr,
-                           &r.proof, st);
+    rc = r.whole ? pkg_prove_r1cs(&rc1, static_cast<uint64_t*>(w), r.blinding_seed, r.domain,
+                                  &r.whir, &r.proof, r.whir_commit_words, r.whir_proof, st)
+                 : pkg_spartan_prove(&rc1, static_cast<uint64_t*>(w), r.blinding_seed, r.domain,
+                                     r.ff, r.lr, &r.proof, st);
     if (rc) r.error = pkg_last_error();
   } else if (r.error.empty()) {
     r.error = pkg_last_error();
@@ -278,7 +295,23 @@ extern "C" int pkg_server_submit(pkg_server* s, const pkg_prove_request* req, ui
   r->domain = req->transcript_domain;
   r->ff = req->folding_factor;
   r->lr = req->log_inv_rate;
-  r->footprint = prove_footprint(r->nc, r->nw, r->nnz, r->ff, r->lr);
+  if (req->whir) {
+    PK_REQUIRE(req->whir_commit_words && req->whir_proof, "null WHIR output buffer");
+    PK_REQUIRE(pkg_whir_proof_words(req->whir, 3) != 0, "invalid WHIR parameters");
+    size_t m = 0, m0 = 0;
+    int rc = pkg_r1cs_sizing(r->nc, r->nw, &m, &m0);
+    if (rc) return rc;
+    PK_REQUIRE(req->whir->num_variables == m,
+               "WHIR parameters for %u variables, the R1CS needs %zu", req->whir->num_variables,
+               m);
+    r->whole = true;
+    r->whir = *req->whir;
+    r->whir_commit_words = req->whir_commit_words;
+    r->whir_proof = req->whir_proof;
+    r->ff = r->whir.folding_factor;
+    r->lr = r->whir.log_inv_rate;
+  }
+  r->footprint = prove_footprint(r->nc, r->nw, r->nnz, r->ff, r->lr, r->whole);
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (r->footprint > s->budget) {

@@ -2,9 +2,10 @@
 device execution (pkg_server_* in the C header)."""
 import ctypes
 
+import numpy as np
 
 from ._lib import check, lib
-from .prover import SpartanProofC
+from .prover import SpartanProofC, whir_params_for
 
 
 class ProveRequestC(ctypes.Structure):
@@ -13,7 +14,8 @@ class ProveRequestC(ctypes.Structure):
                 ("vals", ctypes.c_void_p * 3), ("nnz", ctypes.c_size_t * 3),
                 ("witness", ctypes.c_void_p), ("blinding_seed", ctypes.c_uint64),
                 ("transcript_domain", ctypes.c_uint64), ("folding_factor", ctypes.c_uint),
-                ("log_inv_rate", ctypes.c_uint)]
+                ("log_inv_rate", ctypes.c_uint), ("whir", ctypes.c_void_p),
+                ("whir_commit_words", ctypes.c_void_p), ("whir_proof", ctypes.c_void_p)]
 
 
 class RequestTimesC(ctypes.Structure):
@@ -29,8 +31,11 @@ class ServerStatsC(ctypes.Structure):
                 ("proofs_per_s", ctypes.c_double)]
 
 
-def make_request(h, blinding_seed=1, transcript_domain=3, folding_factor=3, log_inv_rate=2):
-    """pkg_prove_request over a HostR1CS (the arrays must outlive submit)."""
+def make_request(h, blinding_seed=1, transcript_domain=3, folding_factor=3, log_inv_rate=2,
+                 whole=None):
+    """pkg_prove_request over a HostR1CS (the arrays must outlive submit).
+    whole: None for the Spartan part, or (WhirParams, commit_words buffer,
+    proof buffer) for a whole proof."""
     req = ProveRequestC()
     req.num_constraints, req.num_witnesses = h.num_constraints, h.num_witnesses
     for k in range(3):
@@ -44,6 +49,11 @@ def make_request(h, blinding_seed=1, transcript_domain=3, folding_factor=3, log_
     req.witness = h.witness.ctypes.data
     req.blinding_seed, req.transcript_domain = blinding_seed, transcript_domain
     req.folding_factor, req.log_inv_rate = folding_factor, log_inv_rate
+    if whole is not None:
+        p, cw, pr = whole
+        req.whir = ctypes.addressof(p)
+        req.whir_commit_words = cw.ctypes.data
+        req.whir_proof = pr.ctypes.data
     return req
 
 
@@ -53,22 +63,34 @@ class ProofServer:
         self._s = ctypes.c_void_p()
         check(lib().pkg_server_create(hbm_budget_bytes, max_inflight, ctypes.byref(self._s)))
 
-    def submit(self, h, **kw) -> int:
-        """Queue a HostR1CS; the server reads its arrays until wait() returns."""
-        req = make_request(h, **kw)
+    def submit(self, h, whole_proof=False, whir=None, **kw) -> int:
+        """Queue a HostR1CS; the server reads its arrays until wait() returns.
+        whole_proof: prove with WHIR's rounds too (whir: WhirParams, by
+        default the reference's configuration for the R1CS's m)."""
+        whole = None
+        if whole_proof or whir is not None:
+            p = whir if whir is not None else whir_params_for(h)
+            whole = (p, np.zeros(p.commit_words(), np.uint64), np.zeros(p.proof_words(3), np.uint64))
+        req = make_request(h, whole=whole, **kw)
         rid = ctypes.c_uint64()
         check(lib().pkg_server_submit(self._s, ctypes.byref(req), ctypes.byref(rid)))
-        self._live[rid.value] = h  # keep the request's buffers alive until wait()
+        self._live[rid.value] = (h, whole)  # keep the request's buffers alive until wait()
         return rid.value
 
     def wait(self, rid: int):
+        """(Spartan fields, times) -- plus (commit words, WHIR proof) appended
+        to the fields as "whir_commit_words" / "whir_proof" for whole proofs."""
         proof, times = SpartanProofC(), RequestTimesC()
         try:
             check(lib().pkg_server_wait(self._s, rid, ctypes.byref(proof), ctypes.byref(times)))
+            _, whole = self._live.get(rid, (None, None))
         finally:
             self._live.pop(rid, None)
-        return proof.as_dict(), {"submit_ns": times.submit_ns, "admit_ns": times.admit_ns,
-                                 "done_ns": times.done_ns, "footprint": times.footprint_bytes}
+        out = proof.as_dict()
+        if whole is not None:
+            out["whir_commit_words"], out["whir_proof"] = whole[1], whole[2]
+        return out, {"submit_ns": times.submit_ns, "admit_ns": times.admit_ns,
+                     "done_ns": times.done_ns, "footprint": times.footprint_bytes}
 
     def stats(self) -> dict:
         st = ServerStatsC()

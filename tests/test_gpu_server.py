@@ -76,3 +76,24 @@ def test_request_above_budget_is_rejected():
     with pytest.raises(PkgError):
         srv.submit(HostR1CS(1, 1 << 16, 1 << 14))
     srv.close()
+
+
+def test_served_whole_proofs_equal_alone_results():
+    """Whole proofs (pkg_prove_r1cs) through the server: Spartan part, WHIR
+    commitment words and WHIR proof equal the same request proved alone."""
+    from provekit_b200.prover import HostR1CS, prove_r1cs
+    from provekit_b200.server import ProofServer
+    sizes = [(12, 10), (14, 12), (13, 11), (15, 13), (12, 10)]
+    reqs = [HostR1CS(700 + i, 1 << lc, 1 << li) for i, (lc, li) in enumerate(sizes)]
+    alone = [prove_r1cs(h.to_device(), blinding_seed=3 + i, transcript_domain=40 + i)
+             for i, h in enumerate(reqs)]
+    srv = ProofServer(hbm_budget_bytes=1 << 30, max_inflight=3)
+    ids = [srv.submit(h, whole_proof=True, blinding_seed=3 + i, transcript_domain=40 + i)
+           for i, h in enumerate(reqs)]
+    for rid, (sp, cw, proof) in zip(ids, alone):
+        got, times = srv.wait(rid)
+        assert np.array_equal(got.pop("whir_commit_words"), cw)
+        assert np.array_equal(got.pop("whir_proof"), proof)
+        same(got, sp)
+        assert times["submit_ns"] <= times["admit_ns"] <= times["done_ns"]
+    srv.close()
