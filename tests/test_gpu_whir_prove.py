@@ -56,6 +56,9 @@ def _device_proof(p, domain, c, cov):
 
 CASES = [
     (6, 2, 1, 24, 0, {}),
+    (4, 4, 1, 20, 1, {}),
+    (12, 3, 2, 30, 2, {"num_rounds": 3, "final_vars": 0, "queries": [20, 12, 9, 7]}),
+    (9, 3, 3, 30, 0, {"num_rounds": 1, "final_vars": 3, "final_pow_bits": 5, "queries": [4, 1]}),
     (8, 2, 1, 32, 2, {}),
     (10, 3, 2, 40, 3, {}),
     (12, 3, 2, 60, 4, {"ood_samples": 2}),
@@ -128,3 +131,15 @@ def test_pow_solutions_are_the_smallest_nonces():
         assert lib().pkg_skyscraper_pow_solve(ch.ctypes.data, thr.ctypes.data,
                                               ctypes.byref(got)) == 0
         assert got.value == O.lib().pko_sky_pow_solve(O.p64(ch), O.p64(thr))
+
+
+def test_largest_commitment_proof_verifies():
+    """2^24 coefficients (a 2 GiB codeword at rate 1/4, ff 4): the device
+    proof of two statements is accepted by the oracle verifier."""
+    n = 24
+    p, po = _params_pair(n, 4, 2, 64, 6, {})
+    c = O.sample_fr(24, 1 << n)
+    cov = O.sample_fr(25, 2 << n)
+    _, _, words, proof, _ = _device_proof(p, 31, c, cov)
+    torch.cuda.empty_cache()
+    assert O.whir_verify(po, 31, cov, 2, words, proof) == 0

@@ -60,6 +60,11 @@ def layout(p, ncov):
 CASES = [
     # n, k, log_inv_rate, security, pow, overrides
     (6, 2, 1, 24, 0, {}),
+    (4, 4, 1, 20, 1, {}),                                            # R = 0, no final variables
+    (12, 3, 2, 30, 2, {"num_rounds": 3, "final_vars": 0,
+                       "queries": [20, 12, 9, 7]}),                  # hand-set schedule, 1 final coeff
+    (9, 3, 3, 30, 0, {"num_rounds": 1, "final_vars": 3, "final_pow_bits": 5,
+                      "queries": [4, 1]}),
     (8, 2, 1, 32, 2, {}),
     (10, 3, 2, 40, 3, {}),
     (12, 3, 2, 60, 4, {"ood_samples": 2}),
