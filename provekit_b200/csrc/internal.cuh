@@ -31,10 +31,14 @@ int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* d_out, 
                cudaStream_t s);
 
 // The WHIR prover's round loop (pkg_whir_prove); values (host, ncov Fr) are
-// the statements' values when the caller already has them, else nullptr.
+// the statements' values when the caller already has them, else nullptr;
+// hat (device, 2^n Fr, overwritten) is zeta(coeffs) when the caller already
+// computed it, else nullptr.
 int whir_prove_device(const pkg_whir_params* p, pkg_transcript* t, const uint64_t* coeffs,
                       const uint64_t* codeword, const uint8_t* layers, const uint64_t* ood_points,
                       const uint64_t* covectors, size_t ncov, const uint64_t* values,
-                      uint64_t* proof, cudaStream_t s);
+                      uint64_t* hat, uint64_t* proof, cudaStream_t s);
+// In place v[b | 2^i] += v[b] over 2^n entries (pkg_subset_transform's zeta).
+int subset_zeta_device(uint64_t* v, unsigned n, cudaStream_t s);
 
 }  // namespace pk

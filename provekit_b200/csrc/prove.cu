@@ -208,7 +208,7 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     // state the WHIR prover starts from
     pkg_transcript tw = out->transcript;
     if ((rc = whir_prove_device(whir, &tw, poly, cw, layers, ood_points, cov, 3, &out->evals[0][0],
-                                whir_proof, s)))
+                                nullptr, whir_proof, s)))
       return rc;
     clk.mark(5);
   }

@@ -128,6 +128,12 @@ cudaMemPool_t lib_pool() {
     if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    // A block freed on one stream is handed to another only once its free
+    // has completed, never with a dependency the driver inserts between the
+    // two streams: proofs running concurrently on their own streams would
+    // otherwise be chained to each other's frees.  The pool grows instead.
+    int no = 0;
+    cudaMemPoolSetAttribute(p, cudaMemPoolReuseAllowInternalDependencies, &no);
     g_pools[dev] = p;
   }
   return g_pools[dev];

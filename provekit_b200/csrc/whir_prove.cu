@@ -233,7 +233,7 @@ class WhirProver {
 
   int run(const uint64_t* coeffs, const uint64_t* codeword, const uint8_t* layers,
           const uint64_t* ood_points, const uint64_t* covectors, size_t ncov,
-          const uint64_t* values);
+          const uint64_t* values, uint64_t* hat);
 
  private:
   void put(const HostFr& x) {
@@ -337,7 +337,7 @@ int WhirProver::add_constraints(const std::vector<HostFr>& points, unsigned nv,
 
 int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint8_t* layers,
                     const uint64_t* ood_points, const uint64_t* covectors, size_t ncov,
-                    const uint64_t* values) {
+                    const uint64_t* values, uint64_t* hat) {
   memset(g_whir_ms, 0, sizeof g_whir_ms);
   const unsigned n = p_->num_variables, k = p_->folding_factor, R = p_->num_rounds;
   const unsigned o = p_->ood_samples;
@@ -350,15 +350,19 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
   std::vector<HostFr> pw;
   {
   PhaseTimer pt(0);
-  PK_TRY(E.alloc(32 * N, s_));
   PK_TRY(W.alloc(32 * N, s_));
   PK_TRY(A.alloc(32 * (N >> k), s_));
   PK_TRY(B.alloc(32 * (N >> k), s_));
-  E_ = E.as<uint64_t>();
   w_ = W.as<uint64_t>();
   size_ = N;
-  PK_CUDA(cudaMemcpyAsync(E_, coeffs, 32 * N, cudaMemcpyDeviceToDevice, s_));
-  PK_TRY(subset_transform_device<true>(E_, n, s_));
+  if (hat) {
+    E_ = hat;  // the caller's zeta(coeffs), folded in place from here on
+  } else {
+    PK_TRY(E.alloc(32 * N, s_));
+    E_ = E.as<uint64_t>();
+    PK_CUDA(cudaMemcpyAsync(E_, coeffs, 32 * N, cudaMemcpyDeviceToDevice, s_));
+    PK_TRY(subset_transform_device<true>(E_, n, s_));
+  }
 
   // the statement values, then the combination randomness over
   // (commitment OOD answers, values)
@@ -508,9 +512,13 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
 int whir_prove_device(const pkg_whir_params* p, pkg_transcript* t, const uint64_t* coeffs,
                       const uint64_t* codeword, const uint8_t* layers, const uint64_t* ood_points,
                       const uint64_t* covectors, size_t ncov, const uint64_t* values,
-                      uint64_t* proof, cudaStream_t s) {
+                      uint64_t* hat, uint64_t* proof, cudaStream_t s) {
   WhirProver prover(p, t, s, proof);
-  return prover.run(coeffs, codeword, layers, ood_points, covectors, ncov, values);
+  return prover.run(coeffs, codeword, layers, ood_points, covectors, ncov, values, hat);
+}
+
+int subset_zeta_device(uint64_t* v, unsigned n, cudaStream_t s) {
+  return subset_transform_device<true>(v, n, s);
 }
 
 }  // namespace pk
@@ -612,7 +620,7 @@ extern "C" int pkg_whir_prove(const pkg_whir_params* p, pkg_transcript* t, const
                  (!ncov || aligned16(covectors)),
              "device buffers must be 16-byte aligned");
   return whir_prove_device(p, t, coeffs, codeword, layers, ood_points, covectors, ncov, nullptr,
-                           proof, as_stream(stream));
+                           nullptr, proof, as_stream(stream));
 }
 
 extern "C" int pkg_last_whir_stages(double ms[PKG_WHIR_STAGES]) {
