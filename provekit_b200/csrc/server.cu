@@ -256,18 +256,39 @@ extern "C" int pkg_server_create(size_t hbm_budget_bytes, int max_inflight, pkg_
              max_inflight);
   size_t free_b = 0, total_b = 0;
   PK_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  PK_REQUIRE(hbm_budget_bytes > 0 && hbm_budget_bytes <= free_b,
-             "budget %zu bytes exceeds free device memory %zu", hbm_budget_bytes, free_b);
+  // memory the library pool holds but does not use is available as well
+  PK_REQUIRE(lib_pool() != nullptr, "could not create the library memory pool");
+  uint64_t reserved = 0, used = 0;
+  PK_CUDA(cudaMemPoolGetAttribute(lib_pool(), cudaMemPoolAttrReservedMemCurrent, &reserved));
+  PK_CUDA(cudaMemPoolGetAttribute(lib_pool(), cudaMemPoolAttrUsedMemCurrent, &used));
+  const size_t avail = free_b + (size_t)(reserved > used ? reserved - used : 0);
+  PK_REQUIRE(hbm_budget_bytes > 0 && hbm_budget_bytes <= avail,
+             "budget %zu bytes exceeds available device memory %zu", hbm_budget_bytes, avail);
   // Twiddles for every transform the admitted sizes can need (codewords up to
   // 2^28): built once here, before any worker runs.
   const uint64_t* roots = nullptr;
   int rc = roots_reserve(size_t(1) << 24, &roots);
   if (rc) return rc;
+  // Request buffers come from the library's pool, which keeps freed memory,
+  // so back-to-back proves reuse it instead of mapping it again.  The budget
+  // is reserved in the pool once, here: allocated and freed on a private
+  // stream and waited for, so every later request, on any worker stream, is
+  // carved from memory whose free has completed -- the pool neither grows
+  // (a physical mapping in the middle of a request) nor chains the workers'
+  // streams while requests run.
+  PK_REQUIRE(lib_pool() != nullptr, "could not create the library memory pool");
+  {
+    cudaStream_t ps = nullptr;
+    PK_CUDA(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
+    void* blk = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&blk, hbm_budget_bytes, lib_pool(), ps);
+    if (e == cudaSuccess) e = cudaFreeAsync(blk, ps);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ps);
+    cudaStreamDestroy(ps);
+    if (e != cudaSuccess) return cuda_status(e, "reserving the server's HBM budget");
+  }
   pkg_server* s = new pkg_server();
   PK_CUDA(cudaGetDevice(&s->device));
-  // Request buffers come from the library's pool, which keeps freed memory,
-  // so back-to-back proves reuse it instead of mapping it again.
-  PK_REQUIRE(lib_pool() != nullptr, "could not create the library memory pool");
   s->budget = hbm_budget_bytes;
   s->slots = max_inflight;
   for (int i = 0; i < max_inflight; i++) s->workers.emplace_back(worker_main, s);
