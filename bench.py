@@ -661,6 +661,7 @@ def run_prove(a):
     # proof written back per proof, as in e2e), so that one proof's host
     # round trips overlap the others' kernels
     nthr, per = 4, max(a.steps // 4, 2)
+    check(L.pkg_reserve_memory(nthr * (3 << 30)))  # four proofs' working sets, mapped up front
     bstreams = [torch.cuda.Stream(device=dev) for _ in range(nthr)]
     bw = [torch.empty_like(d.witness) for _ in range(nthr)]
     blat = [[] for _ in range(nthr)]

@@ -569,6 +569,14 @@ int pkg_fr_mul_batch(const uint64_t *a, const uint64_t *b, uint64_t *out, size_t
  * Returns unused pool memory on the current device to the driver, keeping at
  * least keep_bytes.  No counterpart in the reference. */
 int pkg_trim_memory(size_t keep_bytes);
+/* Grows the pool on the current device to hold at least `bytes` more (one
+ * allocation, freed and waited for).  The pool hands a block freed on one
+ * stream to another stream only once its free has completed, so work on
+ * several streams at once (proofs on their own streams, server workers)
+ * otherwise grows the pool while it runs; reserving first keeps those
+ * physical mappings out of the timed work.  No counterpart in the
+ * reference. */
+int pkg_reserve_memory(size_t bytes);
 
 /* ---- diagnostics ---------------------------------------------------------- */
 /* Synchronous device -> host copy of library-owned memory (e.g. batch buffers). */

@@ -143,6 +143,24 @@ cudaMemPool_t lib_pool() {
 
 using namespace pk;
 
+extern "C" int pkg_reserve_memory(size_t bytes) {
+  cudaMemPool_t p = lib_pool();
+  if (!p) {
+    set_last_error("could not create the library memory pool");
+    return PKG_ERR_CUDA;
+  }
+  if (bytes == 0) return PKG_OK;
+  cudaStream_t ps = nullptr;
+  PK_CUDA(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
+  void* blk = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&blk, bytes, p, ps);
+  if (e == cudaSuccess) e = cudaFreeAsync(blk, ps);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ps);
+  cudaStreamDestroy(ps);
+  if (e != cudaSuccess) return cuda_status(e, "pkg_reserve_memory");
+  return PKG_OK;
+}
+
 extern "C" int pkg_trim_memory(size_t keep_bytes) {
   cudaMemPool_t p = lib_pool();
   if (!p) {

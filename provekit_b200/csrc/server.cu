@@ -276,17 +276,7 @@ extern "C" int pkg_server_create(size_t hbm_budget_bytes, int max_inflight, pkg_
   // carved from memory whose free has completed -- the pool neither grows
   // (a physical mapping in the middle of a request) nor chains the workers'
   // streams while requests run.
-  PK_REQUIRE(lib_pool() != nullptr, "could not create the library memory pool");
-  {
-    cudaStream_t ps = nullptr;
-    PK_CUDA(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
-    void* blk = nullptr;
-    cudaError_t e = cudaMallocFromPoolAsync(&blk, hbm_budget_bytes, lib_pool(), ps);
-    if (e == cudaSuccess) e = cudaFreeAsync(blk, ps);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ps);
-    cudaStreamDestroy(ps);
-    if (e != cudaSuccess) return cuda_status(e, "reserving the server's HBM budget");
-  }
+  if ((rc = pkg_reserve_memory(hbm_budget_bytes))) return rc;
   pkg_server* s = new pkg_server();
   PK_CUDA(cudaGetDevice(&s->device));
   s->budget = hbm_budget_bytes;
