@@ -90,3 +90,33 @@ def test_whole_proof_at_2p20_constraints_verifies():
     sp, cw, proof = prove_r1cs(d, p, blinding_seed=1, transcript_domain=3)
     wp = O.whir_params(21, 3, 2, 128, 10)
     assert O.verify_r1cs_whir(h, wp, 3, sp, cw, proof) == 0
+
+
+def test_concurrent_whole_proofs_equal_sequential():
+    """Four host threads with their own streams prove the same resident
+    circuit at once (the batched bench's pattern); each proof equals the
+    same call made alone."""
+    import threading
+    from provekit_b200._lib import check, lib
+    from provekit_b200.prover import HostR1CS, prove_r1cs, whir_params_for
+    h = HostR1CS(41, 1 << 13, 1 << 11)
+    d = h.to_device()
+    p = whir_params_for(d, 3, 2, 64, 4)
+    alone = [prove_r1cs(d, p, blinding_seed=10 + i, transcript_domain=20 + i) for i in range(8)]
+    check(lib().pkg_reserve_memory(1 << 30))
+    streams = [torch.cuda.Stream() for _ in range(4)]
+    got = [None] * 8
+
+    def worker(j):
+        for i in range(j, 8, 4):
+            got[i] = prove_r1cs(d, p, blinding_seed=10 + i, transcript_domain=20 + i,
+                                stream=streams[j])
+
+    th = [threading.Thread(target=worker, args=(j,)) for j in range(4)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for (sp, cw, pr), (esp, ecw, epr) in zip(got, alone):
+        assert_same(sp, esp)
+        assert np.array_equal(cw, ecw) and np.array_equal(pr, epr)
