@@ -484,10 +484,21 @@ typedef struct pkg_whir_params_s {
   uint32_t ood_samples;     /* OOD samples per commitment (0..4)            */
   uint32_t pow_bits;        /* grinding per round (0..27, 0 = none)         */
   uint32_t final_pow_bits;
+  uint32_t batch_size;      /* polynomials committed together: 1, 2 or 4  */
   uint32_t queries[PKG_WHIR_MAX_ROUNDS + 1]; /* rounds 0..R-1, final at R   */
 } pkg_whir_params;
 /* Schedule: R + 1 = max(1, ceil((n - 6) / k)) folds; queries[r] =
- * ceil(2 (security - pow) / rate_r), rate_r = log_inv_rate + r (k - 1). */
+ * ceil(2 (security - pow) / rate_r), rate_r = log_inv_rate + r (k - 1);
+ * batch_size 1.
+ * Batches (whir's ZK commitment, as the reference's Go verifier reads it:
+ * RunZKWhir and parseBatchedCommitment, recursive-verifier/app/circuit/whir.go:53-218,
+ * mtUtilities.go:51-119): batch_size polynomials f_i of 2^n coefficients are
+ * committed in one tree whose row holds f_0's 2^k values, then f_1's, ...
+ * (pkg_whir_commit of their concatenation with folding factor k +
+ * log2 batch_size); after every polynomial's OOD answers a batching
+ * challenge b is drawn, the statement values are sent per polynomial, the
+ * rounds prove c = sum_i b^i f_i, and the first codeword's openings are the
+ * wide rows. */
 int pkg_whir_params_init(pkg_whir_params *p, unsigned num_variables, unsigned folding_factor,
                          unsigned log_inv_rate, unsigned security_bits, unsigned pow_bits);
 size_t pkg_whir_commit_words(const pkg_whir_params *p);
@@ -502,18 +513,22 @@ int pkg_transcript_squeeze_bytes(pkg_transcript *t, uint8_t *out, size_t n);
 #define PKG_SUBSET_ZETA 0
 #define PKG_SUBSET_MOBIUS_T 1
 int pkg_subset_transform(uint64_t *v, unsigned n, int mode, pkg_stream_t stream);
-/* The commitment's transcript part, after pkg_whir_commit(coeffs, 2^n,
- * folding_factor, log_inv_rate, no masks, PKG_LEAF_CANONICAL): absorb the root,
- * draw ood_samples points, absorb f(z).  coeffs, layers: device;
- * commit_words (4 + 4 ood_samples: root, answers), ood_points: host.
+/* The commitment's transcript part, after pkg_whir_commit(coeffs,
+ * batch_size 2^n, folding_factor + log2 batch_size, log_inv_rate, no masks,
+ * PKG_LEAF_CANONICAL): absorb the root, draw ood_samples points, absorb
+ * f_i(z_j) polynomial by polynomial, and for a batch draw the batching
+ * challenge.  coeffs (batch_size x 2^n, concatenated), layers: device;
+ * commit_words (4 + 4 ood_samples batch_size: root, answers), ood_points
+ * (ood_samples, then the batching challenge for a batch): host.
  * Synchronous. */
 int pkg_whir_commit_ood(const pkg_whir_params *p, pkg_transcript *t, const uint64_t *coeffs,
                         const uint8_t *layers, uint64_t *commit_words, uint64_t *ood_points,
                         pkg_stream_t stream);
 /* The proof of num_covectors (<= 16) statements: covectors device
- * (num_covectors x 2^n Fr, coefficient space); coeffs, codeword, layers the
- * commitment (device); ood_points from pkg_whir_commit_ood; proof: host,
- * pkg_whir_proof_words words.  Synchronous; t advances past the proof. */
+ * (num_covectors x 2^n Fr, coefficient space); coeffs (batch_size x 2^n),
+ * codeword, layers the commitment (device); ood_points from
+ * pkg_whir_commit_ood; proof: host, pkg_whir_proof_words words.
+ * Synchronous; t advances past the proof. */
 int pkg_whir_prove(const pkg_whir_params *p, pkg_transcript *t, const uint64_t *coeffs,
                    const uint64_t *codeword, const uint8_t *layers, const uint64_t *ood_points,
                    const uint64_t *covectors, size_t num_covectors, uint64_t *proof,

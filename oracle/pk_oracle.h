@@ -205,6 +205,7 @@ typedef struct {
     uint32_t ood_samples;     /* out-of-domain samples per commitment         */
     uint32_t pow_bits;        /* grinding per round (0: none)                 */
     uint32_t final_pow_bits;
+    uint32_t batch_size;      /* polynomials committed together: 1, 2 or 4  */
     uint32_t queries[PKO_WHIR_MAX_ROUNDS + 1]; /* STIR queries of rounds 0..R-1, final at R */
 } pko_whir_params;
 /* The schedule: R + 1 = max(1, ceil((n - 6) / k)) folds of k variables,
@@ -219,16 +220,30 @@ void pko_transcript_squeeze_bytes(pko_transcript *t, uint8_t *out, size_t n);
 /* In place over 2^n entries: zeta: v[b | 2^i] += v[b]; mobius_t: v[b] -= v[b | 2^i]. */
 void pko_subset_zeta(uint64_t *v, unsigned n);
 void pko_subset_mobius_t(uint64_t *v, unsigned n);
-/* The commitment: codeword (2^(n + log_inv_rate) Fr) of 2^k contiguous
+/* Batches (the ZK commitment, RunZKWhir + parseBatchedCommitment,
+ * recursive-verifier/app/circuit/whir.go:53-218, mtUtilities.go:51-119):
+ * batch_size polynomials f_0..f_{B-1} of 2^n coefficients each are committed
+ * in one tree whose row i holds f_0's 2^k values, then f_1's, ...: the
+ * commitment of their concatenation with folding factor k + log2 B.  After
+ * the OOD answers of every polynomial a batching challenge b is drawn; the
+ * proof is about c = sum_i b^i f_i, with every statement's value sent per
+ * polynomial, and the first codeword's openings are the wide rows, which
+ * the verifier collapses with powers of b (rlcBatchedLeaves) before folding.
+ *
+ * The commitment: codeword (2^(n + log_inv_rate) Fr) of 2^k contiguous
  * messages and its tree over canonical leaves (2 L - 1 digests). */
 int pko_whir_commit(const uint64_t *coeffs, size_t num_coeffs, unsigned k, unsigned log_inv_rate,
                     uint64_t *codeword, uint8_t *layers);
-/* Absorb the root, draw the commitment's OOD points, absorb f(z).  words:
- * root (4) + answers (4 ood); ood_points: 4 ood. */
+/* Absorb the root, draw the commitment's OOD points, absorb f_i(z_j)
+ * (polynomial-major), and with batch_size > 1 draw the batching challenge.
+ * coeffs: batch_size x 2^n (concatenated).  words: root (4) + answers
+ * (4 batch_size ood); ood_points: 4 ood, then the batching challenge when
+ * batch_size > 1. */
 int pko_whir_commit_ood(const pko_whir_params *p, pko_transcript *t, const uint64_t *coeffs,
                         const uint8_t root[32], uint64_t *commit_words, uint64_t *ood_points);
 /* The proof (pko_whir_proof_words words) of the ncov covectors (ncov x 2^n,
- * coefficient space) against the commitment. */
+ * coefficient space) against the commitment (coeffs: batch_size x 2^n;
+ * codeword and layers: the commitment of their concatenation). */
 int pko_whir_prove(const pko_whir_params *p, pko_transcript *t, const uint64_t *coeffs,
                    const uint64_t *codeword, const uint8_t *layers, const uint64_t *commit_words,
                    const uint64_t *ood_points, const uint64_t *covectors, size_t ncov,

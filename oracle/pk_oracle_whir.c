@@ -58,6 +58,7 @@ static int params_ok(const pko_whir_params *p) {
     if (p->log_inv_rate < 1 || p->log_inv_rate > 8) return 0;
     if ((R + 1) * k + p->final_vars != n) return 0;
     if (p->ood_samples > 4 || p->pow_bits > 27 || p->final_pow_bits > 27) return 0;
+    if (p->batch_size != 1 && p->batch_size != 2 && p->batch_size != 4) return 0;
     if (n + p->log_inv_rate < k + R + 1) return 0; /* every codeword has >= 2 rows */
     for (unsigned r = 0; r <= R; r++)
         if (p->queries[r] < 1 || p->queries[r] > 4096) return 0;
@@ -81,6 +82,7 @@ int pko_whir_params_init(pko_whir_params *p, unsigned n, unsigned k, unsigned lo
     p->ood_samples = 1;
     p->pow_bits = pow_bits;
     p->final_pow_bits = pow_bits;
+    p->batch_size = 1;
     for (unsigned r = 0; r <= p->num_rounds; r++) {
         unsigned rate = log_inv_rate + r * (k - 1);
         unsigned q = (2 * (security_bits - pow_bits) + rate - 1) / rate;
@@ -89,18 +91,27 @@ int pko_whir_params_init(pko_whir_params *p, unsigned n, unsigned k, unsigned lo
     return params_ok(p) ? 0 : PKO_WHIR_BAD_PARAMS;
 }
 
-size_t pko_whir_commit_words(const pko_whir_params *p) { return 4 + 4 * (size_t)p->ood_samples; }
+size_t pko_whir_commit_words(const pko_whir_params *p) {
+    return 4 + 4 * (size_t)p->ood_samples * p->batch_size;
+}
+
+/* Fr per opened row of codeword r: the first codeword holds every batched
+ * polynomial's values. */
+static size_t row_fr(const pko_whir_params *p, unsigned r) {
+    return ((size_t)1 << p->folding_factor) * (r == 0 ? p->batch_size : 1);
+}
 
 size_t pko_whir_proof_words(const pko_whir_params *p, size_t ncov) {
     if (!params_ok(p)) return 0;
-    const size_t K = (size_t)1 << p->folding_factor, k = p->folding_factor;
-    size_t w = 4 * ncov + 12 * k;
+    const size_t k = p->folding_factor;
+    size_t w = 4 * ncov * p->batch_size + 12 * k;
     for (unsigned r = 0; r < p->num_rounds; r++)
         w += 4 + 4 * (size_t)p->ood_samples + (p->pow_bits ? 1 : 0) +
-             (size_t)p->queries[r] * (4 * K + 4 * rows_log(p, r)) + 12 * k;
+             (size_t)p->queries[r] * (4 * row_fr(p, r) + 4 * rows_log(p, r)) + 12 * k;
     const unsigned R = p->num_rounds;
     w += 4 * ((size_t)1 << p->final_vars) + (p->final_pow_bits ? 1 : 0) +
-         (size_t)p->queries[R] * (4 * K + 4 * rows_log(p, R)) + 12 * (size_t)p->final_vars;
+         (size_t)p->queries[R] * (4 * row_fr(p, R) + 4 * rows_log(p, R)) +
+         12 * (size_t)p->final_vars;
     return w;
 }
 
@@ -292,6 +303,7 @@ static int stir_indices_from(pko_transcript *t, size_t q, size_t L, uint64_t *id
 
 static int stir_prove(pko_transcript *t, size_t q, size_t L, size_t K, const uint64_t *cw,
                       const uint8_t *layers, uint64_t *idx, cursor *c) {
+    /* K: Fr per row (the batch's width for the first codeword) */
     int depth = stir_indices_from(t, q, L, idx);
     if (depth < 0) return depth;
     for (size_t i = 0; i < q; i++) {
@@ -314,11 +326,15 @@ int pko_whir_commit_ood(const pko_whir_params *p, pko_transcript *t, const uint6
     pko_transcript_absorb(t, rm);
     cp4(commit_words, rc);
     const size_t N = (size_t)1 << p->num_variables;
-    for (unsigned j = 0; j < p->ood_samples; j++) pko_transcript_squeeze(t, ood_points + 4 * j);
-    for (unsigned j = 0; j < p->ood_samples; j++) {
-        pko_poly_eval(commit_words + 4 + 4 * j, coeffs, N, ood_points + 4 * j);
-        pko_transcript_absorb(t, commit_words + 4 + 4 * j);
-    }
+    const unsigned o = p->ood_samples;
+    for (unsigned j = 0; j < o; j++) pko_transcript_squeeze(t, ood_points + 4 * j);
+    for (unsigned i = 0; i < p->batch_size; i++)
+        for (unsigned j = 0; j < o; j++) {
+            uint64_t *ans = commit_words + 4 + 4 * (i * o + j);
+            pko_poly_eval(ans, coeffs + 4 * N * i, N, ood_points + 4 * j);
+            pko_transcript_absorb(t, ans);
+        }
+    if (p->batch_size > 1) pko_transcript_squeeze(t, ood_points + 4 * o);
     return 0;
 }
 
@@ -346,15 +362,27 @@ int pko_whir_prove(const pko_whir_params *p, pko_transcript *t, const uint64_t *
         rc = -2;
         goto done;
     }
-    memcpy(E, coeffs, 32 * N);
+    /* the batch: c = sum_i b^i f_i (b drawn at the commitment) */
+    const unsigned Bn = p->batch_size;
+    uint64_t bp[4 * 4];
+    powers(bp, ood_points + 4 * o, Bn);
+    memset(f, 0, 32 * N);
+    for (unsigned i = 0; i < Bn; i++)
+        for (size_t b = 0; b < N; b++) {
+            uint64_t x[4];
+            pko_fr_mul(x, bp + 4 * i, coeffs + 4 * (N * i + b));
+            pko_fr_add(f + 4 * b, f + 4 * b, x);
+        }
+    memcpy(E, f, 32 * N);
     pko_subset_zeta(E, n);
 
-    /* statement values */
-    for (size_t a = 0; a < ncov; a++) {
-        pko_dot(proof + c.pos, covectors + 4 * N * a, coeffs, N);
-        pko_transcript_absorb(t, proof + c.pos);
-        c.pos += 4;
-    }
+    /* statement values, polynomial by polynomial */
+    for (unsigned i = 0; i < Bn; i++)
+        for (size_t a = 0; a < ncov; a++) {
+            pko_dot(proof + c.pos, covectors + 4 * N * a, coeffs + 4 * N * i, N);
+            pko_transcript_absorb(t, proof + c.pos);
+            c.pos += 4;
+        }
     pko_transcript_squeeze(t, gamma);
     powers(pw, gamma, o + ncov);
     for (size_t a = 0; a < ncov; a++) {
@@ -373,7 +401,6 @@ int pko_whir_prove(const pko_whir_params *p, pko_transcript *t, const uint64_t *
     size_t size = N;
     if ((rc = sc_prove(t, E, w, &size, k, alpha, &c))) goto done;
 
-    memcpy(f, coeffs, 32 * N);
     unsigned nv = n;
     const uint64_t *cw_r = codeword;
     const uint8_t *lay_r = layers;
@@ -404,7 +431,7 @@ int pko_whir_prove(const pko_whir_params *p, pko_transcript *t, const uint64_t *
         }
         if (p->pow_bits) pow_prove(t, p->pow_bits, &c);
         const size_t Lr = (size_t)1 << rows_log(p, r), q = p->queries[r];
-        if ((rc = stir_prove(t, q, Lr, K, cw_r, lay_r, idx, &c))) goto done;
+        if ((rc = stir_prove(t, q, Lr, row_fr(p, r), cw_r, lay_r, idx, &c))) goto done;
         pko_rs_evaluation_points(Lr, (const size_t *)idx, q, upts + 4 * o);
         pko_transcript_squeeze(t, gamma);
         powers(pw, gamma, o + q);
@@ -433,7 +460,8 @@ int pko_whir_prove(const pko_whir_params *p, pko_transcript *t, const uint64_t *
         pko_transcript_absorb(t, g + 4 * i);
     }
     if (p->final_pow_bits) pow_prove(t, p->final_pow_bits, &c);
-    if ((rc = stir_prove(t, p->queries[R], (size_t)1 << rows_log(p, R), K, cw_r, lay_r, idx, &c)))
+    if ((rc = stir_prove(t, p->queries[R], (size_t)1 << rows_log(p, R), row_fr(p, R), cw_r, lay_r,
+                         idx, &c)))
         goto done;
     {
         uint64_t *rfin = (uint64_t *)malloc(32 * (nv ? nv : 1));
@@ -513,14 +541,17 @@ static int pow_verify(pko_transcript *t, reader *rd, unsigned bits) {
     return less4(h, thr) ? 0 : PKO_WHIR_REJECT_POW;
 }
 
-/* Reads q openings of a codeword of L rows, checks them against root and
- * writes their folds (MultivarPoly with ralpha) and evaluation points. */
+/* Reads q openings of a codeword of L rows of `batch` polynomials, checks
+ * them against root, collapses each row with the powers bp of the batching
+ * challenge (rlcBatchedLeaves, mtUtilities.go:98-119) and writes the folds
+ * (MultivarPoly with ralpha) and the evaluation points. */
 static int stir_verify(pko_transcript *t, reader *rd, size_t q, size_t L, unsigned k,
-                       const uint64_t root[4], const uint64_t *ralpha, uint64_t *folds,
-                       uint64_t *points) {
-    const size_t K = (size_t)1 << k;
+                       unsigned batch, const uint64_t *bp, const uint64_t root[4],
+                       const uint64_t *ralpha, uint64_t *folds, uint64_t *points) {
+    const size_t K = (size_t)1 << k, W = K * batch;
     uint64_t *idx = (uint64_t *)malloc(8 * q);
-    uint64_t *row = (uint64_t *)malloc(32 * K), *canon = (uint64_t *)malloc(32 * K);
+    uint64_t *row = (uint64_t *)malloc(32 * W), *canon = (uint64_t *)malloc(32 * W);
+    uint64_t col[64 * 4];
     int rc = 0;
     if (!idx || !row || !canon) {
         rc = -2;
@@ -532,7 +563,7 @@ static int stir_verify(pko_transcript *t, reader *rd, size_t q, size_t L, unsign
         goto out;
     }
     for (size_t i = 0; i < q; i++) {
-        for (size_t j = 0; j < K; j++) cp4(row + 4 * j, get_fr(rd));
+        for (size_t j = 0; j < W; j++) cp4(row + 4 * j, get_fr(rd));
         if (rd->bad || rd->pos + 4 * (size_t)depth > rd->len) {
             rd->bad = 1;
             rc = PKO_WHIR_REJECT_FORMAT;
@@ -540,13 +571,21 @@ static int stir_verify(pko_transcript *t, reader *rd, size_t q, size_t L, unsign
         }
         const uint8_t *path = (const uint8_t *)(rd->p + rd->pos);
         rd->pos += 4 * (size_t)depth;
-        memcpy(canon, row, 32 * K);
-        pko_from_mont_many(canon, K);
-        if (!pko_merkle_verify(canon, K, idx[i], path, (size_t)depth, (const uint8_t *)root)) {
+        memcpy(canon, row, 32 * W);
+        pko_from_mont_many(canon, W);
+        if (!pko_merkle_verify(canon, W, idx[i], path, (size_t)depth, (const uint8_t *)root)) {
             rc = PKO_WHIR_REJECT_MERKLE;
             goto out;
         }
-        pko_whir_fold_rows(row, 1, k, ralpha, folds + 4 * i);
+        for (size_t j = 0; j < K; j++) {
+            uint64_t acc[4] = {0, 0, 0, 0}, x[4];
+            for (unsigned b = 0; b < batch; b++) {
+                pko_fr_mul(x, bp + 4 * b, row + 4 * (b * K + j));
+                pko_fr_add(acc, acc, x);
+            }
+            cp4(col + 4 * j, acc);
+        }
+        pko_whir_fold_rows(col, 1, k, ralpha, folds + 4 * i);
     }
     pko_rs_evaluation_points(L, (const size_t *)idx, q, points);
 out:
@@ -570,17 +609,18 @@ int pko_whir_verify_commit(const pko_whir_params *p, pko_transcript *t,
     pko_fr_to_mont(rm, commit_words);
     pko_transcript_absorb(t, rm);
     for (unsigned j = 0; j < p->ood_samples; j++) pko_transcript_squeeze(t, ood_points + 4 * j);
-    for (unsigned j = 0; j < p->ood_samples; j++) {
+    for (unsigned j = 0; j < p->ood_samples * p->batch_size; j++) {
         if (!is_canon(commit_words + 4 + 4 * j)) return PKO_WHIR_REJECT_FORMAT;
         pko_transcript_absorb(t, commit_words + 4 + 4 * j);
     }
+    if (p->batch_size > 1) pko_transcript_squeeze(t, ood_points + 4 * p->ood_samples);
     return 0;
 }
 
 int pko_whir_verify(const pko_whir_params *p, pko_transcript *t, const uint64_t *covectors,
                     size_t ncov, const uint64_t *commit_words, const uint64_t *proof,
                     size_t proof_words) {
-    uint64_t z[4 * 4];
+    uint64_t z[5 * 4];
     int rc = pko_whir_verify_commit(p, t, commit_words, z);
     if (rc) return rc;
     return pko_whir_verify_proof(p, t, covectors, ncov, commit_words, z, proof, proof_words);
@@ -613,20 +653,34 @@ int pko_whir_verify_proof(const pko_whir_params *p, pko_transcript *t, const uin
     /* the commitment's root and OOD points (pko_whir_verify_commit) */
     cp4(root, commit_words);
     if (o) memcpy(z0, ood_points, 32 * o);
-    /* statement values and the initial claimed sum */
-    uint64_t vals[16 * 4];
-    for (size_t a = 0; a < ncov; a++) {
-        cp4(vals + 4 * a, get_fr(&rd));
-        if (rd.bad) {
-            rc = PKO_WHIR_REJECT_FORMAT;
-            goto done;
+    /* statement values (per polynomial) and the initial claimed sum over
+     * the batch's combination c = sum_i b^i f_i */
+    const unsigned Bn = p->batch_size;
+    uint64_t bp[4 * 4], vals[16 * 4], cans[4 * 4];
+    powers(bp, ood_points + 4 * o, Bn);
+    memset(vals, 0, sizeof vals);
+    memset(cans, 0, sizeof cans);
+    for (unsigned i = 0; i < Bn; i++)
+        for (size_t a = 0; a < ncov; a++) {
+            uint64_t v[4];
+            cp4(v, get_fr(&rd));
+            if (rd.bad) {
+                rc = PKO_WHIR_REJECT_FORMAT;
+                goto done;
+            }
+            pko_transcript_absorb(t, v);
+            pko_fr_mul(x, bp + 4 * i, v);
+            pko_fr_add(vals + 4 * a, vals + 4 * a, x);
         }
-        pko_transcript_absorb(t, vals + 4 * a);
-    }
+    for (unsigned i = 0; i < Bn; i++)
+        for (unsigned j = 0; j < o; j++) {
+            pko_fr_mul(x, bp + 4 * i, commit_words + 4 + 4 * (i * o + j));
+            pko_fr_add(cans + 4 * j, cans + 4 * j, x);
+        }
     pko_transcript_squeeze(t, gamma);
     powers(pw0, gamma, o + ncov);
     for (unsigned j = 0; j < o; j++) {
-        pko_fr_mul(x, pw0 + 4 * j, commit_words + 4 + 4 * j);
+        pko_fr_mul(x, pw0 + 4 * j, cans + 4 * j);
         pko_fr_add(last, last, x);
     }
     for (size_t a = 0; a < ncov; a++) {
@@ -667,8 +721,8 @@ int pko_whir_verify_proof(const pko_whir_params *p, pko_transcript *t, const uin
         }
         if (p->pow_bits && (rc = pow_verify(t, &rd, p->pow_bits))) goto done;
         reverse_fr(ralpha, r_all + 4 * (nr - k), k);
-        if ((rc = stir_verify(t, &rd, q, (size_t)1 << rows_log(p, r), k, prev_root, ralpha, folds,
-                              rc_r->pts + 4 * o)))
+        if ((rc = stir_verify(t, &rd, q, (size_t)1 << rows_log(p, r), k, r == 0 ? Bn : 1, bp,
+                              prev_root, ralpha, folds, rc_r->pts + 4 * o)))
             goto done;
         pko_transcript_squeeze(t, gamma);
         powers(rc_r->coef, gamma, o + q);
@@ -696,7 +750,8 @@ int pko_whir_verify_proof(const pko_whir_params *p, pko_transcript *t, const uin
     {
         const size_t q = p->queries[R];
         reverse_fr(ralpha, r_all + 4 * (nr - k), k);
-        if ((rc = stir_verify(t, &rd, q, (size_t)1 << rows_log(p, R), k, root, ralpha, folds, ypts)))
+        if ((rc = stir_verify(t, &rd, q, (size_t)1 << rows_log(p, R), k, R == 0 ? Bn : 1, bp, root,
+                              ralpha, folds, ypts)))
             goto done;
         for (size_t i = 0; i < q; i++) {
             pko_poly_eval(x, fc, (size_t)1 << nf, ypts + 4 * i);

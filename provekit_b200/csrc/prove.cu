@@ -89,6 +89,7 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     PK_REQUIRE(pkg_whir_proof_words(whir, 3) != 0, "invalid WHIR parameters");
     PK_REQUIRE(whir->num_variables == m, "WHIR parameters for %u variables, the R1CS needs %zu",
                whir->num_variables, m);
+    PK_REQUIRE(whir->batch_size == 1, "batched WHIR parameters are not supported here");
   }
   memset(out, 0, sizeof *out);
   memset(g_stage_ms, 0, sizeof g_stage_ms);

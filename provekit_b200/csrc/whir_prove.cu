@@ -123,6 +123,11 @@ static unsigned rows_log(const pkg_whir_params* p, unsigned r) {
   return p->num_variables + p->log_inv_rate - p->folding_factor - r;
 }
 
+// Fr per opened row of codeword r: the first holds every batched polynomial.
+static size_t row_fr(const pkg_whir_params* p, unsigned r) {
+  return (size_t(1) << p->folding_factor) * (r == 0 ? p->batch_size : 1);
+}
+
 static bool params_ok(const pkg_whir_params* p) {
   if (!p) return false;
   const unsigned n = p->num_variables, k = p->folding_factor, R = p->num_rounds;
@@ -130,6 +135,7 @@ static bool params_ok(const pkg_whir_params* p) {
   if (p->log_inv_rate < 1 || p->log_inv_rate > 8) return false;
   if ((R + 1) * k + p->final_vars != n) return false;
   if (p->ood_samples > 4 || p->pow_bits > 27 || p->final_pow_bits > 27) return false;
+  if (p->batch_size != 1 && p->batch_size != 2 && p->batch_size != 4) return false;
   if (n + p->log_inv_rate < k + R + 1) return false;
   for (unsigned r = 0; r <= R; r++)
     if (p->queries[r] < 1 || p->queries[r] > 4096) return false;
@@ -242,7 +248,7 @@ class WhirProver {
   }
   int sumcheck_phase(unsigned rounds, std::vector<HostFr>& rands);
   int pow_step(unsigned bits);
-  int stir_step(size_t q, size_t L, const uint64_t* cw, const uint8_t* layers,
+  int stir_step(size_t q, size_t L, size_t row, const uint64_t* cw, const uint8_t* layers,
                 std::vector<uint64_t>& idx);
   int add_constraints(const std::vector<HostFr>& points, unsigned nv,
                       const std::vector<HostFr>& coefs);
@@ -303,10 +309,10 @@ int WhirProver::pow_step(unsigned bits) {
 
 // getStirChallenges (circuit/whir_utilities.go:49-78) on a codeword of L
 // rows, then each queried row and its authentication path into the proof.
-int WhirProver::stir_step(size_t q, size_t L, const uint64_t* cw, const uint8_t* layers,
+int WhirProver::stir_step(size_t q, size_t L, size_t K, const uint64_t* cw, const uint8_t* layers,
                           std::vector<uint64_t>& idx) {
+  // K: Fr per row (the batch's width for the first codeword)
   const int depth = log2_exact(L);
-  const size_t K = size_t(1) << p_->folding_factor;
   const size_t nb = (size_t)(depth + 7) / 8;
   std::vector<uint8_t> bytes(q * nb + 1);
   PK_TRY(pkg_transcript_squeeze_bytes(t_, bytes.data(), q * nb));
@@ -344,10 +350,14 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
   const size_t N = size_t(1) << n, K = size_t(1) << k;
   const pkg_stream_t ps = reinterpret_cast<pkg_stream_t>(s_);
 
-  PoolBuf E, W, A, B, cw_own, lay_own, cw_next, lay_next;
-  std::vector<HostFr> vals(ncov);
+  PoolBuf E, W, A, B, Cb, cw_own, lay_own, cw_next, lay_next;
+  const unsigned nb = p_->batch_size;
+  std::vector<HostFr> vals(ncov * nb);
   HostFr gamma;
   std::vector<HostFr> pw;
+  // the batch's combination c = sum_i b^i f_i (b drawn at the commitment);
+  // a single polynomial is c itself
+  const uint64_t* poly = coeffs;
   {
   PhaseTimer pt(0);
   PK_TRY(W.alloc(32 * N, s_));
@@ -355,25 +365,41 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
   PK_TRY(B.alloc(32 * (N >> k), s_));
   w_ = W.as<uint64_t>();
   size_ = N;
-  if (hat) {
+  const std::vector<HostFr> bp =
+      powers_of(nb > 1 ? HostFr::from_limbs(ood_points + 4 * o) : HostFr::one(), nb);
+  if (nb > 1) {
+    PK_TRY(Cb.alloc(32 * N, s_));
+    CovParams P;
+    memset(&P, 0, sizeof P);
+    P.cov = coeffs;
+    P.stride = N;
+    P.ncov = (int)nb;
+    for (unsigned i = 0; i < nb; i++) memcpy(P.coef[i], bp[i].l, 32);
+    combine_covectors_kernel<<<ew_grid(N), 256, 0, s_>>>(Cb.as<uint64_t>(), N, P);
+    PK_CHECK_LAUNCH("combine_covectors_kernel");
+    poly = Cb.as<uint64_t>();
+  }
+  if (hat && nb == 1) {
     E_ = hat;  // the caller's zeta(coeffs), folded in place from here on
   } else {
     PK_TRY(E.alloc(32 * N, s_));
     E_ = E.as<uint64_t>();
-    PK_CUDA(cudaMemcpyAsync(E_, coeffs, 32 * N, cudaMemcpyDeviceToDevice, s_));
+    PK_CUDA(cudaMemcpyAsync(E_, poly, 32 * N, cudaMemcpyDeviceToDevice, s_));
     PK_TRY(subset_transform_device<true>(E_, n, s_));
   }
 
-  // the statement values, then the combination randomness over
-  // (commitment OOD answers, values)
-  for (size_t a = 0; a < ncov; a++) {
-    if (values)
-      memcpy(vals[a].l, values + 4 * a, 32);
-    else
-      PK_TRY(pkg_dot(covectors + 4 * N * a, coeffs, N, vals[a].l, ps));
-    put(vals[a]);
-  }
-  gamma = absorb_squeeze(t_, vals.data(), ncov);
+  // the statement values, polynomial by polynomial, then the combination
+  // randomness over (commitment OOD answers, values)
+  for (unsigned i = 0; i < nb; i++)
+    for (size_t a = 0; a < ncov; a++) {
+      HostFr& v = vals[i * ncov + a];
+      if (values)
+        memcpy(v.l, values + 4 * (i * ncov + a), 32);
+      else
+        PK_TRY(pkg_dot(covectors + 4 * N * a, coeffs + 4 * N * i, N, v.l, ps));
+      put(v);
+    }
+  gamma = absorb_squeeze(t_, vals.data(), ncov * nb);
   pw = powers_of(gamma, o + ncov);
   if (ncov) {
     CovParams P;
@@ -401,7 +427,7 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
     PK_TRY(sumcheck_phase(k, alpha));
   }
 
-  const uint64_t* f = coeffs;  // current polynomial's coefficients
+  const uint64_t* f = poly;  // current polynomial's coefficients
   unsigned nv = n;
   const uint64_t* cw_r = codeword;
   const uint8_t* lay_r = layers;
@@ -454,7 +480,7 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
     const size_t Lr = size_t(1) << rows_log(p_, r), q = p_->queries[r];
     {
       PhaseTimer pt(5);
-      PK_TRY(stir_step(q, Lr, cw_r, lay_r, idx));
+      PK_TRY(stir_step(q, Lr, row_fr(p_, r), cw_r, lay_r, idx));
       std::vector<size_t> sidx(idx.begin(), idx.end());
       points.resize(o + q);
       PK_TRY(pkg_rs_evaluation_points(Lr, sidx.data(), q, points[o].l));
@@ -498,7 +524,8 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
   }
   {
     PhaseTimer pt(5);
-    PK_TRY(stir_step(p_->queries[R], size_t(1) << rows_log(p_, R), cw_r, lay_r, idx));
+    PK_TRY(stir_step(p_->queries[R], size_t(1) << rows_log(p_, R), row_fr(p_, R), cw_r, lay_r,
+                     idx));
   }
   {
     PhaseTimer pt(1);
@@ -545,6 +572,7 @@ extern "C" int pkg_whir_params_init(pkg_whir_params* p, unsigned n, unsigned k,
   p->ood_samples = 1;
   p->pow_bits = pow_bits;
   p->final_pow_bits = pow_bits;
+  p->batch_size = 1;
   for (unsigned r = 0; r <= p->num_rounds; r++) {
     const unsigned rate = log_inv_rate + r * (k - 1);
     const unsigned q = (2 * (security_bits - pow_bits) + rate - 1) / rate;
@@ -555,19 +583,20 @@ extern "C" int pkg_whir_params_init(pkg_whir_params* p, unsigned n, unsigned k,
 }
 
 extern "C" size_t pkg_whir_commit_words(const pkg_whir_params* p) {
-  return p ? 4 + 4 * (size_t)p->ood_samples : 0;
+  return p ? 4 + 4 * (size_t)p->ood_samples * p->batch_size : 0;
 }
 
 extern "C" size_t pkg_whir_proof_words(const pkg_whir_params* p, size_t ncov) {
   if (!params_ok(p)) return 0;
-  const size_t K = size_t(1) << p->folding_factor, k = p->folding_factor;
-  size_t w = 4 * ncov + 12 * k;
+  const size_t k = p->folding_factor;
+  size_t w = 4 * ncov * p->batch_size + 12 * k;
   for (unsigned r = 0; r < p->num_rounds; r++)
     w += 4 + 4 * (size_t)p->ood_samples + (p->pow_bits ? 1 : 0) +
-         (size_t)p->queries[r] * (4 * K + 4 * rows_log(p, r)) + 12 * k;
+         (size_t)p->queries[r] * (4 * row_fr(p, r) + 4 * rows_log(p, r)) + 12 * k;
   const unsigned R = p->num_rounds;
   w += 4 * (size_t(1) << p->final_vars) + (p->final_pow_bits ? 1 : 0) +
-       (size_t)p->queries[R] * (4 * K + 4 * rows_log(p, R)) + 12 * (size_t)p->final_vars;
+       (size_t)p->queries[R] * (4 * row_fr(p, R) + 4 * rows_log(p, R)) +
+       12 * (size_t)p->final_vars;
   return w;
 }
 
@@ -597,13 +626,18 @@ extern "C" int pkg_whir_commit_ood(const pkg_whir_params* p, pkg_transcript* t,
   pkg_transcript_absorb(t, rm.l);
   memcpy(commit_words, root.l, 32);
   const unsigned o = p->ood_samples;
+  const size_t N = size_t(1) << p->num_variables;
   for (unsigned j = 0; j < o; j++) pkg_transcript_squeeze(t, ood_points + 4 * j);
-  if (o) {
-    int rc = pkg_poly_eval_many(coeffs, size_t(1) << p->num_variables, ood_points, o,
-                                commit_words + 4, stream);
+  // f_i(z_j), polynomial by polynomial (parseBatchedCommitment,
+  // recursive-verifier/app/circuit/mtUtilities.go:51-76)
+  for (unsigned i = 0; o && i < p->batch_size; i++) {
+    int rc = pkg_poly_eval_many(coeffs + 4 * N * i, N, ood_points, o, commit_words + 4 + 4 * o * i,
+                                stream);
     if (rc) return rc;
   }
-  for (unsigned j = 0; j < o; j++) pkg_transcript_absorb(t, commit_words + 4 + 4 * j);
+  for (unsigned j = 0; j < o * p->batch_size; j++)
+    pkg_transcript_absorb(t, commit_words + 4 + 4 * j);
+  if (p->batch_size > 1) pkg_transcript_squeeze(t, ood_points + 4 * o);  // batching challenge
   return PKG_OK;
 }
 

@@ -108,6 +108,7 @@ class WhirParams(ctypes.Structure):
                 ("log_inv_rate", ctypes.c_uint32), ("num_rounds", ctypes.c_uint32),
                 ("final_vars", ctypes.c_uint32), ("ood_samples", ctypes.c_uint32),
                 ("pow_bits", ctypes.c_uint32), ("final_pow_bits", ctypes.c_uint32),
+                ("batch_size", ctypes.c_uint32),
                 ("queries", ctypes.c_uint32 * (MAX_ROUNDS + 1))]
 
     @classmethod
@@ -153,23 +154,26 @@ def squeeze_bytes(transcript, n: int) -> bytes:
 
 
 def commit(coeffs, params: WhirParams, stream=None):
-    """pkg_whir_commit of the 2^n coefficients with canonical leaves: (codeword, layers)."""
+    """pkg_whir_commit of the batch's batch_size x 2^n coefficients
+    (concatenated) with canonical leaves: (codeword, layers)."""
     fr_tensor(coeffs, "coeffs")
-    n, k, lr = params.num_variables, params.folding_factor, params.log_inv_rate
-    if coeffs.shape[0] != 1 << n:
-        raise ValueError("coeffs must hold 2^num_variables entries")
+    n, k, lr, nb = params.num_variables, params.folding_factor, params.log_inv_rate, \
+        params.batch_size
+    if coeffs.shape[0] != nb << n:
+        raise ValueError("coeffs must hold batch_size x 2^num_variables entries")
+    kb = k + {1: 0, 2: 1, 4: 2}[nb]
     L = (1 << (n - k)) << lr
-    cw = torch.empty(((1 << n) << lr, 4), dtype=torch.int64, device=coeffs.device)
+    cw = torch.empty(((nb << n) << lr, 4), dtype=torch.int64, device=coeffs.device)
     layers = torch.empty(((2 * L - 1) * 32,), dtype=torch.uint8, device=coeffs.device)
-    check(lib().pkg_whir_commit(ptr(coeffs), 1 << n, k, lr, None, 0, PKG_LEAF_CANONICAL, ptr(cw),
-                                ptr(layers), stream_handle(stream)))
+    check(lib().pkg_whir_commit(ptr(coeffs), nb << n, kb, lr, None, 0, PKG_LEAF_CANONICAL,
+                                ptr(cw), ptr(layers), stream_handle(stream)))
     return cw, layers
 
 
 def commit_ood(params: WhirParams, transcript, coeffs, layers, stream=None):
     """Root and OOD answers into the transcript: (commit_words, ood_points)."""
     words = np.zeros(params.commit_words(), np.uint64)
-    ood = np.zeros((max(params.ood_samples, 1), 4), np.uint64)
+    ood = np.zeros((params.ood_samples + 1, 4), np.uint64)
     check(lib().pkg_whir_commit_ood(ctypes.byref(params), ctypes.byref(transcript), ptr(coeffs),
                                     ptr(layers), words.ctypes.data, ood.ctypes.data,
                                     stream_handle(stream)))

@@ -83,7 +83,7 @@ def verify_r1cs_whir(h, wp, domain, spartan, cwords, proof):
     """The WHIR part of a whole proof: the commitment half on a fresh
     transcript, the proof half from the state the WHIR prover started from."""
     t0 = transcript(domain)
-    z = np.zeros((4, 4), np.uint64)
+    z = np.zeros((5, 4), np.uint64)
     rc = lib().pko_whir_verify_commit(ctypes.byref(wp), ctypes.byref(t0), p64(cwords), p64(z))
     if rc:
         return rc
@@ -196,6 +196,7 @@ class WhirParams(ctypes.Structure):
                 ("log_inv_rate", ctypes.c_uint32), ("num_rounds", ctypes.c_uint32),
                 ("final_vars", ctypes.c_uint32), ("ood_samples", ctypes.c_uint32),
                 ("pow_bits", ctypes.c_uint32), ("final_pow_bits", ctypes.c_uint32),
+                ("batch_size", ctypes.c_uint32),
                 ("queries", ctypes.c_uint32 * (WHIR_MAX_ROUNDS + 1))]
 
 
@@ -227,16 +228,21 @@ def whir_commit(coeffs: np.ndarray, k: int, log_inv_rate: int):
     return cw, layers
 
 
+def batch_log(p) -> int:
+    return {1: 0, 2: 1, 4: 2}[p.batch_size]
+
+
 def whir_prove(p: WhirParams, domain: int, coeffs: np.ndarray, covectors: np.ndarray):
-    """Commit + prove with a fresh transcript; returns (commit_words, proof)."""
+    """Commit + prove with a fresh transcript; returns (commit_words, proof).
+    coeffs: batch_size x 2^n (the batch's polynomials concatenated)."""
     c = np.ascontiguousarray(coeffs, dtype=np.uint64).reshape(-1, 4)
     cov = np.ascontiguousarray(covectors, dtype=np.uint64).reshape(-1, 4)
-    ncov = cov.shape[0] // max(c.shape[0], 1)
-    cw, layers = whir_commit(c, p.folding_factor, p.log_inv_rate)
+    ncov = cov.shape[0] >> p.num_variables
+    cw, layers = whir_commit(c, p.folding_factor + batch_log(p), p.log_inv_rate)
     root = np.ascontiguousarray(layers[-32:])
     t = transcript(domain)
     cwords = np.zeros(lib().pko_whir_commit_words(ctypes.byref(p)), np.uint64)
-    ood = np.zeros((max(p.ood_samples, 1), 4), np.uint64)
+    ood = np.zeros((p.ood_samples + 1, 4), np.uint64)
     assert lib().pko_whir_commit_ood(ctypes.byref(p), ctypes.byref(t), p64(c), p8(root),
                                      p64(cwords), p64(ood)) == 0
     proof = np.zeros(lib().pko_whir_proof_words(ctypes.byref(p), ncov), np.uint64)

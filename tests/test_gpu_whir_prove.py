@@ -50,7 +50,7 @@ def _device_proof(p, domain, c, cov):
     proof = W.prove(p, t, dc, cw, layers, ood, dcov)
     torch.cuda.synchronize()
     assert (dcov is None and cov.shape[0] == 0) or dcov.shape[0] == cov.shape[0]
-    assert N == dc.shape[0]
+    assert p.batch_size * N == dc.shape[0]
     return cw, layers, words, proof, (list(t.l), list(t.r))
 
 
@@ -68,6 +68,9 @@ CASES = [
     (16, 6, 2, 24, 0, {"ood_samples": 3}),
     (12, 1, 3, 20, 1, {}),
     (11, 3, 2, 40, 2, {"ood_samples": 0}),
+    (10, 3, 2, 40, 3, {"batch_size": 2}),
+    (12, 2, 1, 30, 2, {"batch_size": 4, "ood_samples": 2}),
+    (8, 4, 1, 20, 1, {"batch_size": 2}),
 ]
 
 
@@ -75,10 +78,10 @@ CASES = [
 def test_device_proof_equals_the_oracle_proof(n, k, lr, sec, pw, over):
     p, po = _params_pair(n, k, lr, sec, pw, over)
     for ncov in (0, 2):
-        c = O.sample_fr(3000 + n + ncov, 1 << n)
+        c = O.sample_fr(3000 + n + ncov, p.batch_size << n)
         cov = O.sample_fr(4000 + n + ncov, ncov << n) if ncov else np.zeros((0, 4), np.uint64)
         cw, layers, words, proof, _ = _device_proof(p, 0xabc + n, c, cov)
-        ocw, olayers = O.whir_commit(c, k, lr)
+        ocw, olayers = O.whir_commit(c, k + O.batch_log(po), lr)
         assert np.array_equal(host(cw), ocw)
         assert np.array_equal(layers.cpu().numpy(), olayers)
         owords, oproof = O.whir_prove(po, 0xabc + n, c, cov)

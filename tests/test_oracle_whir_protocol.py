@@ -17,10 +17,10 @@ import oracle_lib as O
 def layout(p, ncov):
     """Word offsets of every section of a proof (the order pko_whir_prove writes)."""
     k, K, o = p.folding_factor, 1 << p.folding_factor, p.ood_samples
-    n, lr = p.num_variables, p.log_inv_rate
+    n, lr, B = p.num_variables, p.log_inv_rate, p.batch_size
     pos = 0
     out = {"values": pos}
-    pos += 4 * ncov
+    pos += 4 * ncov * B
     out["sc0"] = pos
     pos += 12 * k
     rounds = []
@@ -34,8 +34,8 @@ def layout(p, ncov):
             pos += 1
         depth = n + lr - k - r
         d["open"] = pos
-        d["row_words"], d["path_words"] = 4 * K, 4 * depth
-        pos += p.queries[r] * (4 * K + 4 * depth)
+        d["row_words"], d["path_words"] = 4 * K * (B if r == 0 else 1), 4 * depth
+        pos += p.queries[r] * (d["row_words"] + 4 * depth)
         d["sc"] = pos
         pos += 12 * k
         rounds.append(d)
@@ -48,8 +48,8 @@ def layout(p, ncov):
         pos += 1
     depth = n + lr - k - R
     fin["open"] = pos
-    fin["row_words"], fin["path_words"] = 4 * K, 4 * depth
-    pos += p.queries[R] * (4 * K + 4 * depth)
+    fin["row_words"], fin["path_words"] = 4 * K * (B if R == 0 else 1), 4 * depth
+    pos += p.queries[R] * (fin["row_words"] + 4 * depth)
     fin["sc"] = pos
     pos += 12 * p.final_vars
     out["final"] = fin
@@ -65,6 +65,9 @@ CASES = [
                        "queries": [20, 12, 9, 7]}),                  # hand-set schedule, 1 final coeff
     (9, 3, 3, 30, 0, {"num_rounds": 1, "final_vars": 3, "final_pow_bits": 5,
                       "queries": [4, 1]}),
+    (10, 3, 2, 40, 3, {"batch_size": 2}),                            # the ZK batch
+    (12, 2, 1, 30, 2, {"batch_size": 4, "ood_samples": 2}),
+    (8, 4, 1, 20, 1, {"batch_size": 2}),                             # R = 0: final opens the batch
     (8, 2, 1, 32, 2, {}),
     (10, 3, 2, 40, 3, {}),
     (12, 3, 2, 60, 4, {"ood_samples": 2}),
@@ -76,9 +79,9 @@ CASES = [
 ]
 
 
-def _problem(n, ncov, seed):
+def _problem(n, ncov, seed, batch=1):
     N = 1 << n
-    return O.sample_fr(seed, N), O.sample_fr(seed + 1, max(ncov, 1) * N)[: ncov * N]
+    return O.sample_fr(seed, batch * N), O.sample_fr(seed + 1, max(ncov, 1) * N)[: ncov * N]
 
 
 @pytest.mark.parametrize("n,k,lr,sec,pw,over", CASES)
@@ -86,18 +89,21 @@ def test_honest_proofs_are_accepted(n, k, lr, sec, pw, over):
     p = O.whir_params(n, k, lr, sec, pw, **over)
     assert (p.num_rounds + 1) * k + p.final_vars == n
     for ncov in (0, 1, 3):
-        c, cov = _problem(n, ncov, 1000 * n + 10 * k + ncov)
+        c, cov = _problem(n, ncov, 1000 * n + 10 * k + ncov, p.batch_size)
         cw, proof = O.whir_prove(p, 0x5eed + n, c, cov)
         lay = layout(p, ncov)
         assert proof.shape[0] == lay["total"] == O.lib().pko_whir_proof_words(
             O.ctypes.byref(p), ncov)
         assert O.whir_verify(p, 0x5eed + n, cov, ncov, cw, proof) == 0
-        # the statement values are the covectors' dot products with c
-        for a in range(ncov):
-            exp = np.zeros(4, np.uint64)
-            O.lib().pko_dot(O.p64(exp), O.p64(np.ascontiguousarray(cov[a << n:(a + 1) << n])),
-                            O.p64(c), 1 << n)
-            assert np.array_equal(proof[4 * a:4 * a + 4], exp)
+        # the statement values are the covectors' dot products with each
+        # polynomial of the batch
+        for i in range(p.batch_size):
+            for a in range(ncov):
+                exp = np.zeros(4, np.uint64)
+                O.lib().pko_dot(O.p64(exp), O.p64(np.ascontiguousarray(cov[a << n:(a + 1) << n])),
+                                O.p64(np.ascontiguousarray(c[i << n:(i + 1) << n])), 1 << n)
+                at = 4 * (i * ncov + a)
+                assert np.array_equal(proof[at:at + 4], exp)
 
 
 def test_params_schedule_of_the_r1cs_config():
@@ -292,3 +298,21 @@ def test_whole_r1cs_proof_verifies(nc, ni):
     bad = dict(sp)
     bad["transcript"] = (list(sp["transcript"][1]), list(sp["transcript"][0]))
     assert O.verify_r1cs_whir(h, wp, 11, bad, cw, proof) != 0
+
+
+def test_batch_tampering_is_rejected():
+    """The ZK batch: the second polynomial's statement value, its half of an
+    opened first-round row, and its OOD answer are all bound."""
+    p = O.whir_params(11, 3, 2, 40, 0, batch_size=2)
+    c, cov = _problem(11, 2, 9191, 2)
+    cw, proof = O.whir_prove(p, 17, c, cov)
+    assert O.whir_verify(p, 17, cov, 2, cw, proof) == 0
+    lay = layout(p, 2)
+    assert O.whir_verify(p, 17, cov, 2, cw, _bump(proof, lay["values"] + 4 * 3)) == -3
+    sec = lay["rounds"][0]
+    row_at = sec["open"] + sec["row_words"] // 2 + 4  # an entry of f_1's half
+    assert O.whir_verify(p, 17, cov, 2, cw, _bump(proof, row_at)) == -5
+    assert O.whir_verify(p, 17, cov, 2, _bump(cw, 4 + 4), proof) != 0  # f_1's OOD answer
+    # a batch proof is not a proof about either polynomial alone
+    p1 = O.whir_params(11, 3, 2, 40, 0)
+    assert O.whir_verify(p1, 17, cov, 2, cw[:8], proof) != 0
