@@ -27,7 +27,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-PROVE_METRIC = ("Spartan+WHIR proofs/s & p99 latency @2^20-constraint R1CS (whole proof: WHIR "
+PROVE_METRIC = ("Spartan+WHIR proofs/s & p99 latency @2^20-constraint R1CS (whole proof: WHIR-ZK "
                 "commit, zk-sumcheck, covector evaluations, WHIR rounds; plain GPU; bit-exact)")
 PROVE_UNIT = "proofs/s"
 METRIC = ("WHIR commit throughput, Spartan+WHIR prover hot path: 2^20 Fr coefficients -> "
@@ -44,10 +44,11 @@ F64_PER_SQR = 11 + 66 + 10 + 140 + 69  # 296
 # from an ncu capture of this workload (profiles/leaf_fold_fr_kernel_whir_commit_2p20.md),
 # keyed by (log2 coeffs, folding factor, log inv rate).
 LEAF_TRAFFIC_BYTES = {(20, 4, 2): 134.264064e6 + 6.855168e6}
-# the same for the whole proof's commit (2^20 leaves of 8 Fr: the witness
-# polynomial of m = 21 at rate 1/4), from an ncu capture of the default command
+# the same for the whole proof's witness commitment (whir-ZK: 2^20 leaves of
+# 16 Fr, the witness and blinding polynomials of m = 21 at rate 1/4), from an
+# ncu capture of the default command
 # (profiles/leaf_fold_fr_kernel_whole_proof_2p20_constraints.md).
-LEAF_TRAFFIC_PROVE_BYTES = 268505344 + 26489856
+LEAF_TRAFFIC_PROVE_BYTES = 537195264 + 33959680
 
 
 def parse_args():
@@ -553,6 +554,9 @@ def prove_config(a, h, wp, proof_bytes=None):
             "num_witnesses": h.num_witnesses, "whir_num_variables": wp.num_variables,
             "folding_factor": wp.folding_factor, "log_inv_rate": wp.log_inv_rate,
             "security_bits": 128, "pow_bits": wp.pow_bits, "whir_rounds": wp.num_rounds,
+            "whir_zk": wp.batch_size == 2,
+            "whir_batch": f"{wp.batch_size} (the witness with a blinding polynomial)"
+            if wp.batch_size == 2 else "1",
             "queries": list(wp.queries[:wp.num_rounds + 1]), "proof_bytes": proof_bytes,
             "seed": a.seed, "parallelism": f"replicas x{a.gpus}",
             "l2": "flushed: 256 MiB device write between timed steps (outside the step events); "
@@ -696,10 +700,10 @@ def run_prove(a):
 
     # the dominant kernel (Merkle leaf hashing of the witness commitment:
     # 2^20 leaves of 8 Fr) timed on its own with CUDA events, L2 flushed
-    M = 1 << wp.folding_factor
-    msg_len = (1 << wp.num_variables) // M
+    M = (1 << wp.folding_factor) * wp.batch_size  # Fr per leaf of the witness commitment
+    msg_len = (wp.batch_size << wp.num_variables) // M
     rows = msg_len << wp.log_inv_rate
-    coeffs = torch.empty((1 << wp.num_variables, 4), dtype=torch.int64, device=dev)
+    coeffs = torch.empty((wp.batch_size << wp.num_variables, 4), dtype=torch.int64, device=dev)
     hc = np.zeros((coeffs.shape[0], 4), np.uint64)
     check(L.pkg_sample_fr(a.seed + 7, hc.shape[0], hc.ctypes.data, 1))
     coeffs.copy_(torch.from_numpy(hc.view(np.int64)))
@@ -735,7 +739,8 @@ def run_prove(a):
     if not a.no_cpu_baseline and a.gpus == 1:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib as O
-        owp = O.whir_params(wp.num_variables, wp.folding_factor, wp.log_inv_rate, 128, wp.pow_bits)
+        owp = O.whir_params(wp.num_variables, wp.folding_factor, wp.log_inv_rate, 128, wp.pow_bits,
+                            batch_size=wp.batch_size)
         t0 = time.perf_counter()
         O.prove_r1cs(h, 1, 3, owp)
         cpu_s = time.perf_counter() - t0
@@ -755,8 +760,8 @@ def run_prove(a):
             "latency_ms": {"p50": p50_max, "p99": p99_max,
                            "note": "per-proof device time, worst rank"},
             "roofline": {
-                "kernel": "leaf_fold_fr_kernel (Skyscraper leaf hashing of the witness "
-                          "commitment: 2^20 leaves of 8 Fr)",
+                "kernel": f"leaf_fold_fr_kernel (Skyscraper leaf hashing of the witness "
+                          f"commitment: {rows} leaves of {M} Fr)",
                 "bound": "fp64", "achieved": f64_achieved / 1e12, "peak": dfma.value / 1e12,
                 "unit": "T fp64-op/s", "frac": f64_achieved / dfma.value,
                 "traffic": LEAF_TRAFFIC_PROVE_BYTES,
@@ -806,7 +811,7 @@ def run_reference_prove(a):
 
     h = HostR1CS(a.seed, PROVE_NC, PROVE_NI)
     m, _ = r1cs_sizing(h.num_constraints, h.num_witnesses)
-    wp = O.whir_params(m, 3, 2, 128, 10)
+    wp = O.whir_params(m, 3, 2, 128, 10, batch_size=2)  # whir-ZK, as the default line
     t0 = time.perf_counter()
     O.prove_r1cs(h, 1, 3, wp)
     t_full = time.perf_counter() - t0
@@ -817,7 +822,7 @@ def run_reference_prove(a):
         shrink += 1
     hs = h if shrink == 0 else HostR1CS(a.seed, PROVE_NC >> shrink, PROVE_NI >> shrink)
     ms_, _ = r1cs_sizing(hs.num_constraints, hs.num_witnesses)
-    wps = wp if shrink == 0 else O.whir_params(ms_, 3, 2, 128, 10)
+    wps = wp if shrink == 0 else O.whir_params(ms_, 3, 2, 128, 10, batch_size=2)
     for _ in range(max(a.warmup - 1, 0)):
         O.prove_r1cs(hs, 1, 3, wps)
     times = []

@@ -584,6 +584,15 @@ int pkg_fr_mul_batch(const uint64_t *a, const uint64_t *b, uint64_t *out, size_t
  * Returns unused pool memory on the current device to the driver, keeping at
  * least keep_bytes.  No counterpart in the reference. */
 int pkg_trim_memory(size_t keep_bytes);
+/* Indexed Fr sampler on the device (no rejection, every element computed
+ * alone): out[i] = lo + hi 2^253 mod p (Montgomery form), lo and hi the two
+ * 32-byte halves of ChaCha20 block start + i (RFC 8439 block function, key =
+ * seed LE, nonce word 1), each read as a little-endian integer masked to 253
+ * bits.  Draws the WHIR-ZK blinding polynomial of pkg_prove_r1cs.  out:
+ * device, 16-byte aligned; async.  No counterpart in the reference (which
+ * draws masks from thread_rng). */
+int pkg_sample_fr_indexed(uint64_t seed, uint64_t start, size_t n, uint64_t *out,
+                          pkg_stream_t stream);
 /* Grows the pool on the current device to hold at least `bytes` more (one
  * allocation, freed and waited for).  The pool hands a block freed on one
  * stream to another stream only once its free has completed, so work on

@@ -211,10 +211,11 @@ static inline uint32_t rotl32(uint32_t x, int n) { return (x << n) | (x >> (32 -
         c += d; b ^= c; b = rotl32(b, 7);                \
     } while (0)
 
-static void chacha20_block(const uint32_t key[8], uint64_t counter, uint32_t out[16]) {
+static void chacha20_block_n(const uint32_t key[8], uint64_t counter, uint32_t nonce,
+                             uint32_t out[16]) {
     uint32_t s[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u,
                       key[0], key[1], key[2], key[3], key[4], key[5], key[6], key[7],
-                      (uint32_t)counter, (uint32_t)(counter >> 32), 0u, 0u};
+                      (uint32_t)counter, (uint32_t)(counter >> 32), nonce, 0u};
     uint32_t x[16];
     memcpy(x, s, sizeof x);
     for (int i = 0; i < 10; i++) {
@@ -228,6 +229,33 @@ static void chacha20_block(const uint32_t key[8], uint64_t counter, uint32_t out
         QR(x[3], x[4], x[9], x[14]);
     }
     for (int i = 0; i < 16; i++) out[i] = x[i] + s[i];
+}
+
+static void chacha20_block(const uint32_t key[8], uint64_t counter, uint32_t out[16]) {
+    chacha20_block_n(key, counter, 0u, out);
+}
+
+void pko_sample_fr_indexed(uint64_t seed, uint64_t start, size_t n, uint64_t *out) {
+    const uint32_t key[8] = {(uint32_t)seed, (uint32_t)(seed >> 32), 0, 0, 0, 0, 0, 0};
+    const uint64_t two253[4] = {0, 0, 0, (uint64_t)1 << 61};
+    uint64_t t[4];
+    pko_fr_to_mont(t, two253);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < n; i++) {
+        uint32_t blk[16];
+        uint64_t lo[4], hi[4], a[4], b[4];
+        chacha20_block_n(key, start + i, 1u, blk);
+        for (int j = 0; j < 4; j++) {
+            lo[j] = (uint64_t)blk[2 * j] | ((uint64_t)blk[2 * j + 1] << 32);
+            hi[j] = (uint64_t)blk[8 + 2 * j] | ((uint64_t)blk[8 + 2 * j + 1] << 32);
+        }
+        lo[3] &= ((uint64_t)1 << 61) - 1;
+        hi[3] &= ((uint64_t)1 << 61) - 1;
+        pko_fr_to_mont(a, lo);
+        pko_fr_to_mont(b, hi);
+        pko_fr_mul(b, b, t);
+        pko_fr_add(out + 4 * i, a, b);
+    }
 }
 
 void pko_sample_fr(uint64_t seed, size_t n, uint64_t *out, int mont) {
@@ -983,8 +1011,12 @@ static int spartan_prove_impl(const pko_r1cs *r1cs, const uint64_t *witness,
     pko_r1cs_sizing(nc, nw, &m, &m0);
     if (m0 > 30 || m > 28 || ff > m) return -1;
     if (whir && (whir->num_variables != m || whir->folding_factor != ff ||
-                 whir->log_inv_rate != lr || whir->ood_samples > 4))
+                 whir->log_inv_rate != lr || whir->ood_samples > 4 ||
+                 (whir->batch_size != 1 && whir->batch_size != 2)))
         return -1;
+    /* whir-ZK (a WHIR batch of 2): the witness polynomial committed with a
+     * blinding polynomial drawn from the indexed sampler */
+    const size_t nb = whir ? whir->batch_size : 1;
     memset(out, 0, sizeof *out);
     out->m = m;
     out->m0 = m0;
@@ -993,20 +1025,21 @@ static int spartan_prove_impl(const pko_r1cs *r1cs, const uint64_t *witness,
     pko_transcript_init(t, dom);
     /* commit: pad, blinding coefficients at offset w1_size */
     size_t n = (size_t)1 << m;
-    uint64_t *poly = (uint64_t *)calloc(n, 32);
+    uint64_t *poly = (uint64_t *)calloc(n * nb, 32);
     uint64_t *g = (uint64_t *)malloc(32 * 4 * m0);
     if (!poly || !g) return -2;
     memcpy(poly, witness, 32 * nw);
     pko_sample_fr(blinding_seed, 4 * m0, g, 1);
     memcpy(poly + 4 * w1_size, g, 32 * 4 * m0);
+    if (nb == 2) pko_sample_fr_indexed(blinding_seed ^ 0x243f6a8885a308d3ULL, 0, n, poly + 4 * n);
     size_t M = (size_t)1 << ff, L = n >> ff, cw_len = L << lr;
-    uint64_t *cw = (uint64_t *)malloc(32 * M * cw_len);
+    uint64_t *cw = (uint64_t *)malloc(32 * M * nb * cw_len);
     uint8_t *layers = (uint8_t *)malloc(32 * (2 * cw_len - 1));
     if (!cw || !layers) return -2;
-    int rc = pko_whir_commit(poly, n, ff, lr, cw, layers);
+    int rc = pko_whir_commit(poly, n * nb, ff + (nb == 2 ? 1 : 0), lr, cw, layers);
     if (rc) return rc;
     memcpy(out->root, layers + 32 * (2 * cw_len - 2), 32);
-    uint64_t ood_points[4 * 4];
+    uint64_t ood_points[4 * 5];
     if (whir) {
         rc = pko_whir_commit_ood(whir, t, poly, out->root, whir_commit_words, ood_points);
         if (rc) return rc;

@@ -41,6 +41,11 @@ void pko_from_mont_many(uint64_t *v, size_t n);
  * key = seed LE in the first 8 bytes).  254-bit mask + rejection; output in
  * Montgomery form when mont != 0. */
 void pko_sample_fr(uint64_t seed, size_t n, uint64_t *out, int mont);
+/* Indexed sampler (no rejection, any element computable alone): out[i] =
+ * lo + hi 2^253 mod p (Montgomery form), lo and hi the two 32-byte halves of
+ * ChaCha20 block start + i (key = seed LE, nonce word 1), each read as a
+ * little-endian integer masked to 253 bits. */
+void pko_sample_fr_indexed(uint64_t seed, uint64_t start, size_t n, uint64_t *out);
 
 /* ---- ntt crate (ntt/src/ntt.rs) --------------------------------------- */
 int  pko_ntt_nr(uint64_t *values, size_t len, size_t codeword_size, size_t num_groups);

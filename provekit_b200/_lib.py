@@ -81,6 +81,7 @@ SIGNATURES = {
     "pkg_last_prove_stages": [ctypes.c_void_p],
     "pkg_trim_memory": [ctypes.c_size_t],
     "pkg_reserve_memory": [ctypes.c_size_t],
+    "pkg_sample_fr_indexed": [ctypes.c_uint64, ctypes.c_uint64, _c_sz, _c_vp, _c_vp],
     "pkg_whir_fold_coeffs": [_c_vp, _c_sz, _c_uint, _c_vp, _c_vp, _c_vp],
     "pkg_whir_fold_rows": [_c_vp, _c_sz, _c_uint, _c_vp, _c_vp, _c_vp],
     "pkg_poly_eval_many": [_c_vp, _c_sz, _c_vp, _c_sz, _c_vp, _c_vp],

@@ -35,6 +35,10 @@ static size_t ceil_log2(size_t n) {  // utils::next_power_of_two (utils/mod.rs:7
 // device time plus their host work.
 thread_local double g_stage_ms[PKG_PROVE_STAGES];
 
+// Seed of the WHIR-ZK blinding polynomial: the blinding seed with the first
+// 64 fraction bits of pi (a fixed, arbitrary domain separator).
+constexpr uint64_t kMaskSeed = 0x243f6a8885a308d3ULL;
+
 struct StageClock {
   std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
   void mark(int k) {
@@ -89,7 +93,9 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     PK_REQUIRE(pkg_whir_proof_words(whir, 3) != 0, "invalid WHIR parameters");
     PK_REQUIRE(whir->num_variables == m, "WHIR parameters for %u variables, the R1CS needs %zu",
                whir->num_variables, m);
-    PK_REQUIRE(whir->batch_size == 1, "batched WHIR parameters are not supported here");
+    PK_REQUIRE(whir->batch_size == 1 || whir->batch_size == 2,
+               "WHIR batch of %u: the witness is committed alone or with one blinding "
+               "polynomial", whir->batch_size);
   }
   memset(out, 0, sizeof *out);
   memset(g_stage_ms, 0, sizeof g_stage_ms);
@@ -104,9 +110,12 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   // ---- commit (whir_r1cs.rs:82-140)
   const size_t n = size_t(1) << m, M = size_t(1) << ff, L = n >> ff, cw_len = L << lr;
   const size_t n0 = size_t(1) << m0;
+  // whir-ZK (a WHIR batch of 2): the witness polynomial is committed with a
+  // random blinding polynomial g of the same length in one tree
+  const unsigned nb = whir ? whir->batch_size : 1;
   Scratch s_poly, s_cw, s_layers, s_tab, s_misc;
-  if ((rc = s_poly.alloc(32 * n, s))) return rc;
-  if ((rc = s_cw.alloc(32 * M * cw_len, s))) return rc;
+  if ((rc = s_poly.alloc(32 * n * nb, s))) return rc;
+  if ((rc = s_cw.alloc(32 * M * nb * cw_len, s))) return rc;
   if ((rc = s_layers.alloc(32 * (2 * cw_len - 1), s))) return rc;
   if ((rc = s_tab.alloc(32 * 3 * n0, s))) return rc;
   uint64_t* poly = static_cast<uint64_t*>(s_poly.ptr);
@@ -120,11 +129,14 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   PK_CUDA(cudaMemcpyAsync(poly, witness, 32 * nw, cudaMemcpyDeviceToDevice, s));
   PK_CUDA(cudaMemsetAsync(poly + 4 * nw, 0, 32 * (n - nw), s));
   PK_CUDA(cudaMemcpyAsync(poly + 4 * w1_size, g.data(), 32 * 4 * m0, cudaMemcpyHostToDevice, s));
-  if ((rc = rs_encode_device(poly, M, L, nullptr, 0, cw_len, cw, s))) return rc;
-  if ((rc = merkle_tree_fr_device(cw, M, cw_len, PKG_LEAF_CANONICAL, layers, s))) return rc;
+  uint64_t* mask = poly + 4 * n;  // the blinding polynomial (batch of 2)
+  if (nb == 2 && (rc = pkg_sample_fr_indexed(blinding_seed ^ kMaskSeed, 0, n, mask, stream)))
+    return rc;
+  if ((rc = rs_encode_device(poly, M * nb, L, nullptr, 0, cw_len, cw, s))) return rc;
+  if ((rc = merkle_tree_fr_device(cw, M * nb, cw_len, PKG_LEAF_CANONICAL, layers, s))) return rc;
   PK_CUDA(cudaMemcpyAsync(out->root, layers + 32 * (2 * cw_len - 2), 32, cudaMemcpyDeviceToHost, s));
   PK_CUDA(cudaStreamSynchronize(s));
-  uint64_t ood_points[4 * 4];
+  uint64_t ood_points[4 * 5];
   if (whir) {
     // whir's commit: the root, then the OOD samples of the committed polynomial
     if ((rc = pkg_whir_commit_ood(whir, &out->transcript, poly, layers, whir_commit_words,
@@ -207,8 +219,16 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   if (whir) {
     // whir's prove of <alpha_k, w> = evals[k]; out->transcript keeps the
     // state the WHIR prover starts from
+    // statement values: <alpha_k, w> (above), and for whir-ZK <alpha_k, g>
+    std::vector<uint64_t> vals(12 * nb);
+    memcpy(vals.data(), &out->evals[0][0], 96);
+    for (int k = 0; nb == 2 && k < 3; k++) {
+      if ((rc = dot_device(cov + 4 * n * (size_t)k, mask, n, dot_out, part, s))) return rc;
+      PK_CUDA(cudaMemcpyAsync(vals.data() + 12 + 4 * k, dot_out, 32, cudaMemcpyDeviceToHost, s));
+    }
+    PK_CUDA(cudaStreamSynchronize(s));
     pkg_transcript tw = out->transcript;
-    if ((rc = whir_prove_device(whir, &tw, poly, cw, layers, ood_points, cov, 3, &out->evals[0][0],
+    if ((rc = whir_prove_device(whir, &tw, poly, cw, layers, ood_points, cov, 3, vals.data(),
                                 nullptr, whir_proof, s)))
       return rc;
     clk.mark(5);

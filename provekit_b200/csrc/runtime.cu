@@ -1,5 +1,6 @@
 // runtime.cu -- library-wide plumbing: last-error storage, version, device
 // properties, the host-side Fr sampler and the IMAD-rate microbenchmark.
+#include <algorithm>
 #include <atomic>
 #include <cstdarg>
 #include <cstring>
@@ -199,6 +200,79 @@ extern "C" int pkg_sample_fr(uint64_t seed, size_t n, uint64_t* out, int mont) {
       got++;
     }
   }
+  return PKG_OK;
+}
+
+namespace pk {
+__device__ __forceinline__ uint32_t rotl32_dev(uint32_t x, int n) {
+  return (x << n) | (x >> (32 - n));
+}
+
+// ChaCha20 block (RFC 8439 layout: constants, 8 key words, 64-bit counter,
+// nonce words) with key = (k0, k1, 0, ...) and nonce word 14 = nonce.
+__device__ void chacha20_block_dev(uint32_t k0, uint32_t k1, uint64_t counter, uint32_t nonce,
+                                   uint32_t out[16]) {
+  const uint32_t s[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u,
+                          k0, k1, 0u, 0u, 0u, 0u, 0u, 0u,
+                          (uint32_t)counter, (uint32_t)(counter >> 32), nonce, 0u};
+  uint32_t x[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) x[i] = s[i];
+#define PK_QR(a, b, c, d)                                   \
+  a += b; d ^= a; d = rotl32_dev(d, 16);                    \
+  c += d; b ^= c; b = rotl32_dev(b, 12);                    \
+  a += b; d ^= a; d = rotl32_dev(d, 8);                     \
+  c += d; b ^= c; b = rotl32_dev(b, 7);
+#pragma unroll 1
+  for (int r = 0; r < 10; r++) {
+    PK_QR(x[0], x[4], x[8], x[12]);
+    PK_QR(x[1], x[5], x[9], x[13]);
+    PK_QR(x[2], x[6], x[10], x[14]);
+    PK_QR(x[3], x[7], x[11], x[15]);
+    PK_QR(x[0], x[5], x[10], x[15]);
+    PK_QR(x[1], x[6], x[11], x[12]);
+    PK_QR(x[2], x[7], x[8], x[13]);
+    PK_QR(x[3], x[4], x[9], x[14]);
+  }
+#undef PK_QR
+#pragma unroll
+  for (int i = 0; i < 16; i++) out[i] = x[i] + s[i];
+}
+
+// out[i] = lo + hi 2^253 mod p (Montgomery) from ChaCha20 block start + i.
+__global__ void sample_indexed_kernel(uint32_t k0, uint32_t k1, uint64_t start, size_t n, Fr t253,
+                                      uint64_t* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t b[16];
+    chacha20_block_dev(k0, k1, start + i, 1u, b);
+    Fr lo, hi;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      lo.v[j] = b[j];
+      hi.v[j] = b[8 + j];
+    }
+    lo.v[7] &= 0x1fffffffu;
+    hi.v[7] &= 0x1fffffffu;
+    fr_store(out, i, fr_add(fr_to_mont(lo), fr_mul(fr_to_mont(hi), t253)));
+  }
+}
+}  // namespace pk
+
+extern "C" int pkg_sample_fr_indexed(uint64_t seed, uint64_t start, size_t n, uint64_t* out,
+                                     pkg_stream_t stream) {
+  if (n == 0) return PKG_OK;
+  PK_REQUIRE(out && aligned16(out), "null or unaligned output");
+  HostFr two253;
+  two253.l[3] = uint64_t(1) << 61;
+  const HostFr t = HostFr::to_mont(two253);
+  Fr t253;
+  memcpy(t253.v, t.l, 32);
+  const int grid = (int)std::min<size_t>((n + 255) / 256, (size_t)sm_count() * 16);
+  sample_indexed_kernel<<<grid, 256, 0, as_stream(stream)>>>((uint32_t)seed,
+                                                              (uint32_t)(seed >> 32), start, n,
+                                                              t253, out);
+  PK_CHECK_LAUNCH("sample_indexed_kernel");
   return PKG_OK;
 }
 

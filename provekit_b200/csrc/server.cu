@@ -70,7 +70,7 @@ static size_t ceil_log2_sz(size_t n) {
 // Device bytes pkg_spartan_prove (with whole, pkg_prove_r1cs) plus the
 // resident request use (upper bound).
 size_t prove_footprint(size_t nc, size_t nw, const size_t nnz[3], unsigned ff, unsigned lr,
-                       bool whole) {
+                       bool whole, unsigned batch) {
   size_t m = ceil_log2_sz(nw), m0 = ceil_log2_sz(nc);
   if (m < 13) m = 13;
   if (m0 < 1) m0 = 1;
@@ -94,6 +94,9 @@ size_t prove_footprint(size_t nc, size_t nw, const size_t nnz[3], unsigned ff, u
     const size_t cw1 = lr >= 1 ? n << (lr - 1) : n;
     b += 32 * 3 * n + 32 * 2 * n + 32 * 2 * (n >> ff);
     b += 2 * (32 * cw1 + 32 * 2 * (cw1 >> ff));
+    // whir-ZK: the blinding polynomial, the second half of the first
+    // codeword, and the batch's combination
+    b += (size_t)(batch - 1) * (32 * n + 32 * cw + 32 * n);
   }
   return b + b / 8 + (16 << 20);                                  // pool slack
 }
@@ -322,7 +325,8 @@ extern "C" int pkg_server_submit(pkg_server* s, const pkg_prove_request* req, ui
     r->ff = r->whir.folding_factor;
     r->lr = r->whir.log_inv_rate;
   }
-  r->footprint = prove_footprint(r->nc, r->nw, r->nnz, r->ff, r->lr, r->whole);
+  r->footprint = prove_footprint(r->nc, r->nw, r->nnz, r->ff, r->lr, r->whole,
+                                 r->whole ? r->whir.batch_size : 1);
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (r->footprint > s->budget) {

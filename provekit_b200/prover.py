@@ -97,11 +97,14 @@ def r1cs_sizing(num_constraints: int, num_witnesses: int):
 
 
 def whir_params_for(r1cs, folding_factor=3, log_inv_rate=2, security_bits=128, pow_bits=10,
-                    **overrides):
+                    zk=True, **overrides):
     """The WHIR parameters of the R1CS's witness commitment (by default the
-    reference's: provekit/r1cs-compiler/src/whir_r1cs.rs:103-118)."""
+    reference's: provekit/r1cs-compiler/src/whir_r1cs.rs:103-118, whir-ZK,
+    i.e. the witness committed in a batch of 2 with a blinding polynomial)."""
     from .whir import WhirParams
     m, _ = r1cs_sizing(r1cs.num_constraints, r1cs.num_witnesses)
+    if zk:
+        overrides.setdefault("batch_size", 2)
     return WhirParams.new(m, folding_factor, log_inv_rate, security_bits, pow_bits, **overrides)
 
 

@@ -117,6 +117,7 @@ def lib():
         L = _lib
         L.pko_fr_mul.argtypes = [_u64p, _u64p, _u64p]
         L.pko_sample_fr.argtypes = [ctypes.c_uint64, _sz, _u64p, ctypes.c_int]
+        L.pko_sample_fr_indexed.argtypes = [ctypes.c_uint64, ctypes.c_uint64, _sz, _u64p]
         L.pko_ntt_nr.argtypes = [_u64p, _sz, _sz, _sz]
         L.pko_intt_rn.argtypes = [_u64p, _sz]
         L.pko_roots_reverse_ordered.argtypes = [_u64p, _sz]

@@ -57,19 +57,21 @@ def test_stage_timers_and_memory_trim_keep_results():
     assert_same(again, first)
 
 
-@pytest.mark.parametrize("log_nc,log_ni,sec,pw", [(10, 8, 40, 3), (12, 11, 64, 5), (14, 12, 128, 10)])
-def test_whole_proof_matches_oracle_and_verifies(log_nc, log_ni, sec, pw):
+@pytest.mark.parametrize("log_nc,log_ni,sec,pw,zk", [(10, 8, 40, 3, False), (12, 11, 64, 5, False),
+                                                    (14, 12, 128, 10, False), (10, 8, 40, 3, True),
+                                                    (13, 11, 64, 5, True)])
+def test_whole_proof_matches_oracle_and_verifies(log_nc, log_ni, sec, pw, zk):
     import ctypes
     from provekit_b200._lib import check, lib
     from provekit_b200.prover import HostR1CS, prove_r1cs, whir_params_for
     h = HostR1CS(300 + log_nc, 1 << log_nc, 1 << log_ni)
     d = h.to_device()
-    p = whir_params_for(d, 3, 2, sec, pw)
+    p = whir_params_for(d, 3, 2, sec, pw, zk=zk)
     sp, cw, proof = prove_r1cs(d, p, blinding_seed=6, transcript_domain=12)
     stages = (ctypes.c_double * 6)()
     check(lib().pkg_last_prove_stages(stages))
     assert all(v > 0 for v in stages), list(stages)
-    wp = O.whir_params(sp["m"], 3, 2, sec, pw)
+    wp = O.whir_params(sp["m"], 3, 2, sec, pw, batch_size=2 if zk else 1)
     assert bytes(wp) == bytes(p)
     esp, ecw, eproof = O.prove_r1cs(h, 6, 12, wp)
     assert_same(sp, esp)
@@ -86,9 +88,10 @@ def test_whole_proof_at_2p20_constraints_verifies():
     h = HostR1CS(3, 1 << 20, 1 << 18)
     d = h.to_device()
     p = whir_params_for(d)
-    assert (p.num_variables, p.folding_factor, p.log_inv_rate, p.pow_bits) == (21, 3, 2, 10)
+    assert (p.num_variables, p.folding_factor, p.log_inv_rate, p.pow_bits, p.batch_size) == \
+        (21, 3, 2, 10, 2)
     sp, cw, proof = prove_r1cs(d, p, blinding_seed=1, transcript_domain=3)
-    wp = O.whir_params(21, 3, 2, 128, 10)
+    wp = O.whir_params(21, 3, 2, 128, 10, batch_size=2)
     assert O.verify_r1cs_whir(h, wp, 3, sp, cw, proof) == 0
 
 
@@ -120,3 +123,15 @@ def test_concurrent_whole_proofs_equal_sequential():
     for (sp, cw, pr), (esp, ecw, epr) in zip(got, alone):
         assert_same(sp, esp)
         assert np.array_equal(cw, ecw) and np.array_equal(pr, epr)
+
+
+@pytest.mark.parametrize("seed,start,n", [(1, 0, 1), (5, 0, 1000), (0xfeedface12345678, 1 << 33, 4097)])
+def test_indexed_sampler_matches_oracle(seed, start, n):
+    """pkg_sample_fr_indexed (the whir-ZK blinding polynomial's source)."""
+    from provekit_b200._lib import check, lib
+    d = torch.empty((n, 4), dtype=torch.int64, device="cuda")
+    check(lib().pkg_sample_fr_indexed(seed, start, n, d.data_ptr(), None))
+    torch.cuda.synchronize()
+    exp = np.zeros((n, 4), np.uint64)
+    O.lib().pko_sample_fr_indexed(seed, start, n, O.p64(exp))
+    assert np.array_equal(d.cpu().numpy().view(np.uint64), exp)

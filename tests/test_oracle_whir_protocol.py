@@ -274,8 +274,9 @@ def test_squeeze_bytes_takes_31_bytes_per_element():
     assert out.tobytes() == exp[:70]
 
 
-@pytest.mark.parametrize("nc,ni", [(1 << 10, 1 << 8), (3000, 500), (1 << 12, 1 << 12)])
-def test_whole_r1cs_proof_verifies(nc, ni):
+@pytest.mark.parametrize("nc,ni,batch", [(1 << 10, 1 << 8, 1), (3000, 500, 1), (1 << 12, 1 << 12, 1),
+                                         (1 << 10, 1 << 8, 2), (3000, 500, 2)])
+def test_whole_r1cs_proof_verifies(nc, ni, batch):
     """pko_prove_r1cs: the Spartan part, then the WHIR proof of the three
     covectors M^T eq(alpha) against the evaluations; the WHIR part verifies
     from the transcript state the prover started it from, and the
@@ -283,11 +284,20 @@ def test_whole_r1cs_proof_verifies(nc, ni):
     from provekit_b200.prover import HostR1CS
     h = HostR1CS(nc + ni, nc, ni)
     m, m0 = O.r1cs_sizing(h.num_constraints, h.num_witnesses)
-    wp = O.whir_params(m, 3, 2, 40, 3)
+    wp = O.whir_params(m, 3, 2, 40, 3, batch_size=batch)
     sp, cw, proof = O.prove_r1cs(h, 5, 11, wp)
     assert (sp["m"], sp["m0"]) == (m, m0)
     assert O.verify_r1cs_whir(h, wp, 11, sp, cw, proof) == 0
-    cov = O.r1cs_covectors(h, sp["alpha"], m0, 1 << m)
+    cov = O.r1cs_covectors(h, sp["alpha"], m0, 1 << m)  # noqa: F841 (used below)
+    if batch == 2:
+        # whir-ZK: the blinding polynomial is the indexed sampler's
+        g = np.zeros((1 << m, 4), np.uint64)
+        O.lib().pko_sample_fr_indexed(5 ^ 0x243f6a8885a308d3, 0, 1 << m, O.p64(g))
+        for k in range(3):
+            d = np.zeros(4, np.uint64)
+            O.lib().pko_dot(O.p64(d), O.p64(np.ascontiguousarray(cov[k << m:(k + 1) << m])),
+                            O.p64(g), 1 << m)
+            assert np.array_equal(proof[12 + 4 * k:16 + 4 * k], d)
     for k in range(3):
         assert np.array_equal(proof[4 * k:4 * k + 4], sp["evals"][k])
         d = np.zeros(4, np.uint64)
