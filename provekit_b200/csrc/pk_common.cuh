@@ -62,6 +62,22 @@ inline cudaStream_t as_stream(pkg_stream_t s) { return reinterpret_cast<cudaStre
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Device -> host reads of small results (sumcheck sums, roots, openings)
+// through a per-thread pinned bounce buffer, then a stream synchronisation:
+// a copy into pageable memory goes through the driver's staging buffer, and
+// the proof path makes dozens of these per proof.  Reads that do not fit
+// the bounce buffer are copied directly.
+struct HostRead {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+int read_small(const HostRead* reads, int n, cudaStream_t s);
+inline int read_small(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  const HostRead r{dst, src, bytes};
+  return read_small(&r, 1, s);
+}
+
 // Stream-ordered scratch allocation (cudaMallocAsync), freed on scope exit
 // in stream order.
 // The library's stream-ordered memory pool on the current device (created on

@@ -134,8 +134,7 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     return rc;
   if ((rc = rs_encode_device(poly, M * nb, L, nullptr, 0, cw_len, cw, s))) return rc;
   if ((rc = merkle_tree_fr_device(cw, M * nb, cw_len, PKG_LEAF_CANONICAL, layers, s))) return rc;
-  PK_CUDA(cudaMemcpyAsync(out->root, layers + 32 * (2 * cw_len - 2), 32, cudaMemcpyDeviceToHost, s));
-  PK_CUDA(cudaStreamSynchronize(s));
+  if ((rc = read_small(out->root, layers + 32 * (2 * cw_len - 2), 32, s))) return rc;
   uint64_t ood_points[4 * 5];
   if (whir) {
     // whir's commit: the root, then the OOD samples of the committed polynomial
@@ -165,11 +164,10 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
 
   // ---- zk sumcheck (whir_r1cs.rs:519-621)
   std::vector<uint64_t> wb(16 * m0);
-  PK_CUDA(cudaMemcpyAsync(wb.data(), poly + 4 * w1_size, 32 * 4 * m0, cudaMemcpyDeviceToHost, s));
   {
     uint32_t h_err = 0;
-    PK_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, s));
-    PK_CUDA(cudaStreamSynchronize(s));
+    const HostRead reads[2] = {{wb.data(), poly + 4 * w1_size, 32 * 4 * m0}, {&h_err, err, 4}};
+    if ((rc = read_small(reads, 2, s))) return rc;
     PK_REQUIRE(!h_err, "R1CS column index out of range");
   }
   clk.mark(1);
@@ -211,8 +209,7 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     if ((rc = spmv_device(rp_t, cl_t, vl_t, nw, nc, eq, alph, err, s))) return rc;
     // create_weights_and_evaluations (:623-642): the zero padding adds nothing
     if ((rc = dot_device(alph, poly, nw, dot_out, part, s))) return rc;
-    PK_CUDA(cudaMemcpyAsync(out->evals[k], dot_out, 32, cudaMemcpyDeviceToHost, s));
-    PK_CUDA(cudaStreamSynchronize(s));
+    if ((rc = read_small(out->evals[k], dot_out, 32, s))) return rc;
     pkg_transcript_absorb(&out->transcript, out->evals[k]);
   }
   clk.mark(4);
@@ -224,9 +221,8 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     memcpy(vals.data(), &out->evals[0][0], 96);
     for (int k = 0; nb == 2 && k < 3; k++) {
       if ((rc = dot_device(cov + 4 * n * (size_t)k, mask, n, dot_out, part, s))) return rc;
-      PK_CUDA(cudaMemcpyAsync(vals.data() + 12 + 4 * k, dot_out, 32, cudaMemcpyDeviceToHost, s));
+      if ((rc = read_small(vals.data() + 12 + 4 * k, dot_out, 32, s))) return rc;
     }
-    PK_CUDA(cudaStreamSynchronize(s));
     pkg_transcript tw = out->transcript;
     if ((rc = whir_prove_device(whir, &tw, poly, cw, layers, ood_points, cov, 3, vals.data(),
                                 nullptr, whir_proof, s)))

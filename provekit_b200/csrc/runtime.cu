@@ -110,6 +110,42 @@ __global__ void dfma_rate_kernel(double* sink, double c, double d, int iters) {
   if (s == -1.0) sink[threadIdx.x] = s;
 }
 
+int read_small(const HostRead* reads, int n, cudaStream_t s) {
+  constexpr size_t kCap = size_t(256) << 10;
+  thread_local uint8_t* bounce = nullptr;
+  thread_local bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, kCap, cudaHostAllocPortable) == cudaSuccess)
+      bounce = static_cast<uint8_t*>(p);
+    else
+      cudaGetLastError();  // no bounce buffer: direct copies below
+  }
+  size_t total = 0;
+  for (int i = 0; i < n; i++) total += (reads[i].bytes + 15) & ~size_t(15);
+  if (!bounce || total > kCap) {
+    for (int i = 0; i < n; i++)
+      PK_CUDA(cudaMemcpyAsync(reads[i].dst, reads[i].src, reads[i].bytes, cudaMemcpyDeviceToHost,
+                              s));
+    PK_CUDA(cudaStreamSynchronize(s));
+    return PKG_OK;
+  }
+  size_t off = 0;
+  for (int i = 0; i < n; i++) {
+    PK_CUDA(cudaMemcpyAsync(bounce + off, reads[i].src, reads[i].bytes, cudaMemcpyDeviceToHost,
+                            s));
+    off += (reads[i].bytes + 15) & ~size_t(15);
+  }
+  PK_CUDA(cudaStreamSynchronize(s));
+  off = 0;
+  for (int i = 0; i < n; i++) {
+    memcpy(reads[i].dst, bounce + off, reads[i].bytes);
+    off += (reads[i].bytes + 15) & ~size_t(15);
+  }
+  return PKG_OK;
+}
+
 namespace {
 std::mutex g_pool_mu;
 cudaMemPool_t g_pools[64] = {};

@@ -256,8 +256,7 @@ int pow_solve_device(const uint64_t challenge[4], const uint64_t threshold[4], c
     const int grid = (int)std::min<uint64_t>((uint64_t)sm_count() * 8, (batch + 255) / 256);
     pow_kernel<<<grid, 256, 0, s>>>(c, t, base, batch, d_best);
     PK_CHECK_LAUNCH("pow_kernel");
-    PK_CUDA(cudaMemcpyAsync(&best, d_best, sizeof best, cudaMemcpyDeviceToHost, s));
-    PK_CUDA(cudaStreamSynchronize(s));
+    if ((rc = read_small(&best, d_best, sizeof best, s))) return rc;
   }
   if (best == none) {
     set_last_error("no nonce found");

@@ -366,9 +366,7 @@ extern "C" int pkg_spartan_round(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t
   uint64_t* d_out = part + 4 * 3 * (size_t)red_grid(q);
   rc = spartan_round_device(a, b, c, eq, size, fold, part, d_out, s);
   if (rc) return rc;
-  PK_CUDA(cudaMemcpyAsync(out, d_out, 96, cudaMemcpyDeviceToHost, s));
-  PK_CUDA(cudaStreamSynchronize(s));
-  return PKG_OK;
+  return read_small(out, d_out, 96, s);
 }
 
 extern "C" int pkg_eq_hypercube(const uint64_t* r, size_t nr, size_t num_entries, uint64_t* out,
@@ -418,9 +416,7 @@ extern "C" int pkg_dot(const uint64_t* a, const uint64_t* b, size_t n, uint64_t 
   uint64_t* part = static_cast<uint64_t*>(scr.ptr);
   rc = dot_device(a, b, n, part + 4 * (size_t)g, part, s);
   if (rc) return rc;
-  PK_CUDA(cudaMemcpyAsync(out, part + 4 * (size_t)g, 32, cudaMemcpyDeviceToHost, s));
-  PK_CUDA(cudaStreamSynchronize(s));
-  return PKG_OK;
+  return read_small(out, part + 4 * (size_t)g, 32, s);
 }
 
 extern "C" int pkg_csr_transpose(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
@@ -516,8 +512,7 @@ extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_
   for (size_t idx = 0; idx < m0; idx++) {  // :550-610
     rc = spartan_round_device(a, b, c, eq, size, idx ? alpha[idx - 1].l : nullptr, part, d_out, s);
     if (rc) return rc;
-    PK_CUDA(cudaMemcpyAsync(h, d_out, 96, cudaMemcpyDeviceToHost, s));
-    PK_CUDA(cudaStreamSynchronize(s));
+    if ((rc = read_small(h, d_out, 96, s))) return rc;
     if (idx) size /= 2;
     HostFr gp[4];
     blinding_coeffs(gv.data(), m0, idx, alpha.data(), gp);

@@ -268,9 +268,7 @@ extern "C" int pkg_poly_eval_many(const uint64_t* coeffs, size_t n, const uint64
     sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, g, d_out + 4 * j);
     PK_CHECK_LAUNCH("sum_partials_kernel");
   }
-  PK_CUDA(cudaMemcpyAsync(out, d_out, 32 * npts, cudaMemcpyDeviceToHost, s));
-  PK_CUDA(cudaStreamSynchronize(s));
-  return PKG_OK;
+  return read_small(out, d_out, 32 * npts, s);
 }
 
 extern "C" int pkg_merkle_open(const uint8_t* layers, size_t num_leaves, const uint64_t* indices,
@@ -348,11 +346,9 @@ int open_rows_device(const uint64_t* codeword, size_t fr_per_row, size_t num_row
                                                            d_paths);
     PK_CHECK_LAUNCH("merkle_open_kernel");
   }
-  PK_CUDA(cudaMemcpyAsync(rows, d_rows, 32 * nq * fr_per_row, cudaMemcpyDeviceToHost, s));
-  if (depth)
-    PK_CUDA(cudaMemcpyAsync(paths, d_paths, 32 * nq * (size_t)depth, cudaMemcpyDeviceToHost, s));
-  PK_CUDA(cudaStreamSynchronize(s));
-  return PKG_OK;
+  const HostRead reads[2] = {{rows, d_rows, 32 * nq * fr_per_row},
+                             {paths, d_paths, depth ? 32 * nq * (size_t)depth : 0}};
+  return read_small(reads, depth ? 2 : 1, s);
 }
 }  // namespace pk
 
@@ -395,9 +391,7 @@ extern "C" int pkg_whir_sumcheck_round(uint64_t* f, uint64_t* w, size_t size, co
   PK_CHECK_LAUNCH("whir_round_kernel");
   sum_partials_kernel<3><<<1, kRedThreads, 0, s>>>(part, g, d_out);
   PK_CHECK_LAUNCH("sum_partials_kernel");
-  PK_CUDA(cudaMemcpyAsync(out, d_out, 96, cudaMemcpyDeviceToHost, s));
-  PK_CUDA(cudaStreamSynchronize(s));
-  return PKG_OK;
+  return read_small(out, d_out, 96, s);
 }
 
 namespace pk {

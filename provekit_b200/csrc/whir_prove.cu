@@ -451,9 +451,7 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
                              0, PKG_LEAF_CANONICAL, cw_next.as<uint64_t>(), lay_next.as<uint8_t>(),
                              ps));
       HostFr root;
-      PK_CUDA(cudaMemcpyAsync(root.l, lay_next.as<uint8_t>() + 32 * (2 * Ln - 2), 32,
-                              cudaMemcpyDeviceToHost, s_));
-      PK_CUDA(cudaStreamSynchronize(s_));
+      PK_TRY(read_small(root.l, lay_next.as<uint8_t>() + 32 * (2 * Ln - 2), 32, s_));
       put(root);
       const HostFr root_m = HostFr::to_mont(root);
       pkg_transcript_absorb(t_, root_m.l);
@@ -511,8 +509,7 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
     PK_TRY(fold_into(g));
     const size_t nfin = size_t(1) << nv;
     std::vector<HostFr> fin(nfin);
-    PK_CUDA(cudaMemcpyAsync(fin[0].l, g, 32 * nfin, cudaMemcpyDeviceToHost, s_));
-    PK_CUDA(cudaStreamSynchronize(s_));
+    PK_TRY(read_small(fin[0].l, g, 32 * nfin, s_));
     for (size_t i = 0; i < nfin; i++) {
       put(fin[i]);
       pkg_transcript_absorb(t_, fin[i].l);
@@ -619,8 +616,10 @@ extern "C" int pkg_whir_commit_ood(const pkg_whir_params* p, pkg_transcript* t,
   cudaStream_t s = as_stream(stream);
   const size_t L = size_t(1) << rows_log(p, 0);
   HostFr root;
-  PK_CUDA(cudaMemcpyAsync(root.l, layers + 32 * (2 * L - 2), 32, cudaMemcpyDeviceToHost, s));
-  PK_CUDA(cudaStreamSynchronize(s));
+  {
+    int rc = read_small(root.l, layers + 32 * (2 * L - 2), 32, s);
+    if (rc) return rc;
+  }
   PK_REQUIRE(root.is_canonical(), "root digest is not a canonical field element");
   const HostFr rm = HostFr::to_mont(root);
   pkg_transcript_absorb(t, rm.l);
