@@ -240,6 +240,7 @@ class WhirProver {
   int run(const uint64_t* coeffs, const uint64_t* codeword, const uint8_t* layers,
           const uint64_t* ood_points, const uint64_t* covectors, size_t ncov,
           const uint64_t* values, uint64_t* hat);
+  size_t words() const { return pos_; }
 
  private:
   void put(const HostFr& x) {
@@ -538,7 +539,14 @@ int whir_prove_device(const pkg_whir_params* p, pkg_transcript* t, const uint64_
                       const uint64_t* covectors, size_t ncov, const uint64_t* values,
                       uint64_t* hat, uint64_t* proof, cudaStream_t s) {
   WhirProver prover(p, t, s, proof);
-  return prover.run(coeffs, codeword, layers, ood_points, covectors, ncov, values, hat);
+  int rc = prover.run(coeffs, codeword, layers, ood_points, covectors, ncov, values, hat);
+  if (rc) return rc;
+  if (prover.words() != pkg_whir_proof_words(p, ncov)) {
+    set_last_error("WHIR proof wrote %zu words, the layout has %zu", prover.words(),
+                   pkg_whir_proof_words(p, ncov));
+    return PKG_ERR_UNSUPPORTED;
+  }
+  return PKG_OK;
 }
 
 int subset_zeta_device(uint64_t* v, unsigned n, cudaStream_t s) {
