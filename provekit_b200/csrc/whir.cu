@@ -195,11 +195,22 @@ __global__ void eq_accumulate_kernel(uint64_t* __restrict__ w, size_t n, int nlo
   const size_t nlo_entries = size_t(1) << nlo;
   for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < n;
        b += (size_t)gridDim.x * blockDim.x) {
-    Fr acc = fr_load(w, b);
-    for (size_t j = 0; j < npts; j++)
-      acc = fr_add(acc, fr_mul_f64(fr_load_ro(hi, j * nhi_entries + (b >> nlo)),
-                                   fr_load_ro(lo, j * nlo_entries + (b & (nlo_entries - 1)))));
-    fr_store(w, b, acc);
+    // two independent products per step, one on the FP64 pipe and one on
+    // the integer pipe (the CIOS routine; the same integers), which issue
+    // side by side
+    const size_t bh = b >> nlo, bl = b & (nlo_entries - 1);
+    Fr acc = fr_load(w, b), acc2 = fr_zero();
+    size_t j = 0;
+    for (; j + 1 < npts; j += 2) {
+      acc = fr_add(acc, fr_mul_f64(fr_load_ro(hi, j * nhi_entries + bh),
+                                   fr_load_ro(lo, j * nlo_entries + bl)));
+      acc2 = fr_add(acc2, fr_mul(fr_load_ro(hi, (j + 1) * nhi_entries + bh),
+                                 fr_load_ro(lo, (j + 1) * nlo_entries + bl)));
+    }
+    if (j < npts)
+      acc = fr_add(acc, fr_mul_f64(fr_load_ro(hi, j * nhi_entries + bh),
+                                   fr_load_ro(lo, j * nlo_entries + bl)));
+    fr_store(w, b, fr_add(acc, acc2));
   }
 }
 
