@@ -246,6 +246,7 @@ typedef struct {
   const uint32_t *cols[3];
   const uint64_t *vals[3];
   size_t nnz[3];
+  size_t num_public_inputs;   /* the public inputs are witness[1 ..= this] */
 } pkg_r1cs;
 
 /* Everything the prover produces before WHIR's own prove rounds. */
@@ -258,6 +259,8 @@ typedef struct {
   uint64_t rho[4], sum_g[4], blinding_eval[4], public_x[4];
   uint64_t evals[3][4];          /* <A^T eq(alpha), w>, <B^T ...>, <C^T ...> */
   pkg_transcript transcript;     /* state after the last message           */
+  uint64_t public_hash[4];       /* PublicInputs::hash (canonical; 0 if none) */
+  uint64_t public_eval[4];       /* <[1, x, .., x^n], w> (0 if no publics)   */
 } pkg_spartan_proof;
 
 /* The prover's work up to WHIR's prove call for a single-commitment R1CS
@@ -378,6 +381,7 @@ typedef struct {
    * (pkg_spartan_prove). */
   const struct pkg_whir_params_s *whir;
   uint64_t *whir_commit_words, *whir_proof;
+  size_t num_public_inputs;   /* witness[1 ..= this] are public */
 } pkg_prove_request;
 typedef struct {
   uint64_t submit_ns, admit_ns, done_ns; /* steady clock */
@@ -545,12 +549,19 @@ int pkg_last_whir_stages(double ms[PKG_WHIR_STAGES]);
 /* A whole proof (WhirR1CSProver::prove_noir with whir's prove,
  * provekit/prover/src/whir_r1cs.rs:143-301): pkg_spartan_prove's work with
  * whir's commitment OOD samples drawn right after the root
- * (pkg_whir_commit_ood: whir_commit_words), then pkg_whir_prove of the three
- * covectors A^T eq(alpha), B^T eq(alpha), C^T eq(alpha) (zero-padded to 2^m)
- * against out->evals (whir_proof: pkg_whir_proof_words(whir, 3) words).
- * whir: pkg_whir_params for pkg_r1cs_sizing's m (folding factor and rate
- * are taken from it).  out->transcript is the state the WHIR prover starts
- * from.  Synchronous. */
+ * (pkg_whir_commit_ood: whir_commit_words), then pkg_whir_prove of the
+ * single-commitment statements in the reference's order (prove_from_alphas,
+ * :258-301): the public weight [1, x, .., x^n] on the first n + 1 entries
+ * when there are n public inputs (make_public_weight,
+ * provekit/common/src/prefix_covector.rs:173-186), A^T eq(alpha),
+ * B^T eq(alpha), C^T eq(alpha) (zero-padded to 2^m), and the blinding
+ * covector expand_powers::<4>(alpha) at the blinding offset (OffsetCovector)
+ * with the zk-sumcheck's blinding_eval as its value -- whir_proof:
+ * pkg_whir_proof_words(whir, 4 + (n > 0)) words.  With batch_size 2
+ * (whir-ZK) the witness is committed with a blinding polynomial drawn by
+ * pkg_sample_fr_indexed.  whir: pkg_whir_params for pkg_r1cs_sizing's m
+ * (folding factor and rate are taken from it).  out->transcript is the state
+ * the WHIR prover starts from.  Synchronous. */
 int pkg_prove_r1cs(const pkg_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
                    uint64_t transcript_domain, const pkg_whir_params *whir,
                    pkg_spartan_proof *out, uint64_t *whir_commit_words, uint64_t *whir_proof,

@@ -997,6 +997,54 @@ int pko_r1cs_covectors(const pko_r1cs *r1cs, const uint64_t *alpha, size_t m0, s
     return 0;
 }
 
+void pko_public_inputs_hash(uint64_t out[4], const uint64_t *v, size_t n) {
+    static const uint64_t zero[4] = {0, 0, 0, 0};
+    if (n == 0) {
+        cpy4(out, zero);
+        return;
+    }
+    if (n == 1) {
+        pko_sky_compress(out, v, zero);
+        return;
+    }
+    uint64_t h[4], t[4];
+    pko_sky_compress(h, v, v + 4);
+    for (size_t i = 2; i < n; i++) {
+        pko_sky_compress(t, h, v + 4 * i);
+        cpy4(h, t);
+    }
+    cpy4(out, h);
+}
+
+int pko_r1cs_statement_covectors(const pko_r1cs *r1cs, const uint64_t public_x[4],
+                                 const uint64_t *alpha, size_t m0, size_t blinding_offset,
+                                 size_t len, uint64_t *out) {
+    const size_t np = r1cs->num_public_inputs;
+    const size_t base = np ? 1 : 0, ncov = base + 4;
+    if (blinding_offset + 4 * m0 > len || np + 1 > len) return -1;
+    memset(out, 0, 32 * ncov * len);
+    if (np) {
+        uint64_t pw[4];
+        cpy4(pw, ONE_MONT);
+        for (size_t i = 0; i <= np; i++) {
+            cpy4(out + 4 * i, pw);
+            pko_fr_mul(pw, pw, public_x);
+        }
+    }
+    int rc = pko_r1cs_covectors(r1cs, alpha, m0, len, out + 4 * len * base);
+    if (rc) return rc;
+    uint64_t *bl = out + 4 * len * (base + 3) + 4 * blinding_offset;
+    for (size_t i = 0; i < m0; i++) {
+        uint64_t pw[4];
+        cpy4(pw, ONE_MONT);
+        for (int k = 0; k < 4; k++) {
+            cpy4(bl + 4 * (4 * i + k), pw);
+            pko_fr_mul(pw, pw, alpha + 4 * i);
+        }
+    }
+    return (int)ncov;
+}
+
 /* With whir == NULL the commitment's root alone enters the transcript and
  * the proof ends at the covector evaluations; with whir, the commitment's
  * OOD samples follow the root (pko_whir_commit_ood) and pko_whir_prove of
@@ -1066,9 +1114,20 @@ static int spartan_prove_impl(const pko_r1cs *r1cs, const uint64_t *witness,
      * the scatter sum over the rows of M, which equals the transposed SpMV */
     uint64_t *cov = (uint64_t *)malloc(32 * 3 * n);
     if (!cov) return -2;
-    /* public weights (whir_r1cs.rs:665-676): hash of no public inputs is 0 */
-    static const uint64_t zero[4] = {0, 0, 0, 0};
-    pko_transcript_absorb(t, zero);
+    /* public weights (whir_r1cs.rs:665-676): the public inputs' hash, then x */
+    const size_t np = r1cs->num_public_inputs;
+    if (np + 1 > nw) return -1;
+    {
+        uint64_t *pv = (uint64_t *)malloc(32 * (np + 1));
+        if (!pv) return -2;
+        memcpy(pv, witness + 4, 32 * np);
+        pko_from_mont_many(pv, np);
+        pko_public_inputs_hash(out->public_hash, pv, np);
+        free(pv);
+        uint64_t hm[4];
+        pko_fr_to_mont(hm, out->public_hash);
+        pko_transcript_absorb(t, hm);
+    }
     pko_transcript_squeeze(t, out->public_x);
     if ((rc = pko_r1cs_covectors(r1cs, &out->alpha[0][0], m0, n, cov))) return rc;
     for (int k = 0; k < 3; k++) {
@@ -1076,10 +1135,28 @@ static int spartan_prove_impl(const pko_r1cs *r1cs, const uint64_t *witness,
         pko_dot(out->evals[k], cov + 4 * n * (size_t)k, poly, nw);
         pko_transcript_absorb(t, out->evals[k]);
     }
+    if (np) { /* compute_public_weight_evaluation (:654-663), then its message (:281) */
+        uint64_t pw[4], x[4];
+        cpy4(pw, ONE_MONT);
+        memset(out->public_eval, 0, 32);
+        for (size_t i = 0; i <= np; i++) {
+            pko_fr_mul(x, pw, poly + 4 * i);
+            pko_fr_add(out->public_eval, out->public_eval, x);
+            pko_fr_mul(pw, pw, out->public_x);
+        }
+        pko_transcript_absorb(t, out->public_eval);
+    }
     if (whir) {
+        /* the statements [public?, A, B, C, blinding] (prove_from_alphas, :258-301) */
+        uint64_t *stmts = (uint64_t *)malloc(32 * 5 * n);
+        if (!stmts) return -2;
+        int ncov = pko_r1cs_statement_covectors(r1cs, out->public_x, &out->alpha[0][0], m0, w1_size,
+                                                n, stmts);
         pko_transcript tw = *t;
-        rc = pko_whir_prove(whir, &tw, poly, cw, layers, whir_commit_words, ood_points, cov, 3,
-                            whir_proof);
+        rc = ncov < 0 ? ncov
+                      : pko_whir_prove(whir, &tw, poly, cw, layers, whir_commit_words, ood_points,
+                                       stmts, (size_t)ncov, whir_proof);
+        free(stmts);
     }
     free(cov); free(poly); free(cw); free(layers);
     return rc;

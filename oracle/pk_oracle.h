@@ -126,6 +126,7 @@ typedef struct {
     const uint64_t *row_ptr[3];   /* A, B, C: num_constraints + 1 */
     const uint32_t *cols[3];
     const uint64_t *vals[3];
+    size_t num_public_inputs;     /* the public inputs are witness[1 ..= this] */
 } pko_r1cs;
 typedef struct {
     size_t m, m0;
@@ -133,6 +134,7 @@ typedef struct {
     uint64_t r[30][4], coeffs[120][4], alpha[30][4];
     uint64_t rho[4], sum_g[4], blinding_eval[4], public_x[4], evals[3][4];
     pko_transcript transcript;
+    uint64_t public_hash[4], public_eval[4]; /* canonical hash; mont eval (0 without publics) */
 } pko_spartan_proof;
 int pko_spartan_prove(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t blinding_seed,
                       uint64_t domain, unsigned folding_factor, unsigned log_inv_rate,
@@ -279,6 +281,19 @@ int pko_whir_verify_proof(const pko_whir_params *p, pko_transcript *t, const uin
  * 3 x len Fr.  Computed as the scatter sum over the rows of M. */
 int pko_r1cs_covectors(const pko_r1cs *r1cs, const uint64_t *alpha, size_t m0, size_t len,
                        uint64_t *out);
+/* The whole proof's WHIR statements in the reference's order
+ * (prove_from_alphas, provekit/prover/src/whir_r1cs.rs:247-301): with public
+ * inputs the public weight [1, x, .., x^n] on the first n + 1 entries
+ * (make_public_weight, provekit/common/src/prefix_covector.rs:173-186), then
+ * A^T eq(alpha), B^T eq(alpha), C^T eq(alpha), then the blinding covector
+ * expand_powers::<4>(alpha) at blinding_offset (OffsetCovector, :90-112).
+ * out: (4 or 5) x len Fr; returns the count. */
+int pko_r1cs_statement_covectors(const pko_r1cs *r1cs, const uint64_t public_x[4],
+                                 const uint64_t *alpha, size_t m0, size_t blinding_offset,
+                                 size_t len, uint64_t *out);
+/* PublicInputs::hash (provekit/common/src/witness/mod.rs:86-97): 0, or
+ * compress(v, 0), or the left fold of compress; canonical in and out. */
+void pko_public_inputs_hash(uint64_t out[4], const uint64_t *values_canonical, size_t n);
 /* WhirR1CSScheme::new_for_r1cs sizing (provekit/r1cs-compiler/src/whir_r1cs.rs:48-92). */
 void pko_r1cs_sizing(size_t num_constraints, size_t num_witnesses, size_t *m, size_t *m0);
 /* A whole proof: pko_spartan_prove with the commitment's OOD samples drawn

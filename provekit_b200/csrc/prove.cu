@@ -18,6 +18,7 @@
 #include "internal.cuh"
 #include "pk_common.cuh"
 #include "rs_internal.cuh"
+#include "sky_host.hpp"
 
 namespace pk {
 
@@ -88,6 +89,8 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   if (rc) return rc;
   PK_REQUIRE(m0 <= 30 && m <= 28 && ff <= m && lr <= 8, "instance too large (m=%zu, m0=%zu)", m,
              m0);
+  PK_REQUIRE(r1cs->num_public_inputs + 1 <= nw, "%zu public inputs but %zu witnesses",
+             r1cs->num_public_inputs, nw);
   if (whir) {
     PK_REQUIRE(whir_commit_words && whir_proof, "null WHIR output");
     PK_REQUIRE(pkg_whir_proof_words(whir, 3) != 0, "invalid WHIR parameters");
@@ -178,22 +181,37 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   clk.mark(2);
 
   // ---- eq(alpha) and the transposed products (sumcheck.rs:195-227)
-  // the covectors: one nw-entry buffer, or (for the WHIR proof) three
-  // zero-padded 2^m-entry ones
+  // The covectors: one nw-entry buffer, or for the WHIR proof the
+  // statements of prove_from_alphas (whir_r1cs.rs:258-301), each 2^m entries:
+  // [public weight?, A^T eq, B^T eq, C^T eq, blinding covector].
+  const size_t np = r1cs->num_public_inputs;
+  const size_t sbase = np ? 1 : 0, nstm = sbase + 4;
   Scratch s_eq, s_alph;
   if ((rc = s_eq.alloc(32 * nc, s))) return rc;
-  if ((rc = s_alph.alloc(32 * (whir ? 3 * n : nw), s))) return rc;
+  if ((rc = s_alph.alloc(32 * (whir ? nstm * n : nw), s))) return rc;
   uint64_t* eq = static_cast<uint64_t*>(s_eq.ptr);
   uint64_t* cov = static_cast<uint64_t*>(s_alph.ptr);
-  if (whir) PK_CUDA(cudaMemsetAsync(cov, 0, 32 * 3 * n, s));
+  if (whir) PK_CUDA(cudaMemsetAsync(cov, 0, 32 * nstm * n, s));
   if ((rc = eq_hypercube_device(&out->alpha[0][0], m0, nc, eq, s))) return rc;
-  // public weights (whir_r1cs.rs:665-676): the hash of no public inputs is 0
-  const uint64_t zero[4] = {0, 0, 0, 0};
-  pkg_transcript_absorb(&out->transcript, zero);
+  // public weights (get_public_weights, whir_r1cs.rs:665-676): the hash of
+  // the public inputs (PublicInputs::hash, common/src/witness/mod.rs:86-97)
+  // into the transcript, then the challenge x
+  std::vector<HostFr> pubw(np + 1);  // w[0 ..= np], Montgomery form
+  if (np) {
+    if ((rc = read_small(pubw[0].l, witness, 32 * (np + 1), s))) return rc;
+    HostFr h = HostSky::compress(HostFr::from_mont(pubw[1]),
+                                 np > 1 ? HostFr::from_mont(pubw[2]) : HostFr::zero());
+    for (size_t i = 3; i <= np; i++) h = HostSky::compress(h, HostFr::from_mont(pubw[i]));
+    memcpy(out->public_hash, h.l, 32);
+  }
+  {
+    const HostFr hm = HostFr::to_mont(HostFr::from_limbs(out->public_hash));
+    pkg_transcript_absorb(&out->transcript, hm.l);
+  }
   pkg_transcript_squeeze(&out->transcript, out->public_x);
   clk.mark(3);
   for (int k = 0; k < 3; k++) {
-    uint64_t* alph = whir ? cov + 4 * n * (size_t)k : cov;
+    uint64_t* alph = whir ? cov + 4 * n * (sbase + (size_t)k) : cov;
     Scratch s_t;
     const size_t nnz = r1cs->nnz[k];
     const size_t rp_bytes = ((8 * (nw + 1) + 255) / 256) * 256;
@@ -212,19 +230,54 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     if ((rc = read_small(out->evals[k], dot_out, 32, s))) return rc;
     pkg_transcript_absorb(&out->transcript, out->evals[k]);
   }
+  // the public weight's evaluation <[1, x, .., x^np], w> and its message
+  // (compute_public_weight_evaluation, :654-663, :275-282)
+  std::vector<HostFr> xpow(np + 1);
+  if (np) {
+    const HostFr x = HostFr::from_limbs(out->public_x);
+    HostFr pw = HostFr::one(), acc = HostFr::zero();
+    for (size_t i = 0; i <= np; i++) {
+      xpow[i] = pw;
+      acc = HostFr::add(acc, HostFr::mul(pw, pubw[i]));
+      pw = HostFr::mul(pw, x);
+    }
+    memcpy(out->public_eval, acc.l, 32);
+    pkg_transcript_absorb(&out->transcript, acc.l);
+  }
   clk.mark(4);
   if (whir) {
-    // whir's prove of <alpha_k, w> = evals[k]; out->transcript keeps the
-    // state the WHIR prover starts from
-    // statement values: <alpha_k, w> (above), and for whir-ZK <alpha_k, g>
-    std::vector<uint64_t> vals(12 * nb);
-    memcpy(vals.data(), &out->evals[0][0], 96);
-    for (int k = 0; nb == 2 && k < 3; k++) {
-      if ((rc = dot_device(cov + 4 * n * (size_t)k, mask, n, dot_out, part, s))) return rc;
-      if ((rc = read_small(vals.data() + 12 + 4 * k, dot_out, 32, s))) return rc;
+    // the public weight and the blinding covector expand_powers::<4>(alpha)
+    // at the blinding offset (OffsetCovector, prefix_covector.rs:90-112)
+    if (np)
+      PK_CUDA(cudaMemcpyAsync(cov, xpow[0].l, 32 * (np + 1), cudaMemcpyHostToDevice, s));
+    std::vector<HostFr> bw(4 * m0);
+    for (size_t i = 0; i < m0; i++) {
+      HostFr pw = HostFr::one();
+      const HostFr a = HostFr::from_limbs(out->alpha[i]);
+      for (int k = 0; k < 4; k++) {
+        bw[4 * i + k] = pw;
+        pw = HostFr::mul(pw, a);
+      }
     }
+    PK_CUDA(cudaMemcpyAsync(cov + 4 * n * (sbase + 3) + 4 * w1_size, bw[0].l, 32 * 4 * m0,
+                            cudaMemcpyHostToDevice, s));
+    // statement values of w: [public_eval?, evals, blinding_eval]; for
+    // whir-ZK also every statement's value on the blinding polynomial g
+    std::vector<uint64_t> vals(4 * nstm * nb);
+    size_t at = 0;
+    if (np) {
+      memcpy(vals.data(), out->public_eval, 32);
+      at = 4;
+    }
+    memcpy(vals.data() + at, &out->evals[0][0], 96);
+    memcpy(vals.data() + at + 12, out->blinding_eval, 32);
+    for (size_t k = 0; nb == 2 && k < nstm; k++) {
+      if ((rc = dot_device(cov + 4 * n * k, mask, n, dot_out, part, s))) return rc;
+      if ((rc = read_small(vals.data() + 4 * (nstm + k), dot_out, 32, s))) return rc;
+    }
+    // host sources above are pageable: staged before the copies returned
     pkg_transcript tw = out->transcript;
-    if ((rc = whir_prove_device(whir, &tw, poly, cw, layers, ood_points, cov, 3, vals.data(),
+    if ((rc = whir_prove_device(whir, &tw, poly, cw, layers, ood_points, cov, nstm, vals.data(),
                                 nullptr, whir_proof, s)))
       return rc;
     clk.mark(5);

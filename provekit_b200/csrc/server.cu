@@ -42,6 +42,7 @@ struct HostRequest {
   const uint32_t* cols[3] = {nullptr, nullptr, nullptr};
   const uint64_t* vals[3] = {nullptr, nullptr, nullptr};
   const uint64_t* witness = nullptr;
+  size_t num_public = 0;
   uint64_t blinding_seed = 0, domain = 0;
   unsigned ff = 3, lr = 2;
   // whole proof: WHIR parameters and the caller's output buffers
@@ -155,6 +156,7 @@ static int run_request(HostRequest& r, cudaStream_t st) {
   memset(&rc1, 0, sizeof rc1);
   rc1.num_constraints = r.nc;
   rc1.num_witnesses = r.nw;
+  rc1.num_public_inputs = r.num_public;
   int rc = PKG_OK;
   // (destination, host source, bytes) of every upload
   struct Up {
@@ -305,6 +307,9 @@ extern "C" int pkg_server_submit(pkg_server* s, const pkg_prove_request* req, ui
     r->vals[k] = req->vals[k];
   }
   r->witness = req->witness;
+  r->num_public = req->num_public_inputs;
+  PK_REQUIRE(r->num_public + 1 <= r->nw, "%zu public inputs but %zu witnesses", r->num_public,
+             r->nw);
   r->blinding_seed = req->blinding_seed;
   r->domain = req->transcript_domain;
   r->ff = req->folding_factor;

@@ -63,6 +63,12 @@ struct HostSky {
   static void permute(HostFr& l, HostFr& r) {
     for (int k = 0; k < 18; k++) round(k, k == 6 || k == 7 || k == 10 || k == 11, l, r);
   }
+  // reference::compress (reference.rs:41-46): permute(l, r).0 + l, canonical
+  static HostFr compress(const HostFr& l, const HostFr& r) {
+    HostFr a = l, b = r;
+    permute(a, b);
+    return HostFr::add(a, l);
+  }
 };
 
 }  // namespace pk

@@ -13,7 +13,8 @@ from .spartan import Transcript
 class R1csC(ctypes.Structure):
     _fields_ = [("num_constraints", ctypes.c_size_t), ("num_witnesses", ctypes.c_size_t),
                 ("row_ptr", ctypes.c_void_p * 3), ("cols", ctypes.c_void_p * 3),
-                ("vals", ctypes.c_void_p * 3), ("nnz", ctypes.c_size_t * 3)]
+                ("vals", ctypes.c_void_p * 3), ("nnz", ctypes.c_size_t * 3),
+                ("num_public_inputs", ctypes.c_size_t)]
 
 
 class SpartanProofC(ctypes.Structure):
@@ -22,7 +23,8 @@ class SpartanProofC(ctypes.Structure):
                 ("alpha", ctypes.c_uint64 * 120), ("rho", ctypes.c_uint64 * 4),
                 ("sum_g", ctypes.c_uint64 * 4), ("blinding_eval", ctypes.c_uint64 * 4),
                 ("public_x", ctypes.c_uint64 * 4), ("evals", ctypes.c_uint64 * 12),
-                ("transcript", Transcript)]
+                ("transcript", Transcript), ("public_hash", ctypes.c_uint64 * 4),
+                ("public_eval", ctypes.c_uint64 * 4)]
 
     def as_dict(self):
         m0 = self.m0
@@ -32,15 +34,21 @@ class SpartanProofC(ctypes.Structure):
                 "rho": np.array(self.rho, np.uint64), "sum_g": np.array(self.sum_g, np.uint64),
                 "blinding_eval": np.array(self.blinding_eval, np.uint64),
                 "public_x": np.array(self.public_x, np.uint64), "evals": arr(self.evals, 3),
-                "transcript": (list(self.transcript.l), list(self.transcript.r))}
+                "transcript": (list(self.transcript.l), list(self.transcript.r)),
+                "public_hash": np.array(self.public_hash, np.uint64),
+                "public_eval": np.array(self.public_eval, np.uint64)}
 
 
 class HostR1CS:
     """Synthetic satisfiable R1CS in host memory (pkg_synthetic_r1cs)."""
 
-    def __init__(self, seed: int, num_constraints: int, num_inputs: int):
+    def __init__(self, seed: int, num_constraints: int, num_inputs: int, num_public_inputs: int = 0):
+        """num_public_inputs: the first inputs (witness[1 ..= this]) are public."""
         nc, ni = num_constraints, num_inputs
+        if num_public_inputs > ni:
+            raise ValueError("more public inputs than inputs")
         self.num_constraints, self.num_inputs = nc, ni
+        self.num_public_inputs = num_public_inputs
         self.num_witnesses = 1 + ni + nc
         self.row_ptr = [np.zeros(nc + 1, np.uint64) for _ in range(3)]
         caps = [3 * nc, 3 * nc, nc]
@@ -65,6 +73,7 @@ class DeviceR1CS:
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(  # noqa: E731
             np.int32 if a.dtype == np.uint32 else np.int64)).to(device)
         self.num_constraints, self.num_witnesses = h.num_constraints, h.num_witnesses
+        self.num_public_inputs = getattr(h, "num_public_inputs", 0)
         self.row_ptr = [t(a) for a in h.row_ptr]
         self.cols = [t(a) for a in h.cols]
         self.vals = [t(a) for a in h.vals]
@@ -74,7 +83,7 @@ class DeviceR1CS:
                        (ctypes.c_void_p * 3)(*[x.data_ptr() for x in self.row_ptr]),
                        (ctypes.c_void_p * 3)(*[x.data_ptr() for x in self.cols]),
                        (ctypes.c_void_p * 3)(*[x.data_ptr() for x in self.vals]),
-                       (ctypes.c_size_t * 3)(*self.nnz))
+                       (ctypes.c_size_t * 3)(*self.nnz), self.num_public_inputs)
 
 
 def spartan_prove(r1cs: DeviceR1CS, witness=None, blinding_seed=1, transcript_domain=3,
@@ -116,9 +125,16 @@ def prove_r1cs(r1cs: DeviceR1CS, whir=None, witness=None, blinding_seed=1, trans
     w = r1cs.witness if witness is None else witness
     out = SpartanProofC()
     cwords = np.zeros(p.commit_words(), np.uint64)
-    proof = np.zeros(p.proof_words(3), np.uint64)
+    proof = np.zeros(p.proof_words(statement_count(r1cs)), np.uint64)
     s = (stream if stream is not None else torch.cuda.current_stream()).cuda_stream
     check(lib().pkg_prove_r1cs(ctypes.byref(r1cs.c), w.data_ptr(), blinding_seed,
                                transcript_domain, ctypes.byref(p), ctypes.byref(out),
                                cwords.ctypes.data, proof.ctypes.data, s))
     return out.as_dict(), cwords, proof
+
+
+def statement_count(r1cs) -> int:
+    """The whole proof's WHIR statements (prove_from_alphas,
+    provekit/prover/src/whir_r1cs.rs:258-301): the public weight when there
+    are public inputs, A^T eq, B^T eq, C^T eq, and the blinding covector."""
+    return 4 + (1 if getattr(r1cs, "num_public_inputs", 0) else 0)

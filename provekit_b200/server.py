@@ -5,7 +5,7 @@ import ctypes
 import numpy as np
 
 from ._lib import check, lib
-from .prover import SpartanProofC, whir_params_for
+from .prover import SpartanProofC, statement_count, whir_params_for
 
 
 class ProveRequestC(ctypes.Structure):
@@ -15,7 +15,8 @@ class ProveRequestC(ctypes.Structure):
                 ("witness", ctypes.c_void_p), ("blinding_seed", ctypes.c_uint64),
                 ("transcript_domain", ctypes.c_uint64), ("folding_factor", ctypes.c_uint),
                 ("log_inv_rate", ctypes.c_uint), ("whir", ctypes.c_void_p),
-                ("whir_commit_words", ctypes.c_void_p), ("whir_proof", ctypes.c_void_p)]
+                ("whir_commit_words", ctypes.c_void_p), ("whir_proof", ctypes.c_void_p),
+                ("num_public_inputs", ctypes.c_size_t)]
 
 
 class RequestTimesC(ctypes.Structure):
@@ -47,6 +48,7 @@ def make_request(h, blinding_seed=1, transcript_domain=3, folding_factor=3, log_
         req.vals[k] = h.vals[k].ctypes.data
         req.nnz[k] = h.nnz[k]
     req.witness = h.witness.ctypes.data
+    req.num_public_inputs = getattr(h, "num_public_inputs", 0)
     req.blinding_seed, req.transcript_domain = blinding_seed, transcript_domain
     req.folding_factor, req.log_inv_rate = folding_factor, log_inv_rate
     if whole is not None:
@@ -70,7 +72,8 @@ class ProofServer:
         whole = None
         if whole_proof or whir is not None:
             p = whir if whir is not None else whir_params_for(h)
-            whole = (p, np.zeros(p.commit_words(), np.uint64), np.zeros(p.proof_words(3), np.uint64))
+            whole = (p, np.zeros(p.commit_words(), np.uint64),
+                     np.zeros(p.proof_words(statement_count(h)), np.uint64))
         req = make_request(h, whole=whole, **kw)
         rid = ctypes.c_uint64()
         check(lib().pkg_server_submit(self._s, ctypes.byref(req), ctypes.byref(rid)))

@@ -24,7 +24,7 @@ class Transcript(ctypes.Structure):
 class R1CS(ctypes.Structure):
     _fields_ = [("num_constraints", ctypes.c_size_t), ("num_witnesses", ctypes.c_size_t),
                 ("row_ptr", ctypes.c_void_p * 3), ("cols", ctypes.c_void_p * 3),
-                ("vals", ctypes.c_void_p * 3)]
+                ("vals", ctypes.c_void_p * 3), ("num_public_inputs", ctypes.c_size_t)]
 
 
 class SpartanProof(ctypes.Structure):
@@ -33,14 +33,21 @@ class SpartanProof(ctypes.Structure):
                 ("alpha", ctypes.c_uint64 * 120), ("rho", ctypes.c_uint64 * 4),
                 ("sum_g", ctypes.c_uint64 * 4), ("blinding_eval", ctypes.c_uint64 * 4),
                 ("public_x", ctypes.c_uint64 * 4), ("evals", ctypes.c_uint64 * 12),
-                ("transcript", Transcript)]
+                ("transcript", Transcript), ("public_hash", ctypes.c_uint64 * 4),
+                ("public_eval", ctypes.c_uint64 * 4)]
 
 
 def _r1cs_c(h):
     return R1CS(h.num_constraints, h.num_witnesses,
                 (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.row_ptr]),
                 (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.cols]),
-                (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.vals]))
+                (ctypes.c_void_p * 3)(*[a.ctypes.data for a in h.vals]),
+                getattr(h, "num_public_inputs", 0))
+
+
+def statement_count(h) -> int:
+    """The whole proof's WHIR statements: [public?, A, B, C, blinding]."""
+    return 4 + (1 if getattr(h, "num_public_inputs", 0) else 0)
 
 
 def spartan_prove(h, blinding_seed, domain, ff, lr):
@@ -64,7 +71,7 @@ def prove_r1cs(h, blinding_seed, domain, wp):
     r = _r1cs_c(h)
     out = SpartanProof()
     cwords = np.zeros(lib().pko_whir_commit_words(ctypes.byref(wp)), np.uint64)
-    proof = np.zeros(lib().pko_whir_proof_words(ctypes.byref(wp), 3), np.uint64)
+    proof = np.zeros(lib().pko_whir_proof_words(ctypes.byref(wp), statement_count(h)), np.uint64)
     rc = lib().pko_prove_r1cs(ctypes.byref(r), p64(np.ascontiguousarray(h.witness)), blinding_seed,
                               domain, ctypes.byref(wp), ctypes.byref(out), p64(cwords), p64(proof))
     assert rc == 0, rc
@@ -91,9 +98,22 @@ def verify_r1cs_whir(h, wp, domain, spartan, cwords, proof):
     l, r = spartan["transcript"]
     t.l[:] = l
     t.r[:] = r
-    cov = r1cs_covectors(h, spartan["alpha"], spartan["m0"], 1 << spartan["m"])
-    return lib().pko_whir_verify_proof(ctypes.byref(wp), ctypes.byref(t), p64(cov), 3, p64(cwords),
-                                       p64(z), p64(np.ascontiguousarray(proof)), proof.shape[0])
+    cov = statement_covectors(h, spartan)
+    return lib().pko_whir_verify_proof(ctypes.byref(wp), ctypes.byref(t), p64(cov),
+                                       cov.shape[0] >> spartan["m"], p64(cwords), p64(z),
+                                       p64(np.ascontiguousarray(proof)), proof.shape[0])
+
+
+def statement_covectors(h, spartan):
+    """[public?, A^T eq, B^T eq, C^T eq, blinding] as (ncov * 2^m, 4)."""
+    n = 1 << spartan["m"]
+    out = np.zeros((5 * n, 4), np.uint64)
+    px = np.ascontiguousarray(spartan["public_x"], dtype=np.uint64)
+    ncov = lib().pko_r1cs_statement_covectors(ctypes.byref(_r1cs_c(h)), p64(px),
+                                              p64(np.ascontiguousarray(spartan["alpha"])),
+                                              spartan["m0"], h.num_witnesses, n, p64(out))
+    assert ncov > 0
+    return out[: ncov * n]
 
 
 def _spartan_dict(out):
@@ -104,7 +124,9 @@ def _spartan_dict(out):
             "rho": np.array(out.rho, np.uint64), "sum_g": np.array(out.sum_g, np.uint64),
             "blinding_eval": np.array(out.blinding_eval, np.uint64),
             "public_x": np.array(out.public_x, np.uint64), "evals": arr(out.evals, 3),
-            "transcript": (list(out.transcript.l), list(out.transcript.r))}
+            "transcript": (list(out.transcript.l), list(out.transcript.r)),
+            "public_hash": np.array(out.public_hash, np.uint64),
+            "public_eval": np.array(out.public_eval, np.uint64)}
 
 
 _lib = None
@@ -181,6 +203,9 @@ def lib():
         L.pko_whir_verify_proof.argtypes = [wp, tp, _u64p, _sz, _u64p, _u64p, _u64p, _sz]
         L.pko_r1cs_sizing.argtypes = [_sz, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]
         L.pko_r1cs_covectors.argtypes = [ctypes.c_void_p, _u64p, _sz, _sz, _u64p]
+        L.pko_r1cs_statement_covectors.argtypes = [ctypes.c_void_p, _u64p, _u64p, _sz, _sz, _sz,
+                                                   _u64p]
+        L.pko_public_inputs_hash.argtypes = [_u64p, _u64p, _sz]
         L.pko_prove_r1cs.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_uint64, wp,
                                      ctypes.c_void_p, _u64p, _u64p]
     return _lib

@@ -57,14 +57,19 @@ def test_stage_timers_and_memory_trim_keep_results():
     assert_same(again, first)
 
 
-@pytest.mark.parametrize("log_nc,log_ni,sec,pw,zk", [(10, 8, 40, 3, False), (12, 11, 64, 5, False),
-                                                    (14, 12, 128, 10, False), (10, 8, 40, 3, True),
-                                                    (13, 11, 64, 5, True)])
-def test_whole_proof_matches_oracle_and_verifies(log_nc, log_ni, sec, pw, zk):
+@pytest.mark.parametrize("log_nc,log_ni,sec,pw,zk,npub", [(10, 8, 40, 3, False, 0),
+                                                         (12, 11, 64, 5, False, 0),
+                                                         (14, 12, 128, 10, False, 0),
+                                                         (10, 8, 40, 3, True, 0),
+                                                         (13, 11, 64, 5, True, 0),
+                                                         (11, 9, 40, 3, False, 1),
+                                                         (12, 10, 64, 4, True, 2),
+                                                         (12, 10, 40, 3, True, 300)])
+def test_whole_proof_matches_oracle_and_verifies(log_nc, log_ni, sec, pw, zk, npub):
     import ctypes
     from provekit_b200._lib import check, lib
     from provekit_b200.prover import HostR1CS, prove_r1cs, whir_params_for
-    h = HostR1CS(300 + log_nc, 1 << log_nc, 1 << log_ni)
+    h = HostR1CS(300 + log_nc, 1 << log_nc, 1 << log_ni, num_public_inputs=npub)
     d = h.to_device()
     p = whir_params_for(d, 3, 2, sec, pw, zk=zk)
     sp, cw, proof = prove_r1cs(d, p, blinding_seed=6, transcript_domain=12)

@@ -277,10 +277,11 @@ def test_squeeze_bytes_takes_31_bytes_per_element():
 @pytest.mark.parametrize("nc,ni,batch", [(1 << 10, 1 << 8, 1), (3000, 500, 1), (1 << 12, 1 << 12, 1),
                                          (1 << 10, 1 << 8, 2), (3000, 500, 2)])
 def test_whole_r1cs_proof_verifies(nc, ni, batch):
-    """pko_prove_r1cs: the Spartan part, then the WHIR proof of the three
-    covectors M^T eq(alpha) against the evaluations; the WHIR part verifies
-    from the transcript state the prover started it from, and the
-    evaluations are the covectors' dot products with the padded witness."""
+    """pko_prove_r1cs: the Spartan part, then the WHIR proof of the
+    covectors M^T eq(alpha) and the blinding covector against the
+    evaluations; the WHIR part verifies from the transcript state the prover
+    started it from, and the evaluations are the covectors' dot products
+    with the padded witness."""
     from provekit_b200.prover import HostR1CS
     h = HostR1CS(nc + ni, nc, ni)
     m, m0 = O.r1cs_sizing(h.num_constraints, h.num_witnesses)
@@ -288,22 +289,27 @@ def test_whole_r1cs_proof_verifies(nc, ni, batch):
     sp, cw, proof = O.prove_r1cs(h, 5, 11, wp)
     assert (sp["m"], sp["m0"]) == (m, m0)
     assert O.verify_r1cs_whir(h, wp, 11, sp, cw, proof) == 0
-    cov = O.r1cs_covectors(h, sp["alpha"], m0, 1 << m)  # noqa: F841 (used below)
+    cov = O.r1cs_covectors(h, sp["alpha"], m0, 1 << m)
+    ncov = O.statement_count(h)  # A, B, C and the blinding covector
+    stm = O.statement_covectors(h, sp)
+    assert stm.shape[0] == ncov << m
     if batch == 2:
         # whir-ZK: the blinding polynomial is the indexed sampler's
         g = np.zeros((1 << m, 4), np.uint64)
         O.lib().pko_sample_fr_indexed(5 ^ 0x243f6a8885a308d3, 0, 1 << m, O.p64(g))
-        for k in range(3):
+        for k in range(ncov):
             d = np.zeros(4, np.uint64)
-            O.lib().pko_dot(O.p64(d), O.p64(np.ascontiguousarray(cov[k << m:(k + 1) << m])),
+            O.lib().pko_dot(O.p64(d), O.p64(np.ascontiguousarray(stm[k << m:(k + 1) << m])),
                             O.p64(g), 1 << m)
-            assert np.array_equal(proof[12 + 4 * k:16 + 4 * k], d)
+            assert np.array_equal(proof[4 * (ncov + k):4 * (ncov + k) + 4], d)
     for k in range(3):
         assert np.array_equal(proof[4 * k:4 * k + 4], sp["evals"][k])
         d = np.zeros(4, np.uint64)
         O.lib().pko_dot(O.p64(d), O.p64(np.ascontiguousarray(cov[k << m:(k << m) + h.num_witnesses])),
                         O.p64(np.ascontiguousarray(h.witness)), h.num_witnesses)
         assert np.array_equal(d, sp["evals"][k])
+    # the fourth statement is the zk-sumcheck's blinding evaluation
+    assert np.array_equal(proof[12:16], sp["blinding_eval"])
     # the WHIR part is bound to the Spartan transcript
     bad = dict(sp)
     bad["transcript"] = (list(sp["transcript"][1]), list(sp["transcript"][0]))
@@ -326,3 +332,43 @@ def test_batch_tampering_is_rejected():
     # a batch proof is not a proof about either polynomial alone
     p1 = O.whir_params(11, 3, 2, 40, 0)
     assert O.whir_verify(p1, 17, cov, 2, cw[:8], proof) != 0
+
+
+
+@pytest.mark.parametrize("npub,batch", [(1, 1), (3, 2), (200, 1)])
+def test_whole_proof_with_public_inputs_verifies(npub, batch):
+    """Public inputs (witness[1 ..= n]): their hash enters the transcript
+    (PublicInputs::hash, provekit/common/src/witness/mod.rs:86-97), the
+    public weight [1, x, .., x^n] is the first statement and its value
+    <weight, w> is sent after the three evaluations."""
+    from provekit_b200.prover import HostR1CS
+    h = HostR1CS(61 + npub, 1 << 10, 1 << 9, num_public_inputs=npub)
+    m, m0 = O.r1cs_sizing(h.num_constraints, h.num_witnesses)
+    wp = O.whir_params(m, 3, 2, 40, 3, batch_size=batch)
+    sp, cw, proof = O.prove_r1cs(h, 2, 21, wp)
+    assert O.statement_count(h) == 5
+    assert O.verify_r1cs_whir(h, wp, 21, sp, cw, proof) == 0
+    # the hash over the canonical public values
+    pub = np.ascontiguousarray(h.witness[1:1 + npub]).copy()
+    O.lib().pko_from_mont_many(O.p64(pub), npub)
+    exp = np.zeros(4, np.uint64)
+    O.lib().pko_public_inputs_hash(O.p64(exp), O.p64(pub), npub)
+    assert np.array_equal(sp["public_hash"], exp)
+    assert np.array_equal(proof[0:4], sp["public_eval"])
+    # another public value changes the hash, hence x and the whole proof
+    h.witness[1] = O.sample_fr(999, 1)[0]
+    sp2, cw2, proof2 = O.prove_r1cs(h, 2, 21, wp)
+    assert not np.array_equal(sp2["public_hash"], sp["public_hash"])
+    assert not np.array_equal(sp2["public_x"], sp["public_x"])
+
+
+def test_public_inputs_hash_cases():
+    """0 for none, compress(v, 0) for one, the left fold for more."""
+    v = O.sample_fr(5, 3, mont=False)
+    out = np.zeros(4, np.uint64)
+    O.lib().pko_public_inputs_hash(O.p64(out), O.p64(v), 0)
+    assert not out.any()
+    O.lib().pko_public_inputs_hash(O.p64(out), O.p64(v), 1)
+    assert np.array_equal(out, O.compress(v[0], np.zeros(4, np.uint64)))
+    O.lib().pko_public_inputs_hash(O.p64(out), O.p64(v), 3)
+    assert np.array_equal(out, O.compress(O.compress(v[0], v[1]), v[2]))
