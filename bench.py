@@ -544,7 +544,7 @@ def run_b200(a):
 
 
 # ---------------------------------------------------------------------------
-# Config 3 (the headline): whole proofs of a synthetic 2^20-constraint R1CS.
+# The headline: whole proofs of a synthetic 2^20-constraint R1CS.
 # ---------------------------------------------------------------------------
 PROVE_NC, PROVE_NI = 1 << 20, 1 << 18
 
@@ -851,7 +851,7 @@ def run_reference_prove(a):
 
 
 # ---------------------------------------------------------------------------
-# Config 4: the batched form vs the plain path.
+# The batched form (256 uneven jobs) vs the plain path.
 # ---------------------------------------------------------------------------
 def batched_sizes(seed, jobs, lo=10, hi=22):
     import numpy as np
@@ -951,7 +951,7 @@ def run_batched(a):
 
 
 # ---------------------------------------------------------------------------
-# Config 5: the served form under open-loop Poisson arrivals.
+# The served form under open-loop Poisson arrivals.
 # ---------------------------------------------------------------------------
 def run_served(a):
     import concurrent.futures as cf
@@ -1039,7 +1039,8 @@ def run_served(a):
 
 
 # ---------------------------------------------------------------------------
-# NTT: 2^24 (the north star's roofline target) and config 1 (2^16).
+# NTT: 2^24 (the size whose FP64-roofline fraction is the transform's target)
+# and the 2^16 single-vector transform.
 # ---------------------------------------------------------------------------
 def run_ntt(a):
     import numpy as np
@@ -1102,7 +1103,7 @@ def run_ntt(a):
                      "hbm_gbs": 2 * 32 * n * ((logn + 8) // 9) / (ms * 1e-3) / 1e9,
                      "intt_rn_ms": ms_inv, "intt_fr_per_s": n / (ms_inv * 1e-3),
                      "round_trip_ok": ok}
-    line = {"metric": "BN254 Fr ntt_nr throughput, 2^24 (roofline target) and 2^16 (config 1)",
+    line = {"metric": "BN254 Fr ntt_nr throughput, 2^24 (roofline target) and 2^16 (single vector)",
             "value": out[24]["fr_per_s"], "unit": "Fr/s", "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": out[24]["ms"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32 (BN254 Fr, 8x32-bit limbs)",

@@ -91,8 +91,8 @@ size_t prove_footprint(size_t nc, size_t nw, const size_t nnz[3], unsigned ff, u
   if (whole) {
     // the WHIR rounds: up to five padded statement covectors (public
     // weight, A, B, C, blinding), f^ and w tables, two folded polynomials,
-    // and two round codewords with their trees at a time (round 1's, the
-    // largest, holds n << (lr - 1) Fr)
+    // and two round codewords with their trees at a time (the first
+    // round's, the largest, holds n << (lr - 1) Fr)
     const size_t cw1 = lr >= 1 ? n << (lr - 1) : n;
     b += 32 * 5 * n + 32 * 2 * n + 32 * 2 * (n >> ff);
     b += 2 * (32 * cw1 + 32 * 2 * (cw1 >> ff));

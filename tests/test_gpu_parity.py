@@ -58,7 +58,7 @@ def test_ntt_nr_interleaved_and_skipped_stages(logn, cols, groups):
     assert np.array_equal(host(d), exp)
 
 
-def test_ntt_config1_2_16_bit_exact_and_round_trip():
+def test_ntt_2_16_single_vector_bit_exact_and_round_trip():
     """2^16 Fr from ChaCha seed 1, ntt_nr(v, 2^16, 1); bit-exact against the
     oracle, and intt_rn round-trips to the input."""
     from provekit_b200.ntt import intt_rn, ntt_nr
