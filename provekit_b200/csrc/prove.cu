@@ -226,10 +226,11 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     if (rc) return rc;
     if ((rc = spmv_device(rp_t, cl_t, vl_t, nw, nc, eq, alph, err, s))) return rc;
     // create_weights_and_evaluations (:623-642): the zero padding adds nothing
-    if ((rc = dot_device(alph, poly, nw, dot_out, part, s))) return rc;
-    if ((rc = read_small(out->evals[k], dot_out, 32, s))) return rc;
-    pkg_transcript_absorb(&out->transcript, out->evals[k]);
+    if ((rc = dot_device(alph, poly, nw, dot_out + 4 * k, part, s))) return rc;
   }
+  // the three evaluations read back at once, then absorbed in order
+  if ((rc = read_small(&out->evals[0][0], dot_out, 96, s))) return rc;
+  for (int k = 0; k < 3; k++) pkg_transcript_absorb(&out->transcript, out->evals[k]);
   // the public weight's evaluation <[1, x, .., x^np], w> and its message
   // (compute_public_weight_evaluation, :654-663, :275-282)
   std::vector<HostFr> xpow(np + 1);
@@ -271,10 +272,9 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     }
     memcpy(vals.data() + at, &out->evals[0][0], 96);
     memcpy(vals.data() + at + 12, out->blinding_eval, 32);
-    for (size_t k = 0; nb == 2 && k < nstm; k++) {
-      if ((rc = dot_device(cov + 4 * n * k, mask, n, dot_out, part, s))) return rc;
-      if ((rc = read_small(vals.data() + 4 * (nstm + k), dot_out, 32, s))) return rc;
-    }
+    for (size_t k = 0; nb == 2 && k < nstm; k++)
+      if ((rc = dot_device(cov + 4 * n * k, mask, n, dot_out + 4 * k, part, s))) return rc;
+    if (nb == 2 && (rc = read_small(vals.data() + 4 * nstm, dot_out, 32 * nstm, s))) return rc;
     // host sources above are pageable: staged before the copies returned
     pkg_transcript tw = out->transcript;
     if ((rc = whir_prove_device(whir, &tw, poly, cw, layers, ood_points, cov, nstm, vals.data(),
