@@ -171,3 +171,45 @@ def test_whir_prove_validation_needs_no_device(L):
                             proof.ctypes.data, None) == PKG_ERR_INVALID_ARGUMENT
     assert L.pkg_subset_transform(None, 4, 0, None) == PKG_ERR_INVALID_ARGUMENT
     assert L.pkg_subset_transform(16, 4, 7, None) == PKG_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("nc,nw", [(1, 1), (3, 5), (1 << 10, 1 << 9), (1000, 70000),
+                                   (1 << 20, (1 << 18) + (1 << 20) + 1), (5, 4 * 13 + 8200)])
+def test_r1cs_sizing_matches_oracle(nc, nw):
+    """new_for_r1cs sizing (m, m0), with the blinding slots' extra variable."""
+    from provekit_b200.prover import r1cs_sizing
+    assert r1cs_sizing(nc, nw) == O.r1cs_sizing(nc, nw)
+
+
+def test_prove_r1cs_validation_needs_no_device(L):
+    """pkg_prove_r1cs refuses bad arguments before any device work: no WHIR
+    parameters, parameters for another variable count, a batch other than
+    1 or 2, as many public inputs as witnesses, null outputs."""
+    from provekit_b200.prover import R1csC, SpartanProofC, r1cs_sizing
+    from provekit_b200.whir import WhirParams
+    from provekit_b200._lib import PKG_ERR_INVALID_ARGUMENT
+    nc, nw = 1 << 10, (1 << 9) + (1 << 10) + 1
+    m, _ = r1cs_sizing(nc, nw)
+    r = R1csC(nc, nw)
+    out = SpartanProofC()
+    w = np.zeros(4 * 16, np.uint64)
+    wptr = (w.ctypes.data + 15) // 16 * 16
+    cw = np.zeros(64, np.uint64)
+
+    def prove(p, r1cs=r, words=cw.ctypes.data, proof=cw.ctypes.data):
+        return L.pkg_prove_r1cs(ctypes.byref(r1cs), wptr, 1, 2,
+                                None if p is None else ctypes.byref(p), ctypes.byref(out),
+                                words, proof, None)
+
+    assert prove(None) == PKG_ERR_INVALID_ARGUMENT
+    assert prove(WhirParams.new(m + 1, 3, 2, 64, 4)) == PKG_ERR_INVALID_ARGUMENT
+    assert prove(WhirParams.new(m, 3, 2, 64, 4, batch_size=4)) == PKG_ERR_INVALID_ARGUMENT
+    good = WhirParams.new(m, 3, 2, 64, 4, batch_size=2)
+    assert prove(good, words=None) == PKG_ERR_INVALID_ARGUMENT
+    assert prove(good, proof=None) == PKG_ERR_INVALID_ARGUMENT
+    many = R1csC(nc, nw)
+    many.num_public_inputs = nw
+    assert prove(good, r1cs=many) == PKG_ERR_INVALID_ARGUMENT
+    assert L.pkg_prove_r1cs(ctypes.byref(r), w.ctypes.data + 8, 1, 2, ctypes.byref(good),
+                            ctypes.byref(out), cw.ctypes.data, cw.ctypes.data,
+                            None) == PKG_ERR_INVALID_ARGUMENT  # unaligned witness
