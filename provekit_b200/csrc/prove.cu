@@ -3,7 +3,7 @@
 // evaluations (provekit/prover/src/whir_r1cs.rs:82-301,
 // provekit/r1cs-compiler/src/whir_r1cs.rs:48-92); pkg_prove_r1cs: the same
 // with whir's commitment OOD samples and the WHIR proof (pkg_whir_prove) of
-// the covector evaluations, a whole proof.
+// the statements' evaluations, a whole proof.
 //
 // Device data: the padded witness polynomial (2^m Fr), its RS codeword and
 // Merkle layers, the a/b/c sumcheck tables (2^m0 Fr each), eq(alpha), the
@@ -75,7 +75,8 @@ extern "C" int pkg_r1cs_sizing(size_t num_constraints, size_t num_witnesses, siz
 // With whir == nullptr the commitment's root alone enters the transcript and
 // the proof ends at the covector evaluations (pkg_spartan_prove); with whir,
 // the commitment's OOD samples follow the root and the WHIR proof of the
-// three zero-padded covectors ends it (pkg_prove_r1cs).
+// statements ends it (pkg_prove_r1cs): the public weight when there are
+// public inputs, the three zero-padded covectors and the blinding covector.
 static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
                               uint64_t blinding_seed, uint64_t transcript_domain, unsigned ff,
                               unsigned lr, pkg_spartan_proof* out, const pkg_whir_params* whir,

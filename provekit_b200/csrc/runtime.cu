@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "fr.cuh"
+#include "fr_f64.cuh"
 #include "fr_host.hpp"
 #include "pk_common.cuh"
 
@@ -275,9 +276,11 @@ __device__ void chacha20_block_dev(uint32_t k0, uint32_t k1, uint64_t counter, u
   for (int i = 0; i < 16; i++) out[i] = x[i] + s[i];
 }
 
-// out[i] = lo + hi 2^253 mod p (Montgomery) from ChaCha20 block start + i.
-__global__ void sample_indexed_kernel(uint32_t k0, uint32_t k1, uint64_t start, size_t n, Fr t253,
-                                      uint64_t* __restrict__ out) {
+// out[i] = lo + hi 2^253 mod p (Montgomery) from ChaCha20 block start + i,
+// as two products on the FP64 pipe: lo * R^2 and hi * (2^253 R^2), each
+// times R^-1 (lo, hi < 2^253 < p).
+__global__ void sample_indexed_kernel(uint32_t k0, uint32_t k1, uint64_t start, size_t n, Fr r2,
+                                      Fr t253r2, uint64_t* __restrict__ out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     uint32_t b[16];
@@ -290,7 +293,7 @@ __global__ void sample_indexed_kernel(uint32_t k0, uint32_t k1, uint64_t start, 
     }
     lo.v[7] &= 0x1fffffffu;
     hi.v[7] &= 0x1fffffffu;
-    fr_store(out, i, fr_add(fr_to_mont(lo), fr_mul(fr_to_mont(hi), t253)));
+    fr_store(out, i, fr_add(fr_mul_f64(lo, r2), fr_mul_f64(hi, t253r2)));
   }
 }
 }  // namespace pk
@@ -299,15 +302,19 @@ extern "C" int pkg_sample_fr_indexed(uint64_t seed, uint64_t start, size_t n, ui
                                      pkg_stream_t stream) {
   if (n == 0) return PKG_OK;
   PK_REQUIRE(out && aligned16(out), "null or unaligned output");
-  HostFr two253;
+  HostFr one, two253;
+  one.l[0] = 1;
   two253.l[3] = uint64_t(1) << 61;
-  const HostFr t = HostFr::to_mont(two253);
-  Fr t253;
-  memcpy(t253.v, t.l, 32);
+  // x R^2 mod p as raw limbs: to_mont applied twice
+  const HostFr r2h = HostFr::to_mont(HostFr::to_mont(one));
+  const HostFr th = HostFr::to_mont(HostFr::to_mont(two253));
+  Fr r2, t253r2;
+  memcpy(r2.v, r2h.l, 32);
+  memcpy(t253r2.v, th.l, 32);
   const int grid = (int)std::min<size_t>((n + 255) / 256, (size_t)sm_count() * 16);
   sample_indexed_kernel<<<grid, 256, 0, as_stream(stream)>>>((uint32_t)seed,
                                                               (uint32_t)(seed >> 32), start, n,
-                                                              t253, out);
+                                                              r2, t253r2, out);
   PK_CHECK_LAUNCH("sample_indexed_kernel");
   return PKG_OK;
 }

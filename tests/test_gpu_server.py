@@ -97,3 +97,27 @@ def test_served_whole_proofs_equal_alone_results():
         same(got, sp)
         assert times["submit_ns"] <= times["admit_ns"] <= times["done_ns"]
     srv.close()
+
+
+def test_served_mix_of_public_inputs_and_zk_equals_alone_results():
+    """A mix of whole proofs with 0, 1 and 3 public inputs, committed with
+    a blinding polynomial (whir-ZK) or alone, served together: each equals
+    the same request proved alone."""
+    from provekit_b200.prover import HostR1CS, prove_r1cs, whir_params_for
+    from provekit_b200.server import ProofServer
+    spec = [(12, 10, 0, True), (13, 11, 1, False), (12, 10, 3, True), (14, 12, 1, True),
+            (11, 9, 3, False), (13, 11, 0, False)]
+    reqs = [HostR1CS(800 + i, 1 << lc, 1 << li, num_public_inputs=npub)
+            for i, (lc, li, npub, _) in enumerate(spec)]
+    params = [whir_params_for(h, zk=zk) for h, (_, _, _, zk) in zip(reqs, spec)]
+    alone = [prove_r1cs(h.to_device(), whir=p, blinding_seed=5 + i, transcript_domain=60 + i)
+             for i, (h, p) in enumerate(zip(reqs, params))]
+    srv = ProofServer(hbm_budget_bytes=1 << 30, max_inflight=3)
+    ids = [srv.submit(h, whir=p, blinding_seed=5 + i, transcript_domain=60 + i)
+           for i, (h, p) in enumerate(zip(reqs, params))]
+    for rid, (sp, cw, proof) in zip(ids, alone):
+        got, _ = srv.wait(rid)
+        assert np.array_equal(got.pop("whir_commit_words"), cw)
+        assert np.array_equal(got.pop("whir_proof"), proof)
+        same(got, sp)
+    srv.close()
