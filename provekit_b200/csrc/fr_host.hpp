@@ -158,14 +158,18 @@ struct HostFr {
   static HostFr root_of_unity(uint64_t n) {
     int k = 0;
     while ((uint64_t(1) << k) < n) k++;
-    uint64_t t[4] = {P[0] - 1, P[1], P[2], P[3]};
-    for (int i = 0; i < 28; i++) {
-      t[0] = (t[0] >> 1) | (t[1] << 63);
-      t[1] = (t[1] >> 1) | (t[2] << 63);
-      t[2] = (t[2] >> 1) | (t[3] << 63);
-      t[3] >>= 1;
-    }
-    HostFr w = pow(from_u64(5), t);
+    // the 2^28-th root, exponentiated once per process (~400 products)
+    static const HostFr w28 = [] {
+      uint64_t t[4] = {P[0] - 1, P[1], P[2], P[3]};
+      for (int i = 0; i < 28; i++) {
+        t[0] = (t[0] >> 1) | (t[1] << 63);
+        t[1] = (t[1] >> 1) | (t[2] << 63);
+        t[2] = (t[2] >> 1) | (t[3] << 63);
+        t[3] >>= 1;
+      }
+      return pow(from_u64(5), t);
+    }();
+    HostFr w = w28;
     for (int i = k; i < 28; i++) w = mul(w, w);
     return w;
   }

@@ -20,9 +20,11 @@ int eq_hypercube_device(const uint64_t* r_host, size_t nr, size_t num_entries, u
 int pow_solve_device(const uint64_t challenge[4], const uint64_t threshold[4], cudaStream_t s,
                      uint64_t* nonce_out);
 // w += sum_j coeffs_j eq(points_j, .) (pkg_eq_accumulate); sync = false only
-// when points and coeffs are pageable host memory.
+// when points and coeffs are pageable host memory.  expanded: points holds
+// npts x nv coordinates; otherwise npts univariate points z, expanded on the
+// device to (z^(2^(nv-1)), .., z^2, z).
 int eq_accumulate_device(uint64_t* w, size_t nv, const uint64_t* points, const uint64_t* coeffs,
-                         size_t npts, cudaStream_t s, bool sync);
+                         size_t npts, cudaStream_t s, bool sync, bool expanded = true);
 // Codeword rows and their Merkle paths for nq indices (host in/out), one sync.
 int open_rows_device(const uint64_t* codeword, size_t fr_per_row, size_t num_rows,
                      const uint8_t* layers, const uint64_t* indices, size_t nq, uint64_t* rows,

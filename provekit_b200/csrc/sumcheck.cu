@@ -267,6 +267,12 @@ static HostFr eval_cubic(const HostFr* c, const HostFr& x) {
   return HostFr::add(acc, c[0]);
 }
 
+// 1/2 in Montgomery form, inverted once (an inversion is ~400 products).
+static const HostFr& half_mont() {
+  static const HostFr h = HostFr::inv(HostFr::add(HostFr::one(), HostFr::one()));
+  return h;
+}
+
 // compute_blinding_coefficients_for_round (whir_r1cs.rs:427-492)
 static void blinding_coeffs(const HostFr* g, size_t n, size_t compute_for, const HostFr* alphas,
                             HostFr out[4]) {
@@ -283,7 +289,7 @@ static void blinding_coeffs(const HostFr* g, size_t n, size_t compute_for, const
                                              eval_cubic(g + 4 * i, HostFr::one())));
   HostFr pm = HostFr::one();
   for (size_t i = 0; i < n - 1 - cf; i++) pm = HostFr::add(pm, pm);
-  HostFr sm = HostFr::mul(pm, HostFr::inv(HostFr::add(HostFr::one(), HostFr::one())));
+  HostFr sm = HostFr::mul(pm, half_mont());
   HostFr cst = HostFr::add(HostFr::mul(pm, prefix), HostFr::mul(sm, suffix));
   const HostFr* cur = g + 4 * cf;
   HostFr res[4] = {HostFr::add(HostFr::mul(pm, cur[0]), cst), HostFr::mul(pm, cur[1]),
@@ -506,7 +512,7 @@ extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_
   HostFr rho = t.squeeze();         // :543
   memcpy(rho_out, rho.l, 32);
   HostFr saved = HostFr::mul(rho, sum_g);
-  const HostFr half = HostFr::inv(HostFr::add(HostFr::one(), HostFr::one()));
+  const HostFr half = half_mont();
   size_t size = n;
   uint64_t h[12];
   for (size_t idx = 0; idx < m0; idx++) {  // :550-610

@@ -188,6 +188,21 @@ __global__ void eq_tables_kernel(const uint64_t* __restrict__ pts, size_t stride
   }
 }
 
+// out[j nv + nv - 1 - i] = z_j^(2^i): the expansion of each univariate point
+// into nv coordinates, the top variable first (ExpandFromUnivariate,
+// recursive-verifier/app/utilities/utilities.go:183-191).
+__global__ void expand_points_kernel(const uint64_t* __restrict__ raw, size_t npts, size_t nv,
+                                     uint64_t* __restrict__ out) {
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npts;
+       j += (size_t)gridDim.x * blockDim.x) {
+    Fr acc = fr_load_ro(raw, j);
+    for (size_t i = 0; i < nv; i++) {
+      fr_store(out, j * nv + nv - 1 - i, acc);
+      acc = fr_sqr_f64(acc);
+    }
+  }
+}
+
 // w[b] += sum_j hi_j[b >> nlo] lo_j[b & (2^nlo - 1)]
 __global__ void eq_accumulate_kernel(uint64_t* __restrict__ w, size_t n, int nlo,
                                      const uint64_t* __restrict__ hi, size_t nhi_entries,
@@ -407,19 +422,27 @@ extern "C" int pkg_whir_sumcheck_round(uint64_t* f, uint64_t* w, size_t size, co
 
 namespace pk {
 int eq_accumulate_device(uint64_t* w, size_t nv, const uint64_t* points, const uint64_t* coeffs,
-                         size_t npts, cudaStream_t s, bool sync) {
+                         size_t npts, cudaStream_t s, bool sync, bool expanded) {
   if (npts == 0) return PKG_OK;
   const int nhi = (int)(nv + 1) / 2, nlo = (int)nv - nhi;
   const size_t nh = size_t(1) << nhi, nl = size_t(1) << nlo, n = size_t(1) << nv;
   Scratch scr;
   const size_t pts_fr = npts * (nv ? nv : 1);
-  int rc = scr.alloc(32 * (pts_fr + npts + npts * (nh + nl)), s);
+  // [expanded points | coefficients | hi tables | lo tables | raw points]
+  int rc = scr.alloc(32 * (pts_fr + npts + npts * (nh + nl) + (expanded ? 0 : npts)), s);
   if (rc) return rc;
   uint64_t* d_pts = static_cast<uint64_t*>(scr.ptr);
   uint64_t* d_cf = d_pts + 4 * pts_fr;
   uint64_t* d_hi = d_cf + 4 * npts;
   uint64_t* d_lo = d_hi + 4 * npts * nh;
-  if (nv) PK_CUDA(cudaMemcpyAsync(d_pts, points, 32 * npts * nv, cudaMemcpyHostToDevice, s));
+  if (nv && expanded) {
+    PK_CUDA(cudaMemcpyAsync(d_pts, points, 32 * npts * nv, cudaMemcpyHostToDevice, s));
+  } else if (nv) {
+    uint64_t* d_raw = d_lo + 4 * npts * nl;
+    PK_CUDA(cudaMemcpyAsync(d_raw, points, 32 * npts, cudaMemcpyHostToDevice, s));
+    expand_points_kernel<<<ew_grid(npts), 256, 0, s>>>(d_raw, npts, nv, d_pts);
+    PK_CHECK_LAUNCH("expand_points_kernel");
+  }
   PK_CUDA(cudaMemcpyAsync(d_cf, coeffs, 32 * npts, cudaMemcpyHostToDevice, s));
   // hi tables carry the coefficient, lo tables are plain eq tables
   eq_tables_kernel<<<ew_grid(npts * nh), 256, 0, s>>>(d_pts, nv, 0, nhi, d_cf, npts, d_hi);

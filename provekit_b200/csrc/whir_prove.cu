@@ -157,16 +157,6 @@ static std::vector<HostFr> powers_of(const HostFr& g, size_t n) {
   return out;
 }
 
-// ExpandFromUnivariate (recursive-verifier/app/utilities/utilities.go:183-191)
-static void expand_into(std::vector<HostFr>& out, const HostFr& z, unsigned m) {
-  HostFr acc = z;
-  const size_t base = out.size();
-  out.resize(base + m);
-  for (unsigned i = 0; i < m; i++) {
-    out[base + m - 1 - i] = acc;
-    acc = HostFr::mul(acc, acc);
-  }
-}
 
 static void pow_threshold(unsigned bits, uint64_t thr[4]) {
   memcpy(thr, HostFr::P, 32);
@@ -334,12 +324,10 @@ int WhirProver::stir_step(size_t q, size_t L, size_t K, const uint64_t* cw, cons
 // w += sum_j coefs_j eq(expand(points_j), .) on the live nv-variable table.
 int WhirProver::add_constraints(const std::vector<HostFr>& points, unsigned nv,
                                 const std::vector<HostFr>& coefs) {
-  std::vector<HostFr> pts;
-  pts.reserve(points.size() * nv);
-  for (const HostFr& z : points) expand_into(pts, z, nv);
-  // pts and coefs are pageable: staged before the copies return, no sync
-  return eq_accumulate_device(w_, nv, pts.empty() ? nullptr : pts[0].l, coefs[0].l, points.size(),
-                              s_, false);
+  // points and coefs are pageable: staged before the copies return, no
+  // sync; the points are expanded on the device
+  if (points.empty()) return PKG_OK;
+  return eq_accumulate_device(w_, nv, points[0].l, coefs[0].l, points.size(), s_, false, false);
 }
 
 int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint8_t* layers,
