@@ -73,6 +73,22 @@ struct HostRead {
   size_t bytes;
 };
 int read_small(const HostRead* reads, int n, cudaStream_t s);
+
+// Per host thread: a mapped pinned buffer of kFusedSlotFr Fr that fused
+// reductions (reduce.cuh's RedOut with a ticket) write their sums to, and a
+// device counter on the current device for their tickets.  One of each per
+// thread is enough because every user launches its fused reductions in
+// stream order on one stream and synchronises before returning, so a
+// thread's fused launches never run at the same time.
+struct FusedSlots {
+  uint64_t* host;    // the buffer, as the host reads it
+  uint64_t* dev;     // the same buffer, as kernels write it
+  unsigned* ticket;  // zero between launches
+};
+constexpr size_t kFusedSlotFr = 64;
+int fused_slots(FusedSlots* f);
+// Waits for the stream, then copies bytes of the thread's slots to dst.
+int fused_read(void* dst, const FusedSlots& f, size_t bytes, cudaStream_t s);
 inline int read_small(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   const HostRead r{dst, src, bytes};
   return read_small(&r, 1, s);

@@ -152,12 +152,14 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   clk.mark(0);
 
   // ---- witness bounds (sumcheck.rs:163-179)
-  // partial sums of dot_device (<= 4 * SMs CTAs) and its result slot
+  // partial sums of dot_device (<= 4 * SMs CTAs); its results go to the
+  // thread's fused slots
   const size_t nparts = 4 * (size_t)sm_count();
-  if ((rc = s_misc.alloc(256 + 32 * (nparts + 8), s))) return rc;
+  FusedSlots fs;
+  if ((rc = fused_slots(&fs))) return rc;
+  if ((rc = s_misc.alloc(256 + 32 * nparts, s))) return rc;
   uint32_t* err = static_cast<uint32_t*>(s_misc.ptr);
   uint64_t* part = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(s_misc.ptr) + 256);
-  uint64_t* dot_out = part + 4 * nparts;
   PK_CUDA(cudaMemsetAsync(err, 0, 4, s));
   PK_CUDA(cudaMemsetAsync(ta, 0, 32 * 3 * n0, s));
   if ((rc = spmv_device(r1cs->row_ptr[0], r1cs->cols[0], r1cs->vals[0], nc, nw, witness, ta, err, s)))
@@ -227,10 +229,10 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     if (rc) return rc;
     if ((rc = spmv_device(rp_t, cl_t, vl_t, nw, nc, eq, alph, err, s))) return rc;
     // create_weights_and_evaluations (:623-642): the zero padding adds nothing
-    if ((rc = dot_device(alph, poly, nw, dot_out + 4 * k, part, s))) return rc;
+    if ((rc = dot_device(alph, poly, nw, fs.dev + 4 * k, part, s, fs.ticket))) return rc;
   }
   // the three evaluations read back at once, then absorbed in order
-  if ((rc = read_small(&out->evals[0][0], dot_out, 96, s))) return rc;
+  if ((rc = fused_read(&out->evals[0][0], fs, 96, s))) return rc;
   for (int k = 0; k < 3; k++) pkg_transcript_absorb(&out->transcript, out->evals[k]);
   // the public weight's evaluation <[1, x, .., x^np], w> and its message
   // (compute_public_weight_evaluation, :654-663, :275-282)
@@ -274,8 +276,9 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     memcpy(vals.data() + at, &out->evals[0][0], 96);
     memcpy(vals.data() + at + 12, out->blinding_eval, 32);
     for (size_t k = 0; nb == 2 && k < nstm; k++)
-      if ((rc = dot_device(cov + 4 * n * k, mask, n, dot_out + 4 * k, part, s))) return rc;
-    if (nb == 2 && (rc = read_small(vals.data() + 4 * nstm, dot_out, 32 * nstm, s))) return rc;
+      if ((rc = dot_device(cov + 4 * n * k, mask, n, fs.dev + 4 * k, part, s, fs.ticket)))
+        return rc;
+    if (nb == 2 && (rc = fused_read(vals.data() + 4 * nstm, fs, 32 * nstm, s))) return rc;
     // host sources above are pageable: staged before the copies returned
     pkg_transcript tw = out->transcript;
     if ((rc = whir_prove_device(whir, &tw, poly, cw, layers, ood_points, cov, nstm, vals.data(),

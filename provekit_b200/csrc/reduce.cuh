@@ -47,6 +47,59 @@ __device__ __forceinline__ void block_sum(Fr (&v)[K]) {
   }
 }
 
+// Where a reduction kernel's CTAs leave their sums.  part: one partial per
+// CTA (K Fr each), summed by sum_partials_kernel.  With a ticket, the kernel
+// finishes the sum itself: every CTA takes a ticket after storing its
+// partial, and the CTA that takes the last one adds all partials, writes the
+// K sums to out (device or mapped host memory) and resets the counter for the
+// next launch -- one launch instead of two, no copy when out is mapped.
+struct RedOut {
+  uint64_t* part;
+  unsigned* ticket;  // nullptr: partials only
+  uint64_t* out;
+};
+
+// 32 bytes through L2 only: partials other CTAs wrote during this launch.
+__device__ __forceinline__ Fr fr_load_cg(const uint64_t* base, size_t idx) {
+  const uint4* q = reinterpret_cast<const uint4*>(base + 4 * idx);
+  const uint4 a = __ldcg(q), b = __ldcg(q + 1);
+  Fr r;
+  r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+  r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+  return r;
+}
+
+// The end of a reduction kernel: block sum, the CTA's partial, and with a
+// ticket the last CTA's final sum.  Every thread of the CTA calls it.
+template <int K>
+__device__ __forceinline__ void block_finish(Fr (&v)[K], const RedOut& ro) {
+  __shared__ bool last;
+  block_sum<K>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) fr_store(ro.part, (size_t)blockIdx.x * K + k, v[k]);
+    if (ro.ticket) {
+      __threadfence();
+      last = atomicAdd(ro.ticket, 1u) == gridDim.x - 1;
+    }
+  }
+  if (!ro.ticket) return;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < K; k++) v[k] = fr_zero();
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = fr_add(v[k], fr_load_cg(ro.part, (size_t)i * K + k));
+  block_sum<K>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) fr_store(ro.out, k, v[k]);
+    *ro.ticket = 0u;
+  }
+}
+
 template <int K>
 __global__ void __launch_bounds__(kRedThreads) sum_partials_kernel(const uint64_t* __restrict__ part,
                                                                  int nparts,

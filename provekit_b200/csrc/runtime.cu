@@ -111,6 +111,49 @@ __global__ void dfma_rate_kernel(double* sink, double c, double d, int iters) {
   if (s == -1.0) sink[threadIdx.x] = s;
 }
 
+int fused_slots(FusedSlots* f) {
+  constexpr int kMaxDevices = 64;
+  thread_local uint64_t* host = nullptr;
+  thread_local uint64_t* dev = nullptr;
+  thread_local unsigned* tickets[kMaxDevices] = {};
+  if (!host) {
+    void* p = nullptr;
+    PK_CUDA(cudaHostAlloc(&p, 32 * kFusedSlotFr, cudaHostAllocMapped | cudaHostAllocPortable));
+    void* d = nullptr;
+    PK_CUDA(cudaHostGetDevicePointer(&d, p, 0));
+    host = static_cast<uint64_t*>(p);
+    dev = static_cast<uint64_t*>(d);
+  }
+  int device = 0;
+  PK_CUDA(cudaGetDevice(&device));
+  PK_REQUIRE(device >= 0 && device < kMaxDevices, "device ordinal %d out of range", device);
+  if (!tickets[device]) {
+    // zeroed on a private stream, waited for: ordered before any later launch
+    // on any stream without touching the legacy default stream
+    void* t = nullptr;
+    PK_CUDA(cudaMalloc(&t, 256));
+    cudaStream_t z = nullptr;
+    PK_CUDA(cudaStreamCreateWithFlags(&z, cudaStreamNonBlocking));
+    const cudaError_t e1 = cudaMemsetAsync(t, 0, 256, z);
+    const cudaError_t e2 = cudaStreamSynchronize(z);
+    cudaStreamDestroy(z);
+    PK_CUDA(e1);
+    PK_CUDA(e2);
+    tickets[device] = static_cast<unsigned*>(t);
+  }
+  f->host = host;
+  f->dev = dev;
+  f->ticket = tickets[device];
+  return PKG_OK;
+}
+
+int fused_read(void* dst, const FusedSlots& f, size_t bytes, cudaStream_t s) {
+  PK_REQUIRE(bytes <= 32 * kFusedSlotFr, "%zu bytes exceed the fused slots", bytes);
+  PK_CUDA(cudaStreamSynchronize(s));
+  memcpy(dst, f.host, bytes);
+  return PKG_OK;
+}
+
 int read_small(const HostRead* reads, int n, cudaStream_t s) {
   constexpr size_t kCap = size_t(256) << 10;
   thread_local uint8_t* bounce = nullptr;

@@ -38,16 +38,12 @@ struct Tables4 {
 // !kFold: size s = 2q, pairs (t[j], t[j+q]).
 template <bool kFold>
 __global__ void __launch_bounds__(kRedThreads) spartan_round_kernel(Tables4 tabs, size_t q,
-                                                                     Fr fold,
-                                                                     uint64_t* __restrict__ part) {
+                                                                     Fr fold, const RedOut ro) {
   Fr acc[3] = {fr_zero(), fr_zero(), fr_zero()};
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < q;
        j += (size_t)gridDim.x * blockDim.x)
     spartan_pair<kFold>(tabs.t, j, q, fold, acc);
-  block_sum<3>(acc);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int k = 0; k < 3; k++) fr_store(part, (size_t)blockIdx.x * 3 + k, acc[k]);
+  block_finish<3>(acc, ro);
 }
 
 // eq over a block of variables: out[x] = prod_i (bit_i(x) ? r_i : 1 - r_i)
@@ -105,13 +101,12 @@ __global__ void hadamard_pad_kernel(const uint64_t* __restrict__ a, const uint64
 
 __global__ void __launch_bounds__(kRedThreads) dot_kernel(const uint64_t* __restrict__ a,
                                                         const uint64_t* __restrict__ b, size_t n,
-                                                        uint64_t* __restrict__ part) {
+                                                        const RedOut ro) {
   Fr acc[1] = {fr_zero()};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
     acc[0] = fr_add(acc[0], fr_mul_f64(fr_load_ro(a, i), fr_load_ro(b, i)));
-  block_sum<1>(acc);
-  if (threadIdx.x == 0) fr_store(part, blockIdx.x, acc[0]);
+  block_finish<1>(acc, ro);
 }
 
 // ---- CSR transpose: count, exclusive scan, scatter ------------------------
@@ -151,28 +146,32 @@ __global__ void widen_kernel(const uint32_t* __restrict__ in, size_t n, unsigned
 
 
 // One Spartan round on device tables; writes 3 Fr (f0, f(-1), f(inf)) to
-// d_out (device).  part: >= red_grid(q) * 3 Fr of scratch.
+// d_out.  part: >= red_grid(q) * 3 Fr of scratch.  With a ticket (the
+// thread's fused slots) the round kernel writes d_out itself.
 int spartan_round_device(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t* eq, size_t size,
                          const uint64_t* fold_host, uint64_t* part, uint64_t* d_out,
-                         cudaStream_t s) {
+                         cudaStream_t s, unsigned* ticket) {
   Tables4 tabs = {{a, b, c, eq}};
   Fr f;
   memset(&f, 0, sizeof f);
   size_t q;
   int g;
+  const RedOut ro = {part, ticket, ticket ? d_out : nullptr};
   if (fold_host) {
     memcpy(f.v, fold_host, 32);
     q = size / 4;
     g = red_grid(q);
-    spartan_round_kernel<true><<<g, kRedThreads, 0, s>>>(tabs, q, f, part);
+    spartan_round_kernel<true><<<g, kRedThreads, 0, s>>>(tabs, q, f, ro);
   } else {
     q = size / 2;
     g = red_grid(q);
-    spartan_round_kernel<false><<<g, kRedThreads, 0, s>>>(tabs, q, f, part);
+    spartan_round_kernel<false><<<g, kRedThreads, 0, s>>>(tabs, q, f, ro);
   }
   PK_CHECK_LAUNCH("spartan_round_kernel");
-  sum_partials_kernel<3><<<1, kRedThreads, 0, s>>>(part, g, d_out);
-  PK_CHECK_LAUNCH("sum_partials_kernel");
+  if (!ticket) {
+    sum_partials_kernel<3><<<1, kRedThreads, 0, s>>>(part, g, d_out);
+    PK_CHECK_LAUNCH("sum_partials_kernel");
+  }
   return PKG_OK;
 }
 
@@ -233,12 +232,14 @@ static int read_err_flag(uint32_t* d_err, cudaStream_t s, const char* what) {
 }
 
 int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* d_out, uint64_t* part,
-               cudaStream_t s) {
+               cudaStream_t s, unsigned* ticket) {
   int g = red_grid(n);
-  dot_kernel<<<g, kRedThreads, 0, s>>>(a, b, n, part);
+  dot_kernel<<<g, kRedThreads, 0, s>>>(a, b, n, RedOut{part, ticket, ticket ? d_out : nullptr});
   PK_CHECK_LAUNCH("dot_kernel");
-  sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, g, d_out);
-  PK_CHECK_LAUNCH("sum_partials_kernel");
+  if (!ticket) {
+    sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, g, d_out);
+    PK_CHECK_LAUNCH("sum_partials_kernel");
+  }
   return PKG_OK;
 }
 
@@ -365,14 +366,15 @@ extern "C" int pkg_spartan_round(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t
              "device buffers must be 16-byte aligned");
   cudaStream_t s = as_stream(stream);
   size_t q = fold ? size / 4 : size / 2;
+  FusedSlots fs;
+  int rc = fused_slots(&fs);
+  if (rc) return rc;
   Scratch scr;
-  int rc = scr.alloc(32 * (3 * (size_t)red_grid(q) + 3), s);
-  if (rc) return rc;
+  if ((rc = scr.alloc(32 * 3 * (size_t)red_grid(q), s))) return rc;
   uint64_t* part = static_cast<uint64_t*>(scr.ptr);
-  uint64_t* d_out = part + 4 * 3 * (size_t)red_grid(q);
-  rc = spartan_round_device(a, b, c, eq, size, fold, part, d_out, s);
+  rc = spartan_round_device(a, b, c, eq, size, fold, part, fs.dev, s, fs.ticket);
   if (rc) return rc;
-  return read_small(out, d_out, 96, s);
+  return fused_read(out, fs, 96, s);
 }
 
 extern "C" int pkg_eq_hypercube(const uint64_t* r, size_t nr, size_t num_entries, uint64_t* out,
@@ -415,14 +417,16 @@ extern "C" int pkg_dot(const uint64_t* a, const uint64_t* b, size_t n, uint64_t 
   }
   PK_REQUIRE(a && b && aligned16(a) && aligned16(b), "null or unaligned pointer");
   cudaStream_t s = as_stream(stream);
+  FusedSlots fs;
+  int rc = fused_slots(&fs);
+  if (rc) return rc;
   Scratch scr;
   int g = red_grid(n);
-  int rc = scr.alloc(32 * ((size_t)g + 1), s);
-  if (rc) return rc;
+  if ((rc = scr.alloc(32 * (size_t)g, s))) return rc;
   uint64_t* part = static_cast<uint64_t*>(scr.ptr);
-  rc = dot_device(a, b, n, part + 4 * (size_t)g, part, s);
+  rc = dot_device(a, b, n, fs.dev, part, s, fs.ticket);
   if (rc) return rc;
-  return read_small(out, part + 4 * (size_t)g, 32, s);
+  return fused_read(out, fs, 32, s);
 }
 
 extern "C" int pkg_csr_transpose(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
@@ -494,14 +498,16 @@ extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_
     r[i] = t.squeeze();
     memcpy(r_out + 4 * i, r[i].l, 32);
   }
-  // scratch: eq table (n Fr), partials, one round result
+  // scratch: eq table (n Fr), partials; each round's sums go to the
+  // thread's fused slots
   const int gmax = red_grid(n / 2);
-  Scratch scr;
-  int rc = scr.alloc(32 * (n + 3 * (size_t)gmax + 3), s);
+  FusedSlots fs;
+  int rc = fused_slots(&fs);
   if (rc) return rc;
+  Scratch scr;
+  if ((rc = scr.alloc(32 * (n + 3 * (size_t)gmax), s))) return rc;
   uint64_t* eq = static_cast<uint64_t*>(scr.ptr);
   uint64_t* part = eq + 4 * n;
-  uint64_t* d_out = part + 4 * 3 * (size_t)gmax;
   rc = eq_hypercube_device(r_out, m0, n, eq, s);  // :530
   if (rc) return rc;
   HostFr g0[4];
@@ -516,9 +522,10 @@ extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_
   size_t size = n;
   uint64_t h[12];
   for (size_t idx = 0; idx < m0; idx++) {  // :550-610
-    rc = spartan_round_device(a, b, c, eq, size, idx ? alpha[idx - 1].l : nullptr, part, d_out, s);
+    rc = spartan_round_device(a, b, c, eq, size, idx ? alpha[idx - 1].l : nullptr, part, fs.dev, s,
+                              fs.ticket);
     if (rc) return rc;
-    if ((rc = read_small(h, d_out, 96, s))) return rc;
+    if ((rc = fused_read(h, fs, 96, s))) return rc;
     if (idx) size /= 2;
     HostFr gp[4];
     blinding_coeffs(gv.data(), m0, idx, alpha.data(), gp);

@@ -90,7 +90,7 @@ __global__ void whir_fold_rows_kernel(const uint64_t* __restrict__ rows, size_t 
 // P.v[0] = y, P.v[1 + b] = z^(2^b).
 __global__ void __launch_bounds__(kRedThreads) poly_eval_kernel(
     const uint64_t* __restrict__ c, size_t n, const __grid_constant__ FrParams<33> P,
-    uint64_t* __restrict__ part) {
+    const RedOut ro) {
   const size_t G = (size_t)gridDim.x * blockDim.x;
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   Fr v[1] = {fr_zero()};
@@ -102,8 +102,7 @@ __global__ void __launch_bounds__(kRedThreads) poly_eval_kernel(
       if ((t >> b) & 1) acc = fr_mul_f64(acc, param_fr(P, 1 + b));
     v[0] = acc;
   }
-  block_sum<1>(v);
-  if (threadIdx.x == 0) fr_store(part, blockIdx.x, v[0]);
+  block_finish<1>(v, ro);
 }
 
 // path[q depth + l] = node (idx[q] >> l) ^ 1 of level l
@@ -142,7 +141,7 @@ __global__ void gather_rows_kernel(const uint64_t* __restrict__ cw, size_t row_f
 template <bool kFold>
 __global__ void __launch_bounds__(kRedThreads) whir_round_kernel(
     uint64_t* __restrict__ f, uint64_t* __restrict__ w, size_t q,
-    const __grid_constant__ FrParams<1> A, uint64_t* __restrict__ part) {
+    const __grid_constant__ FrParams<1> A, const RedOut ro) {
   Fr acc[3] = {fr_zero(), fr_zero(), fr_zero()};
   const Fr alpha = param_fr(A, 0);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < q;
@@ -163,10 +162,7 @@ __global__ void __launch_bounds__(kRedThreads) whir_round_kernel(
     const Fr f2 = fr_sub(fr_add(f1, f1), f0), w2 = fr_sub(fr_add(w1, w1), w0);
     acc[2] = fr_add(acc[2], fr_mul_f64(f2, w2));
   }
-  block_sum<3>(acc);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int k = 0; k < 3; k++) fr_store(part, (size_t)blockIdx.x * 3 + k, acc[k]);
+  block_finish<3>(acc, ro);
 }
 
 // tables[j][x] = scale_j * prod_i (bit i of x, top first ? p_j[i] : 1 - p_j[i])
@@ -275,11 +271,16 @@ extern "C" int pkg_poly_eval_many(const uint64_t* coeffs, size_t n, const uint64
   cudaStream_t s = as_stream(stream);
   const int g = red_grid(n);
   const size_t G = (size_t)g * kRedThreads;
-  Scratch scr;
-  int rc = scr.alloc(32 * ((size_t)g + npts), s);
+  // up to kFusedSlotFr points: each launch writes its value to the thread's
+  // fused slots; more points: partials, one summing launch per point
+  FusedSlots fs;
+  int rc = fused_slots(&fs);
   if (rc) return rc;
+  const bool fused = npts <= kFusedSlotFr;
+  Scratch scr;
+  if ((rc = scr.alloc(32 * ((size_t)g + (fused ? 0 : npts)), s))) return rc;
   uint64_t* part = static_cast<uint64_t*>(scr.ptr);
-  uint64_t* d_out = part + 4 * (size_t)g;
+  uint64_t* d_out = fused ? fs.dev : part + 4 * (size_t)g;
   for (size_t j = 0; j < npts; j++) {
     const HostFr z = HostFr::from_limbs(points + 4 * j);
     FrParams<33> P;
@@ -289,12 +290,15 @@ extern "C" int pkg_poly_eval_many(const uint64_t* coeffs, size_t n, const uint64
       put_param(P, 1 + b, sq);
       sq = HostFr::mul(sq, sq);
     }
-    poly_eval_kernel<<<g, kRedThreads, 0, s>>>(coeffs, n, P, part);
+    const RedOut ro = {part, fused ? fs.ticket : nullptr, fused ? d_out + 4 * j : nullptr};
+    poly_eval_kernel<<<g, kRedThreads, 0, s>>>(coeffs, n, P, ro);
     PK_CHECK_LAUNCH("poly_eval_kernel");
-    sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, g, d_out + 4 * j);
-    PK_CHECK_LAUNCH("sum_partials_kernel");
+    if (!fused) {
+      sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, g, d_out + 4 * j);
+      PK_CHECK_LAUNCH("sum_partials_kernel");
+    }
   }
-  return read_small(out, d_out, 32 * npts, s);
+  return fused ? fused_read(out, fs, 32 * npts, s) : read_small(out, d_out, 32 * npts, s);
 }
 
 extern "C" int pkg_merkle_open(const uint8_t* layers, size_t num_leaves, const uint64_t* indices,
@@ -402,22 +406,22 @@ extern "C" int pkg_whir_sumcheck_round(uint64_t* f, uint64_t* w, size_t size, co
   cudaStream_t s = as_stream(stream);
   const size_t q = fold ? size / 4 : size / 2;
   const int g = red_grid(q);
-  Scratch scr;
-  int rc = scr.alloc(32 * (3 * (size_t)g + 3), s);
+  FusedSlots fs;
+  int rc = fused_slots(&fs);
   if (rc) return rc;
+  Scratch scr;
+  if ((rc = scr.alloc(32 * 3 * (size_t)g, s))) return rc;
   uint64_t* part = static_cast<uint64_t*>(scr.ptr);
-  uint64_t* d_out = part + 12 * (size_t)g;
   FrParams<1> A;
   memset(&A, 0, sizeof A);
   if (fold) memcpy(A.v[0], fold, 32);
+  const RedOut ro = {part, fs.ticket, fs.dev};
   if (fold)
-    whir_round_kernel<true><<<g, kRedThreads, 0, s>>>(f, w, q, A, part);
+    whir_round_kernel<true><<<g, kRedThreads, 0, s>>>(f, w, q, A, ro);
   else
-    whir_round_kernel<false><<<g, kRedThreads, 0, s>>>(f, w, q, A, part);
+    whir_round_kernel<false><<<g, kRedThreads, 0, s>>>(f, w, q, A, ro);
   PK_CHECK_LAUNCH("whir_round_kernel");
-  sum_partials_kernel<3><<<1, kRedThreads, 0, s>>>(part, g, d_out);
-  PK_CHECK_LAUNCH("sum_partials_kernel");
-  return read_small(out, d_out, 96, s);
+  return fused_read(out, fs, 96, s);
 }
 
 namespace pk {
