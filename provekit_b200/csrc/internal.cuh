@@ -14,8 +14,9 @@ int merkle_tree_fr_device(const uint64_t* cw, size_t fr_per_leaf, size_t num_lea
 int spmv_device(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
                 size_t num_rows, size_t num_cols, const uint64_t* x, uint64_t* y, uint32_t* err,
                 cudaStream_t s);
+// eq(r, .) over the first num_entries points; sync: wait for the copy of r
 int eq_hypercube_device(const uint64_t* r_host, size_t nr, size_t num_entries, uint64_t* out,
-                        cudaStream_t s);
+                        cudaStream_t s, bool sync = true);
 // Skyscraper PoW on stream s (synchronous): generic::solve's answer.
 int pow_solve_device(const uint64_t challenge[4], const uint64_t threshold[4], cudaStream_t s,
                      uint64_t* nonce_out);
@@ -26,9 +27,11 @@ int pow_solve_device(const uint64_t challenge[4], const uint64_t threshold[4], c
 int eq_accumulate_device(uint64_t* w, size_t nv, const uint64_t* points, const uint64_t* coeffs,
                          size_t npts, cudaStream_t s, bool sync, bool expanded = true);
 // Codeword rows and their Merkle paths for nq indices (host in/out), one sync.
+// sync = false: rows and paths are pinned host memory that the copies fill
+// in stream order, and the caller synchronises before reading them.
 int open_rows_device(const uint64_t* codeword, size_t fr_per_row, size_t num_rows,
                      const uint8_t* layers, const uint64_t* indices, size_t nq, uint64_t* rows,
-                     uint8_t* paths, cudaStream_t s);
+                     uint8_t* paths, cudaStream_t s, bool sync = true);
 // <a, b> to d_out; part: red_grid(n) Fr of scratch.  With a ticket (the
 // thread's fused slots) one launch writes d_out.
 int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* d_out, uint64_t* part,

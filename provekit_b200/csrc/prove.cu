@@ -195,7 +195,8 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   uint64_t* eq = static_cast<uint64_t*>(s_eq.ptr);
   uint64_t* cov = static_cast<uint64_t*>(s_alph.ptr);
   if (whir) PK_CUDA(cudaMemsetAsync(cov, 0, 32 * nstm * n, s));
-  if ((rc = eq_hypercube_device(&out->alpha[0][0], m0, nc, eq, s))) return rc;
+  // out->alpha stays valid and unchanged until the evaluations' read below
+  if ((rc = eq_hypercube_device(&out->alpha[0][0], m0, nc, eq, s, false))) return rc;
   // public weights (get_public_weights, whir_r1cs.rs:665-676): the hash of
   // the public inputs (PublicInputs::hash, common/src/witness/mod.rs:86-97)
   // into the transcript, then the challenge x

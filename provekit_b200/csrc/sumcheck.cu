@@ -176,7 +176,7 @@ int spartan_round_device(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t* eq, si
 }
 
 int eq_hypercube_device(const uint64_t* r_host, size_t nr, size_t num_entries, uint64_t* out,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool sync) {
   if (num_entries == 0) return PKG_OK;
   PK_REQUIRE(nr < 40 && num_entries <= (size_t(1) << nr), "num_entries %zu exceeds 2^%zu",
              num_entries, nr);
@@ -202,8 +202,9 @@ int eq_hypercube_device(const uint64_t* r_host, size_t nr, size_t num_entries, u
   PK_CHECK_LAUNCH("eq_small_kernel");
   eq_combine_kernel<<<ew_grid(num_entries), 256, 0, s>>>(d_hi, d_lo, nlo, num_entries, out);
   PK_CHECK_LAUNCH("eq_combine_kernel");
-  // the host copy of r above must outlive the async copy
-  PK_CUDA(cudaStreamSynchronize(s));
+  // a pinned r must outlive the async copy: callers whose r stays valid
+  // until their next synchronisation pass sync = false
+  if (sync) PK_CUDA(cudaStreamSynchronize(s));
   return PKG_OK;
 }
 
@@ -379,7 +380,7 @@ extern "C" int pkg_spartan_round(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t
 
 extern "C" int pkg_eq_hypercube(const uint64_t* r, size_t nr, size_t num_entries, uint64_t* out,
                                 pkg_stream_t stream) {
-  return eq_hypercube_device(r, nr, num_entries, out, as_stream(stream));
+  return eq_hypercube_device(r, nr, num_entries, out, as_stream(stream), true);
 }
 
 extern "C" int pkg_spmv_csr(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
@@ -508,7 +509,7 @@ extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_
   if ((rc = scr.alloc(32 * (n + 3 * (size_t)gmax), s))) return rc;
   uint64_t* eq = static_cast<uint64_t*>(scr.ptr);
   uint64_t* part = eq + 4 * n;
-  rc = eq_hypercube_device(r_out, m0, n, eq, s);  // :530
+  rc = eq_hypercube_device(r_out, m0, n, eq, s, false);  // :530; the rounds synchronise
   if (rc) return rc;
   HostFr g0[4];
   blinding_coeffs(gv.data(), m0, 0, nullptr, g0);  // sum_over_hypercube, :494-501

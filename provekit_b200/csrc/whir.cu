@@ -353,7 +353,7 @@ namespace pk {
 // one synchronisation.
 int open_rows_device(const uint64_t* codeword, size_t fr_per_row, size_t num_rows,
                      const uint8_t* layers, const uint64_t* indices, size_t nq, uint64_t* rows,
-                     uint8_t* paths, cudaStream_t s) {
+                     uint8_t* paths, cudaStream_t s, bool sync) {
   if (nq == 0) return PKG_OK;
   const int depth = log2_exact(num_rows);
   for (size_t q = 0; q < nq; q++)
@@ -375,6 +375,12 @@ int open_rows_device(const uint64_t* codeword, size_t fr_per_row, size_t num_row
     merkle_open_kernel<<<ew_grid(nq * depth), 256, 0, s>>>(layers, num_rows, depth, d_idx, nq,
                                                            d_paths);
     PK_CHECK_LAUNCH("merkle_open_kernel");
+  }
+  if (!sync) {
+    PK_CUDA(cudaMemcpyAsync(rows, d_rows, 32 * nq * fr_per_row, cudaMemcpyDeviceToHost, s));
+    if (depth)
+      PK_CUDA(cudaMemcpyAsync(paths, d_paths, 32 * nq * (size_t)depth, cudaMemcpyDeviceToHost, s));
+    return PKG_OK;
   }
   const HostRead reads[2] = {{rows, d_rows, 32 * nq * fr_per_row},
                              {paths, d_paths, depth ? 32 * nq * (size_t)depth : 0}};

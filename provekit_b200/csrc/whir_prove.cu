@@ -222,6 +222,39 @@ struct PhaseTimer {
     if (_rc) return _rc;      \
   } while (0)
 
+// Pinned staging for one proof's STIR openings.  Openings feed no transcript
+// value, so their copies run behind the proof's later steps and are moved
+// into the proof after its last synchronisation.  One buffer per host thread
+// and device (grow-only); the event marks the last copy into it, so a proof
+// that ended early cannot leave copies landing in the next one's openings.
+struct OpeningStage {
+  uint8_t* buf = nullptr;
+  size_t cap = 0;
+  cudaEvent_t copied = nullptr;
+};
+
+static int opening_stage(size_t bytes, OpeningStage** out) {
+  constexpr int kMaxDevices = 64;
+  thread_local OpeningStage stages[kMaxDevices];
+  int device = 0;
+  PK_CUDA(cudaGetDevice(&device));
+  PK_REQUIRE(device >= 0 && device < kMaxDevices, "device ordinal %d out of range", device);
+  OpeningStage& st = stages[device];
+  if (!st.copied) PK_CUDA(cudaEventCreateWithFlags(&st.copied, cudaEventDisableTiming));
+  PK_CUDA(cudaEventSynchronize(st.copied));
+  if (bytes > st.cap) {
+    if (st.buf) cudaFreeHost(st.buf);
+    st.buf = nullptr;
+    st.cap = 0;
+    void* p = nullptr;
+    PK_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocPortable));
+    st.buf = static_cast<uint8_t*>(p);
+    st.cap = bytes;
+  }
+  *out = &st;
+  return PKG_OK;
+}
+
 class WhirProver {
  public:
   WhirProver(const pkg_whir_params* p, pkg_transcript* t, cudaStream_t s, uint64_t* proof)
@@ -249,6 +282,13 @@ class WhirProver {
   cudaStream_t s_;
   uint64_t* out_;
   size_t pos_ = 0;
+  // STIR openings: staged copies and where each lands in the proof
+  struct Placement {
+    size_t word, src, bytes;
+  };
+  OpeningStage* stage_ = nullptr;
+  size_t stage_off_ = 0;
+  std::vector<Placement> place_;
   uint64_t* E_ = nullptr;  // f^ table (live size size_)
   uint64_t* w_ = nullptr;  // weight table
   size_t size_ = 0;
@@ -299,7 +339,8 @@ int WhirProver::pow_step(unsigned bits) {
 }
 
 // getStirChallenges (circuit/whir_utilities.go:49-78) on a codeword of L
-// rows, then each queried row and its authentication path into the proof.
+// rows, then each queried row and its authentication path into the proof
+// (copied into the staging buffer now, placed at the end of the proof).
 int WhirProver::stir_step(size_t q, size_t L, size_t K, const uint64_t* cw, const uint8_t* layers,
                           std::vector<uint64_t>& idx) {
   // K: Fr per row (the batch's width for the first codeword)
@@ -309,15 +350,21 @@ int WhirProver::stir_step(size_t q, size_t L, size_t K, const uint64_t* cw, cons
   PK_TRY(pkg_transcript_squeeze_bytes(t_, bytes.data(), q * nb));
   idx.assign(q, 0);
   PK_TRY(pkg_stir_indices(bytes.data(), L, q, idx.data()));
-  std::vector<uint64_t> rows(q * K * 4);
-  std::vector<uint8_t> paths(q * (size_t)depth * 32 + 1);
-  PK_TRY(open_rows_device(cw, K, L, layers, idx.data(), q, rows.data(), paths.data(), s_));
+  const size_t row_bytes = 32 * K, path_bytes = 32 * (size_t)depth;
+  PK_REQUIRE(stage_off_ + q * (row_bytes + path_bytes) <= stage_->cap,
+             "opening staging too small");
+  uint8_t* rows = stage_->buf + stage_off_;
+  uint8_t* paths = rows + q * row_bytes;
+  PK_TRY(open_rows_device(cw, K, L, layers, idx.data(), q, reinterpret_cast<uint64_t*>(rows),
+                          paths, s_, false));
+  PK_CUDA(cudaEventRecord(stage_->copied, s_));
   for (size_t i = 0; i < q; i++) {
-    memcpy(out_ + pos_, rows.data() + i * K * 4, 32 * K);
+    place_.push_back({pos_, stage_off_ + i * row_bytes, row_bytes});
     pos_ += 4 * K;
-    memcpy(out_ + pos_, paths.data() + i * (size_t)depth * 32, 32 * (size_t)depth);
+    place_.push_back({pos_, stage_off_ + q * row_bytes + i * path_bytes, path_bytes});
     pos_ += 4 * (size_t)depth;
   }
+  stage_off_ += q * (row_bytes + path_bytes);
   return PKG_OK;
 }
 
@@ -338,6 +385,15 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
   const unsigned o = p_->ood_samples;
   const size_t N = size_t(1) << n, K = size_t(1) << k;
   const pkg_stream_t ps = reinterpret_cast<pkg_stream_t>(s_);
+  {
+    // every round's openings: rows of row_fr Fr and paths of rows_log digests
+    size_t stage_bytes = 32;
+    for (unsigned r = 0; r <= R; r++)
+      stage_bytes += (size_t)p_->queries[r] * 32 * (row_fr(p_, r) + rows_log(p_, r));
+    PK_TRY(opening_stage(stage_bytes, &stage_));
+    stage_off_ = 0;
+    place_.clear();
+  }
 
   PoolBuf E, W, A, B, Cb, cw_own, lay_own, cw_next, lay_next;
   const unsigned nb = p_->batch_size;
@@ -519,6 +575,8 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
     PK_TRY(sumcheck_phase(nv, rfin));
     PK_CUDA(cudaStreamSynchronize(s_));
   }
+  // the staged openings into their places
+  for (const Placement& pl : place_) memcpy(out_ + pl.word, stage_->buf + pl.src, pl.bytes);
   return PKG_OK;
 }
 
