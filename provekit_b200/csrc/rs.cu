@@ -9,6 +9,7 @@
 // pipeline of ntt.cu.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "fr.cuh"
@@ -106,6 +107,36 @@ int rs_encode_device(const uint64_t* messages, size_t num_messages, size_t messa
   return PKG_OK;
 }
 
+// Powers of the order-2^bits root g, split at lo = bits / 2: lo[j] = g^j
+// (j < 2^lo) and hi[j] = g^(j 2^lo) (j < 2^(bits - lo)), so g^k is one
+// product.  Built once per order on first use (2^lo + 2^(bits - lo)
+// products) and kept: every proof opens the same few codeword lengths.
+struct PowerTables {
+  int lo_bits = 0;
+  std::vector<HostFr> lo, hi;
+};
+
+static const PowerTables& power_tables(int bits) {
+  static std::mutex mu;
+  static PowerTables tables[29];
+  static bool built[29] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  PowerTables& t = tables[bits];
+  if (!built[bits]) {
+    const HostFr g = HostFr::root_of_unity(uint64_t(1) << bits);
+    t.lo_bits = bits / 2;
+    t.lo.resize(size_t(1) << t.lo_bits);
+    t.hi.resize(size_t(1) << (bits - t.lo_bits));
+    t.lo[0] = HostFr::one();
+    for (size_t j = 1; j < t.lo.size(); j++) t.lo[j] = HostFr::mul(t.lo[j - 1], g);
+    const HostFr step = HostFr::mul(t.lo.back(), g);  // g^(2^lo)
+    t.hi[0] = HostFr::one();
+    for (size_t j = 1; j < t.hi.size(); j++) t.hi[j] = HostFr::mul(t.hi[j - 1], step);
+    built[bits] = true;
+  }
+  return t;
+}
+
 }  // namespace pk
 
 using namespace pk;
@@ -136,25 +167,18 @@ extern "C" int pkg_rs_evaluation_points(size_t codeword_length, const size_t* in
   PK_REQUIRE(codeword_length >= 1, "codeword_length must be >= 1");
   PK_REQUIRE(is_pow2(codeword_length) && codeword_length <= (size_t(1) << 28),
              "no root of unity of order %zu", codeword_length);
-  int bits = log2_exact(codeword_length);
-  HostFr g = HostFr::root_of_unity(codeword_length);
-  // g^(2^b) for b < bits: a point is then at most `bits` products
-  HostFr sq[64];
-  sq[0] = g;
-  for (int b = 1; b < bits; b++) sq[b] = HostFr::mul(sq[b - 1], sq[b - 1]);
+  const int bits = log2_exact(codeword_length);
+  const PowerTables& t = power_tables(bits);
+  const size_t lo_mask = (size_t(1) << t.lo_bits) - 1;
   for (size_t x = 0; x < n; x++) {
-    size_t i = indices[x];
-    size_t k = i;
-    if (bits) {  // i.reverse_bits() >> (usize::BITS - bits)
+    const size_t i = indices[x];
+    size_t k = 0;  // bits = 0: g = 1, every power is 1
+    if (bits) {    // i.reverse_bits() >> (usize::BITS - bits)
       size_t r = 0;
       for (int b = 0; b < 64; b++) r |= ((i >> b) & 1) << (63 - b);
       k = r >> (64 - bits);
-    } else {
-      k = 0;  // g = 1: every power is 1
     }
-    HostFr v = HostFr::one();
-    for (int b = 0; b < bits; b++)
-      if ((k >> b) & 1) v = HostFr::mul(v, sq[b]);
+    const HostFr v = HostFr::mul(t.lo[k & lo_mask], t.hi[k >> t.lo_bits]);
     memcpy(out + 4 * x, v.l, 32);
   }
   return PKG_OK;

@@ -275,6 +275,25 @@ static const HostFr& half_mont() {
   return h;
 }
 
+// g_i(0) + g_i(1) of one blinding cubic
+static HostFr cubic_sum01(const HostFr* c) {
+  return HostFr::add(eval_cubic(c, HostFr::zero()), eval_cubic(c, HostFr::one()));
+}
+
+// The coefficients of compute_blinding_coefficients_for_round for
+// cf < n from its two sums: prefix = sum_{i < cf} g_i(alpha_i), suffix =
+// sum_{i > cf} (g_i(0) + g_i(1)).
+static void blinding_from_sums(const HostFr* g, size_t n, size_t cf, const HostFr& prefix,
+                               const HostFr& suffix, HostFr res[4]) {
+  HostFr pm = HostFr::one();
+  for (size_t i = 0; i < n - 1 - cf; i++) pm = HostFr::add(pm, pm);
+  HostFr sm = HostFr::mul(pm, half_mont());
+  HostFr cst = HostFr::add(HostFr::mul(pm, prefix), HostFr::mul(sm, suffix));
+  const HostFr* cur = g + 4 * cf;
+  res[0] = HostFr::add(HostFr::mul(pm, cur[0]), cst);
+  for (int k = 1; k < 4; k++) res[k] = HostFr::mul(pm, cur[k]);
+}
+
 // compute_blinding_coefficients_for_round (whir_r1cs.rs:427-492)
 static void blinding_coeffs(const HostFr* g, size_t n, size_t compute_for, const HostFr* alphas,
                             HostFr out[4]) {
@@ -286,9 +305,11 @@ static void blinding_coeffs(const HostFr* g, size_t n, size_t compute_for, const
   }
   HostFr prefix = HostFr::zero(), suffix = HostFr::zero();
   for (size_t i = 0; i < cf; i++) prefix = HostFr::add(prefix, eval_cubic(g + 4 * i, alphas[i]));
-  for (size_t i = cf + 1; i < n; i++)
-    suffix = HostFr::add(suffix, HostFr::add(eval_cubic(g + 4 * i, HostFr::zero()),
-                                             eval_cubic(g + 4 * i, HostFr::one())));
+  for (size_t i = cf + 1; i < n; i++) suffix = HostFr::add(suffix, cubic_sum01(g + 4 * i));
+  if (!all_fixed) {
+    blinding_from_sums(g, n, cf, prefix, suffix, out);
+    return;
+  }
   HostFr pm = HostFr::one();
   for (size_t i = 0; i < n - 1 - cf; i++) pm = HostFr::add(pm, pm);
   HostFr sm = HostFr::mul(pm, half_mont());
@@ -522,6 +543,9 @@ extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_
   const HostFr half = half_mont();
   size_t size = n;
   uint64_t h[12];
+  // the blinding coefficients' two sums, kept as running sums over the rounds
+  HostFr bprefix = HostFr::zero(), bsuffix = HostFr::zero();
+  for (size_t i = 1; i < m0; i++) bsuffix = HostFr::add(bsuffix, cubic_sum01(&gv[4 * i]));
   for (size_t idx = 0; idx < m0; idx++) {  // :550-610
     rc = spartan_round_device(a, b, c, eq, size, idx ? alpha[idx - 1].l : nullptr, part, fs.dev, s,
                               fs.ticket);
@@ -529,7 +553,11 @@ extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_
     if ((rc = fused_read(h, fs, 96, s))) return rc;
     if (idx) size /= 2;
     HostFr gp[4];
-    blinding_coeffs(gv.data(), m0, idx, alpha.data(), gp);
+    if (idx) {
+      bprefix = HostFr::add(bprefix, eval_cubic(&gv[4 * (idx - 1)], alpha[idx - 1]));
+      bsuffix = HostFr::sub(bsuffix, cubic_sum01(&gv[4 * idx]));
+    }
+    blinding_from_sums(gv.data(), m0, idx, bprefix, bsuffix, gp);
     HostFr h0 = HostFr::from_limbs(h), hem1 = HostFr::from_limbs(h + 4),
            hinf = HostFr::from_limbs(h + 8);
     HostFr cf[4];

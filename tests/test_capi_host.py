@@ -55,8 +55,10 @@ def test_rs_host_helpers_match_oracle(L):
     for n in (1, 2, 1024, 1 << 20, 1 << 28):
         g = rs.generator(n)
         assert unpack(g.reshape(1, 4))[0] == root_of_unity(n)
-    for cw in (1, 2, 16, 64):
-        idx = list(range(cw)) + [cw + 3]
+    rng = np.random.default_rng(5)
+    for cw in (1, 2, 16, 64, 1 << 19, 1 << 20, 1 << 23, 1 << 28):
+        idx = list(range(min(cw, 64))) + [cw + 3, cw - 1]
+        idx += [int(x) for x in rng.integers(0, cw, 40)]
         got = rs.evaluation_points(0, cw, idx)
         exp = np.zeros((len(idx), 4), np.uint64)
         arr = (ctypes.c_size_t * len(idx))(*idx)
