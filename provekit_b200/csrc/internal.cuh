@@ -32,10 +32,10 @@ int eq_accumulate_device(uint64_t* w, size_t nv, const uint64_t* points, const u
 int open_rows_device(const uint64_t* codeword, size_t fr_per_row, size_t num_rows,
                      const uint8_t* layers, const uint64_t* indices, size_t nq, uint64_t* rows,
                      uint8_t* paths, cudaStream_t s, bool sync = true);
-// <a, b> to d_out; part: red_grid(n) Fr of scratch.  With a ticket (the
-// thread's fused slots) one launch writes d_out.
-int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* d_out, uint64_t* part,
-               cudaStream_t s, unsigned* ticket = nullptr);
+// <a, b> to out, a slot of the thread's fused slots (FusedSlots: out within
+// dev, ticket its ticket), in one launch; part: red_grid(n) Fr of scratch.
+int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* out, uint64_t* part,
+               cudaStream_t s, unsigned* ticket);
 
 // The WHIR prover's round loop (pkg_whir_prove); values (host, ncov Fr) are
 // the statements' values when the caller already has them, else nullptr;

@@ -145,18 +145,18 @@ __global__ void widen_kernel(const uint32_t* __restrict__ in, size_t n, unsigned
 }
 
 
-// One Spartan round on device tables; writes 3 Fr (f0, f(-1), f(inf)) to
-// d_out.  part: >= red_grid(q) * 3 Fr of scratch.  With a ticket (the
-// thread's fused slots) the round kernel writes d_out itself.
+// One Spartan round on device tables; the round kernel writes 3 Fr (f0,
+// f(-1), f(inf)) to out (the thread's fused slots, whose ticket it takes).
+// part: >= red_grid(q) * 3 Fr of scratch.
 int spartan_round_device(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t* eq, size_t size,
-                         const uint64_t* fold_host, uint64_t* part, uint64_t* d_out,
+                         const uint64_t* fold_host, uint64_t* part, uint64_t* out,
                          cudaStream_t s, unsigned* ticket) {
   Tables4 tabs = {{a, b, c, eq}};
   Fr f;
   memset(&f, 0, sizeof f);
   size_t q;
   int g;
-  const RedOut ro = {part, ticket, ticket ? d_out : nullptr};
+  const RedOut ro = {part, ticket, out};
   if (fold_host) {
     memcpy(f.v, fold_host, 32);
     q = size / 4;
@@ -168,10 +168,6 @@ int spartan_round_device(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t* eq, si
     spartan_round_kernel<false><<<g, kRedThreads, 0, s>>>(tabs, q, f, ro);
   }
   PK_CHECK_LAUNCH("spartan_round_kernel");
-  if (!ticket) {
-    sum_partials_kernel<3><<<1, kRedThreads, 0, s>>>(part, g, d_out);
-    PK_CHECK_LAUNCH("sum_partials_kernel");
-  }
   return PKG_OK;
 }
 
@@ -232,15 +228,11 @@ static int read_err_flag(uint32_t* d_err, cudaStream_t s, const char* what) {
   return PKG_OK;
 }
 
-int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* d_out, uint64_t* part,
+int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* out, uint64_t* part,
                cudaStream_t s, unsigned* ticket) {
-  int g = red_grid(n);
-  dot_kernel<<<g, kRedThreads, 0, s>>>(a, b, n, RedOut{part, ticket, ticket ? d_out : nullptr});
+  PK_REQUIRE(ticket && out, "dot_device needs the thread's fused slots");
+  dot_kernel<<<red_grid(n), kRedThreads, 0, s>>>(a, b, n, RedOut{part, ticket, out});
   PK_CHECK_LAUNCH("dot_kernel");
-  if (!ticket) {
-    sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, g, d_out);
-    PK_CHECK_LAUNCH("sum_partials_kernel");
-  }
   return PKG_OK;
 }
 

@@ -73,6 +73,16 @@ def test_poly_eval_matches_oracle(n):
         assert np.array_equal(got[j], O.poly_eval(c, pts[j]))
 
 
+def test_poly_eval_of_more_points_than_fused_slots():
+    """70 points (above the 64 fused result slots): the partials path."""
+    from provekit_b200.whir import poly_eval_many
+    c = O.sample_fr(77, 1000)
+    pts = O.sample_fr(78, 70)
+    got = poly_eval_many(dev(c), pts)
+    for j in range(70):
+        assert np.array_equal(got[j], O.poly_eval(c, pts[j]))
+
+
 def test_merkle_openings_of_the_commit_verify():
     from provekit_b200._lib import PKG_LEAF_CANONICAL
     from provekit_b200.merkle import whir_commit
