@@ -84,6 +84,7 @@ struct FusedSlots {
   uint64_t* host;    // the buffer, as the host reads it
   uint64_t* dev;     // the same buffer, as kernels write it
   unsigned* ticket;  // zero between launches
+  uint64_t* part;    // device partials: 3 Fr for each of up to 4 CTAs per SM
 };
 constexpr size_t kFusedSlotFr = 64;
 int fused_slots(FusedSlots* f);

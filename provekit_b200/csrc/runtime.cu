@@ -128,10 +128,11 @@ int fused_slots(FusedSlots* f) {
   PK_CUDA(cudaGetDevice(&device));
   PK_REQUIRE(device >= 0 && device < kMaxDevices, "device ordinal %d out of range", device);
   if (!tickets[device]) {
-    // zeroed on a private stream, waited for: ordered before any later launch
-    // on any stream without touching the legacy default stream
+    // the counter (zeroed on a private stream, waited for: ordered before any
+    // later launch on any stream without touching the legacy default stream)
+    // followed by the partials of one reduction launch
     void* t = nullptr;
-    PK_CUDA(cudaMalloc(&t, 256));
+    PK_CUDA(cudaMalloc(&t, 256 + 32 * 3 * 4 * (size_t)sm_count()));
     cudaStream_t z = nullptr;
     PK_CUDA(cudaStreamCreateWithFlags(&z, cudaStreamNonBlocking));
     const cudaError_t e1 = cudaMemsetAsync(t, 0, 256, z);
@@ -144,6 +145,7 @@ int fused_slots(FusedSlots* f) {
   f->host = host;
   f->dev = dev;
   f->ticket = tickets[device];
+  f->part = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(tickets[device]) + 256);
   return PKG_OK;
 }
 

@@ -379,14 +379,10 @@ extern "C" int pkg_spartan_round(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t
   PK_REQUIRE(aligned16(a) && aligned16(b) && aligned16(c) && aligned16(eq),
              "device buffers must be 16-byte aligned");
   cudaStream_t s = as_stream(stream);
-  size_t q = fold ? size / 4 : size / 2;
   FusedSlots fs;
   int rc = fused_slots(&fs);
   if (rc) return rc;
-  Scratch scr;
-  if ((rc = scr.alloc(32 * 3 * (size_t)red_grid(q), s))) return rc;
-  uint64_t* part = static_cast<uint64_t*>(scr.ptr);
-  rc = spartan_round_device(a, b, c, eq, size, fold, part, fs.dev, s, fs.ticket);
+  rc = spartan_round_device(a, b, c, eq, size, fold, fs.part, fs.dev, s, fs.ticket);
   if (rc) return rc;
   return fused_read(out, fs, 96, s);
 }
@@ -434,11 +430,7 @@ extern "C" int pkg_dot(const uint64_t* a, const uint64_t* b, size_t n, uint64_t 
   FusedSlots fs;
   int rc = fused_slots(&fs);
   if (rc) return rc;
-  Scratch scr;
-  int g = red_grid(n);
-  if ((rc = scr.alloc(32 * (size_t)g, s))) return rc;
-  uint64_t* part = static_cast<uint64_t*>(scr.ptr);
-  rc = dot_device(a, b, n, fs.dev, part, s, fs.ticket);
+  rc = dot_device(a, b, n, fs.dev, fs.part, s, fs.ticket);
   if (rc) return rc;
   return fused_read(out, fs, 32, s);
 }

@@ -278,8 +278,8 @@ extern "C" int pkg_poly_eval_many(const uint64_t* coeffs, size_t n, const uint64
   if (rc) return rc;
   const bool fused = npts <= kFusedSlotFr;
   Scratch scr;
-  if ((rc = scr.alloc(32 * ((size_t)g + (fused ? 0 : npts)), s))) return rc;
-  uint64_t* part = static_cast<uint64_t*>(scr.ptr);
+  if (!fused && (rc = scr.alloc(32 * ((size_t)g + npts), s))) return rc;
+  uint64_t* part = fused ? fs.part : static_cast<uint64_t*>(scr.ptr);
   uint64_t* d_out = fused ? fs.dev : part + 4 * (size_t)g;
   for (size_t j = 0; j < npts; j++) {
     const HostFr z = HostFr::from_limbs(points + 4 * j);
@@ -415,9 +415,7 @@ extern "C" int pkg_whir_sumcheck_round(uint64_t* f, uint64_t* w, size_t size, co
   FusedSlots fs;
   int rc = fused_slots(&fs);
   if (rc) return rc;
-  Scratch scr;
-  if ((rc = scr.alloc(32 * 3 * (size_t)g, s))) return rc;
-  uint64_t* part = static_cast<uint64_t*>(scr.ptr);
+  uint64_t* part = fs.part;  // g <= 4 CTAs per SM
   FrParams<1> A;
   memset(&A, 0, sizeof A);
   if (fold) memcpy(A.v[0], fold, 32);
