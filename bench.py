@@ -28,7 +28,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PROVE_METRIC = ("Spartan+WHIR proofs/s & p99 latency @2^20-constraint R1CS (whole proof: WHIR-ZK "
-                "commit, zk-sumcheck, covector evaluations, WHIR rounds; plain GPU; bit-exact)")
+                "commit, zk-sumcheck, covector evaluations, WHIR rounds; plain GPU; bit-exact "
+                "with the C restatement of the prover)")
 PROVE_UNIT = "proofs/s"
 METRIC = ("WHIR commit throughput, Spartan+WHIR prover hot path: 2^20 Fr coefficients -> "
           "RS rate-1/4 coset NTT -> 2^22 evaluations -> Skyscraper Merkle tree (bit-exact)")
@@ -614,7 +615,7 @@ def run_prove(a):
         for i in range(a.steps):
             flush.zero_()
             evs[i][0].record(stream)
-            _, _, proof = prove_r1cs(d, wp, stream=stream)
+            last = prove_r1cs(d, wp, stream=stream)
             evs[i][1].record(stream)
     stream.synchronize()
     torch.cuda.synchronize()
@@ -736,18 +737,31 @@ def run_prove(a):
     f64_achieved = f64_per_launch / leaf_s
 
     cpu = None
+    parity = {"result": "not checked in this run (the oracle leg runs on rank 0 at N=1 only)"}
     if not a.no_cpu_baseline and a.gpus == 1:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib as O
         owp = O.whir_params(wp.num_variables, wp.folding_factor, wp.log_inv_rate, 128, wp.pow_bits,
                             batch_size=wp.batch_size)
         t0 = time.perf_counter()
-        O.prove_r1cs(h, 1, 3, owp)
+        esp, ecw, eproof = O.prove_r1cs(h, 1, 3, owp)
         cpu_s = time.perf_counter() - t0
         cpu = {"value": 1.0 / cpu_s, "unit": PROVE_UNIT, "cores": O.lib().pko_num_threads(),
                "kind": "port",
                "sample": "one whole proof of the same 2^20-constraint instance on the host (C "
                          "restatement, OpenMP); not the reference binary (no Rust toolchain)"}
+        # the last timed proof (blinding seed 1, domain 3) against the
+        # oracle's proof of the same instance, field by field and word by word
+        gsp, gcw, gproof = last
+        same = (all(np.array_equal(gsp[k], esp[k]) if isinstance(gsp[k], np.ndarray)
+                    else gsp[k] == esp[k] for k in esp)
+                and np.array_equal(gcw, ecw) and np.array_equal(gproof, eproof))
+        parity = {"result": "bit-exact" if same else "MISMATCH",
+                  "against": "the oracle's whole proof of the same instance and seeds (C "
+                             "restatement; whir's and spongefish's own bytes cannot be built "
+                             "here, so this is equality with the restatement)",
+                  "words": int(gproof.shape[0] + gcw.shape[0])}
+    proof = last[2]
     proof_bytes = 8 * proof.shape[0]
     line = {"metric": PROVE_METRIC,
             "value": a.gpus * a.steps / (total_max * 1e-3), "unit": PROVE_UNIT,
@@ -756,7 +770,9 @@ def run_prove(a):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32/f64 (BN254 Fr: 8x32-bit limbs, products on the FP64 pipe)",
             "data": "synthetic R1CS (pkg_synthetic_r1cs, seeded)",
-            "config": dict(prove_config(a, h, wp, proof_bytes), host_generation_s=gen_s),
+            "config": prove_config(a, h, wp, proof_bytes),
+            "host_generation_s": gen_s,
+            "parity": parity,
             "latency_ms": {"p50": p50_max, "p99": p99_max,
                            "note": "per-proof device time, worst rank"},
             "roofline": {
@@ -802,26 +818,29 @@ def run_prove(a):
 def run_reference_prove(a):
     """The CPU arm: the oracle restatement's whole proof on the same
     instance (the reference is Rust and cannot be built here), OpenMP over
-    all host threads; rank 0 only."""
+    all host threads; rank 0 only.  Nothing of the CUDA library is loaded:
+    the instance comes from the oracle's own generator (pko_synthetic_r1cs,
+    equal entry for entry to the library's, tests/test_capi_host.py)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
-    from provekit_b200.prover import HostR1CS, r1cs_sizing
 
-    h = HostR1CS(a.seed, PROVE_NC, PROVE_NI)
-    m, _ = r1cs_sizing(h.num_constraints, h.num_witnesses)
+    t0 = time.perf_counter()
+    h = O.SyntheticR1CS(a.seed, PROVE_NC, PROVE_NI)
+    gen_s = time.perf_counter() - t0
+    m, _ = O.r1cs_sizing(h.num_constraints, h.num_witnesses)
     wp = O.whir_params(m, 3, 2, 128, 10, batch_size=2)  # whir-ZK, as the default line
     t0 = time.perf_counter()
-    O.prove_r1cs(h, 1, 3, wp)
+    _, _, full_proof = O.prove_r1cs(h, 1, 3, wp)
     t_full = time.perf_counter() - t0
     # keep the whole run within a few minutes: smaller instances of the same
     # shape when one full proof is too slow for steps + warmup of them
     budget_s, shrink = 180.0, 0
     while t_full / (1 << shrink) * (a.steps + a.warmup) > budget_s and shrink < 6:
         shrink += 1
-    hs = h if shrink == 0 else HostR1CS(a.seed, PROVE_NC >> shrink, PROVE_NI >> shrink)
-    ms_, _ = r1cs_sizing(hs.num_constraints, hs.num_witnesses)
+    hs = h if shrink == 0 else O.SyntheticR1CS(a.seed, PROVE_NC >> shrink, PROVE_NI >> shrink)
+    ms_, _ = O.r1cs_sizing(hs.num_constraints, hs.num_witnesses)
     wps = wp if shrink == 0 else O.whir_params(ms_, 3, 2, 128, 10, batch_size=2)
     for _ in range(max(a.warmup - 1, 0)):
         O.prove_r1cs(hs, 1, 3, wps)
@@ -839,8 +858,10 @@ def run_reference_prove(a):
     line = {"impl": "reference", "metric": PROVE_METRIC, "value": value, "unit": PROVE_UNIT,
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u64 (BN254 Fr)", "data": "synthetic R1CS (pkg_synthetic_r1cs, seeded)",
-            "config": prove_config(a, h, wp),
+            "dtype": "u64 (BN254 Fr)",
+            "data": "synthetic R1CS (seeded; the oracle's generator, equal to pkg_synthetic_r1cs)",
+            "config": prove_config(a, h, wp, 8 * full_proof.shape[0]),
+            "host_generation_s": gen_s,
             "cpu_baseline": {"value": value, "unit": PROVE_UNIT, "cores": cores, "kind": "port",
                              "sample": sample + "; C restatement of the whole prover (Spartan "
                                        "zk-sumcheck + WHIR rounds), OpenMP, not the reference "

@@ -514,7 +514,7 @@ static void bar(uint64_t x[4]) {
  * compression depends only on its value mod p. */
 static inline void msq(uint64_t r[4], const uint64_t x[4]) { pko_fr_mul(r, x, x); }
 
-/* generic::compress (skyscraper/core/src/generic.rs:137-161). */
+/* generic::compress (skyscraper/core/src/generic.rs:77-102). */
 void pko_sky_compress(uint64_t out[4], const uint64_t lin[4], const uint64_t rin[4]) {
     static const int is_bar[18] = {0, 0, 0, 0, 0, 0, 1, 1, 0, 0, 1, 1, 0, 0, 0, 0, 0, 0};
     uint64_t l[4], r[4], t[4], f[4], nl[4];
@@ -973,6 +973,71 @@ void pko_r1cs_sizing(size_t num_constraints, size_t num_witnesses, size_t *m_out
     if (((size_t)1 << m) - num_witnesses < 4 * m0) m++;
     *m_out = m;
     *m0_out = m0;
+}
+
+/* splitmix64 (Steele, Lea & Flood, "Fast splittable pseudorandom number
+ * generators", OOPSLA 2014): the integer choices of the synthetic R1CS. */
+static uint64_t splitmix64_next(uint64_t *s) {
+    uint64_t z = (*s += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+static uint64_t splitmix64_below(uint64_t *s, uint64_t n) {
+    return n ? splitmix64_next(s) % n : 0;
+}
+
+int pko_synthetic_r1cs(uint64_t seed, size_t nc, size_t ni, uint64_t *row_ptr[3],
+                       uint32_t *cols[3], uint64_t *vals[3], size_t nnz_out[3],
+                       uint64_t *witness) {
+    if (ni + nc + 1 >= ((size_t)1 << 32)) return -1;
+    uint64_t rng = seed;
+    /* the row structure first: every row's two nonzero counts */
+    uint8_t *ka = malloc(nc ? nc : 1), *kb = malloc(nc ? nc : 1);
+    size_t total = 0;
+    for (size_t i = 0; i < nc; i++) {
+        ka[i] = (uint8_t)(1 + splitmix64_below(&rng, 3));
+        kb[i] = (uint8_t)(1 + splitmix64_below(&rng, 3));
+        total += (size_t)ka[i] + kb[i];
+    }
+    uint64_t *coef = malloc(32 * (total ? total : 1));
+    pko_sample_fr(seed + 1, total, coef, 1);
+    cpy4(witness, ONE_MONT);
+    pko_sample_fr(seed, ni, witness + 4, 1);
+    size_t e[2] = {0, 0}, used = 0;
+    row_ptr[0][0] = row_ptr[1][0] = row_ptr[2][0] = 0;
+    for (size_t i = 0; i < nc; i++) {
+        const uint64_t hi = ni + i + 1; /* columns in [0, ni + i] */
+        uint64_t dot[2][4];
+        for (int m = 0; m < 2; m++) {
+            const int k = m == 0 ? ka[i] : kb[i];
+            uint64_t acc[4] = {0, 0, 0, 0}, t[4];
+            for (int j = 0; j < k; j++) {
+                const uint32_t col = (uint32_t)splitmix64_below(&rng, hi);
+                cols[m][e[m]] = col;
+                cpy4(vals[m] + 4 * e[m], coef + 4 * used);
+                pko_fr_mul(t, coef + 4 * used, witness + 4 * (size_t)col);
+                pko_fr_add(acc, acc, t);
+                used++;
+                e[m]++;
+            }
+            row_ptr[m][i + 1] = e[m];
+            cpy4(dot[m], acc);
+        }
+        const size_t out_col = ni + 1 + i;
+        cols[2][i] = (uint32_t)out_col;
+        cpy4(vals[2] + 4 * i, ONE_MONT);
+        row_ptr[2][i + 1] = i + 1;
+        pko_fr_mul(witness + 4 * out_col, dot[0], dot[1]);
+    }
+    nnz_out[0] = e[0];
+    nnz_out[1] = e[1];
+    nnz_out[2] = nc;
+    free(ka);
+    free(kb);
+    free(coef);
+    return 0;
 }
 
 int pko_r1cs_covectors(const pko_r1cs *r1cs, const uint64_t *alpha, size_t m0, size_t len,

@@ -296,6 +296,19 @@ int pko_r1cs_statement_covectors(const pko_r1cs *r1cs, const uint64_t public_x[4
 void pko_public_inputs_hash(uint64_t out[4], const uint64_t *values_canonical, size_t n);
 /* WhirR1CSScheme::new_for_r1cs sizing (provekit/r1cs-compiler/src/whir_r1cs.rs:48-92). */
 void pko_r1cs_sizing(size_t num_constraints, size_t num_witnesses, size_t *m, size_t *m0);
+/* The synthetic satisfiable R1CS of the prove workload, generated on the
+ * host without the CUDA library: w[0] = 1, w[1 ..= ni] from
+ * pko_sample_fr(seed); row i: A_i and B_i hold 1-3 nonzeros (counts drawn
+ * for every row first) at uniform columns in [0, ni + i] with coefficients
+ * from pko_sample_fr(seed + 1), C_i = e_{ni+1+i}, w[ni+1+i] = <A_i,w><B_i,w>.
+ * Integer choices from splitmix64(seed).  The reference compiles its R1CS
+ * from Noir programs; this workload has no counterpart there.  Capacities as
+ * for pko_r1cs: row_ptr nc+1; cols/vals 3 nc for A and B, nc for C; witness
+ * 1 + ni + nc Fr (Montgomery form).  Returns 0, or -1 when the witness count
+ * does not fit u32 columns. */
+int pko_synthetic_r1cs(uint64_t seed, size_t nc, size_t ni, uint64_t *row_ptr[3],
+                       uint32_t *cols[3], uint64_t *vals[3], size_t nnz_out[3],
+                       uint64_t *witness);
 /* A whole proof: pko_spartan_prove with the commitment's OOD samples drawn
  * after its root and the WHIR proof of the three zero-padded covectors
  * M^T eq(alpha) against their evaluations; whir->num_variables must be the

@@ -1,5 +1,5 @@
 // skyscraper.cuh -- Skyscraper v2 two-to-one compression over BN254 Fr on the
-// device (skyscraper/core/src/generic.rs:137-161, reference.rs:41-98).
+// device (skyscraper/core/src/generic.rs:77-102, reference.rs:41-98).
 //
 // Inputs and outputs are canonical little-endian limbs (not Montgomery).
 // Every intermediate value is kept fully reduced in [0, p): the reference's

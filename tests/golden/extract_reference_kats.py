@@ -18,7 +18,7 @@ The vectors are read as text from the reference's Rust test modules:
   two-adicity, C5 = Z^((p-1)/2^28)), i.e. the 2^28-th root of unity that
   ark-bn254's ``Fr::get_root_of_unity`` raises to the NTT's order.
 
-Run from the repository root:  python tests/golden/extract_reference_kats.py
+Run from the repository root:  python tests/golden/extract_reference_kats.py <reference checkout>
 (the reference checkout is only needed to regenerate the JSON; the tests read
 the committed JSON).
 """
@@ -27,7 +27,7 @@ import os
 import re
 import sys
 
-REF = os.environ.get("PROVEKIT_REFERENCE", "/root/reference")
+REF = ""  # the reference checkout, set from the command line
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 
@@ -132,8 +132,10 @@ def root_of_unity_kats():
 
 
 def main():
-    if not os.path.isdir(REF):
-        sys.exit(f"reference checkout not found at {REF}")
+    global REF
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: extract_reference_kats.py <reference checkout directory>")
+    REF = sys.argv[1]
     kats = {"skyscraper": skyscraper_kats(), "sumcheck": sumcheck_kats(), "poseidon2": poseidon2_kats(),
             "root_of_unity": root_of_unity_kats()}
     with open(OUT, "w") as f:

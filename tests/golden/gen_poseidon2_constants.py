@@ -4,7 +4,7 @@ load_rc_partial, load_rc_full2 for t = 4), laid out as the reference's
 Poseidon2Config builds them (poseidon2/src/permutation.rs:29-65): 64 rounds x 4
 lanes, partial rounds only in lane 0.
 
-    python provekit_b200/csrc/gen_poseidon2_constants.py
+    python tests/golden/gen_poseidon2_constants.py <reference checkout>
 
 Writes provekit_b200/csrc/poseidon2_t4_constants.h and
 oracle/poseidon2_t4_constants.h (same content: canonical and Montgomery u64
@@ -14,7 +14,6 @@ import os
 import re
 import sys
 
-REF = os.environ.get("PROVEKIT_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 P = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
@@ -40,8 +39,8 @@ def limbs(x):
     return ", ".join("0x%016xULL" % ((x >> (64 * i)) & (2**64 - 1)) for i in range(4))
 
 
-def main():
-    src = open(os.path.join(REF, "poseidon2/src/constants.rs")).read()
+def main(ref):
+    src = open(os.path.join(ref, "poseidon2/src/constants.rs")).read()
     diag = hexes(arm(src, "load_diag"))
     full1 = rows(arm(src, "load_rc_full1"))
     partial = hexes(arm(src, "load_rc_partial"))
@@ -49,7 +48,7 @@ def main():
     assert len(diag) == 4 and len(full1) == 4 and len(full2) == 4 and len(partial) == 56
     rc = [r for r in full1] + [[v, 0, 0, 0] for v in partial] + [r for r in full2]
     assert len(rc) == 64 and all(len(r) == 4 for r in rc)
-    out = ["// Generated by provekit_b200/csrc/gen_poseidon2_constants.py from the reference's",
+    out = ["// Generated by tests/golden/gen_poseidon2_constants.py from the reference's",
            "// poseidon2/src/constants.rs (t = 4).  Do not edit.",
            "#pragma once", "#include <stdint.h>", ""]
     for name, conv in (("", lambda v: v), ("_MONT", lambda v: v * R % P)):
@@ -62,7 +61,7 @@ def main():
         out.append("};")
         out.append("")
     text = "\n".join(out)
-    for path in (os.path.join(HERE, "poseidon2_t4_constants.h"),
+    for path in (os.path.join(ROOT, "provekit_b200", "csrc", "poseidon2_t4_constants.h"),
                  os.path.join(ROOT, "oracle", "poseidon2_t4_constants.h")):
         with open(path, "w") as f:
             f.write(text)
@@ -70,6 +69,6 @@ def main():
 
 
 if __name__ == "__main__":
-    if not os.path.isdir(REF):
-        sys.exit(f"reference checkout not found at {REF}")
-    main()
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: gen_poseidon2_constants.py <reference checkout directory>")
+    main(sys.argv[1])

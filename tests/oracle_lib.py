@@ -60,6 +60,35 @@ def spartan_prove(h, blinding_seed, domain, ff, lr):
     return _spartan_dict(out)
 
 
+class SyntheticR1CS:
+    """The synthetic satisfiable R1CS of the prove workload, generated by the
+    oracle (pko_synthetic_r1cs) without loading the CUDA library; the same
+    attributes as provekit_b200.prover.HostR1CS."""
+
+    def __init__(self, seed: int, num_constraints: int, num_inputs: int,
+                 num_public_inputs: int = 0):
+        nc, ni = num_constraints, num_inputs
+        if num_public_inputs > ni:
+            raise ValueError("more public inputs than inputs")
+        self.num_constraints, self.num_inputs = nc, ni
+        self.num_public_inputs = num_public_inputs
+        self.num_witnesses = 1 + ni + nc
+        self.row_ptr = [np.zeros(nc + 1, np.uint64) for _ in range(3)]
+        caps = [3 * nc, 3 * nc, nc]
+        cols = [np.zeros(max(c, 1), np.uint32) for c in caps]
+        vals = [np.zeros((max(c, 1), 4), np.uint64) for c in caps]
+        self.witness = np.zeros((self.num_witnesses, 4), np.uint64)
+        nnz = (ctypes.c_size_t * 3)()
+        rp = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.row_ptr])
+        cl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in cols])
+        vl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in vals])
+        rc = lib().pko_synthetic_r1cs(seed, nc, ni, rp, cl, vl, nnz, p64(self.witness))
+        assert rc == 0, rc
+        self.nnz = list(nnz)
+        self.cols = [np.ascontiguousarray(c[:n]) for c, n in zip(cols, self.nnz)]
+        self.vals = [np.ascontiguousarray(v[:n]) for v, n in zip(vals, self.nnz)]
+
+
 def r1cs_sizing(nc, nw):
     m, m0 = ctypes.c_size_t(0), ctypes.c_size_t(0)
     lib().pko_r1cs_sizing(nc, nw, ctypes.byref(m), ctypes.byref(m0))
@@ -202,6 +231,8 @@ def lib():
         L.pko_whir_verify_commit.argtypes = [wp, tp, _u64p, _u64p]
         L.pko_whir_verify_proof.argtypes = [wp, tp, _u64p, _sz, _u64p, _u64p, _u64p, _sz]
         L.pko_r1cs_sizing.argtypes = [_sz, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]
+        L.pko_synthetic_r1cs.argtypes = [ctypes.c_uint64, _sz, _sz, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _u64p]
         L.pko_r1cs_covectors.argtypes = [ctypes.c_void_p, _u64p, _sz, _sz, _u64p]
         L.pko_r1cs_statement_covectors.argtypes = [ctypes.c_void_p, _u64p, _u64p, _sz, _sz, _sz,
                                                    _u64p]

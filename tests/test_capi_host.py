@@ -215,3 +215,35 @@ def test_prove_r1cs_validation_needs_no_device(L):
     assert L.pkg_prove_r1cs(ctypes.byref(r), w.ctypes.data + 8, 1, 2, ctypes.byref(good),
                             ctypes.byref(out), cw.ctypes.data, cw.ctypes.data,
                             None) == PKG_ERR_INVALID_ARGUMENT  # unaligned witness
+
+
+@pytest.mark.parametrize("seed,log_nc,log_ni,npub", [(1, 0, 0, 0), (3, 6, 4, 2), (7, 12, 10, 0),
+                                                     (1003, 16, 14, 5)])
+def test_synthetic_r1cs_matches_oracle_generator(L, seed, log_nc, log_ni, npub):
+    """pkg_synthetic_r1cs (the library's host-side generator of the prove
+    workload) and the oracle's pko_synthetic_r1cs produce the same matrices
+    and witness entry for entry, so a CPU arm can build the instance without
+    loading the CUDA library; the instance is satisfiable."""
+    from provekit_b200.prover import HostR1CS
+    nc, ni = 1 << log_nc, 1 << log_ni
+    got = HostR1CS(seed, nc, ni, num_public_inputs=npub)
+    exp = O.SyntheticR1CS(seed, nc, ni, num_public_inputs=npub)
+    assert got.num_witnesses == exp.num_witnesses and got.nnz == exp.nnz
+    for k in range(3):
+        assert np.array_equal(got.row_ptr[k], exp.row_ptr[k]), k
+        assert np.array_equal(got.cols[k], exp.cols[k]), k
+        assert np.array_equal(got.vals[k], exp.vals[k]), k
+    assert np.array_equal(got.witness, exp.witness)
+    # satisfiable: (A w) o (B w) == C w, checked with the oracle's SpMV
+    w = np.ascontiguousarray(exp.witness)
+    ys = []
+    for k in range(3):
+        y = np.zeros((nc, 4), np.uint64)
+        O.lib().pko_spmv(O.p64(exp.row_ptr[k]), O.p32(exp.cols[k]), O.p64(exp.vals[k]), nc,
+                         O.p64(w), O.p64(y))
+        ys.append(y)
+    for i in range(nc):
+        ab = np.zeros(4, np.uint64)
+        O.lib().pko_fr_mul(O.p64(ab), O.p64(np.ascontiguousarray(ys[0][i])),
+                           O.p64(np.ascontiguousarray(ys[1][i])))
+        assert np.array_equal(ab, ys[2][i]), i

@@ -85,18 +85,31 @@ def test_whole_proof_matches_oracle_and_verifies(log_nc, log_ni, sec, pw, zk, np
     assert O.verify_r1cs_whir(h, wp, 12, sp, cw, proof) == 0
 
 
-def test_whole_proof_at_2p20_constraints_verifies():
-    """The prove workload's instance (2^20 constraints, 2^18 inputs, m = 21)
-    with the reference's WHIR configuration: the oracle verifier accepts the
-    device proof (the oracle prover is not run at this size)."""
+def test_whole_proof_at_2p20_constraints_matches_oracle():
+    """The headline bench instance itself -- the synthetic R1CS of seed 2
+    with 2^20 constraints and 2^18 inputs (m = 21, m0 = 20), whir-ZK (batch
+    of 2), ff 3, rate 1/4, 128 bits, 10 PoW bits, blinding seed 1, domain 3:
+    the device proof equals the oracle's in every Spartan field, every
+    commitment word and every WHIR proof word, and the oracle verifier
+    accepts it."""
     from provekit_b200.prover import HostR1CS, prove_r1cs, whir_params_for
-    h = HostR1CS(3, 1 << 20, 1 << 18)
+    h = HostR1CS(2, 1 << 20, 1 << 18)
     d = h.to_device()
     p = whir_params_for(d)
     assert (p.num_variables, p.folding_factor, p.log_inv_rate, p.pow_bits, p.batch_size) == \
         (21, 3, 2, 10, 2)
     sp, cw, proof = prove_r1cs(d, p, blinding_seed=1, transcript_domain=3)
+    del d
+    torch.cuda.empty_cache()
     wp = O.whir_params(21, 3, 2, 128, 10, batch_size=2)
+    assert bytes(wp) == bytes(p)
+    esp, ecw, eproof = O.prove_r1cs(h, 1, 3, wp)
+    assert_same(sp, esp)
+    assert np.array_equal(cw, ecw)
+    assert proof.shape == eproof.shape
+    if not np.array_equal(proof, eproof):
+        first = int(np.nonzero(proof != eproof)[0][0])
+        pytest.fail(f"proofs differ first at word {first} of {proof.shape[0]}")
     assert O.verify_r1cs_whir(h, wp, 3, sp, cw, proof) == 0
 
 

@@ -83,6 +83,22 @@ def test_poly_eval_of_more_points_than_fused_slots():
         assert np.array_equal(got[j], O.poly_eval(c, pts[j]))
 
 
+def test_poly_eval_at_fused_capacity_and_full_grid():
+    """Exactly 64 points (every fused result slot) on 2^18 coefficients, so
+    each of the 64 back-to-back launches runs the largest reduction grid (4
+    CTAs per SM) and reuses the one ticket the previous launch's last CTA
+    reset: every value equals the oracle's."""
+    from provekit_b200.whir import poly_eval_many
+    n = 1 << 18
+    props = torch.cuda.get_device_properties(0)
+    assert (n + 255) // 256 >= 4 * props.multi_processor_count  # the grid is at its cap
+    c = O.sample_fr(79, n)
+    pts = O.sample_fr(80, 64)
+    got = poly_eval_many(dev(c), pts)
+    for j in range(64):
+        assert np.array_equal(got[j], O.poly_eval(c, pts[j])), j
+
+
 def test_merkle_openings_of_the_commit_verify():
     from provekit_b200._lib import PKG_LEAF_CANONICAL
     from provekit_b200.merkle import whir_commit

@@ -109,6 +109,28 @@ def test_reference_config_at_2p20_verifies():
     assert O.whir_verify(po, 77, cov, 3, words, bad) != 0
 
 
+@pytest.mark.parametrize("n,batch", [(20, 1), (21, 1), (21, 2)])
+def test_reference_config_word_for_word(n, batch):
+    """The reference's R1CS WHIR configuration (ff 3, rate 1/4, 128 bits,
+    10 PoW bits) at the whole proof's sizes -- 2^20 and 2^21 coefficients,
+    plain and as the whir-ZK batch of 2 -- with three covectors: the device
+    proof equals the oracle's word for word (a verifier accepting a proof
+    does not make it the same proof: another nonce, query or opening order
+    would verify too)."""
+    p, po = _params_pair(n, 3, 2, 128, 10, {"batch_size": batch})
+    c = O.sample_fr(6000 + n + batch, batch << n)
+    cov = O.sample_fr(7000 + n + batch, 3 << n)
+    _, _, words, proof, _ = _device_proof(p, 0x5eed + n, c, cov)
+    torch.cuda.empty_cache()
+    owords, oproof = O.whir_prove(po, 0x5eed + n, c, cov)
+    assert np.array_equal(words, owords)
+    assert proof.shape == oproof.shape
+    if not np.array_equal(proof, oproof):
+        first = int(np.nonzero(proof != oproof)[0][0])
+        pytest.fail(f"proofs differ first at word {first} of {proof.shape[0]}")
+    assert O.whir_verify(po, 0x5eed + n, cov, 3, words, proof) == 0
+
+
 @pytest.mark.parametrize("n", [1, 3, 4, 5, 8, 13, 17, 20])
 def test_subset_transforms_match_the_oracle(n):
     from provekit_b200.whir import SUBSET_MOBIUS_T, SUBSET_ZETA, subset_transform

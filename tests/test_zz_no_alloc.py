@@ -46,6 +46,35 @@ def test_noalloc_matches_allocating_entry_point_on_consecutive_calls(L):
         assert np.array_equal(got, want), f"mismatch at 2^{logn}"
 
 
+@pytest.mark.parametrize("logn", [0, 1, 2, 5, 9, 10, 16])
+def test_noalloc_small_and_edge_lengths(L, logn):
+    # Below 2^10 the allocating path uses a padded order-1024 twiddle table
+    # while this one builds a table of exactly len/2 entries (len 2: one
+    # entry, a kernel with log_half = 0); len 1 is the identity.  Compared
+    # with pkg_intt_rn and, independently, with the oracle's intt_rn.
+    x = O.sample_fr(800 + logn, 1 << logn)
+    want = _run(L, L.pkg_intt_rn, x)
+    got = _run(L, L.pkg_intt_rn_noalloc, x)
+    assert np.array_equal(got, want), f"mismatch at 2^{logn}"
+    exp = x.copy()
+    assert O.intt_rn(exp) == 0
+    assert np.array_equal(got.reshape(-1, 4), exp)
+
+
+def test_noalloc_on_a_non_default_stream(L):
+    x = O.sample_fr(901, 1 << 12)
+    want = _run(L, L.pkg_intt_rn, x)
+    s = torch.cuda.Stream()
+    d = torch.from_numpy(x.view(np.int64).copy()).cuda()
+    torch.cuda.synchronize()
+    for _ in range(2):  # the second call must not see the first one's scratch
+        d.copy_(torch.from_numpy(x.view(np.int64).copy()))
+        torch.cuda.synchronize()
+        assert L.pkg_intt_rn_noalloc(d.data_ptr(), x.shape[0], s.cuda_stream) == 0
+        s.synchronize()
+        assert np.array_equal(d.cpu().numpy().view(np.uint64), want)
+
+
 def test_noalloc_rejects_lengths_beyond_its_scratch(L):
     d = torch.zeros((1 << 17, 4), dtype=torch.int64, device="cuda")
     rc = L.pkg_intt_rn_noalloc(d.data_ptr(), 1 << 17, None)
