@@ -247,7 +247,26 @@ typedef struct {
   const uint64_t *vals[3];
   size_t nnz[3];
   size_t num_public_inputs;   /* the public inputs are witness[1 ..= this] */
+  /* Optional, all three or none: the transposes of A, B, C (num_witnesses
+   * rows: row_ptr_t num_witnesses + 1 entries, cols_t / vals_t nnz[k]
+   * entries, column indices < num_constraints), built once for a resident
+   * circuit with
+   * pkg_r1cs_build_transposes or pkg_csr_transpose
+   * (transpose_r1cs_matrices, provekit/common/src/utils/sumcheck.rs:195-206).
+   * NULL: every proof transposes the matrices itself. */
+  const uint64_t *row_ptr_t[3];
+  const uint32_t *cols_t[3];
+  const uint64_t *vals_t[3];
 } pkg_r1cs;
+
+/* Bytes of device memory the three transposes of r1cs take (row pointers,
+ * columns and values, each 256-byte aligned).  Host only. */
+size_t pkg_r1cs_transposes_bytes(const pkg_r1cs *r1cs);
+/* Builds the three transposes into buf (device, pkg_r1cs_transposes_bytes
+ * long, 256-byte aligned) and points r1cs->row_ptr_t / cols_t / vals_t into
+ * it.  Synchronous.  Out-of-range column indices are reported as
+ * PKG_ERR_INVALID_ARGUMENT. */
+int pkg_r1cs_build_transposes(pkg_r1cs *r1cs, void *buf, pkg_stream_t stream);
 
 /* Everything the prover produces before WHIR's own prove rounds. */
 typedef struct {
@@ -567,6 +586,95 @@ int pkg_prove_r1cs(const pkg_r1cs *r1cs, const uint64_t *witness, uint64_t blind
                    pkg_spartan_proof *out, uint64_t *whir_commit_words, uint64_t *whir_proof,
                    pkg_stream_t stream);
 
+/* ---- Prover handles (tooling/provekit-ffi/src/ffi.rs, types.rs) ----------
+ * The reference's FFI hands out an opaque PKProver (a prepared circuit) and
+ * returns proofs in a PKBuf that the library allocated and pk_free_buf
+ * releases.  Same conventions here, over the device prover: the handle holds
+ * the circuit resident on the device that was current at creation, with its
+ * transposes built once; a proof comes back in a pkg_buf.  Calls on one
+ * handle are serialised (one proof at a time, synchronous); different
+ * handles prove concurrently.  Statuses are this header's PKG_* codes (the
+ * reference's PKStatus values are positive: INTEGRATION.md maps them). */
+/* PKBuf (tooling/provekit-ffi/src/types.rs:8-40, include/provekit_ffi.h:14-22):
+ * library-allocated bytes, released exactly once by pkg_free_buf. */
+typedef struct {
+  uint8_t *ptr;
+  size_t len;
+  size_t cap;
+} pkg_buf;
+/* pk_free_buf (ffi.rs:744-750); an empty buffer (ptr NULL) is a no-op. */
+void pkg_free_buf(pkg_buf buf);
+/* pk_get_last_error (ffi.rs:73-89): the calling thread's last message as
+ * UTF-8 bytes (empty buffer if none), then cleared; free with pkg_free_buf. */
+int pkg_get_last_error(pkg_buf *out);
+/* pk_init (ffi.rs:92-97): checks that a CUDA device is present.  Optional
+ * (every entry point initialises what it needs on first use). */
+int pkg_init(void);
+
+typedef struct pkg_prover pkg_prover;  /* PKProver (types.rs) */
+typedef struct {
+  unsigned folding_factor;   /* WHIR folding factor (reference default 3)   */
+  unsigned log_inv_rate;     /* starting rate 2^-log_inv_rate (default 2)   */
+  unsigned security_bits;    /* default 128                                 */
+  unsigned pow_bits;         /* default 10                                  */
+  int zk;                    /* 1: whir-ZK, the witness committed with a    */
+                             /* blinding polynomial (WhirZkConfig, default) */
+  uint64_t transcript_domain;/* Fiat-Shamir domain separator               */
+} pkg_prover_config;
+/* The reference's configuration (provekit/r1cs-compiler/src/whir_r1cs.rs:94-117). */
+int pkg_prover_config_default(pkg_prover_config *cfg);
+/* A prepared prover from an R1CS in host memory (CSR A, B, C over
+ * num_witnesses columns, one Fr per nonzero, Montgomery form; witness[1 ..=
+ * num_public_inputs] are public).  Replaces pk_prepare / pk_load_prover
+ * (ffi.rs:160-265) as far as the prover goes: the reference compiles a Noir
+ * circuit or reads a .pkp file, which is outside this library (Noir
+ * compilation and the .pkp serde layout of the un-vendored whir / spongefish
+ * types).  Row pointers and column indices are validated on the host.
+ * Synchronous; the handle is freed by pkg_prover_free. */
+int pkg_prover_create(size_t num_constraints, size_t num_witnesses, size_t num_public_inputs,
+                      const uint64_t *const row_ptr[3], const uint32_t *const cols[3],
+                      const uint64_t *const vals[3], const size_t nnz[3],
+                      const pkg_prover_config *cfg, pkg_prover **out);
+/* pk_free_prover (ffi.rs:703-718); NULL is a no-op. */
+void pkg_prover_free(pkg_prover *prover);
+typedef struct {
+  size_t num_constraints, num_witnesses, num_public_inputs;
+  size_t m, m0;              /* committed and sumcheck variables            */
+  size_t num_statements;     /* WHIR statements: 4, or 5 with public inputs */
+  size_t proof_bytes;        /* length of every proof this handle returns   */
+  int device;
+  pkg_whir_params whir;
+} pkg_prover_info;
+int pkg_prover_get_info(const pkg_prover *prover, pkg_prover_info *info);
+/* A whole proof (pkg_prove_r1cs) of a solved witness: num_witnesses Fr in
+ * host memory (Montgomery form).  Replaces pk_prove_json / pk_prove_toml
+ * (ffi.rs:537-666), whose input maps go through Noir's witness solver first.
+ * out_proof receives a library-owned buffer (pkg_free_buf) in this layout,
+ * all integers little-endian:
+ *   "PKGPROOF", u32 version (1), u32 0,
+ *   u64 m, m0, num_public_inputs, num_statements, commit_words, proof_words,
+ *       transcript_domain,
+ *   the WHIR parameters as a pkg_whir_params struct: 104 bytes,
+ *   root (32 bytes), then Fr (4 u64 each): r[m0], round coefficients[4 m0],
+ *   alpha[m0], rho, sum_g, blinding_eval, public_x, evals[3], public_hash
+ *   (canonical), public_eval, the transcript state before the WHIR proof (l,
+ *   r; a verifier recomputes it),
+ *   commit_words u64 (root, OOD answers), proof_words u64 (the WHIR proof).
+ * The reference's .np layout (header + postcard + zstd over whir's and
+ * spongefish's proof types) cannot be produced without those crates. */
+int pkg_prover_prove(pkg_prover *prover, const uint64_t *witness, uint64_t blinding_seed,
+                     pkg_buf *out_proof);
+/* pk_serialize_prover / pk_load_prover_bytes (ffi.rs:329-362, 455-482) over
+ * this library's own layout: "PKGPROVR", u32 version (1), u32 0, u64
+ * num_constraints, num_witnesses, num_public_inputs, nnz[3], u32
+ * folding_factor, log_inv_rate, security_bits, pow_bits, zk, 0, u64
+ * transcript_domain, u64 0, then per matrix row_ptr (u64 x
+ * num_constraints + 1), cols (u32 x nnz, zero-padded to 8 bytes), vals (Fr x
+ * nnz).  Loading validates every size against the input length and the
+ * matrices as pkg_prover_create does. */
+int pkg_prover_serialize(const pkg_prover *prover, pkg_buf *out);
+int pkg_prover_load_bytes(const uint8_t *ptr, size_t len, pkg_prover **out);
+
 /* ---- field arithmetic (skyscraper/bn254-multiplier/src/scalar.rs:12-132,
  *      ark-ff Montgomery conversion) ---------------------------------------- */
 /* out[i] = op(a[i], b[i]) over n Fr (4 x u64 LE each, device, 16-byte
@@ -612,6 +720,19 @@ int pkg_sample_fr_indexed(uint64_t seed, uint64_t start, size_t n, uint64_t *out
  * physical mappings out of the timed work.  No counterpart in the
  * reference. */
 int pkg_reserve_memory(size_t bytes);
+
+/* A host thread that proves keeps a few small resources for its later calls:
+ * a mapped pinned buffer for reduction results (2 KiB), a pinned bounce
+ * buffer for small reads (256 KiB), and per device a ~60 KiB device block
+ * (reduction counter, partials, PoW word) and a grow-only pinned staging
+ * buffer for a proof's STIR openings (about 0.3 MB at 2^20 constraints).
+ * They are released when the thread exits; this releases the calling
+ * thread's now (they are re-created on its next call).  The thread must have
+ * no work of this library in flight.  No counterpart in the reference. */
+int pkg_release_thread_resources(void);
+/* Bytes those per-thread resources hold over all live threads: pinned host
+ * memory and device memory.  Diagnostics; no counterpart in the reference. */
+int pkg_thread_resource_bytes(size_t *host_bytes, size_t *device_bytes);
 
 /* ---- diagnostics ---------------------------------------------------------- */
 /* Synchronous device -> host copy of library-owned memory (e.g. batch buffers). */

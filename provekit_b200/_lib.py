@@ -102,7 +102,24 @@ SIGNATURES = {
     "pkg_whir_commit_ood": [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
     "pkg_whir_prove": [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_sz, _c_vp, _c_vp],
     "pkg_version": [],
+    "pkg_release_thread_resources": [],
+    "pkg_r1cs_build_transposes": [_c_vp, _c_vp, _c_vp],
+    "pkg_get_last_error": [_c_vp],
+    "pkg_init": [],
+    "pkg_prover_config_default": [_c_vp],
+    "pkg_prover_create": [_c_sz, _c_sz, _c_sz, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+    "pkg_prover_get_info": [_c_vp, _c_vp],
+    "pkg_prover_prove": [_c_vp, _c_vp, ctypes.c_uint64, _c_vp],
+    "pkg_prover_serialize": [_c_vp, _c_vp],
+    "pkg_prover_load_bytes": [_c_vp, _c_sz, _c_vp],
+    "pkg_thread_resource_bytes": [_c_vp, _c_vp],
 }
+
+
+class PkgBuf(ctypes.Structure):
+    """pkg_buf: library-owned bytes, released by pkg_free_buf."""
+    _fields_ = [("ptr", ctypes.POINTER(ctypes.c_uint8)), ("len", ctypes.c_size_t),
+                ("cap", ctypes.c_size_t)]
 
 
 class PkgError(RuntimeError):
@@ -133,6 +150,12 @@ def lib():
         L.pkg_batch_destroy.restype = None
         L.pkg_server_destroy.argtypes = [_c_vp]
         L.pkg_server_destroy.restype = None
+        L.pkg_free_buf.argtypes = [PkgBuf]
+        L.pkg_free_buf.restype = None
+        L.pkg_prover_free.argtypes = [_c_vp]
+        L.pkg_prover_free.restype = None
+        L.pkg_r1cs_transposes_bytes.argtypes = [_c_vp]
+        L.pkg_r1cs_transposes_bytes.restype = ctypes.c_size_t
         for name in ("pkg_whir_commit_words", "pkg_whir_proof_words"):
             fn = getattr(L, name)
             fn.argtypes = [_c_vp] if name == "pkg_whir_commit_words" else [_c_vp, _c_sz]
@@ -156,4 +179,5 @@ def check(rc: int):
 def exported_symbols():
     return sorted(SIGNATURES) + ["pkg_last_error", "pkg_kernel_launches", "pkg_batch_destroy",
                                   "pkg_server_destroy", "pkg_whir_commit_words",
-                                  "pkg_whir_proof_words"]
+                                  "pkg_whir_proof_words", "pkg_r1cs_transposes_bytes",
+                                  "pkg_free_buf", "pkg_prover_free"]

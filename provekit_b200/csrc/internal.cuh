@@ -11,6 +11,10 @@ namespace pk {
 
 int merkle_tree_fr_device(const uint64_t* cw, size_t fr_per_leaf, size_t num_leaves, int encoding,
                           uint8_t* layers, cudaStream_t s);
+// a = A w, b = B w, c = a o b over the R1CS's rows, zero-padded to padded
+// entries (calculate_witness_bounds), one launch; err: device word, zeroed.
+int witness_bounds_device(const pkg_r1cs* r1cs, const uint64_t* w, size_t padded, uint64_t* ta,
+                          uint64_t* tb, uint64_t* tc, uint32_t* err, cudaStream_t s);
 int spmv_device(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
                 size_t num_rows, size_t num_cols, const uint64_t* x, uint64_t* y, uint32_t* err,
                 cudaStream_t s);

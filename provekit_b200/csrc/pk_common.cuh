@@ -79,17 +79,38 @@ int read_small(const HostRead* reads, int n, cudaStream_t s);
 // device counter on the current device for their tickets.  One of each per
 // thread is enough because every user launches its fused reductions in
 // stream order on one stream and synchronises before returning, so a
-// thread's fused launches never run at the same time.
+// thread's fused launches never run at the same time.  Builds with
+// -DPK_DEBUG_FUSED check that rule: a fused use that begins while the
+// thread's previous one has not synchronised fails.
 struct FusedSlots {
   uint64_t* host;    // the buffer, as the host reads it
   uint64_t* dev;     // the same buffer, as kernels write it
   unsigned* ticket;  // zero between launches
   uint64_t* part;    // device partials: 3 Fr for each of up to 4 CTAs per SM
+  unsigned long long* pow;  // device word of the PoW search (its own, after the partials)
 };
 constexpr size_t kFusedSlotFr = 64;
 int fused_slots(FusedSlots* f);
 // Waits for the stream, then copies bytes of the thread's slots to dst.
 int fused_read(void* dst, const FusedSlots& f, size_t bytes, cudaStream_t s);
+
+// Per host thread and device: a grow-only pinned staging buffer and an event
+// that marks the last copy into it (the WHIR prover's STIR openings).
+// Waits for that event before handing the buffer out again.
+struct PinnedStage {
+  uint8_t* buf = nullptr;
+  size_t cap = 0;
+  cudaEvent_t copied = nullptr;
+};
+int pinned_stage(size_t bytes, PinnedStage** out);
+
+// The per-thread resources above (fused slots, their device counters and
+// partials, the read_small bounce buffer, the pinned stages) are owned by one
+// thread_local object: released when the thread exits, or earlier by
+// pkg_release_thread_resources.  Live totals over all threads, for
+// pkg_thread_resource_bytes.
+void thread_resource_totals(size_t* host_bytes, size_t* device_bytes);
+
 inline int read_small(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   const HostRead r{dst, src, bytes};
   return read_small(&r, 1, s);

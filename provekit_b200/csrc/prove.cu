@@ -161,12 +161,8 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   uint32_t* err = static_cast<uint32_t*>(s_misc.ptr);
   uint64_t* part = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(s_misc.ptr) + 256);
   PK_CUDA(cudaMemsetAsync(err, 0, 4, s));
-  PK_CUDA(cudaMemsetAsync(ta, 0, 32 * 3 * n0, s));
-  if ((rc = spmv_device(r1cs->row_ptr[0], r1cs->cols[0], r1cs->vals[0], nc, nw, witness, ta, err, s)))
-    return rc;
-  if ((rc = spmv_device(r1cs->row_ptr[1], r1cs->cols[1], r1cs->vals[1], nc, nw, witness, tb, err, s)))
-    return rc;
-  if ((rc = pkg_hadamard_pad(ta, tb, nc, nc, tc, stream))) return rc;
+  // a = A w, b = B w, c = a o b, zero-padded to 2^m0: one launch
+  if ((rc = witness_bounds_device(r1cs, witness, n0, ta, tb, tc, err, s))) return rc;
 
   // ---- zk sumcheck (whir_r1cs.rs:519-621)
   std::vector<uint64_t> wb(16 * m0);
@@ -214,20 +210,32 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   }
   pkg_transcript_squeeze(&out->transcript, out->public_x);
   clk.mark(3);
+  // the transposes: the resident circuit's (built once), else built here
+  const bool cached = r1cs->row_ptr_t[0] && r1cs->row_ptr_t[1] && r1cs->row_ptr_t[2];
   for (int k = 0; k < 3; k++) {
     uint64_t* alph = whir ? cov + 4 * n * (sbase + (size_t)k) : cov;
     Scratch s_t;
-    const size_t nnz = r1cs->nnz[k];
-    const size_t rp_bytes = ((8 * (nw + 1) + 255) / 256) * 256;
-    const size_t cl_bytes = ((4 * (nnz ? nnz : 1) + 255) / 256) * 256;
-    if ((rc = s_t.alloc(rp_bytes + cl_bytes + 32 * (nnz ? nnz : 1), s))) return rc;
-    uint8_t* base = static_cast<uint8_t*>(s_t.ptr);
-    uint64_t* rp_t = reinterpret_cast<uint64_t*>(base);
-    uint32_t* cl_t = reinterpret_cast<uint32_t*>(base + rp_bytes);
-    uint64_t* vl_t = reinterpret_cast<uint64_t*>(base + rp_bytes + cl_bytes);
-    rc = pkg_csr_transpose(r1cs->row_ptr[k], r1cs->cols[k], r1cs->vals[k], nc, nw, nnz, rp_t, cl_t,
-                           vl_t, stream);
-    if (rc) return rc;
+    const uint64_t* rp_t = r1cs->row_ptr_t[k];
+    const uint32_t* cl_t = r1cs->cols_t[k];
+    const uint64_t* vl_t = r1cs->vals_t[k];
+    if (!cached) {
+      const size_t nnz = r1cs->nnz[k];
+      const size_t rp_bytes = ((8 * (nw + 1) + 255) / 256) * 256;
+      const size_t cl_bytes = ((4 * (nnz ? nnz : 1) + 255) / 256) * 256;
+      if ((rc = s_t.alloc(rp_bytes + cl_bytes + 32 * (nnz ? nnz : 1), s))) return rc;
+      uint8_t* base = static_cast<uint8_t*>(s_t.ptr);
+      uint64_t* rp = reinterpret_cast<uint64_t*>(base);
+      uint32_t* cl = reinterpret_cast<uint32_t*>(base + rp_bytes);
+      uint64_t* vl = reinterpret_cast<uint64_t*>(base + rp_bytes + cl_bytes);
+      rc = pkg_csr_transpose(r1cs->row_ptr[k], r1cs->cols[k], r1cs->vals[k], nc, nw, nnz, rp, cl,
+                             vl, stream);
+      if (rc) return rc;
+      rp_t = rp;
+      cl_t = cl;
+      vl_t = vl;
+    } else {
+      PK_REQUIRE(cl_t && vl_t, "transpose %d of the R1CS is incomplete", k);
+    }
     if ((rc = spmv_device(rp_t, cl_t, vl_t, nw, nc, eq, alph, err, s))) return rc;
     // create_weights_and_evaluations (:623-642): the zero padding adds nothing
     if ((rc = dot_device(alph, poly, nw, fs.dev + 4 * k, part, s, fs.ticket))) return rc;

@@ -111,82 +111,210 @@ __global__ void dfma_rate_kernel(double* sink, double c, double d, int iters) {
   if (s == -1.0) sink[threadIdx.x] = s;
 }
 
+// ---------------------------------------------------------------------------
+// Per-thread resources, owned by one thread_local object and released when
+// the thread exits (or by pkg_release_thread_resources).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kMaxDevices = 64;
+constexpr size_t kBounceCap = size_t(256) << 10;
+std::atomic<int64_t> g_res_host{0}, g_res_dev{0};
+
+// the device block of one thread on one device: the ticket counter, the
+// partials of one reduction launch (3 Fr for each of 4 CTAs per SM), then the
+// PoW search's word
+size_t fused_block_bytes() { return 256 + 32 * 3 * 4 * (size_t)sm_count() + 256; }
+
+struct ThreadResources {
+  uint64_t* fused_host = nullptr;  // mapped pinned, portable
+  uint64_t* fused_dev = nullptr;
+  struct PerDevice {
+    uint8_t* block = nullptr;  // ticket, partials, PoW word
+    size_t block_bytes = 0;
+    PinnedStage stage;
+  };
+  PerDevice dev[kMaxDevices];
+  uint8_t* bounce = nullptr;
+  bool bounce_tried = false;
+#ifdef PK_DEBUG_FUSED
+  bool fused_busy = false;
+#endif
+
+  void release() {
+    int cur = -1;
+    const bool have_cur = cudaGetDevice(&cur) == cudaSuccess;
+    for (int d = 0; d < kMaxDevices; d++) {
+      PerDevice& pd = dev[d];
+      if (!pd.block && !pd.stage.buf && !pd.stage.copied) continue;
+      cudaSetDevice(d);
+      // copies into the stage may still be in flight: wait for the last one
+      if (pd.stage.copied) {
+        cudaEventSynchronize(pd.stage.copied);
+        cudaEventDestroy(pd.stage.copied);
+      }
+      if (pd.stage.buf) {
+        cudaFreeHost(pd.stage.buf);
+        g_res_host -= (int64_t)pd.stage.cap;
+      }
+      if (pd.block) {
+        cudaFree(pd.block);  // waits for the device's outstanding work
+        g_res_dev -= (int64_t)pd.block_bytes;
+      }
+      pd = PerDevice();
+    }
+    if (have_cur) cudaSetDevice(cur);
+    if (fused_host) {
+      cudaFreeHost(fused_host);
+      g_res_host -= (int64_t)(32 * kFusedSlotFr);
+    }
+    if (bounce) {
+      cudaFreeHost(bounce);
+      g_res_host -= (int64_t)kBounceCap;
+    }
+    fused_host = fused_dev = nullptr;
+    bounce = nullptr;
+    bounce_tried = false;
+    cudaGetLastError();  // a teardown-time failure is not the caller's error
+  }
+  ~ThreadResources() { release(); }
+};
+
+thread_local ThreadResources t_res;
+
+}  // namespace
+
+void thread_resource_totals(size_t* host_bytes, size_t* device_bytes) {
+  *host_bytes = (size_t)std::max<int64_t>(0, g_res_host.load());
+  *device_bytes = (size_t)std::max<int64_t>(0, g_res_dev.load());
+}
+
 int fused_slots(FusedSlots* f) {
-  constexpr int kMaxDevices = 64;
-  thread_local uint64_t* host = nullptr;
-  thread_local uint64_t* dev = nullptr;
-  thread_local unsigned* tickets[kMaxDevices] = {};
-  if (!host) {
+  ThreadResources& tr = t_res;
+#ifdef PK_DEBUG_FUSED
+  PK_REQUIRE(!tr.fused_busy,
+             "fused slots: a fused use began before the thread's previous one synchronised");
+  tr.fused_busy = true;
+#endif
+  if (!tr.fused_host) {
     void* p = nullptr;
     PK_CUDA(cudaHostAlloc(&p, 32 * kFusedSlotFr, cudaHostAllocMapped | cudaHostAllocPortable));
     void* d = nullptr;
-    PK_CUDA(cudaHostGetDevicePointer(&d, p, 0));
-    host = static_cast<uint64_t*>(p);
-    dev = static_cast<uint64_t*>(d);
+    const cudaError_t e = cudaHostGetDevicePointer(&d, p, 0);
+    if (e != cudaSuccess) {
+      cudaFreeHost(p);
+      return cuda_status(e, "cudaHostGetDevicePointer");
+    }
+    tr.fused_host = static_cast<uint64_t*>(p);
+    tr.fused_dev = static_cast<uint64_t*>(d);
+    g_res_host += (int64_t)(32 * kFusedSlotFr);
   }
   int device = 0;
   PK_CUDA(cudaGetDevice(&device));
   PK_REQUIRE(device >= 0 && device < kMaxDevices, "device ordinal %d out of range", device);
-  if (!tickets[device]) {
+  ThreadResources::PerDevice& pd = tr.dev[device];
+  if (!pd.block) {
     // the counter (zeroed on a private stream, waited for: ordered before any
     // later launch on any stream without touching the legacy default stream)
-    // followed by the partials of one reduction launch
+    // followed by the partials of one reduction launch and the PoW word
+    const size_t bytes = fused_block_bytes();
     void* t = nullptr;
-    PK_CUDA(cudaMalloc(&t, 256 + 32 * 3 * 4 * (size_t)sm_count()));
+    PK_CUDA(cudaMalloc(&t, bytes));
     cudaStream_t z = nullptr;
-    PK_CUDA(cudaStreamCreateWithFlags(&z, cudaStreamNonBlocking));
-    const cudaError_t e1 = cudaMemsetAsync(t, 0, 256, z);
-    const cudaError_t e2 = cudaStreamSynchronize(z);
-    cudaStreamDestroy(z);
-    PK_CUDA(e1);
-    PK_CUDA(e2);
-    tickets[device] = static_cast<unsigned*>(t);
+    cudaError_t e = cudaStreamCreateWithFlags(&z, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+      e = cudaMemsetAsync(t, 0, 256, z);
+      const cudaError_t e2 = cudaStreamSynchronize(z);
+      if (e == cudaSuccess) e = e2;
+      cudaStreamDestroy(z);
+    }
+    if (e != cudaSuccess) {
+      cudaFree(t);
+      return cuda_status(e, "fused slots: zeroing the ticket");
+    }
+    pd.block = static_cast<uint8_t*>(t);
+    pd.block_bytes = bytes;
+    g_res_dev += (int64_t)bytes;
   }
-  f->host = host;
-  f->dev = dev;
-  f->ticket = tickets[device];
-  f->part = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(tickets[device]) + 256);
+  f->host = tr.fused_host;
+  f->dev = tr.fused_dev;
+  f->ticket = reinterpret_cast<unsigned*>(pd.block);
+  f->part = reinterpret_cast<uint64_t*>(pd.block + 256);
+  f->pow = reinterpret_cast<unsigned long long*>(pd.block + pd.block_bytes - 256);
   return PKG_OK;
 }
 
 int fused_read(void* dst, const FusedSlots& f, size_t bytes, cudaStream_t s) {
   PK_REQUIRE(bytes <= 32 * kFusedSlotFr, "%zu bytes exceed the fused slots", bytes);
   PK_CUDA(cudaStreamSynchronize(s));
+#ifdef PK_DEBUG_FUSED
+  t_res.fused_busy = false;
+#endif
   memcpy(dst, f.host, bytes);
   return PKG_OK;
 }
 
-int read_small(const HostRead* reads, int n, cudaStream_t s) {
-  constexpr size_t kCap = size_t(256) << 10;
-  thread_local uint8_t* bounce = nullptr;
-  thread_local bool tried = false;
-  if (!tried) {
-    tried = true;
+int pinned_stage(size_t bytes, PinnedStage** out) {
+  int device = 0;
+  PK_CUDA(cudaGetDevice(&device));
+  PK_REQUIRE(device >= 0 && device < kMaxDevices, "device ordinal %d out of range", device);
+  PinnedStage& st = t_res.dev[device].stage;
+  if (!st.copied) PK_CUDA(cudaEventCreateWithFlags(&st.copied, cudaEventDisableTiming));
+  PK_CUDA(cudaEventSynchronize(st.copied));
+  if (bytes > st.cap) {
+    if (st.buf) {
+      cudaFreeHost(st.buf);
+      g_res_host -= (int64_t)st.cap;
+    }
+    st.buf = nullptr;
+    st.cap = 0;
     void* p = nullptr;
-    if (cudaHostAlloc(&p, kCap, cudaHostAllocPortable) == cudaSuccess)
-      bounce = static_cast<uint8_t*>(p);
-    else
+    PK_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocPortable));
+    st.buf = static_cast<uint8_t*>(p);
+    st.cap = bytes;
+    g_res_host += (int64_t)bytes;
+  }
+  *out = &st;
+  return PKG_OK;
+}
+
+int read_small(const HostRead* reads, int n, cudaStream_t s) {
+  ThreadResources& tr = t_res;
+  if (!tr.bounce_tried) {
+    tr.bounce_tried = true;
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, kBounceCap, cudaHostAllocPortable) == cudaSuccess) {
+      tr.bounce = static_cast<uint8_t*>(p);
+      g_res_host += (int64_t)kBounceCap;
+    } else {
       cudaGetLastError();  // no bounce buffer: direct copies below
+    }
   }
   size_t total = 0;
   for (int i = 0; i < n; i++) total += (reads[i].bytes + 15) & ~size_t(15);
-  if (!bounce || total > kCap) {
+  if (!tr.bounce || total > kBounceCap) {
     for (int i = 0; i < n; i++)
       PK_CUDA(cudaMemcpyAsync(reads[i].dst, reads[i].src, reads[i].bytes, cudaMemcpyDeviceToHost,
                               s));
     PK_CUDA(cudaStreamSynchronize(s));
+#ifdef PK_DEBUG_FUSED
+    tr.fused_busy = false;
+#endif
     return PKG_OK;
   }
   size_t off = 0;
   for (int i = 0; i < n; i++) {
-    PK_CUDA(cudaMemcpyAsync(bounce + off, reads[i].src, reads[i].bytes, cudaMemcpyDeviceToHost,
+    PK_CUDA(cudaMemcpyAsync(tr.bounce + off, reads[i].src, reads[i].bytes, cudaMemcpyDeviceToHost,
                             s));
     off += (reads[i].bytes + 15) & ~size_t(15);
   }
   PK_CUDA(cudaStreamSynchronize(s));
+#ifdef PK_DEBUG_FUSED
+  tr.fused_busy = false;
+#endif
   off = 0;
   for (int i = 0; i < n; i++) {
-    memcpy(reads[i].dst, bounce + off, reads[i].bytes);
+    memcpy(reads[i].dst, tr.bounce + off, reads[i].bytes);
     off += (reads[i].bytes + 15) & ~size_t(15);
   }
   return PKG_OK;
@@ -255,6 +383,17 @@ extern "C" int pkg_trim_memory(size_t keep_bytes) {
 }
 
 extern "C" const char* pkg_last_error(void) { return g_last_error; }
+
+extern "C" int pkg_release_thread_resources(void) {
+  t_res.release();
+  return PKG_OK;
+}
+
+extern "C" int pkg_thread_resource_bytes(size_t* host_bytes, size_t* device_bytes) {
+  PK_REQUIRE(host_bytes && device_bytes, "null output");
+  thread_resource_totals(host_bytes, device_bytes);
+  return PKG_OK;
+}
 
 extern "C" int pkg_version(void) { return 100; }
 

@@ -242,12 +242,12 @@ int pow_solve_device(const uint64_t challenge[4], const uint64_t threshold[4], c
   bool thr_zero = true;
   for (int i = 0; i < 8; i++) thr_zero &= (t.v[i] == 0);
   PK_REQUIRE(!thr_zero, "threshold 0 admits no nonce");
-  // the best nonce in the thread's fused-reduction partials (free between
-  // that thread's synchronous calls): no pool allocation per PoW
+  // the best nonce in the thread's own PoW word (after the fused
+  // reductions' partials, which it never overlaps): no pool allocation per PoW
   FusedSlots fs;
   int rc = fused_slots(&fs);
   if (rc) return rc;
-  unsigned long long* d_best = reinterpret_cast<unsigned long long*>(fs.part);
+  unsigned long long* d_best = fs.pow;
   PK_CUDA(cudaMemsetAsync(d_best, 0xff, sizeof(unsigned long long), s));
   const unsigned long long none = ~0ULL;
   unsigned long long best = none;

@@ -92,6 +92,48 @@ __global__ void spmv_csr_kernel(const uint64_t* __restrict__ row_ptr, const uint
   }
 }
 
+// calculate_witness_bounds (sumcheck.rs:163-179) in one pass over the rows:
+// a_i = <A_i, w>, b_i = <B_i, w>, c_i = a_i b_i for i < num_rows, and zeros
+// up to the padded size (the three tables of the zk-sumcheck).  Column
+// indices >= num_cols are skipped and flagged in *err.
+__global__ void witness_bounds_kernel(const uint64_t* __restrict__ rpa,
+                                      const uint32_t* __restrict__ ca,
+                                      const uint64_t* __restrict__ va,
+                                      const uint64_t* __restrict__ rpb,
+                                      const uint32_t* __restrict__ cb,
+                                      const uint64_t* __restrict__ vb, size_t num_rows,
+                                      size_t num_cols, size_t padded,
+                                      const uint64_t* __restrict__ w, uint64_t* __restrict__ ta,
+                                      uint64_t* __restrict__ tb, uint64_t* __restrict__ tc,
+                                      uint32_t* __restrict__ err) {
+  for (size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x; row < padded;
+       row += (size_t)gridDim.x * blockDim.x) {
+    Fr a = fr_zero(), b = fr_zero(), c = fr_zero();
+    if (row < num_rows) {
+      for (uint64_t k = rpa[row]; k < rpa[row + 1]; k++) {
+        const uint32_t col = ca[k];
+        if (col >= num_cols) {
+          atomicOr(err, 1u);
+          continue;
+        }
+        a = fr_add(a, fr_mul_f64(fr_load_ro(va, k), fr_load_ro(w, col)));
+      }
+      for (uint64_t k = rpb[row]; k < rpb[row + 1]; k++) {
+        const uint32_t col = cb[k];
+        if (col >= num_cols) {
+          atomicOr(err, 1u);
+          continue;
+        }
+        b = fr_add(b, fr_mul_f64(fr_load_ro(vb, k), fr_load_ro(w, col)));
+      }
+      c = fr_mul_f64(a, b);
+    }
+    fr_store(ta, row, a);
+    fr_store(tb, row, b);
+    fr_store(tc, row, c);
+  }
+}
+
 __global__ void hadamard_pad_kernel(const uint64_t* __restrict__ a, const uint64_t* __restrict__ b,
                                     size_t n, size_t padded, uint64_t* __restrict__ c) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < padded;
@@ -201,6 +243,20 @@ int eq_hypercube_device(const uint64_t* r_host, size_t nr, size_t num_entries, u
   // a pinned r must outlive the async copy: callers whose r stays valid
   // until their next synchronisation pass sync = false
   if (sync) PK_CUDA(cudaStreamSynchronize(s));
+  return PKG_OK;
+}
+
+// err: device word, zeroed by the caller before the launch.
+int witness_bounds_device(const pkg_r1cs* r1cs, const uint64_t* w, size_t padded, uint64_t* ta,
+                          uint64_t* tb, uint64_t* tc, uint32_t* err, cudaStream_t s) {
+  if (padded == 0) return PKG_OK;
+  PK_REQUIRE(aligned16(ta) && aligned16(tb) && aligned16(tc) && aligned16(w) &&
+                 aligned16(r1cs->vals[0]) && aligned16(r1cs->vals[1]),
+             "null or unaligned device pointer");
+  witness_bounds_kernel<<<ew_grid(padded), 256, 0, s>>>(
+      r1cs->row_ptr[0], r1cs->cols[0], r1cs->vals[0], r1cs->row_ptr[1], r1cs->cols[1],
+      r1cs->vals[1], r1cs->num_constraints, r1cs->num_witnesses, padded, w, ta, tb, tc, err);
+  PK_CHECK_LAUNCH("witness_bounds_kernel");
   return PKG_OK;
 }
 
@@ -574,5 +630,42 @@ extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_
   t.absorb(acc);  // prover_message(&blinding_eval), :618
   memcpy(transcript->l, t.l.l, 32);
   memcpy(transcript->r, t.r.l, 32);
+  return PKG_OK;
+}
+
+namespace {
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+}  // namespace
+
+extern "C" size_t pkg_r1cs_transposes_bytes(const pkg_r1cs* r1cs) {
+  if (!r1cs) return 0;
+  size_t total = 0;
+  for (int k = 0; k < 3; k++) {
+    const size_t nnz = r1cs->nnz[k] ? r1cs->nnz[k] : 1;
+    total += align256(8 * (r1cs->num_witnesses + 1)) + align256(4 * nnz) + align256(32 * nnz);
+  }
+  return total;
+}
+
+extern "C" int pkg_r1cs_build_transposes(pkg_r1cs* r1cs, void* buf, pkg_stream_t stream) {
+  PK_REQUIRE(r1cs && buf, "null pointer");
+  PK_REQUIRE((reinterpret_cast<uintptr_t>(buf) & 255) == 0, "buffer must be 256-byte aligned");
+  uint8_t* at = static_cast<uint8_t*>(buf);
+  const size_t nw = r1cs->num_witnesses, nc = r1cs->num_constraints;
+  for (int k = 0; k < 3; k++) {
+    const size_t nnz = r1cs->nnz[k] ? r1cs->nnz[k] : 1;
+    uint64_t* rp = reinterpret_cast<uint64_t*>(at);
+    at += align256(8 * (nw + 1));
+    uint32_t* cl = reinterpret_cast<uint32_t*>(at);
+    at += align256(4 * nnz);
+    uint64_t* vl = reinterpret_cast<uint64_t*>(at);
+    at += align256(32 * nnz);
+    const int rc = pkg_csr_transpose(r1cs->row_ptr[k], r1cs->cols[k], r1cs->vals[k], nc, nw,
+                                     r1cs->nnz[k], rp, cl, vl, stream);
+    if (rc) return rc;
+    r1cs->row_ptr_t[k] = rp;
+    r1cs->cols_t[k] = cl;
+    r1cs->vals_t[k] = vl;
+  }
   return PKG_OK;
 }

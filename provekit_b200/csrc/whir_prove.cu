@@ -222,38 +222,12 @@ struct PhaseTimer {
     if (_rc) return _rc;      \
   } while (0)
 
-// Pinned staging for one proof's STIR openings.  Openings feed no transcript
-// value, so their copies run behind the proof's later steps and are moved
-// into the proof after its last synchronisation.  One buffer per host thread
-// and device (grow-only); the event marks the last copy into it, so a proof
-// that ended early cannot leave copies landing in the next one's openings.
-struct OpeningStage {
-  uint8_t* buf = nullptr;
-  size_t cap = 0;
-  cudaEvent_t copied = nullptr;
-};
-
-static int opening_stage(size_t bytes, OpeningStage** out) {
-  constexpr int kMaxDevices = 64;
-  thread_local OpeningStage stages[kMaxDevices];
-  int device = 0;
-  PK_CUDA(cudaGetDevice(&device));
-  PK_REQUIRE(device >= 0 && device < kMaxDevices, "device ordinal %d out of range", device);
-  OpeningStage& st = stages[device];
-  if (!st.copied) PK_CUDA(cudaEventCreateWithFlags(&st.copied, cudaEventDisableTiming));
-  PK_CUDA(cudaEventSynchronize(st.copied));
-  if (bytes > st.cap) {
-    if (st.buf) cudaFreeHost(st.buf);
-    st.buf = nullptr;
-    st.cap = 0;
-    void* p = nullptr;
-    PK_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocPortable));
-    st.buf = static_cast<uint8_t*>(p);
-    st.cap = bytes;
-  }
-  *out = &st;
-  return PKG_OK;
-}
+// The proof's STIR openings feed no transcript value, so their copies run
+// behind the proof's later steps into the thread's pinned stage
+// (pinned_stage: one grow-only buffer per host thread and device, whose
+// event marks the last copy into it, so a proof that ended early cannot leave
+// copies landing in the next one's openings) and are moved into the proof
+// after its last synchronisation.
 
 class WhirProver {
  public:
@@ -286,7 +260,7 @@ class WhirProver {
   struct Placement {
     size_t word, src, bytes;
   };
-  OpeningStage* stage_ = nullptr;
+  PinnedStage* stage_ = nullptr;
   size_t stage_off_ = 0;
   std::vector<Placement> place_;
   uint64_t* E_ = nullptr;  // f^ table (live size size_)
@@ -390,7 +364,7 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
     size_t stage_bytes = 32;
     for (unsigned r = 0; r <= R; r++)
       stage_bytes += (size_t)p_->queries[r] * 32 * (row_fr(p_, r) + rows_log(p_, r));
-    PK_TRY(opening_stage(stage_bytes, &stage_));
+    PK_TRY(pinned_stage(stage_bytes, &stage_));
     stage_off_ = 0;
     place_.clear();
   }

@@ -14,7 +14,8 @@ class R1csC(ctypes.Structure):
     _fields_ = [("num_constraints", ctypes.c_size_t), ("num_witnesses", ctypes.c_size_t),
                 ("row_ptr", ctypes.c_void_p * 3), ("cols", ctypes.c_void_p * 3),
                 ("vals", ctypes.c_void_p * 3), ("nnz", ctypes.c_size_t * 3),
-                ("num_public_inputs", ctypes.c_size_t)]
+                ("num_public_inputs", ctypes.c_size_t), ("row_ptr_t", ctypes.c_void_p * 3),
+                ("cols_t", ctypes.c_void_p * 3), ("vals_t", ctypes.c_void_p * 3)]
 
 
 class SpartanProofC(ctypes.Structure):
@@ -64,12 +65,16 @@ class HostR1CS:
         self.cols = [np.ascontiguousarray(c[:n]) for c, n in zip(self.cols, self.nnz)]
         self.vals = [np.ascontiguousarray(v[:n]) for v, n in zip(self.vals, self.nnz)]
 
-    def to_device(self, device="cuda"):
-        return DeviceR1CS(self, device)
+    def to_device(self, device="cuda", transposes=True):
+        return DeviceR1CS(self, device, transposes)
 
 
 class DeviceR1CS:
-    def __init__(self, h: HostR1CS, device="cuda"):
+    """An R1CS resident on the device.  transposes: build A^T, B^T, C^T once
+    (pkg_r1cs_build_transposes) so that proofs of this circuit skip the
+    per-proof transposes; False leaves them to every proof."""
+
+    def __init__(self, h: HostR1CS, device="cuda", transposes=True):
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(  # noqa: E731
             np.int32 if a.dtype == np.uint32 else np.int64)).to(device)
         self.num_constraints, self.num_witnesses = h.num_constraints, h.num_witnesses
@@ -84,6 +89,13 @@ class DeviceR1CS:
                        (ctypes.c_void_p * 3)(*[x.data_ptr() for x in self.cols]),
                        (ctypes.c_void_p * 3)(*[x.data_ptr() for x in self.vals]),
                        (ctypes.c_size_t * 3)(*self.nnz), self.num_public_inputs)
+        self.transposes = None
+        if transposes:
+            nbytes = lib().pkg_r1cs_transposes_bytes(ctypes.byref(self.c))
+            self.transposes = torch.empty(nbytes, dtype=torch.uint8, device=device)
+            s = torch.cuda.current_stream(self.transposes.device).cuda_stream
+            check(lib().pkg_r1cs_build_transposes(ctypes.byref(self.c),
+                                                  self.transposes.data_ptr(), s))
 
 
 def spartan_prove(r1cs: DeviceR1CS, witness=None, blinding_seed=1, transcript_domain=3,

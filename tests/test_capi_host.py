@@ -247,3 +247,92 @@ def test_synthetic_r1cs_matches_oracle_generator(L, seed, log_nc, log_ni, npub):
         O.lib().pko_fr_mul(O.p64(ab), O.p64(np.ascontiguousarray(ys[0][i])),
                            O.p64(np.ascontiguousarray(ys[1][i])))
         assert np.array_equal(ab, ys[2][i]), i
+
+
+def prover_bytes(h, folding_factor=3, log_inv_rate=2, security_bits=128, pow_bits=10, zk=1,
+                 domain=0) -> bytes:
+    """The pkg_prover_serialize layout written independently from the header's
+    description (a test of the loader and of the serializer on the GPU)."""
+    import struct
+    out = [b"PKGPROVR", struct.pack("<II", 1, 0),
+           struct.pack("<6Q", h.num_constraints, h.num_witnesses,
+                       getattr(h, "num_public_inputs", 0), *h.nnz),
+           struct.pack("<6I", folding_factor, log_inv_rate, security_bits, pow_bits, zk, 0),
+           struct.pack("<QQ", domain, 0)]
+    for k in range(3):
+        out.append(np.ascontiguousarray(h.row_ptr[k], np.uint64).tobytes())
+        c = np.ascontiguousarray(h.cols[k][: h.nnz[k]], np.uint32).tobytes()
+        out.append(c + b"\0" * (-len(c) % 8))
+        out.append(np.ascontiguousarray(h.vals[k][: h.nnz[k]], np.uint64).tobytes())
+    return b"".join(out)
+
+
+def test_get_last_error_takes_and_clears(L):
+    from provekit_b200.handle import last_error_taken
+    assert L.pkg_ntt_nr(None, 6, 4, 1, None) == -1
+    msg = last_error_taken()
+    assert msg  # the validation message, as UTF-8 bytes in a library-owned buffer
+    assert last_error_taken() == ""  # cleared by the first take
+
+
+def _bad_variants(h):
+    """(description, mutated HostR1CS-like copy) with one malformed matrix each."""
+    import copy
+    out = []
+    for what in ("start", "decrease", "end", "column"):
+        g = copy.deepcopy(h)
+        if what == "start":
+            g.row_ptr[1] = g.row_ptr[1].copy()
+            g.row_ptr[1][0] = 1
+        elif what == "decrease":
+            g.row_ptr[0] = g.row_ptr[0].copy()
+            g.row_ptr[0][2] = g.row_ptr[0][1] - 1 if g.row_ptr[0][1] else 5
+        elif what == "end":
+            g.nnz = list(g.nnz)
+            g.nnz[2] += 1
+        else:
+            g.cols[0] = g.cols[0].copy()
+            g.cols[0][3] = g.num_witnesses
+        out.append((what, g))
+    return out
+
+
+def test_prover_create_rejects_malformed_circuits_before_device_work(L):
+    """Row pointers that do not start at 0, decrease or do not end at nnz,
+    and columns that are not witness indices, are rejected on the host:
+    the kernels that walk the rows never see them."""
+    from provekit_b200._lib import PkgError
+    from provekit_b200.handle import Prover
+    h = O.SyntheticR1CS(5, 64, 16)
+    for what, g in _bad_variants(h):
+        with pytest.raises(PkgError) as e:
+            Prover.create(g)
+        assert e.value.code == -1, what
+
+
+def test_prover_load_bytes_validates_the_layout(L):
+    """Bad magic, an unknown version, truncation anywhere, trailing bytes and
+    malformed matrices are rejected before any device work; a well-formed
+    string gets as far as the device (which this machine lacks)."""
+    import ctypes
+    h = O.SyntheticR1CS(6, 64, 16, num_public_inputs=2)
+    good = prover_bytes(h)
+
+    def load(b):
+        out = ctypes.c_void_p()
+        buf = (ctypes.c_uint8 * max(len(b), 1)).from_buffer_copy(b or b"\0")
+        return L.pkg_prover_load_bytes(buf, len(b), ctypes.byref(out)), out
+
+    assert load(b"XKGPROVR" + good[8:])[0] == -1
+    assert load(good[:8] + b"\2" + good[9:])[0] == -1
+    for cut in (4, 20, 60, 104, 300, len(good) - 1):
+        rc, out = load(good[:cut])
+        assert rc == -1 and not out.value, cut
+    assert load(good + b"\0")[0] == -1
+    for what, g in _bad_variants(h):
+        assert load(prover_bytes(g))[0] == -1, what
+    rc, out = load(good)
+    if rc == 0:  # a device is present after all
+        L.pkg_prover_free(out)
+    else:
+        assert rc == -2 and not out.value  # CUDA: past every host check
