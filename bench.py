@@ -64,6 +64,9 @@ def parse_args():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plugin-e2e", action="store_true")
+    p.add_argument("--no-north-star", action="store_true",
+                   help="prove: skip the 2^24 NTT, batched and served measurements after the "
+                        "headline")
     p.add_argument("--workload", choices=["commit", "prove", "batched", "served", "ntt", "whir_ops",
                                           "poseidon2"],
                    default="prove",
@@ -670,6 +673,8 @@ def run_prove(a):
     bstreams = [torch.cuda.Stream(device=dev) for _ in range(nthr)]
     bw = [torch.empty_like(d.witness) for _ in range(nthr)]
     blat = [[] for _ in range(nthr)]
+    bdone = [[] for _ in range(nthr)]  # completion times from the common start
+    t_common = [0.0]
 
     def batch_worker(j, count):
         torch.cuda.set_device(dev)
@@ -678,7 +683,9 @@ def run_prove(a):
             with torch.cuda.stream(bstreams[j]):
                 bw[j].copy_(w_pinned, non_blocking=True)
                 prove_r1cs(d, wp, witness=bw[j], blinding_seed=1 + i, stream=bstreams[j])
-            blat[j].append((time.perf_counter() - t1) * 1e3)
+            t2 = time.perf_counter()
+            blat[j].append((t2 - t1) * 1e3)
+            bdone[j].append((t2 - t_common[0]) * 1e3)
 
     th = [threading.Thread(target=batch_worker, args=(j, 1)) for j in range(nthr)]  # warm-up
     for t in th:
@@ -686,8 +693,21 @@ def run_prove(a):
     for t in th:
         t.join()
     blat = [[] for _ in range(nthr)]
+    bdone = [[] for _ in range(nthr)]
+    torch.cuda.synchronize()
+    # the same requests (all arriving at once) proved one at a time by one
+    # thread: completion times from the common start
+    nreq = nthr * per
+    seq_done = []
+    t0 = time.perf_counter()
+    with torch.cuda.stream(bstreams[0]):
+        for i in range(nreq):
+            bw[0].copy_(w_pinned, non_blocking=True)
+            prove_r1cs(d, wp, witness=bw[0], blinding_seed=1 + i, stream=bstreams[0])
+            seq_done.append((time.perf_counter() - t0) * 1e3)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    t_common[0] = t0
     th = [threading.Thread(target=batch_worker, args=(j, per)) for j in range(nthr)]
     for t in th:
         t.start()
@@ -696,8 +716,8 @@ def run_prove(a):
     torch.cuda.synchronize()
     batched_s = time.perf_counter() - t0
     batched_max = max_over_ranks(batched_s, device=dev)
-    nreq = nthr * per
     lat = sorted(x for v in blat for x in v)
+    done_b = [x for v in bdone for x in v]
 
     # the dominant kernel (Merkle leaf hashing of the witness commitment:
     # 2^20 leaves of 8 Fr) timed on its own with CUDA events, L2 flushed
@@ -763,6 +783,39 @@ def run_prove(a):
                   "words": int(gproof.shape[0] + gcw.shape[0])}
     proof = last[2]
     proof_bytes = 8 * proof.shape[0]
+
+    # the north star's targets, measured in the same run: the 2^24 NTT
+    # against both rooflines, the batched form on the 256-job mix against
+    # the same jobs one at a time, and the served form under an open-loop
+    # Poisson stream against sequential plain proving
+    north = None
+    if a.gpus == 1 and not a.no_north_star:
+        north = {}
+        imad = ctypes.c_double(0)
+        check(L.pkg_measure_imad_rate(ctypes.byref(imad)))
+        with torch.cuda.device(dev):
+            north["ntt_2p24"] = ntt_measure(L, stream, flush, 24, 10, 3, dfma.value, imad.value)
+        torch.cuda.empty_cache()
+        t0 = time.perf_counter()
+        b = batched_compare(batched_sizes(a.seed, 256), a.seed, 3, 3)
+        b["wall_s"] = time.perf_counter() - t0
+        b["config"] = ("256 jobs, NTT sizes log-uniform on 2^10..2^22, each: NTT, WHIR commit "
+                       "(ff 3, rate 1/4), zk-sumcheck; one CUDA graph, replayed")
+        north["batched_256_jobs"] = b
+        torch.cuda.empty_cache()
+        t0 = time.perf_counter()
+        logs, reqs, rng = make_requests(a.seed, 32, 14, 20)
+        sgen_s = time.perf_counter() - t0
+        free_b, _ = torch.cuda.mem_get_info()
+        budget = int(min(free_b * 0.5, 48e9))
+        cap, sweeps = served_compare(reqs, (1.0, 2.0), budget, rng)
+        north["served_short_stream"] = {
+            "config": f"{len(reqs)} whole-proof requests, log2 constraints uniform on [14, 20] "
+                      f"(the full sweep to 2^22: --workload served), whir-ZK ff 3, rate 1/4, "
+                      f"128 bits, 10 PoW bits; budget {budget / 1e9:.0f} GB, 8 slots",
+            "log2_constraints": logs, "generation_s": sgen_s,
+            "sequential_capacity_per_s": cap, "sweeps": sweeps,
+            "wall_s": time.perf_counter() - t0}
     line = {"metric": PROVE_METRIC,
             "value": a.gpus * a.steps / (total_max * 1e-3), "unit": PROVE_UNIT,
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
@@ -804,12 +857,21 @@ def run_prove(a):
                                                       int(np.ceil(0.99 * len(lat))) - 1)]},
                         "vs_plain_e2e": (a.gpus * nreq / batched_max) /
                                         (a.gpus * a.steps / (e2e_max * 1e-3)),
+                        "same_requests_at_once": {
+                            "note": f"the same {nreq} requests arriving together: completion "
+                                    "time of each from the common start, batched (4 in flight) "
+                                    "against plain proving one at a time (measured, one thread)",
+                            "batched_ms": {"p50": _pct(done_b, 0.5), "p99": _pct(done_b, 0.99)},
+                            "plain_sequential_ms": {"p50": _pct(seq_done, 0.5),
+                                                    "p99": _pct(seq_done, 0.99)},
+                            "plain_sequential_proofs_per_s": nreq / (seq_done[-1] * 1e-3)},
                         "note": "one resident circuit, many witnesses: 4 host threads with their "
                                 "own streams call pkg_prove_r1cs concurrently (witness from "
                                 "pinned host memory, proof back to host per proof); wall clock "
                                 "from the first call to the last proof"},
             "gpu_launches": int(launches),
-            "clocks": clk}
+            "clocks": clk,
+            "north_star": north}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -880,7 +942,11 @@ def batched_sizes(seed, jobs, lo=10, hi=22):
     return [int(x) for x in rng.integers(lo, hi + 1, size=jobs)]
 
 
-def run_batched(a):
+def batched_compare(sizes, seed, steps, warmup, tune=False):
+    """The batched form (every phase one grouped launch over all jobs, the
+    whole batch one CUDA graph, replayed) against the same jobs one at a time
+    through the plain entry points (pkg_ntt_nr, pkg_whir_commit,
+    pkg_spartan_sumcheck), inputs resident; spot parity of every 32nd job."""
     import numpy as np
     import torch
 
@@ -891,36 +957,28 @@ def run_batched(a):
     from provekit_b200.spartan import Transcript, spartan_sumcheck
 
     L = _lib.lib()
-    torch.cuda.set_device(0)
-    sizes = batched_sizes(a.seed, a.jobs)
     total_fr = sum(1 << k for k in sizes)
     t0 = time.perf_counter()
-    b = Batch(sizes, seed=a.seed)
+    b = Batch(sizes, seed=seed)
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.Stream()
     tuned = None
-    if a.tune:
+    if tune:
         k, e, ms = b.tune(stream)
         tuned = {"kmax": k, "log_elems_per_cta": e, "ms": ms}
     b.run(use_graph=True, stream=stream)  # capture
-    for _ in range(a.warmup):
+    for _ in range(warmup):
         b.run(use_graph=True, stream=stream)
     stream.synchronize()
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
-    clocks = ClockSampler(physical_gpu_index(0))
-    clocks.start()
-    time.sleep(0.3)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
     launches0 = L.pkg_kernel_launches()
-    for i in range(a.steps):
+    for i in range(steps):
         evs[i][0].record(stream)
         b.run(use_graph=True, stream=stream)
         evs[i][1].record(stream)
     stream.synchronize()
     launches = L.pkg_kernel_launches() - launches0
-    clk = clocks.stop()
     ms = [e[0].elapsed_time(e[1]) for e in evs]
-    # plain path: the same jobs one at a time (pkg_ntt_nr, pkg_whir_commit,
-    # pkg_spartan_sumcheck), device-resident inputs
     plain_ms = 0.0
     mismatches = 0
     with torch.cuda.stream(stream):
@@ -951,49 +1009,65 @@ def run_batched(a):
             if j % 32 == 0:  # spot parity (the full check is in tests/test_gpu_batch.py)
                 got = b.sumcheck_result(j)
                 if not (np.array_equal(got["alpha"], sc["alpha"])
-                        and Batch.read(job.layers, 32 * (2 * job.num_leaves - 1)) == lay.cpu().numpy().tobytes()):
+                        and Batch.read(job.layers, 32 * (2 * job.num_leaves - 1))
+                        == lay.cpu().numpy().tobytes()):
                     mismatches += 1
+    b.close()
     batch_ms = statistics.mean(ms)
+    return {"jobs": len(sizes), "log_sizes": sizes, "total_fr": total_fr,
+            "log2_total_fr": float(np.log2(total_fr)), "setup_s": setup_s, "tuned": tuned,
+            "batch_ms": batch_ms, "jobs_per_s": len(sizes) / (batch_ms * 1e-3),
+            "fr_per_s": total_fr / (batch_ms * 1e-3),
+            "plain_ms": plain_ms, "plain_jobs_per_s": len(sizes) / (plain_ms * 1e-3),
+            "speedup_vs_plain": plain_ms / batch_ms, "spot_parity_mismatches": mismatches,
+            "launches_per_batch": int(launches) // max(steps, 1)}
+
+
+def run_batched(a):
+    import torch
+
+    torch.cuda.set_device(0)
+    sizes = batched_sizes(a.seed, a.jobs)
+    clocks = ClockSampler(physical_gpu_index(0))
+    clocks.start()
+    r = batched_compare(sizes, a.seed, a.steps, a.warmup, a.tune)
+    clk = clocks.stop()
     line = {"metric": "batched form: 256 uneven jobs (NTT + WHIR commit + zk-sumcheck each) as one "
                       "CUDA graph vs the same jobs one at a time",
-            "value": len(sizes) / (batch_ms * 1e-3), "unit": "jobs/s", "n_gpus": 1,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": batch_ms,
+            "value": r["jobs_per_s"], "unit": "jobs/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": r["batch_ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32 (BN254 Fr, 8x32-bit limbs)", "data": "synthetic (ChaCha20-seeded Fr)",
-            "config": {"workload": "batched", "jobs": len(sizes), "log_sizes": sizes,
-                       "total_fr": total_fr, "log2_total_fr": float(np.log2(total_fr)),
-                       "setup_s": setup_s, "tuned": tuned},
-            "fr_per_s": total_fr / (batch_ms * 1e-3),
-            "plain": {"value": len(sizes) / (plain_ms * 1e-3), "unit": "jobs/s", "ms": plain_ms},
-            "speedup_vs_plain": plain_ms / batch_ms, "spot_parity_mismatches": mismatches,
-            "gpu_launches": int(launches), "clocks": clk}
+            "config": {"workload": "batched", "jobs": r["jobs"], "log_sizes": r["log_sizes"],
+                       "total_fr": r["total_fr"], "log2_total_fr": r["log2_total_fr"],
+                       "setup_s": r["setup_s"], "tuned": r["tuned"]},
+            "fr_per_s": r["fr_per_s"],
+            "plain": {"value": r["plain_jobs_per_s"], "unit": "jobs/s", "ms": r["plain_ms"]},
+            "speedup_vs_plain": r["speedup_vs_plain"],
+            "spot_parity_mismatches": r["spot_parity_mismatches"],
+            "gpu_launches": r["launches_per_batch"] * a.steps, "clocks": clk}
     print(json.dumps(line), flush=True)
-    b.close()
 
 
 # ---------------------------------------------------------------------------
 # The served form under open-loop Poisson arrivals.
 # ---------------------------------------------------------------------------
-def run_served(a):
-    import concurrent.futures as cf
-
+def _pct(v, p):
     import numpy as np
-    import torch
+    v = sorted(v)
+    return v[min(len(v) - 1, max(0, int(np.ceil(p * len(v))) - 1))]
 
-    from provekit_b200.prover import HostR1CS
+
+def served_compare(reqs, mults, budget, rng, max_inflight=8):
+    """Sequential plain proving (one request at a time on the server's one
+    slot) gives each request's service time and the sequential capacity; then
+    for every arrival-rate multiple of that capacity, an open-loop Poisson
+    stream of the same requests goes to a server with max_inflight slots,
+    against sequential proving under the same arrivals (FIFO, the measured
+    service times).  Latency is from submit to completion."""
+    import numpy as np
+
     from provekit_b200.server import ProofServer
-
-    torch.cuda.set_device(0)
-    rng = np.random.default_rng(a.seed)
-    logs = [int(x) for x in rng.integers(14, 23, size=a.requests)]
-    t0 = time.perf_counter()
-    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
-        reqs = list(ex.map(lambda i: HostR1CS(10_000 + i, 1 << logs[i], 1 << (logs[i] - 2)),
-                           range(a.requests)))
-    gen_s = time.perf_counter() - t0
-    free_b, _ = torch.cuda.mem_get_info()
-    budget = int(min(free_b * 0.8, 120e9))
-    # sequential plain proving: one request at a time (1 slot), service times
     srv = ProofServer(budget, max_inflight=1)
     srv.wait(srv.submit(reqs[0], whole_proof=True, blinding_seed=0, transcript_domain=0))  # warm-up
     service = []
@@ -1002,22 +1076,16 @@ def run_served(a):
         service.append((tm["done_ns"] - tm["submit_ns"]) * 1e-9)
     srv.close()
     cap = len(service) / sum(service)
-
-    def pct(v, p):
-        v = sorted(v)
-        return v[min(len(v) - 1, max(0, int(np.ceil(p * len(v))) - 1))]
-
     sweeps = []
-    for mult in (0.5, 1.0, 1.5, 2.0, 3.0):
+    for mult in mults:
         lam = cap * mult
         arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(reqs)))
-        # sequential plain proving under the same arrivals (FIFO, measured service times)
         fin, seq_lat = 0.0, []
         for t_arr, sv in zip(arrivals, service):
             start = max(t_arr, fin)
             fin = start + sv
             seq_lat.append(fin - t_arr)
-        srv = ProofServer(budget, max_inflight=8)
+        srv = ProofServer(budget, max_inflight=max_inflight)
         ids = [None] * len(reqs)
         t_start = time.perf_counter()
         for i, (t_arr, h) in enumerate(zip(arrivals, reqs)):
@@ -1033,19 +1101,52 @@ def run_served(a):
             svc.append((tm["done_ns"] - tm["admit_ns"]) * 1e-9)
         st = srv.stats()
         srv.close()
-        served_span = max(arrivals[-1], 0) + 0  # for reference only
         sweeps.append({
             "rate_per_s": lam, "rate_vs_sequential_capacity": mult,
-            "served": {"proofs_per_s": st["proofs_per_s"], "p50_ms": 1e3 * pct(lat, 0.5),
-                       "p99_ms": 1e3 * pct(lat, 0.99), "p999_ms": 1e3 * pct(lat, 0.999),
+            "served": {"proofs_per_s": st["proofs_per_s"], "p50_ms": 1e3 * _pct(lat, 0.5),
+                       "p99_ms": 1e3 * _pct(lat, 0.99), "p999_ms": 1e3 * _pct(lat, 0.999),
                        "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9,
-                       "queue_wait_ms": {"p50": 1e3 * pct(qwait, 0.5), "p99": 1e3 * pct(qwait, 0.99)},
-                       "service_ms": {"p50": 1e3 * pct(svc, 0.5), "p99": 1e3 * pct(svc, 0.99),
+                       "queue_wait_ms": {"p50": 1e3 * _pct(qwait, 0.5),
+                                         "p99": 1e3 * _pct(qwait, 0.99)},
+                       "service_ms": {"p50": 1e3 * _pct(svc, 0.5), "p99": 1e3 * _pct(svc, 0.99),
                                       "max": 1e3 * max(svc)}},
-            "sequential": {"proofs_per_s": len(reqs) / fin, "p50_ms": 1e3 * pct(seq_lat, 0.5),
-                           "p99_ms": 1e3 * pct(seq_lat, 0.99), "p999_ms": 1e3 * pct(seq_lat, 0.999)},
+            "sequential": {"proofs_per_s": len(reqs) / fin, "p50_ms": 1e3 * _pct(seq_lat, 0.5),
+                           "p99_ms": 1e3 * _pct(seq_lat, 0.99),
+                           "p999_ms": 1e3 * _pct(seq_lat, 0.999)},
         })
-        del served_span
+        s = sweeps[-1]
+        s["served_beats_sequential"] = (s["served"]["proofs_per_s"] >= s["sequential"]["proofs_per_s"]
+                                        and s["served"]["p99_ms"] <= s["sequential"]["p99_ms"])
+    return cap, sweeps
+
+
+def make_requests(seed, count, lo, hi):
+    """count synthetic R1CS requests, log2 constraints uniform on [lo, hi],
+    a quarter as many inputs, per-request seeds; generated on all host
+    threads."""
+    import concurrent.futures as cf
+
+    import numpy as np
+
+    from provekit_b200.prover import HostR1CS
+    rng = np.random.default_rng(seed)
+    logs = [int(x) for x in rng.integers(lo, hi + 1, size=count)]
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        reqs = list(ex.map(lambda i: HostR1CS(10_000 + i, 1 << logs[i], 1 << (logs[i] - 2)),
+                           range(count)))
+    return logs, reqs, rng
+
+
+def run_served(a):
+    import torch
+
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    logs, reqs, rng = make_requests(a.seed, a.requests, 14, 22)
+    gen_s = time.perf_counter() - t0
+    free_b, _ = torch.cuda.mem_get_info()
+    budget = int(min(free_b * 0.9, 180e9))
+    cap, sweeps = served_compare(reqs, (0.5, 1.0, 1.5, 2.0, 3.0), budget, rng)
     line = {"metric": "served form: open-loop Poisson prove requests (whole proofs: Spartan + WHIR), "
                       "log2 constraints uniform on [14, 22]; proofs/s and p50/p99/p99.9 latency vs "
                       "sequential plain-GPU proving",
@@ -1053,7 +1154,8 @@ def run_served(a):
             "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32/f64 (BN254 Fr: 8x32-bit limbs, products on the FP64 pipe)",
             "data": "synthetic R1CS (pkg_synthetic_r1cs)",
-            "config": {"workload": "served", "whir": "ff 3, rate 1/4, 128 bits, 10 PoW bits", "requests": len(reqs), "log2_constraints": logs,
+            "config": {"workload": "served", "whir": "ff 3, rate 1/4, 128 bits, 10 PoW bits",
+                       "requests": len(reqs), "log2_constraints": logs,
                        "hbm_budget_gb": budget / 1e9, "max_inflight": 8, "generation_s": gen_s},
             "sequential_capacity_per_s": cap, "sweeps": sweeps}
     print(json.dumps(line), flush=True)
@@ -1063,8 +1165,67 @@ def run_served(a):
 # NTT: 2^24 (the size whose FP64-roofline fraction is the transform's target)
 # and the 2^16 single-vector transform.
 # ---------------------------------------------------------------------------
-def run_ntt(a):
+def ntt_measure(L, stream, flush, logn, steps, warmup, dfma_rate, imad_rate):
+    """ntt_nr at 2^logn (one vector, L2 flushed between steps, CUDA events on
+    the launching stream) and intt_rn on its output with the round trip
+    checked; throughput against the FP64-pipe roofline (measured DFMA rate /
+    binary64 instructions per product) and the integer-pipe one (measured
+    IMAD rate / 264 per 8x32 CIOS product)."""
     import numpy as np
+    import torch
+
+    from provekit_b200._lib import check
+    n = 1 << logn
+    h = np.zeros((n, 4), np.uint64)
+    check(L.pkg_sample_fr(1 if logn == 16 else logn, n, h.ctypes.data, 1))
+    src_t = torch.from_numpy(h.view(np.int64)).cuda()
+    d = torch.empty_like(src_t)
+    check(L.pkg_ntt_engine_reserve(n))
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            d.copy_(src_t)
+            check(L.pkg_ntt_nr(d.data_ptr(), n, n, 1, stream.cuda_stream))
+    stream.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for i in range(steps):
+            d.copy_(src_t)
+            flush.zero_()
+            evs[i][0].record(stream)
+            check(L.pkg_ntt_nr(d.data_ptr(), n, n, 1, stream.cuda_stream))
+            evs[i][1].record(stream)
+    stream.synchronize()
+    ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    evi = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for i in range(steps):
+            d.copy_(src_t)
+            check(L.pkg_ntt_nr(d.data_ptr(), n, n, 1, stream.cuda_stream))
+            flush.zero_()
+            evi[i][0].record(stream)
+            check(L.pkg_intt_rn(d.data_ptr(), n, stream.cuda_stream))
+            evi[i][1].record(stream)
+        ok = bool(torch.equal(d, src_t))
+    stream.synchronize()
+    ms_inv = statistics.mean(e[0].elapsed_time(e[1]) for e in evi)
+    products = (n // 2) * logn
+    rate = products / (ms * 1e-3)
+    del d, src_t
+    return {"log2_n": logn, "ms": ms, "fr_per_s": n / (ms * 1e-3), "gmont_per_s": rate / 1e9,
+            "frac_fp64": rate / (dfma_rate / F64_PER_MUL),
+            "frac_int": rate / (imad_rate / IMAD_PER_MONT),
+            "peak_gmont_fp64": dfma_rate / F64_PER_MUL / 1e9,
+            "peak_gmont_int": imad_rate / IMAD_PER_MONT / 1e9,
+            "hbm_gbs": 2 * 32 * n * ((logn + 8) // 9) / (ms * 1e-3) / 1e9,
+            "intt_rn_ms": ms_inv, "round_trip_ok": ok,
+            "note": "CUDA events around one ntt_nr launch sequence, L2 flushed (256 MiB write) "
+                    "before each; frac_fp64 against the measured binary64 fma rate / "
+                    f"{F64_PER_MUL} per product (the butterflies multiply on the FP64 pipe), "
+                    f"frac_int against the measured IMAD rate / {IMAD_PER_MONT} per 8x32 CIOS "
+                    "product (the north star's integer roofline)"}
+
+
+def run_ntt(a):
     import torch
 
     from provekit_b200 import _lib
@@ -1077,53 +1238,9 @@ def run_ntt(a):
     check(L.pkg_measure_imad_rate(ctypes.byref(imad)))
     dfma = ctypes.c_double(0)
     check(L.pkg_measure_dfma_rate(ctypes.byref(dfma)))
-    mont_peak = imad.value / IMAD_PER_MONT
-    f64_peak = dfma.value / F64_PER_MUL  # butterfly products per second on the FP64 pipe
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    out = {}
-    for logn in (24, 16):
-        n = 1 << logn
-        h = np.zeros((n, 4), np.uint64)
-        check(L.pkg_sample_fr(1 if logn == 16 else 24, n, h.ctypes.data, 1))
-        src = torch.from_numpy(h.view(np.int64)).cuda()
-        d = torch.empty_like(src)
-        check(L.pkg_ntt_engine_reserve(n))
-        with torch.cuda.stream(stream):
-            for _ in range(a.warmup):
-                d.copy_(src)
-                check(L.pkg_ntt_nr(d.data_ptr(), n, n, 1, stream.cuda_stream))
-        stream.synchronize()
-        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
-        with torch.cuda.stream(stream):
-            for i in range(a.steps):
-                d.copy_(src)
-                flush.zero_()
-                evs[i][0].record(stream)
-                check(L.pkg_ntt_nr(d.data_ptr(), n, n, 1, stream.cuda_stream))
-                evs[i][1].record(stream)
-        stream.synchronize()
-        ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
-        # intt_rn round trip on the transform's output (ntt/src/ntt.rs:326-348)
-        evi = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(a.steps)]
-        ok = True
-        with torch.cuda.stream(stream):
-            for i in range(a.steps):
-                d.copy_(src)
-                check(L.pkg_ntt_nr(d.data_ptr(), n, n, 1, stream.cuda_stream))
-                flush.zero_()
-                evi[i][0].record(stream)
-                check(L.pkg_intt_rn(d.data_ptr(), n, stream.cuda_stream))
-                evi[i][1].record(stream)
-            ok = bool(torch.equal(d, src))
-        stream.synchronize()
-        ms_inv = statistics.mean(e[0].elapsed_time(e[1]) for e in evi)
-        products = (n // 2) * logn
-        out[logn] = {"ms": ms, "fr_per_s": n / (ms * 1e-3), "gmont_per_s": products / (ms * 1e-3) / 1e9,
-                     "roofline_frac": products / (ms * 1e-3) / f64_peak,
-                     "int_pipe_frac": products / (ms * 1e-3) / mont_peak,
-                     "hbm_gbs": 2 * 32 * n * ((logn + 8) // 9) / (ms * 1e-3) / 1e9,
-                     "intt_rn_ms": ms_inv, "intt_fr_per_s": n / (ms_inv * 1e-3),
-                     "round_trip_ok": ok}
+    out = {logn: ntt_measure(L, stream, flush, logn, a.steps, a.warmup, dfma.value, imad.value)
+           for logn in (24, 16)}
     line = {"metric": "BN254 Fr ntt_nr throughput, 2^24 (roofline target) and 2^16 (single vector)",
             "value": out[24]["fr_per_s"], "unit": "Fr/s", "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": out[24]["ms"], "higher_is_better": True,
@@ -1131,14 +1248,15 @@ def run_ntt(a):
             "data": "synthetic (ChaCha20-seeded Fr)",
             "config": {"workload": "ntt", "log2_n": 24, "l2": "flushed between steps"},
             "roofline": {"kernel": "ntt_pass_kernel", "bound": "fp64",
-                         "achieved": out[24]["gmont_per_s"], "peak": f64_peak / 1e9,
-                         "unit": "Gmont/s", "frac": out[24]["roofline_frac"],
+                         "achieved": out[24]["gmont_per_s"],
+                         "peak": out[24]["peak_gmont_fp64"],
+                         "unit": "Gmont/s", "frac": out[24]["frac_fp64"],
                          "algorithmic": f"(n/2) log2 n Montgomery products per transform, "
                                         f"{F64_PER_MUL} binary64 instructions each",
                          "peak_source": f"measured binary64 fma rate {dfma.value / 1e12:.3f} T/s "
                                         f"(pkg_measure_dfma_rate) / {F64_PER_MUL}",
-                         "int_pipe_alt": {"peak_gmont_per_s": mont_peak / 1e9,
-                                          "frac": out[24]["int_pipe_frac"]}},
+                         "int_pipe_alt": {"peak_gmont_per_s": out[24]["peak_gmont_int"],
+                                          "frac": out[24]["frac_int"]}},
             "ntt_2p24": out[24], "ntt_2p16": out[16]}
     print(json.dumps(line), flush=True)
 

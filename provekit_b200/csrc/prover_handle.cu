@@ -136,13 +136,16 @@ struct Reader {
   }
 };
 
-// Fr in the Spartan part of a proof: m0 challenges r, 4 m0 round
-// coefficients, m0 challenges alpha, rho, sum_g, blinding_eval, public_x,
-// 3 evaluations, public_hash, public_eval, the transcript (2 Fr).
-size_t spartan_fr(size_t m0) { return 6 * m0 + 12; }
+// Fr in the Spartan part of a proof after the root: m0 challenges r, 4 m0
+// round coefficients, m0 challenges alpha, rho, sum_g, blinding_eval,
+// public_x, 3 evaluations, public_hash, public_eval, the transcript (2 Fr).
+size_t spartan_fr(size_t m0) { return 6 * m0 + 11; }
+
+// magic, version, reserved word, seven u64 fields
+constexpr size_t kProofHeader = 8 + 4 + 4 + 7 * 8;
 
 size_t proof_bytes(const pkg_prover* p, size_t nstm) {
-  return 64 + 104 + 32 + 32 * spartan_fr(p->m0) + 8 * pkg_whir_commit_words(&p->whir) +
+  return kProofHeader + 104 + 32 + 32 * spartan_fr(p->m0) + 8 * pkg_whir_commit_words(&p->whir) +
          8 * pkg_whir_proof_words(&p->whir, nstm);
 }
 
@@ -327,7 +330,7 @@ extern "C" int pkg_prover_prove(pkg_prover* p, const uint64_t* witness, uint64_t
   }
   const size_t cwords = pkg_whir_commit_words(&p->whir);
   const size_t pwords = pkg_whir_proof_words(&p->whir, nstm);
-  uint8_t* spartan_at = buf + 64 + 104;
+  uint8_t* spartan_at = buf + kProofHeader + 104;
   uint64_t* commit_at = reinterpret_cast<uint64_t*>(spartan_at + 32 + 32 * spartan_fr(p->m0));
   uint64_t* proof_at = commit_at + cwords;
   // the witness through the host stager (pinned chunks, threaded host

@@ -112,4 +112,8 @@ def test_explicit_release_then_reuse():
     assert after[0] < before[0] and after[1] < before[1]
     b = prove_r1cs(d, p, blinding_seed=4, transcript_domain=6)
     assert (a[1] == b[1]).all() and (a[2] == b[2]).all()
-    assert totals() == before
+    # re-created for this proof: the device block at its fixed size; the
+    # staging buffer at this proof's size (earlier, larger proofs of this
+    # thread had grown it)
+    again = totals()
+    assert again[1] == before[1] and after[0] < again[0] <= before[0]
