@@ -1115,8 +1115,9 @@ def served_compare(reqs, mults, budget, rng, max_inflight=8):
                            "p999_ms": 1e3 * _pct(seq_lat, 0.999)},
         })
         s = sweeps[-1]
-        s["served_beats_sequential"] = (s["served"]["proofs_per_s"] >= s["sequential"]["proofs_per_s"]
-                                        and s["served"]["p99_ms"] <= s["sequential"]["p99_ms"])
+        s["served_beats_sequential"] = bool(
+            s["served"]["proofs_per_s"] >= s["sequential"]["proofs_per_s"]
+            and s["served"]["p99_ms"] <= s["sequential"]["p99_ms"])
     return cap, sweeps
 
 
