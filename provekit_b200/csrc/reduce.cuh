@@ -10,6 +10,7 @@
 #include <algorithm>
 
 #include "fr.cuh"
+#include "fr_f64.cuh"
 #include "pk_common.cuh"
 
 namespace pk {
@@ -71,11 +72,17 @@ __device__ __forceinline__ Fr fr_load_cg(const uint64_t* base, size_t idx) {
 
 // The end of a reduction kernel: block sum, the CTA's partial, and with a
 // ticket the last CTA's final sum.  Every thread of the CTA calls it.
+// scale (or nullptr): each CTA sum is multiplied by it (Montgomery product)
+// before it is stored -- the 2^8 that lazily reduced sums (fr_lazy.cuh) owe.
 template <int K>
-__device__ __forceinline__ void block_finish(Fr (&v)[K], const RedOut& ro) {
+__device__ __forceinline__ void block_finish(Fr (&v)[K], const RedOut& ro,
+                                             const Fr* scale = nullptr) {
   __shared__ bool last;
   block_sum<K>(v);
   if (threadIdx.x == 0) {
+    if (scale)
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = fr_mul_f64(v[k], *scale);
 #pragma unroll
     for (int k = 0; k < K; k++) fr_store(ro.part, (size_t)blockIdx.x * K + k, v[k]);
     if (ro.ticket) {

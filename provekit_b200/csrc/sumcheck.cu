@@ -22,6 +22,7 @@
 #include "fr.cuh"
 #include "fr_f64.cuh"
 #include "fr_host.hpp"
+#include "fr_lazy.cuh"
 #include "pk_common.cuh"
 #include "reduce.cuh"
 #include "sky_host.hpp"
@@ -141,14 +142,29 @@ __global__ void hadamard_pad_kernel(const uint64_t* __restrict__ a, const uint64
     fr_store(c, i, i < n ? fr_mul_f64(fr_load_ro(a, i), fr_load_ro(b, i)) : fr_zero());
 }
 
+// The products are summed unreduced (fr_lazy.cuh) and reduced once per
+// thread; each CTA's sum is then scaled by 2^8 (the lazy reduction divides
+// by 2^264 where a Montgomery product divides by 2^256).
 __global__ void __launch_bounds__(kRedThreads) dot_kernel(const uint64_t* __restrict__ a,
                                                         const uint64_t* __restrict__ b, size_t n,
                                                         const RedOut ro) {
   Fr acc[1] = {fr_zero()};
+  lazy::Acc la;
+  la.zero();
+  int terms = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    acc[0] = fr_add(acc[0], fr_mul_f64(fr_load_ro(a, i), fr_load_ro(b, i)));
-  block_finish<1>(acc, ro);
+       i += (size_t)gridDim.x * blockDim.x) {
+    la.mac(fr_load_ro(a, i), fr_load_ro(b, i));
+    if (++terms % lazy::kCarryEvery == 0) la.carry();
+    if (terms == lazy::kMaxTerms) {
+      acc[0] = fr_add(acc[0], la.finish());
+      la.zero();
+      terms = 0;
+    }
+  }
+  if (terms) acc[0] = fr_add(acc[0], la.finish());
+  const Fr s8 = lazy::mont_2e8();
+  block_finish<1>(acc, ro, &s8);
 }
 
 // ---- CSR transpose: count, exclusive scan, scatter ------------------------

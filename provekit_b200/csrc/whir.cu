@@ -15,12 +15,14 @@
 //                            evaluations at 0, 1, 2 (utilities.go:149-171)
 //   pkg_eq_accumulate        w += sum_j c_j eq(p_j, .) for new constraints
 //   pkg_stir_indices         getStirChallenges (whir_utilities.go:49-79), host
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
 #include "fr.cuh"
 #include "fr_f64.cuh"
 #include "fr_host.hpp"
+#include "fr_lazy.cuh"
 #include "internal.cuh"
 #include "pk_common.cuh"
 #include "reduce.cuh"
@@ -224,6 +226,37 @@ __global__ void eq_accumulate_kernel(uint64_t* __restrict__ w, size_t n, int nlo
     fr_store(w, b, fr_add(acc, acc2));
   }
 }
+
+// The same sum with the products accumulated unreduced (fr_lazy.cuh) and
+// reduced once per chunk of lazy::kMaxTerms points: the hi tables carry the
+// coefficients times 2^8, which the lazy reduction's 2^-264 takes back to
+// a Montgomery product's 2^-256.
+__global__ void __launch_bounds__(128, 4) eq_accumulate_lazy_kernel(
+    uint64_t* __restrict__ w, size_t n, int nlo, const uint64_t* __restrict__ hi,
+    size_t nhi_entries, const uint64_t* __restrict__ lo, size_t npts) {
+  const size_t nlo_entries = size_t(1) << nlo;
+  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < n;
+       b += (size_t)gridDim.x * blockDim.x) {
+    const size_t bh = b >> nlo, bl = b & (nlo_entries - 1);
+    Fr sum = fr_load(w, b);
+    for (size_t j0 = 0; j0 < npts; j0 += lazy::kMaxTerms) {
+      const size_t j1 = npts - j0 < (size_t)lazy::kMaxTerms ? npts : j0 + lazy::kMaxTerms;
+      lazy::Acc acc;
+      acc.zero();
+#pragma unroll 1
+      for (size_t j = j0; j < j1; j++) {
+        acc.mac(fr_load_ro(hi, j * nhi_entries + bh), fr_load_ro(lo, j * nlo_entries + bl));
+        if ((j - j0) % lazy::kCarryEvery == lazy::kCarryEvery - 1) acc.carry();
+      }
+      sum = fr_add(sum, acc.finish());
+    }
+    fr_store(w, b, sum);
+  }
+}
+
+// Points at and above which the lazy sum is cheaper than a product per term
+// (its one reduction per entry costs about a product).
+constexpr size_t kLazyEqMinPoints = 4;
 
 }  // namespace pk
 
@@ -451,14 +484,31 @@ int eq_accumulate_device(uint64_t* w, size_t nv, const uint64_t* points, const u
     expand_points_kernel<<<ew_grid(npts), 256, 0, s>>>(d_raw, npts, nv, d_pts);
     PK_CHECK_LAUNCH("expand_points_kernel");
   }
-  PK_CUDA(cudaMemcpyAsync(d_cf, coeffs, 32 * npts, cudaMemcpyHostToDevice, s));
-  // hi tables carry the coefficient, lo tables are plain eq tables
+  // hi tables carry the coefficient (times 2^8 for the lazy sum), lo tables
+  // are plain eq tables
+  const bool use_lazy = npts >= kLazyEqMinPoints;
+  if (use_lazy) {
+    // pageable: staged before cudaMemcpyAsync returns
+    std::vector<HostFr> cf8(npts);
+    const HostFr m8 = HostFr::from_limbs(lazy::kMont2e8);
+    for (size_t j = 0; j < npts; j++) cf8[j] = HostFr::mul(HostFr::from_limbs(coeffs + 4 * j), m8);
+    PK_CUDA(cudaMemcpyAsync(d_cf, cf8[0].l, 32 * npts, cudaMemcpyHostToDevice, s));
+  } else {
+    PK_CUDA(cudaMemcpyAsync(d_cf, coeffs, 32 * npts, cudaMemcpyHostToDevice, s));
+  }
   eq_tables_kernel<<<ew_grid(npts * nh), 256, 0, s>>>(d_pts, nv, 0, nhi, d_cf, npts, d_hi);
   PK_CHECK_LAUNCH("eq_tables_kernel");
   eq_tables_kernel<<<ew_grid(npts * nl), 256, 0, s>>>(d_pts, nv, nhi, nlo, nullptr, npts, d_lo);
   PK_CHECK_LAUNCH("eq_tables_kernel");
-  eq_accumulate_kernel<<<ew_grid(n), 256, 0, s>>>(w, n, nlo, d_hi, nh, d_lo, npts);
-  PK_CHECK_LAUNCH("eq_accumulate_kernel");
+  if (use_lazy) {
+    const int grid = (int)std::max<size_t>(
+        1, std::min<size_t>((n + 127) / 128, (size_t)sm_count() * 4 * 8));
+    eq_accumulate_lazy_kernel<<<grid, 128, 0, s>>>(w, n, nlo, d_hi, nh, d_lo, npts);
+    PK_CHECK_LAUNCH("eq_accumulate_lazy_kernel");
+  } else {
+    eq_accumulate_kernel<<<ew_grid(n), 256, 0, s>>>(w, n, nlo, d_hi, nh, d_lo, npts);
+    PK_CHECK_LAUNCH("eq_accumulate_kernel");
+  }
   // host sources in pinned memory must outlive their async copies; pageable
   // ones are staged before cudaMemcpyAsync returns
   if (sync) PK_CUDA(cudaStreamSynchronize(s));

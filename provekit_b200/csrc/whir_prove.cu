@@ -27,6 +27,7 @@
 #include "fr.cuh"
 #include "fr_f64.cuh"
 #include "fr_host.hpp"
+#include "fr_lazy.cuh"
 #include "internal.cuh"
 #include "pk_common.cuh"
 #include "reduce.cuh"
@@ -105,6 +106,55 @@ __global__ void combine_covectors_kernel(uint64_t* __restrict__ w, size_t n,
     }
     fr_store(w, b, acc);
   }
+}
+
+// The same sum with the products accumulated unreduced and reduced once per
+// entry (fr_lazy.cuh); the coefficients carry a factor 2^8 (see
+// combine_covectors).
+__global__ void __launch_bounds__(128, 4) combine_covectors_lazy_kernel(
+    uint64_t* __restrict__ w, size_t n, const __grid_constant__ CovParams P) {
+  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < n;
+       b += (size_t)gridDim.x * blockDim.x) {
+    lazy::Acc acc;
+    acc.zero();
+    for (int a = 0; a < P.ncov; a++) {
+      Fr c;
+#pragma unroll
+      for (int i = 0; i < 8; i++) c.v[i] = P.coef[a][i];
+      acc.mac(c, fr_load_ro(P.cov, (size_t)a * P.stride + b));
+    }
+    fr_store(w, b, acc.finish());  // kMaxCovectors < kCarryEvery: no carry needed
+  }
+}
+
+static_assert(kMaxCovectors < lazy::kCarryEvery, "one carry-free lazy sum per entry");
+
+// w = sum_a coefs[a] cov[a] over n entries (coefs host, Montgomery form):
+// the lazy sum from four covectors on, where its one reduction per entry
+// costs less than the products it saves.
+static int combine_covectors(uint64_t* w, size_t n, const uint64_t* cov, size_t stride,
+                             const HostFr* coefs, size_t ncov, cudaStream_t s) {
+  CovParams P;
+  memset(&P, 0, sizeof P);
+  P.cov = cov;
+  P.stride = stride;
+  P.ncov = (int)ncov;
+  const bool use_lazy = ncov >= 4;
+  const HostFr m8 = HostFr::from_limbs(lazy::kMont2e8);
+  for (size_t a = 0; a < ncov; a++) {
+    const HostFr c = use_lazy ? HostFr::mul(coefs[a], m8) : coefs[a];
+    memcpy(P.coef[a], c.l, 32);
+  }
+  if (use_lazy) {
+    const int grid = (int)std::max<size_t>(
+        1, std::min<size_t>((n + 127) / 128, (size_t)sm_count() * 4 * 8));
+    combine_covectors_lazy_kernel<<<grid, 128, 0, s>>>(w, n, P);
+    PK_CHECK_LAUNCH("combine_covectors_lazy_kernel");
+  } else {
+    combine_covectors_kernel<<<ew_grid(n), 256, 0, s>>>(w, n, P);
+    PK_CHECK_LAUNCH("combine_covectors_kernel");
+  }
+  return PKG_OK;
 }
 
 // t[i] += r (t[i + h] - t[i]) for both tables: bind the top variable.
@@ -388,14 +438,7 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
       powers_of(nb > 1 ? HostFr::from_limbs(ood_points + 4 * o) : HostFr::one(), nb);
   if (nb > 1) {
     PK_TRY(Cb.alloc(32 * N, s_));
-    CovParams P;
-    memset(&P, 0, sizeof P);
-    P.cov = coeffs;
-    P.stride = N;
-    P.ncov = (int)nb;
-    for (unsigned i = 0; i < nb; i++) memcpy(P.coef[i], bp[i].l, 32);
-    combine_covectors_kernel<<<ew_grid(N), 256, 0, s_>>>(Cb.as<uint64_t>(), N, P);
-    PK_CHECK_LAUNCH("combine_covectors_kernel");
+    PK_TRY(combine_covectors(Cb.as<uint64_t>(), N, coeffs, N, bp.data(), nb, s_));
     poly = Cb.as<uint64_t>();
   }
   if (hat && nb == 1) {
@@ -421,14 +464,7 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
   gamma = absorb_squeeze(t_, vals.data(), ncov * nb);
   pw = powers_of(gamma, o + ncov);
   if (ncov) {
-    CovParams P;
-    memset(&P, 0, sizeof P);
-    P.cov = covectors;
-    P.stride = N;
-    P.ncov = (int)ncov;
-    for (size_t a = 0; a < ncov; a++) memcpy(P.coef[a], pw[o + a].l, 32);
-    combine_covectors_kernel<<<ew_grid(N), 256, 0, s_>>>(w_, N, P);
-    PK_CHECK_LAUNCH("combine_covectors_kernel");
+    PK_TRY(combine_covectors(w_, N, covectors, N, pw.data() + o, ncov, s_));
     PK_TRY(subset_transform_device<false>(w_, n, s_));
   } else {
     PK_CUDA(cudaMemsetAsync(w_, 0, 32 * N, s_));

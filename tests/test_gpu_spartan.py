@@ -113,6 +113,32 @@ def test_hadamard_and_dot():
     assert np.array_equal(dot(dev(a), dev(b)), exp)
 
 
+@pytest.mark.parametrize("n", [1, 7, 33, 5_000_011])
+def test_dot_lazy_sums_match_oracle(n):
+    """pkg_dot sums its products unreduced and reduces once per thread; at
+    5M entries every thread sums more than 32 terms (the carry step)."""
+    from provekit_b200.spartan import dot
+    a, b = O.sample_fr(30 + n % 7, n), O.sample_fr(31 + n % 5, n)
+    exp = np.zeros(4, np.uint64)
+    O.lib().pko_dot(O.p64(exp), O.p64(a), O.p64(b), n)
+    assert np.array_equal(dot(dev(a), dev(b)), exp)
+
+
+def test_dot_of_maximal_values_past_one_lazy_chunk():
+    """2^28 + 3 entries of p - 1 (Montgomery limbs) in both vectors: the
+    largest operands, and more than 1024 terms per thread, so each thread
+    finishes several lazy sums.  The expected value is computed in Python
+    integers: n (p-1)^2 2^-256 mod p."""
+    from provekit_b200.spartan import dot
+    n = (1 << 28) + 3
+    pm1 = np.array([P - 1 >> (64 * i) & (2**64 - 1) for i in range(4)], np.uint64)
+    a = torch.from_numpy(pm1.view(np.int64)).cuda().reshape(1, 4).expand(n, 4).contiguous()
+    got = unpack(dot(a, a).reshape(1, 4))[0]
+    del a
+    torch.cuda.empty_cache()
+    assert got == n * (P - 1) ** 2 * pow(2, -256, P) % P
+
+
 @pytest.mark.parametrize("size,fold", [(2, False), (4, False), (4, True), (8, True), (1 << 12, True), (1 << 20, False), (1 << 20, True)])
 def test_spartan_round(size, fold):
     from provekit_b200.spartan import spartan_round

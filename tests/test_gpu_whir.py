@@ -161,8 +161,11 @@ def test_sumcheck_rounds_match_oracle_to_the_end():
 
 
 def test_eq_accumulate_matches_oracle():
+    """Fewer than four points take a product per term; from four on the
+    products are summed unreduced (fr_lazy.cuh), past 32 points with carry
+    steps and past 1024 in several lazy chunks."""
     from provekit_b200.whir import eq_accumulate
-    for nv, npts in ((0, 2), (1, 3), (9, 7), (17, 40)):
+    for nv, npts in ((0, 2), (1, 3), (9, 7), (17, 40), (3, 4), (6, 33), (4, 1100), (12, 119)):
         w = O.sample_fr(900 + nv, 1 << nv)
         pts = O.sample_fr(901, max(npts * nv, 1))[: npts * nv]
         cf = O.sample_fr(902, npts)
