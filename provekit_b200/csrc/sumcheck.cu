@@ -389,6 +389,38 @@ static void blinding_coeffs(const HostFr* g, size_t n, size_t compute_for, const
   for (int k = 0; k < 4; k++) out[k] = res[k];
 }
 
+// Tables of at most this many entries finish their rounds on the host.
+constexpr size_t kHostTailEntries = 64;
+
+// spartan_round_kernel on host tables: with fold, bind the top variable
+// first (t[j] += fold (t[j + size/2] - t[j])) and halve size; then the sums
+// f(0), f(-1), f(inf) over the pairs (j, j + size/2) (whir_r1cs.rs:552-558),
+// as canonical Montgomery limbs into out.
+static void host_spartan_round(std::vector<HostFr> (&t)[4], size_t size, const HostFr* fold,
+                               uint64_t out[12]) {
+  if (fold) {
+    const size_t h = size / 2;
+    for (auto& v : t)
+      for (size_t j = 0; j < h; j++) v[j] = HostFr::add(v[j], HostFr::mul(*fold, HostFr::sub(v[j + h], v[j])));
+    size = h;
+  }
+  const size_t q = size / 2;
+  HostFr f0 = HostFr::zero(), fm1 = HostFr::zero(), finf = HostFr::zero();
+  for (size_t j = 0; j < q; j++) {
+    const HostFr a0 = t[0][j], a1 = t[0][j + q], b0 = t[1][j], b1 = t[1][j + q];
+    const HostFr c0 = t[2][j], c1 = t[2][j + q], e0 = t[3][j], e1 = t[3][j + q];
+    f0 = HostFr::add(f0, HostFr::mul(e0, HostFr::sub(HostFr::mul(a0, b0), c0)));
+    const HostFr a2 = HostFr::sub(HostFr::add(a0, a0), a1), b2 = HostFr::sub(HostFr::add(b0, b0), b1);
+    const HostFr c2 = HostFr::sub(HostFr::add(c0, c0), c1), e2 = HostFr::sub(HostFr::add(e0, e0), e1);
+    fm1 = HostFr::add(fm1, HostFr::mul(e2, HostFr::sub(HostFr::mul(a2, b2), c2)));
+    finf = HostFr::add(finf, HostFr::mul(HostFr::sub(e1, e0),
+                                         HostFr::mul(HostFr::sub(a1, a0), HostFr::sub(b1, b0))));
+  }
+  memcpy(out, f0.l, 32);
+  memcpy(out + 4, fm1.l, 32);
+  memcpy(out + 8, finf.l, 32);
+}
+
 }  // namespace pk
 
 using namespace pk;
@@ -602,11 +634,26 @@ extern "C" int pkg_spartan_sumcheck(uint64_t* a, uint64_t* b, uint64_t* c, size_
   // the blinding coefficients' two sums, kept as running sums over the rounds
   HostFr bprefix = HostFr::zero(), bsuffix = HostFr::zero();
   for (size_t i = 1; i < m0; i++) bsuffix = HostFr::add(bsuffix, cubic_sum01(&gv[4 * i]));
+  // the last rounds, on tables of at most kHostTailEntries, run on the host
+  // (a device round there is launch and round-trip latency)
+  std::vector<HostFr> tab[4];
+  bool on_host = false;
   for (size_t idx = 0; idx < m0; idx++) {  // :550-610
-    rc = spartan_round_device(a, b, c, eq, size, idx ? alpha[idx - 1].l : nullptr, part, fs.dev, s,
-                              fs.ticket);
-    if (rc) return rc;
-    if ((rc = fused_read(h, fs, 96, s))) return rc;
+    if (!on_host && size <= kHostTailEntries) {
+      for (int k = 0; k < 4; k++) tab[k].resize(size);
+      const HostRead reads[4] = {{tab[0][0].l, a, 32 * size}, {tab[1][0].l, b, 32 * size},
+                                 {tab[2][0].l, c, 32 * size}, {tab[3][0].l, eq, 32 * size}};
+      if ((rc = read_small(reads, 4, s))) return rc;
+      on_host = true;
+    }
+    if (on_host) {
+      host_spartan_round(tab, size, idx ? &alpha[idx - 1] : nullptr, h);
+    } else {
+      rc = spartan_round_device(a, b, c, eq, size, idx ? alpha[idx - 1].l : nullptr, part, fs.dev,
+                                s, fs.ticket);
+      if (rc) return rc;
+      if ((rc = fused_read(h, fs, 96, s))) return rc;
+    }
     if (idx) size /= 2;
     HostFr gp[4];
     if (idx) {

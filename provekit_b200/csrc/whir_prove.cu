@@ -294,7 +294,7 @@ class WhirProver {
     memcpy(out_ + pos_, x.l, 32);
     pos_ += 4;
   }
-  int sumcheck_phase(unsigned rounds, std::vector<HostFr>& rands);
+  int sumcheck_phase(unsigned rounds, std::vector<HostFr>& rands, bool last = false);
   int pow_step(unsigned bits);
   int stir_step(size_t q, size_t L, size_t row, const uint64_t* cw, const uint8_t* layers,
                 std::vector<uint64_t>& idx);
@@ -318,12 +318,58 @@ class WhirProver {
   size_t size_ = 0;
 };
 
+// Tables of at most this many entries run the proof's last sumcheck on the
+// host (a device round there is launch and round-trip latency).
+constexpr size_t kHostTailEntries = 64;
+
+// whir_round_kernel on host tables: fold the top variable by fold (if any,
+// halving size), then h(0), h(1), h(2) of sum_b f(X, b) w(X, b).
+static void host_whir_round(std::vector<HostFr>& f, std::vector<HostFr>& w, size_t& size,
+                            const HostFr* fold, uint64_t out[12]) {
+  if (fold) {
+    const size_t h = size / 2;
+    for (auto* t : {&f, &w})
+      for (size_t j = 0; j < h; j++)
+        (*t)[j] = HostFr::add((*t)[j], HostFr::mul(*fold, HostFr::sub((*t)[j + h], (*t)[j])));
+    size = h;
+  }
+  const size_t q = size / 2;
+  HostFr h0 = HostFr::zero(), h1 = HostFr::zero(), h2 = HostFr::zero();
+  for (size_t j = 0; j < q; j++) {
+    const HostFr f0 = f[j], f1 = f[j + q], w0 = w[j], w1 = w[j + q];
+    h0 = HostFr::add(h0, HostFr::mul(f0, w0));
+    h1 = HostFr::add(h1, HostFr::mul(f1, w1));
+    h2 = HostFr::add(h2, HostFr::mul(HostFr::sub(HostFr::add(f1, f1), f0),
+                                     HostFr::sub(HostFr::add(w1, w1), w0)));
+  }
+  memcpy(out, h0.l, 32);
+  memcpy(out + 4, h1.l, 32);
+  memcpy(out + 8, h2.l, 32);
+}
+
 // k rounds of the weighted sumcheck (runWhirSumcheckRounds,
 // circuit/whir_utilities.go:103-126): send h(0), h(1), h(2), draw r.  The fold
-// by r rides on the next round's kernel; the last one is done here.
-int WhirProver::sumcheck_phase(unsigned rounds, std::vector<HostFr>& rands) {
+// by r rides on the next round's kernel; the last one is done here.  The
+// proof's last phase (last: nothing reads the tables afterwards) runs on
+// the host when its tables are small.
+int WhirProver::sumcheck_phase(unsigned rounds, std::vector<HostFr>& rands, bool last) {
   rands.clear();
   rands.reserve(rounds);
+  if (last && rounds && size_ <= kHostTailEntries) {
+    std::vector<HostFr> f(size_), w(size_);
+    const HostRead reads[2] = {{f[0].l, E_, 32 * size_}, {w[0].l, w_, 32 * size_}};
+    PK_TRY(read_small(reads, 2, s_));
+    size_t size = size_;
+    for (unsigned i = 0; i < rounds; i++) {
+      uint64_t h[12];
+      host_whir_round(f, w, size, i ? &rands.back() : nullptr, h);
+      memcpy(out_ + pos_, h, 96);
+      pos_ += 12;
+      HostFr hs[3] = {HostFr::from_limbs(h), HostFr::from_limbs(h + 4), HostFr::from_limbs(h + 8)};
+      rands.push_back(absorb_squeeze(t_, hs, 3));
+    }
+    return PKG_OK;
+  }
   const uint64_t* pending = nullptr;
   HostFr r;
   for (unsigned i = 0; i < rounds; i++) {
@@ -582,7 +628,7 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
   {
     PhaseTimer pt(1);
     std::vector<HostFr> rfin;
-    PK_TRY(sumcheck_phase(nv, rfin));
+    PK_TRY(sumcheck_phase(nv, rfin, true));
     PK_CUDA(cudaStreamSynchronize(s_));
   }
   // the staged openings into their places
