@@ -35,14 +35,30 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-I", os.path.join(ROOT, "include"), "-o", LIB, *sources(), "-lcudart"]
+def _compile(src: str, obj: str, verbose: bool) -> None:
+    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-c",
+           "-I", os.path.join(ROOT, "include"), "-o", obj, src]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every translation unit to an object in parallel (each is
+    self-contained: no device code crosses files), then link the shared
+    library."""
+    import concurrent.futures as cf
+
+    if not force and up_to_date():
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(objdir, os.path.basename(c)[:-3] + ".o") for c in srcs]
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 4))) as ex:
+        for f in [ex.submit(_compile, c, o, verbose) for c, o in zip(srcs, objs)]:
+            f.result()
+    subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"], check=True)
     return LIB
 
 

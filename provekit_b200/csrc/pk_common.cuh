@@ -111,6 +111,12 @@ int pinned_stage(size_t bytes, PinnedStage** out);
 // pkg_thread_resource_bytes.
 void thread_resource_totals(size_t* host_bytes, size_t* device_bytes);
 
+// Allocates the calling thread's per-thread resources on the current device
+// now (fused slots and their device block, the bounce buffer, a pinned stage
+// of at least stage_bytes), so that a long-lived thread's first proof does
+// not pay for them.
+int warm_thread_resources(size_t stage_bytes);
+
 inline int read_small(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   const HostRead r{dst, src, bytes};
   return read_small(&r, 1, s);

@@ -278,18 +278,35 @@ int pinned_stage(size_t bytes, PinnedStage** out) {
   return PKG_OK;
 }
 
+// The bounce buffer of read_small, allocated on the thread's first use; a
+// thread that cannot get one copies directly.
+static void ensure_bounce(ThreadResources& tr) {
+  if (tr.bounce_tried) return;
+  tr.bounce_tried = true;
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, kBounceCap, cudaHostAllocPortable) == cudaSuccess) {
+    tr.bounce = static_cast<uint8_t*>(p);
+    g_res_host += (int64_t)kBounceCap;
+  } else {
+    cudaGetLastError();  // no bounce buffer: direct copies
+  }
+}
+
+int warm_thread_resources(size_t stage_bytes) {
+  FusedSlots f;
+  int rc = fused_slots(&f);
+  if (rc) return rc;
+#ifdef PK_DEBUG_FUSED
+  t_res.fused_busy = false;
+#endif
+  ensure_bounce(t_res);
+  PinnedStage* st = nullptr;
+  return pinned_stage(stage_bytes, &st);
+}
+
 int read_small(const HostRead* reads, int n, cudaStream_t s) {
   ThreadResources& tr = t_res;
-  if (!tr.bounce_tried) {
-    tr.bounce_tried = true;
-    void* p = nullptr;
-    if (cudaHostAlloc(&p, kBounceCap, cudaHostAllocPortable) == cudaSuccess) {
-      tr.bounce = static_cast<uint8_t*>(p);
-      g_res_host += (int64_t)kBounceCap;
-    } else {
-      cudaGetLastError();  // no bounce buffer: direct copies below
-    }
-  }
+  ensure_bounce(tr);
   size_t total = 0;
   for (int i = 0; i < n; i++) total += (reads[i].bytes + 15) & ~size_t(15);
   if (!tr.bounce || total > kBounceCap) {

@@ -220,10 +220,17 @@ static int run_request(HostRequest& r, cudaStream_t st) {
   return rc;
 }
 
+// Pinned staging each worker allocates at start: a whole proof's STIR
+// openings at 2^22 constraints take ~0.4 MB.
+constexpr size_t kWorkerStageBytes = size_t(1) << 20;
+
 static void worker_main(pkg_server* s) {
   cudaSetDevice(s->device);
   cudaStream_t st;
   cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  // the worker's per-thread buffers before its first request, not inside it
+  // (a failure here only leaves them to the first request)
+  if (warm_thread_resources(kWorkerStageBytes)) cudaGetLastError();
   for (;;) {
     std::shared_ptr<HostRequest> r;
     {
