@@ -8,9 +8,10 @@
 //   pkg_whir_commit               RS encode + Merkle tree of one polynomial
 //
 // One thread owns one compression chain (a leaf's left fold, or one node);
-// 32-byte chunks are read as two 128-bit vector loads.  The top of the tree
-// (<= kTopNodes nodes) is finished by one CTA in shared memory, so a tree
-// costs log2(leaves) - log2(kTopNodes) + 2 launches.
+// 32-byte chunks are read as two 128-bit vector loads.  Levels above
+// kSubtreeMax nodes take one launch each; below it one launch reduces
+// 256-node subtrees per CTA by eight levels, and one CTA finishes the top in
+// shared memory.
 #include <algorithm>
 #include <cstring>
 
@@ -135,6 +136,59 @@ __global__ void __launch_bounds__(512) merkle_top_kernel(const uint8_t* __restri
   }
 }
 
+// The levels from kSubtreeMax nodes down: each CTA (one warp per SM
+// sub-partition) reduces kSubNodes consecutive nodes of the current level by
+// kSubLevels levels in shared memory and writes every level's digests to
+// their slots, so the latency-bound small levels cost one launch instead of
+// one each; the kSubNodes-fold fewer subroots go to merkle_top_kernel.
+constexpr int kSubThreads = 128;
+constexpr int kSubNodes = 2 * kSubThreads;
+constexpr int kSubLevels = 8;  // kSubNodes = 2^kSubLevels
+constexpr size_t kSubtreeMax = size_t(1) << 15;
+static_assert(kSubNodes == 1 << kSubLevels, "a CTA reduces its nodes to one subroot");
+static_assert(kSubtreeMax / kSubNodes <= (size_t)kTopNodes, "the subroots fit the top kernel");
+
+__global__ void __launch_bounds__(kSubThreads) merkle_subtree_kernel(uint8_t* __restrict__ lvl,
+                                                                     size_t n) {
+  __shared__ uint4 buf[2 * kSubNodes];
+  const size_t c = blockIdx.x;  // this CTA's nodes: [c kSubNodes, (c + 1) kSubNodes)
+  for (int i = threadIdx.x; i < kSubNodes; i += blockDim.x) {
+    const uint4* q = reinterpret_cast<const uint4*>(lvl + 32 * (c * kSubNodes + i));
+    buf[2 * i] = q[0];
+    buf[2 * i + 1] = q[1];
+  }
+  __syncthreads();
+  uint8_t* level = lvl;  // first node of the current level
+  size_t level_n = n;
+  int cnt = kSubNodes;
+#pragma unroll 1
+  for (int l = 0; l < kSubLevels; l++) {
+    const int half = cnt / 2;
+    const int i = threadIdx.x;
+    Fr h;
+    if (i < half) {
+      Fr a, b;
+      const uint4 x0 = buf[4 * i], x1 = buf[4 * i + 1], y0 = buf[4 * i + 2], y1 = buf[4 * i + 3];
+      a.v[0] = x0.x; a.v[1] = x0.y; a.v[2] = x0.z; a.v[3] = x0.w;
+      a.v[4] = x1.x; a.v[5] = x1.y; a.v[6] = x1.z; a.v[7] = x1.w;
+      b.v[0] = y0.x; b.v[1] = y0.y; b.v[2] = y0.z; b.v[3] = y0.w;
+      b.v[4] = y1.x; b.v[5] = y1.y; b.v[6] = y1.z; b.v[7] = y1.w;
+      h = sky_compress(a, b);
+    }
+    __syncthreads();
+    uint8_t* next = level + 32 * level_n;
+    if (i < half) {
+      buf[2 * i] = make_uint4(h.v[0], h.v[1], h.v[2], h.v[3]);
+      buf[2 * i + 1] = make_uint4(h.v[4], h.v[5], h.v[6], h.v[7]);
+      store_raw(next + 32 * (c * half + i), h);
+    }
+    __syncthreads();
+    level = next;
+    level_n /= 2;
+    cnt = half;
+  }
+}
+
 static int grid_for(size_t n, int threads) {
   size_t b = (n + threads - 1) / threads;
   size_t cap = (size_t)sm_count() * 64;
@@ -167,15 +221,25 @@ int hash_many_device(size_t size, const uint8_t* in, size_t count, uint8_t* out,
   return PKG_OK;
 }
 
-// Internal levels above the leaf digests already in layers[0..n).
+// Internal levels above the leaf digests already in layers[0..n) (n a power
+// of two): one launch per level while a level has more than kSubtreeMax
+// nodes, then the subtree kernel's kSubLevels levels, then the top.
 int merkle_levels_device(uint8_t* layers, size_t n, cudaStream_t s) {
   uint8_t* cur = layers;
-  while (n > (size_t)kTopNodes) {
+  while (n > kSubtreeMax) {
     uint8_t* next = cur + 32 * n;
     merkle_level_kernel<<<grid_for(n / 2, 128), 128, 0, s>>>(cur, n / 2, next);
     PK_CHECK_LAUNCH("merkle_level_kernel");
     cur = next;
     n /= 2;
+  }
+  if (n >= (size_t)kSubNodes * 2) {
+    merkle_subtree_kernel<<<(unsigned)(n / kSubNodes), kSubThreads, 0, s>>>(cur, n);
+    PK_CHECK_LAUNCH("merkle_subtree_kernel");
+    for (int l = 0; l < kSubLevels; l++) {
+      cur += 32 * n;
+      n /= 2;
+    }
   }
   if (n > 1) {
     merkle_top_kernel<<<1, 512, 0, s>>>(cur, n, cur + 32 * n);

@@ -214,8 +214,13 @@ def test_hash_many_rejects_unsupported_size():
 # --------------------------------------------------------------------------
 # Merkle trees and the commit
 # --------------------------------------------------------------------------
-@pytest.mark.parametrize("count,leaf", [(1, 64), (2, 32), (8, 128), (1024, 256), (2048, 64), (4096, 512)])
+@pytest.mark.parametrize("count,leaf", [(1, 64), (2, 32), (8, 128), (256, 64), (512, 32), (1024, 256),
+                                        (2048, 64), (4096, 512), (1 << 15, 64), (1 << 16, 32),
+                                        (1 << 17, 64)])
 def test_merkle_tree_bytes(count, leaf):
+    """Leaf counts on both sides of the tree's launch thresholds: the top
+    kernel alone (<= 256 nodes), the 256-node subtree kernel from 512 nodes,
+    and per-level launches above 2^15 nodes."""
     from provekit_b200.merkle import merkle_tree
     rng = np.random.default_rng(count + leaf)
     data = rng.integers(0, 256, size=count * leaf, dtype=np.uint8)
