@@ -41,6 +41,11 @@ IMAD_PER_MONT = 264  # mad.lo/madc.hi/mul.lo per 8x32 CIOS product (fr.cuh: 8 x 
 # step plus normalisation (69).
 F64_PER_MUL = 22 + 121 + 140 + 69      # 352
 F64_PER_SQR = 11 + 66 + 10 + 140 + 69  # 296
+# integer multiply-adds of one Montgomery->canonical REDC (fr.cuh
+# fr_from_mont: 8 x (1 + 16)); B200 runs them on the same throughput as the
+# binary64 fmas (a kernel mixing the two runs at the rate of either alone),
+# so the leaf kernel's multiply work is its squarings plus these.
+IMAD_PER_REDC = 8 * (1 + 16)  # 136
 # dram__bytes_read.sum + dram__bytes_write.sum of one leaf_fold_fr_kernel launch
 # from an ncu capture of this workload (profiles/leaf_fold_fr_kernel_whir_commit_2p20.md),
 # keyed by (log2 coeffs, folding factor, log inv rate).
@@ -472,9 +477,9 @@ def run_b200(a):
     mont_peak = imad.value / IMAD_PER_MONT
     num_leaves = cw_len
     mont_per_leaf_launch = num_leaves * ((M - 1) * 14 + M)
-    # the M Montgomery->canonical conversions per leaf run on the integer pipe
-    # (REDC), so only the squarings count against the FP64 pipe
-    f64_per_leaf_launch = num_leaves * (M - 1) * 14 * F64_PER_SQR
+    # the squarings' binary64 instructions plus the M Montgomery->canonical
+    # REDCs per leaf (integer multiply-adds on the same shared throughput)
+    f64_per_leaf_launch = num_leaves * ((M - 1) * 14 * F64_PER_SQR + M * IMAD_PER_REDC)
     leaf_avg_s = statistics.mean(leaf_ms) * 1e-3
     achieved = mont_per_leaf_launch / leaf_avg_s
     f64_achieved = f64_per_leaf_launch / leaf_avg_s
@@ -498,16 +503,18 @@ def run_b200(a):
         "config": workload_config(a),
         "roofline": {
             "kernel": "leaf_fold_fr_kernel (Skyscraper leaf hashing)", "bound": "fp64",
-            "achieved": f64_achieved / 1e12, "peak": dfma.value / 1e12, "unit": "T fp64-op/s",
+            "achieved": f64_achieved / 1e12, "peak": dfma.value / 1e12, "unit": "T multiply-op/s",
             "frac": f64_achieved / dfma.value,
             "traffic": LEAF_TRAFFIC_BYTES.get((a.log_coeffs, a.folding_factor, a.log_inv_rate)),
             "traffic_algorithmic": 32 * total_fr + 32 * num_leaves,
             "peak_source": f"measured binary64 fma rate {dfma.value / 1e12:.3f} T/s "
                            "(pkg_measure_dfma_rate, this GPU, this run)",
-            "algorithmic": f"{num_leaves} leaves x {M - 1} compressions x 14 squarings x "
-                           f"{F64_PER_SQR} = {f64_per_leaf_launch} fp64 instructions per launch "
-                           f"({mont_per_leaf_launch} Fr products including the {M} "
-                           "Montgomery->canonical REDCs per leaf, which run on the integer pipe)",
+            "algorithmic": f"{num_leaves} leaves x ({M - 1} compressions x 14 squarings x "
+                           f"{F64_PER_SQR} binary64 instructions + {M} Montgomery->canonical "
+                           f"REDCs x {IMAD_PER_REDC} integer multiply-adds) = "
+                           f"{f64_per_leaf_launch} multiply-pipe instructions per launch "
+                           f"({mont_per_leaf_launch} Fr products and REDCs); the integer "
+                           "multiply-adds share the binary64 fma throughput on B200",
             "achieved_gmont_per_s": achieved / 1e9,
             "int_pipe_alt": {"peak_gmont_per_s": mont_peak / 1e9, "frac": achieved / mont_peak,
                              "note": f"the same products against the IMAD roofline (measured "
@@ -779,7 +786,7 @@ def run_prove(a):
         return
     dfma = ctypes.c_double(0)
     check(L.pkg_measure_dfma_rate(ctypes.byref(dfma)))
-    f64_per_launch = rows * (M - 1) * 14 * F64_PER_SQR
+    f64_per_launch = rows * ((M - 1) * 14 * F64_PER_SQR + M * IMAD_PER_REDC)
     f64_achieved = f64_per_launch / leaf_s
 
     cpu = None
@@ -858,13 +865,16 @@ def run_prove(a):
                 "kernel": f"leaf_fold_fr_kernel (Skyscraper leaf hashing of the witness "
                           f"commitment: {rows} leaves of {M} Fr)",
                 "bound": "fp64", "achieved": f64_achieved / 1e12, "peak": dfma.value / 1e12,
-                "unit": "T fp64-op/s", "frac": f64_achieved / dfma.value,
+                "unit": "T multiply-op/s", "frac": f64_achieved / dfma.value,
                 "traffic": LEAF_TRAFFIC_PROVE_BYTES,
                 "traffic_algorithmic": 32 * rows * M + 32 * rows,
                 "peak_source": f"measured binary64 fma rate {dfma.value / 1e12:.3f} T/s "
                                "(pkg_measure_dfma_rate, this GPU, this run)",
-                "algorithmic": f"{rows} leaves x {M - 1} compressions x 14 squarings x "
-                               f"{F64_PER_SQR} = {f64_per_launch} fp64 instructions per launch",
+                "algorithmic": f"{rows} leaves x ({M - 1} compressions x 14 squarings x "
+                               f"{F64_PER_SQR} binary64 instructions + {M} Montgomery->"
+                               f"canonical REDCs x {IMAD_PER_REDC} integer multiply-adds) = "
+                               f"{f64_per_launch} multiply-pipe instructions per launch; the "
+                               "integer multiply-adds share the binary64 fma throughput on B200",
                 "launch_ms": leaf_s * 1e3,
             },
             "stages_ms_last_step": stage_ms, "whir_phases_ms_last_step": whir_ms,

@@ -15,9 +15,11 @@ int merkle_tree_fr_device(const uint64_t* cw, size_t fr_per_leaf, size_t num_lea
 // entries (calculate_witness_bounds), one launch; err: device word, zeroed.
 int witness_bounds_device(const pkg_r1cs* r1cs, const uint64_t* w, size_t padded, uint64_t* ta,
                           uint64_t* tb, uint64_t* tc, uint32_t* err, cudaStream_t s);
+// y = M x for a CSR matrix; err: device word, zeroed; nnz: row_ptr[num_rows]
+// if known (large matrices then take two balanced passes), else 0.
 int spmv_device(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
                 size_t num_rows, size_t num_cols, const uint64_t* x, uint64_t* y, uint32_t* err,
-                cudaStream_t s);
+                cudaStream_t s, size_t nnz);
 // eq(r, .) over the first num_entries points; sync: wait for the copy of r
 int eq_hypercube_device(const uint64_t* r_host, size_t nr, size_t num_entries, uint64_t* out,
                         cudaStream_t s, bool sync = true);

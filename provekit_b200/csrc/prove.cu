@@ -236,7 +236,7 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     } else {
       PK_REQUIRE(cl_t && vl_t, "transpose %d of the R1CS is incomplete", k);
     }
-    if ((rc = spmv_device(rp_t, cl_t, vl_t, nw, nc, eq, alph, err, s))) return rc;
+    if ((rc = spmv_device(rp_t, cl_t, vl_t, nw, nc, eq, alph, err, s, r1cs->nnz[k]))) return rc;
     // create_weights_and_evaluations (:623-642): the zero padding adds nothing
     if ((rc = dot_device(alph, poly, nw, fs.dev + 4 * k, part, s, fs.ticket))) return rc;
   }

@@ -93,6 +93,38 @@ __global__ void spmv_csr_kernel(const uint64_t* __restrict__ row_ptr, const uint
   }
 }
 
+// The same product in two balanced passes, for large matrices whose row
+// lengths vary (a transposed R1CS matrix: 0 to ~10 entries per witness
+// column): one thread per nonzero forms vals[k] * x[cols[k]] into prod[k],
+// then one thread per row adds its run of prod -- so a warp's Montgomery
+// products no longer wait for its longest row.
+__global__ void spmv_products_kernel(const uint32_t* __restrict__ cols,
+                                     const uint64_t* __restrict__ vals, size_t nnz,
+                                     size_t num_cols, const uint64_t* __restrict__ x,
+                                     uint64_t* __restrict__ prod, uint32_t* __restrict__ err) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nnz;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t col = cols[k];
+    Fr v = fr_zero();
+    if (col >= num_cols)
+      atomicOr(err, 1u);
+    else
+      v = fr_mul_f64(fr_load_ro(vals, k), fr_load_ro(x, col));
+    fr_store(prod, k, v);
+  }
+}
+
+__global__ void spmv_rowsum_kernel(const uint64_t* __restrict__ row_ptr,
+                                   const uint64_t* __restrict__ prod, size_t num_rows,
+                                   uint64_t* __restrict__ y) {
+  for (size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x; row < num_rows;
+       row += (size_t)gridDim.x * blockDim.x) {
+    Fr acc = fr_zero();
+    for (uint64_t k = row_ptr[row]; k < row_ptr[row + 1]; k++) acc = fr_add(acc, fr_load_ro(prod, k));
+    fr_store(y, row, acc);
+  }
+}
+
 // calculate_witness_bounds (sumcheck.rs:163-179) in one pass over the rows:
 // a_i = <A_i, w>, b_i = <B_i, w>, c_i = a_i b_i for i < num_rows, and zeros
 // up to the padded size (the three tables of the zk-sumcheck).  Column
@@ -276,16 +308,33 @@ int witness_bounds_device(const pkg_r1cs* r1cs, const uint64_t* w, size_t padded
   return PKG_OK;
 }
 
-// err: device word, zeroed by the caller before the launch.
+// Nonzeros from which the two balanced passes replace the one-row-per-thread
+// kernel (below it the product temporary is not worth its traffic).
+constexpr size_t kSpmvBalancedNnz = size_t(1) << 16;
+
+// err: device word, zeroed by the caller before the launch.  nnz: the
+// matrix's nonzero count (row_ptr[num_rows]), or 0 if the caller does not
+// know it (one thread per row then).
 int spmv_device(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* vals,
                 size_t num_rows, size_t num_cols, const uint64_t* x, uint64_t* y, uint32_t* err,
-                cudaStream_t s) {
+                cudaStream_t s, size_t nnz) {
   if (num_rows == 0) return PKG_OK;
   PK_REQUIRE(row_ptr && y && aligned16(y) && aligned16(vals) && aligned16(x),
              "null or unaligned device pointer");
-  spmv_csr_kernel<<<ew_grid(num_rows), 256, 0, s>>>(row_ptr, cols, vals, num_rows, num_cols, x, y,
-                                                   err);
-  PK_CHECK_LAUNCH("spmv_csr_kernel");
+  if (nnz < kSpmvBalancedNnz) {
+    spmv_csr_kernel<<<ew_grid(num_rows), 256, 0, s>>>(row_ptr, cols, vals, num_rows, num_cols, x,
+                                                     y, err);
+    PK_CHECK_LAUNCH("spmv_csr_kernel");
+    return PKG_OK;
+  }
+  Scratch tmp;
+  int rc = tmp.alloc(32 * nnz, s);
+  if (rc) return rc;
+  uint64_t* prod = static_cast<uint64_t*>(tmp.ptr);
+  spmv_products_kernel<<<ew_grid(nnz), 256, 0, s>>>(cols, vals, nnz, num_cols, x, prod, err);
+  PK_CHECK_LAUNCH("spmv_products_kernel");
+  spmv_rowsum_kernel<<<ew_grid(num_rows), 256, 0, s>>>(row_ptr, prod, num_rows, y);
+  PK_CHECK_LAUNCH("spmv_rowsum_kernel");
   return PKG_OK;
 }
 
@@ -506,7 +555,12 @@ extern "C" int pkg_spmv_csr(const uint64_t* row_ptr, const uint32_t* cols, const
   if (rc) return rc;
   uint32_t* err = static_cast<uint32_t*>(scr.ptr);
   PK_CUDA(cudaMemsetAsync(err, 0, 4, s));
-  rc = spmv_device(row_ptr, cols, vals, num_rows, num_cols, x, y, err, s);
+  PK_REQUIRE(row_ptr, "null row pointers");
+  uint64_t nnz = 0;  // row_ptr[num_rows], for the balanced passes
+  if ((rc = read_small(&nnz, row_ptr + num_rows, 8, s))) return rc;
+  PK_REQUIRE(nnz < (uint64_t(1) << 40), "row_ptr[num_rows] = %llu is not a nonzero count",
+             (unsigned long long)nnz);
+  rc = spmv_device(row_ptr, cols, vals, num_rows, num_cols, x, y, err, s, (size_t)nnz);
   if (rc) return rc;
   return read_err_flag(err, s, "pkg_spmv_csr");
 }

@@ -87,24 +87,50 @@ __global__ void whir_fold_rows_kernel(const uint64_t* __restrict__ rows, size_t 
   }
 }
 
-// Thread t of G owns coefficients t, t + G, t + 2G, ...: Horner in y = z^G
-// from the top, times z^t (from the squares z^(2^b)); CTA sums to part.
-// P.v[0] = y, P.v[1 + b] = z^(2^b).
+// CTA b owns the C coefficients [bC, (b + 1)C) (C a multiple of the CTA
+// size); its thread j takes bC + j + 256k for k = 0, 1, ..: Horner in
+// y = z^256 from the top.  A power tree in shared memory combines the 256
+// thread values, level l joining neighbours 2^l apart with z^(2^l), to
+// sum_j acc_j z^j; thread 0 scales it by z^(bC) (from the squares
+// z^(C 2^b)), and the CTA values are summed.  Per coefficient one product,
+// per thread one more: a per-thread z^t would cost up to log2(threads)
+// products per thread, more than the coefficients at mid sizes.
+// P.v[0] = z^256, P.v[1 + l] = z^(2^l) (l < 8), P.v[9 + b] = z^(C 2^b).
+constexpr int kEvalTreeLevels = 8;  // kRedThreads = 2^8
+constexpr int kEvalScaleBits = 10;  // CTAs < 2^10
+static_assert(kRedThreads == 1 << kEvalTreeLevels, "one tree level per thread-index bit");
+
 __global__ void __launch_bounds__(kRedThreads) poly_eval_kernel(
-    const uint64_t* __restrict__ c, size_t n, const __grid_constant__ FrParams<33> P,
-    const RedOut ro) {
-  const size_t G = (size_t)gridDim.x * blockDim.x;
-  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  Fr v[1] = {fr_zero()};
-  if (t < n) {
+    const uint64_t* __restrict__ c, size_t n, size_t C,
+    const __grid_constant__ FrParams<1 + kEvalTreeLevels + kEvalScaleBits> P, const RedOut ro) {
+  __shared__ Fr tree[kRedThreads];
+  const unsigned j = threadIdx.x;
+  const size_t c0 = blockIdx.x * C;
+  Fr acc = fr_zero();
+  if (c0 + j < n) {
     const Fr y = param_fr(P, 0);
-    Fr acc = fr_zero();
-    for (size_t k = (n - 1 - t) / G + 1; k-- > 0;) acc = fr_add(fr_mul_f64(acc, y), fr_load_ro(c, t + k * G));
-    for (int b = 0; b < 32; b++)
-      if ((t >> b) & 1) acc = fr_mul_f64(acc, param_fr(P, 1 + b));
-    v[0] = acc;
+    const size_t end = n < c0 + C ? n : c0 + C;
+    for (size_t k = (end - 1 - c0 - j) / kRedThreads + 1; k-- > 0;)
+      acc = fr_add(fr_mul_f64(acc, y), fr_load_ro(c, c0 + j + (size_t)kRedThreads * k));
   }
-  block_finish<1>(v, ro);
+  Fr scale = fr_one_mont();
+  if (j == 0)
+    for (int b = 0; b < kEvalScaleBits; b++)
+      if ((blockIdx.x >> b) & 1) scale = fr_mul_f64(scale, param_fr(P, 1 + kEvalTreeLevels + b));
+  tree[j] = acc;
+  __syncthreads();
+#pragma unroll 1
+  for (int l = 0; l < kEvalTreeLevels; l++) {
+    const unsigned half = kRedThreads >> (l + 1);
+    Fr v;
+    if (j < half) v = fr_add(tree[2 * j], fr_mul_f64(param_fr(P, 1 + l), tree[2 * j + 1]));
+    __syncthreads();
+    if (j < half) tree[j] = v;
+    __syncthreads();
+  }
+  Fr out[1] = {fr_zero()};
+  if (j == 0) out[0] = fr_mul_f64(tree[0], scale);
+  block_finish<1>(out, ro);
 }
 
 // path[q depth + l] = node (idx[q] >> l) ^ 1 of level l
@@ -302,8 +328,15 @@ extern "C" int pkg_poly_eval_many(const uint64_t* coeffs, size_t n, const uint64
   PK_REQUIRE(coeffs && aligned16(coeffs), "null or unaligned coefficients");
   PK_REQUIRE(n < (size_t(1) << 40), "too many coefficients");
   cudaStream_t s = as_stream(stream);
-  const int g = red_grid(n);
-  const size_t G = (size_t)g * kRedThreads;
+  // at least kEvalMin coefficients per thread, up to 4 CTAs per SM (and
+  // fewer than 2^kEvalScaleBits CTAs); C coefficients per CTA
+  constexpr size_t kEvalMin = 4;
+  const size_t gmax = std::min<size_t>((size_t)sm_count() * 4, (size_t(1) << kEvalScaleBits) - 1);
+  size_t g = std::max<size_t>(1, std::min(gmax, (n + kRedThreads * kEvalMin - 1) /
+                                                    (kRedThreads * kEvalMin)));
+  const size_t per = (n + kRedThreads * g - 1) / (kRedThreads * g);
+  const size_t C = per * kRedThreads;
+  g = (n + C - 1) / C;
   // up to kFusedSlotFr points: each launch writes its value to the thread's
   // fused slots; more points: partials, one summing launch per point
   FusedSlots fs;
@@ -316,18 +349,23 @@ extern "C" int pkg_poly_eval_many(const uint64_t* coeffs, size_t n, const uint64
   uint64_t* d_out = fused ? fs.dev : part + 4 * (size_t)g;
   for (size_t j = 0; j < npts; j++) {
     const HostFr z = HostFr::from_limbs(points + 4 * j);
-    FrParams<33> P;
-    put_param(P, 0, HostFr::pow_u64(z, G));
+    FrParams<1 + kEvalTreeLevels + kEvalScaleBits> P;
     HostFr sq = z;
-    for (int b = 0; b < 32; b++) {
-      put_param(P, 1 + b, sq);
+    for (int l = 0; l < kEvalTreeLevels; l++) {  // z^(2^l), then z^256
+      put_param(P, 1 + l, sq);
+      sq = HostFr::mul(sq, sq);
+    }
+    put_param(P, 0, sq);
+    sq = HostFr::pow_u64(z, C);
+    for (int b = 0; b < kEvalScaleBits; b++) {  // z^(C 2^b)
+      put_param(P, 1 + kEvalTreeLevels + b, sq);
       sq = HostFr::mul(sq, sq);
     }
     const RedOut ro = {part, fused ? fs.ticket : nullptr, fused ? d_out + 4 * j : nullptr};
-    poly_eval_kernel<<<g, kRedThreads, 0, s>>>(coeffs, n, P, ro);
+    poly_eval_kernel<<<(unsigned)g, kRedThreads, 0, s>>>(coeffs, n, C, P, ro);
     PK_CHECK_LAUNCH("poly_eval_kernel");
     if (!fused) {
-      sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, g, d_out + 4 * j);
+      sum_partials_kernel<1><<<1, kRedThreads, 0, s>>>(part, (int)g, d_out + 4 * j);
       PK_CHECK_LAUNCH("sum_partials_kernel");
     }
   }

@@ -185,6 +185,21 @@ def test_spartan_sumcheck_matches_oracle(m0):
     assert list(tr.l) == list(t.l) and list(tr.r) == list(t.r)
 
 
+def test_spmv_balanced_path_rejects_out_of_range_column():
+    """Above 2^16 nonzeros the product runs as two balanced passes; a column
+    index past the vector is still reported, not read."""
+    from provekit_b200 import PkgError
+    from provekit_b200.spartan import CsrMatrix
+    rng = np.random.default_rng(31)
+    rows, cols = 1 << 15, 1 << 14
+    row_ptr, col, vals = random_csr(rng, rows, cols, max_nnz=6)
+    assert int(row_ptr[-1]) >= 1 << 16
+    col[len(col) // 2] = cols + 5
+    m = CsrMatrix.from_host(rows, cols, row_ptr, col, vals)
+    with pytest.raises(PkgError):
+        m.mul(dev(O.sample_fr(2, cols)))
+
+
 def test_spmv_rejects_out_of_range_column():
     from provekit_b200 import PkgError
     from provekit_b200.spartan import CsrMatrix

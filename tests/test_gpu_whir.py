@@ -84,19 +84,32 @@ def test_poly_eval_of_more_points_than_fused_slots():
 
 
 def test_poly_eval_at_fused_capacity_and_full_grid():
-    """Exactly 64 points (every fused result slot) on 2^18 coefficients, so
-    each of the 64 back-to-back launches runs the largest reduction grid (4
-    CTAs per SM) and reuses the one ticket the previous launch's last CTA
-    reset: every value equals the oracle's."""
+    """Exactly 64 points (every fused result slot) on 2^20 coefficients, so
+    each of the 64 back-to-back launches runs the largest evaluation grid (4
+    CTAs per SM at 4 coefficients per thread and up) and reuses the one
+    ticket the previous launch's last CTA reset: every value equals the
+    oracle's."""
     from provekit_b200.whir import poly_eval_many
-    n = 1 << 18
+    n = 1 << 20
     props = torch.cuda.get_device_properties(0)
-    assert (n + 255) // 256 >= 4 * props.multi_processor_count  # the grid is at its cap
+    assert n // (256 * 4) >= 4 * props.multi_processor_count  # the grid is at its cap
     c = O.sample_fr(79, n)
     pts = O.sample_fr(80, 64)
     got = poly_eval_many(dev(c), pts)
     for j in range(64):
         assert np.array_equal(got[j], O.poly_eval(c, pts[j])), j
+
+
+@pytest.mark.parametrize("n", [1, 2, 255, 256, 257, 1025, 4099, 65536 + 3, (1 << 21) + 5])
+def test_poly_eval_ragged_sizes(n):
+    """Sizes that leave the last CTA's chunk, or a thread's strided run,
+    short: each CTA's power tree and its z^(bC) scale against the oracle."""
+    from provekit_b200.whir import poly_eval_many
+    c = O.sample_fr(900 + n % 97, n)
+    pts = O.sample_fr(901, 2)
+    got = poly_eval_many(dev(c), pts)
+    for j in range(2):
+        assert np.array_equal(got[j], O.poly_eval(c, pts[j])), (n, j)
 
 
 def test_merkle_openings_of_the_commit_verify():
