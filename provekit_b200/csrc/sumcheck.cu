@@ -321,7 +321,9 @@ int spmv_device(const uint64_t* row_ptr, const uint32_t* cols, const uint64_t* v
   if (num_rows == 0) return PKG_OK;
   PK_REQUIRE(row_ptr && y && aligned16(y) && aligned16(vals) && aligned16(x),
              "null or unaligned device pointer");
-  if (nnz < kSpmvBalancedNnz) {
+  // rows of at most ~one entry (a transposed C: one constraint per output
+  // column) leave nothing to balance
+  if (nnz < kSpmvBalancedNnz || nnz <= num_rows) {
     spmv_csr_kernel<<<ew_grid(num_rows), 256, 0, s>>>(row_ptr, cols, vals, num_rows, num_cols, x,
                                                      y, err);
     PK_CHECK_LAUNCH("spmv_csr_kernel");

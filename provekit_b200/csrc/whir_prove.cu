@@ -37,47 +37,77 @@ namespace pk {
 static_assert(sizeof(HostFr) == 32, "vectors of HostFr are arrays of 4 x u64 limbs");
 
 // ---- subset transforms ----------------------------------------------------
-// NB bits [lo, lo + NB) of the index per pass: each thread loads the 2^NB
-// entries of one group (stride 2^lo), runs NB butterfly stages in registers
-// and stores them.  Zeta: v[b | 2^i] += v[b]; mobius^T: v[b] -= v[b | 2^i].
-template <bool kZeta, int NB>
-__global__ void __launch_bounds__(256) subset_pass_kernel(uint64_t* __restrict__ v, size_t groups,
-                                                         int lo) {
-  constexpr int G = 1 << NB;
-  const size_t low_mask = (size_t(1) << lo) - 1;
-  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < groups;
-       g += (size_t)gridDim.x * blockDim.x) {
-    const size_t base = ((g >> lo) << (lo + NB)) | (g & low_mask);
-    Fr x[G];
-#pragma unroll
-    for (int j = 0; j < G; j++) x[j] = fr_load(v, base + ((size_t)j << lo));
-#pragma unroll
-    for (int b = 0; b < NB; b++) {
-#pragma unroll
-      for (int j = 0; j < G; j++) {
-        if (kZeta && (j >> b & 1)) x[j] = fr_add(x[j], x[j ^ (1 << b)]);
-        if (!kZeta && !(j >> b & 1)) x[j] = fr_sub(x[j], x[j | (1 << b)]);
-      }
+// Zeta: v[b | 2^i] += v[b]; mobius^T: v[b] -= v[b | 2^i], over every index
+// bit i.  A pass covers bits [lo, lo + nb): each CTA stages a tile of 2^nb
+// rows (those bits) x 2^logw consecutive indices (the low bits, for
+// coalesced 32-byte runs) in shared memory as two planes of 16-byte halves,
+// runs its nb stages of additions there and writes the tile back.  The
+// transform is memory-bound, so the pass count is what costs: a tile of
+// kSubsetTile entries takes 10 bits in the first pass and 7 in each later
+// one (21 bits: 3 passes).
+constexpr int kSubsetLogTile = 10;
+constexpr int kSubsetTile = 1 << kSubsetLogTile;  // Fr per CTA (32 KiB)
+constexpr int kSubsetLogW = 3;                    // 8 consecutive indices after the first pass
+
+__device__ __forceinline__ Fr tile_load(const uint4* t0, const uint4* t1, int e) {
+  const uint4 a = t0[e], b = t1[e];
+  Fr r;
+  r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+  r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+  return r;
+}
+
+__device__ __forceinline__ void tile_store(uint4* t0, uint4* t1, int e, const Fr& x) {
+  t0[e] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+  t1[e] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+}
+
+template <bool kZeta>
+__global__ void __launch_bounds__(256) subset_tile_kernel(uint64_t* __restrict__ v, int lo, int nb,
+                                                          int logw) {
+  __shared__ uint4 t0[kSubsetTile], t1[kSubsetTile];
+  const int E = 1 << (nb + logw), W = 1 << logw;
+  // this CTA: a block of W low indices (of 2^(lo - logw)) and a high part
+  const size_t lblocks_log = (size_t)(lo - logw);
+  const size_t lb = blockIdx.x & ((size_t(1) << lblocks_log) - 1);
+  const size_t hi = (size_t)blockIdx.x >> lblocks_log;
+  const size_t base = (hi << (lo + nb)) | (lb << logw);
+  for (int e = threadIdx.x; e < E; e += blockDim.x) {
+    const uint4* q = reinterpret_cast<const uint4*>(
+        v + 4 * (base + ((size_t)(e >> logw) << lo) + (e & (W - 1))));
+    t0[e] = q[0];
+    t1[e] = q[1];
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int b = 0; b < nb; b++) {
+    for (int p = threadIdx.x; p < E / 2; p += blockDim.x) {
+      const int c = p & (W - 1), rp = p >> logw;
+      const int r = ((rp >> b) << (b + 1)) | (rp & ((1 << b) - 1));  // row with bit b clear
+      const int e0 = (r << logw) | c, e1 = ((r | (1 << b)) << logw) | c;
+      const Fr x0 = tile_load(t0, t1, e0), x1 = tile_load(t0, t1, e1);
+      if (kZeta)
+        tile_store(t0, t1, e1, fr_add(x1, x0));
+      else
+        tile_store(t0, t1, e0, fr_sub(x0, x1));
     }
-#pragma unroll
-    for (int j = 0; j < G; j++) fr_store(v, base + ((size_t)j << lo), x[j]);
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < E; e += blockDim.x) {
+    uint4* q = reinterpret_cast<uint4*>(v + 4 * (base + ((size_t)(e >> logw) << lo) + (e & (W - 1))));
+    q[0] = t0[e];
+    q[1] = t1[e];
   }
 }
 
 template <bool kZeta>
 static int subset_transform_device(uint64_t* v, unsigned n, cudaStream_t s) {
-  const size_t N = size_t(1) << n;
   for (unsigned lo = 0; lo < n;) {
-    const int nb = (int)std::min(4u, n - lo);
-    const size_t groups = N >> nb;
-    const int grid = ew_grid(groups);
-    switch (nb) {
-      case 4: subset_pass_kernel<kZeta, 4><<<grid, 256, 0, s>>>(v, groups, (int)lo); break;
-      case 3: subset_pass_kernel<kZeta, 3><<<grid, 256, 0, s>>>(v, groups, (int)lo); break;
-      case 2: subset_pass_kernel<kZeta, 2><<<grid, 256, 0, s>>>(v, groups, (int)lo); break;
-      default: subset_pass_kernel<kZeta, 1><<<grid, 256, 0, s>>>(v, groups, (int)lo); break;
-    }
-    PK_CHECK_LAUNCH("subset_pass_kernel");
+    const int logw = lo == 0 ? 0 : (int)std::min<unsigned>(lo, kSubsetLogW);
+    const int nb = (int)std::min<unsigned>(kSubsetLogTile - logw, n - lo);
+    const size_t ctas = size_t(1) << (n - nb - logw);
+    subset_tile_kernel<kZeta><<<(unsigned)ctas, 256, 0, s>>>(v, (int)lo, nb, logw);
+    PK_CHECK_LAUNCH("subset_tile_kernel");
     lo += nb;
   }
   return PKG_OK;

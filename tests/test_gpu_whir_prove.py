@@ -131,8 +131,10 @@ def test_reference_config_word_for_word(n, batch):
     assert O.whir_verify(po, 0x5eed + n, cov, 3, words, proof) == 0
 
 
-@pytest.mark.parametrize("n", [1, 3, 4, 5, 8, 13, 17, 20])
+@pytest.mark.parametrize("n", [0, 1, 2, 3, 4, 5, 8, 10, 11, 13, 17, 18, 20, 21, 22])
 def test_subset_transforms_match_the_oracle(n):
+    """Every pass split of the tiled transform: one pass (n <= 10), the
+    first pass plus a partial one, and full 7-bit passes after it."""
     from provekit_b200.whir import SUBSET_MOBIUS_T, SUBSET_ZETA, subset_transform
     v = O.sample_fr(500 + n, 1 << n)
     for mode, fn in ((SUBSET_ZETA, "pko_subset_zeta"), (SUBSET_MOBIUS_T, "pko_subset_mobius_t")):
