@@ -23,6 +23,16 @@
 #include "host_stage.cuh"
 #include "pk_common.cuh"
 
+// Most stages per pass (a pass kernel exists for 1..9).  Eight: a 9-stage
+// pass stages 2 x 2^8 x 11 doubles of twiddle digits (45 KiB) besides its
+// 16 KiB tile, which holds it to 3 CTAs per SM; the whole proof's 18-stage
+// witness encode ran 0.39 ms faster per proof as three 6-stage passes than as
+// two 9-stage ones (18.65 vs 19.04 ms), and two 9-stage lines per CTA (512
+// threads, 2 CTAs per SM) gained nothing.
+#ifndef PK_NTT_KMAX
+#define PK_NTT_KMAX 8
+#endif
+
 namespace pk {
 
 // ---------------------------------------------------------------------------
@@ -288,7 +298,7 @@ int ntt_stages(uint64_t* data, size_t N, size_t M, int t_begin, int t_end, const
                cudaStream_t stream, const NttSource* src) {
   const int S = log2_exact(N);
   (void)S;
-  const int kmax = 9;
+  const int kmax = PK_NTT_KMAX;
   int total = t_end - t_begin;
   if (total <= 0) return PKG_OK;
   int npasses = (total + kmax - 1) / kmax;

@@ -91,7 +91,12 @@ struct FusedSlots {
 };
 constexpr size_t kFusedSlotFr = 64;
 int fused_slots(FusedSlots* f);
-// Waits for the stream, then copies bytes of the thread's slots to dst.
+// The completion number for the next fused launch of this thread on the
+// current device (its RedOut's seq; never 0).
+unsigned fused_next_seq();
+// Waits until the thread's last fused launch has written its sums (its
+// completion word, else the stream's completion), then copies bytes of the
+// thread's slots to dst.  Work enqueued after that launch may still run.
 int fused_read(void* dst, const FusedSlots& f, size_t bytes, cudaStream_t s);
 
 // Per host thread and device: a grow-only pinned staging buffer and an event

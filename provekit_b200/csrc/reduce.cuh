@@ -54,10 +54,17 @@ __device__ __forceinline__ void block_sum(Fr (&v)[K]) {
 // partial, and the CTA that takes the last one adds all partials, writes the
 // K sums to out (device or mapped host memory) and resets the counter for the
 // next launch -- one launch instead of two, no copy when out is mapped.
+//
+// A fused launch also announces its completion to the host: after writing
+// the sums, the last CTA stores seq (fused_next_seq(), nonzero) into a word
+// of mapped host memory whose device address sits in the ticket's block
+// (ticket + 2, see fused_slots), so fused_read can poll that word instead of
+// waiting for the stream.
 struct RedOut {
   uint64_t* part;
   unsigned* ticket;  // nullptr: partials only
   uint64_t* out;
+  unsigned seq;      // 0: no completion word
 };
 
 // 32 bytes through L2 only: partials other CTAs wrote during this launch.
@@ -104,6 +111,11 @@ __device__ __forceinline__ void block_finish(Fr (&v)[K], const RedOut& ro,
 #pragma unroll
     for (int k = 0; k < K; k++) fr_store(ro.out, k, v[k]);
     *ro.ticket = 0u;
+    if (ro.seq) {
+      volatile unsigned* word = *reinterpret_cast<unsigned* const*>(ro.ticket + 2);
+      __threadfence_system();  // the sums before the completion word
+      *word = ro.seq;
+    }
   }
 }
 

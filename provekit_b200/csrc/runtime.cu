@@ -119,6 +119,8 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 constexpr size_t kBounceCap = size_t(256) << 10;
+// the fused slots, then the completion word fused launches write (64 bytes)
+constexpr size_t kFusedHostBytes = 32 * kFusedSlotFr + 64;
 std::atomic<int64_t> g_res_host{0}, g_res_dev{0};
 
 // the device block of one thread on one device: the ticket counter, the
@@ -132,6 +134,7 @@ struct ThreadResources {
   struct PerDevice {
     uint8_t* block = nullptr;  // ticket, partials, PoW word
     size_t block_bytes = 0;
+    unsigned seq = 0;          // the last completion number handed out
     PinnedStage stage;
   };
   PerDevice dev[kMaxDevices];
@@ -166,7 +169,7 @@ struct ThreadResources {
     if (have_cur) cudaSetDevice(cur);
     if (fused_host) {
       cudaFreeHost(fused_host);
-      g_res_host -= (int64_t)(32 * kFusedSlotFr);
+      g_res_host -= (int64_t)kFusedHostBytes;
     }
     if (bounce) {
       cudaFreeHost(bounce);
@@ -198,7 +201,8 @@ int fused_slots(FusedSlots* f) {
 #endif
   if (!tr.fused_host) {
     void* p = nullptr;
-    PK_CUDA(cudaHostAlloc(&p, 32 * kFusedSlotFr, cudaHostAllocMapped | cudaHostAllocPortable));
+    PK_CUDA(cudaHostAlloc(&p, kFusedHostBytes, cudaHostAllocMapped | cudaHostAllocPortable));
+    memset(p, 0, kFusedHostBytes);
     void* d = nullptr;
     const cudaError_t e = cudaHostGetDevicePointer(&d, p, 0);
     if (e != cudaSuccess) {
@@ -207,23 +211,29 @@ int fused_slots(FusedSlots* f) {
     }
     tr.fused_host = static_cast<uint64_t*>(p);
     tr.fused_dev = static_cast<uint64_t*>(d);
-    g_res_host += (int64_t)(32 * kFusedSlotFr);
+    g_res_host += (int64_t)kFusedHostBytes;
   }
   int device = 0;
   PK_CUDA(cudaGetDevice(&device));
   PK_REQUIRE(device >= 0 && device < kMaxDevices, "device ordinal %d out of range", device);
   ThreadResources::PerDevice& pd = tr.dev[device];
   if (!pd.block) {
-    // the counter (zeroed on a private stream, waited for: ordered before any
-    // later launch on any stream without touching the legacy default stream)
+    // the counter and, 8 bytes in, the device address of the completion word
+    // (written on a private stream, waited for: ordered before any later
+    // launch on any stream without touching the legacy default stream),
     // followed by the partials of one reduction launch and the PoW word
     const size_t bytes = fused_block_bytes();
     void* t = nullptr;
     PK_CUDA(cudaMalloc(&t, bytes));
+    unsigned* word_dev = reinterpret_cast<unsigned*>(
+        reinterpret_cast<uint8_t*>(tr.fused_dev) + 32 * kFusedSlotFr);
     cudaStream_t z = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&z, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
       e = cudaMemsetAsync(t, 0, 256, z);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(static_cast<uint8_t*>(t) + 8, &word_dev, sizeof word_dev,
+                            cudaMemcpyHostToDevice, z);
       const cudaError_t e2 = cudaStreamSynchronize(z);
       if (e == cudaSuccess) e = e2;
       cudaStreamDestroy(z);
@@ -244,9 +254,40 @@ int fused_slots(FusedSlots* f) {
   return PKG_OK;
 }
 
+unsigned fused_next_seq() {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return 0;
+  ThreadResources::PerDevice& pd = t_res.dev[device];
+  if (++pd.seq == 0) pd.seq = 1;  // 0 means "no completion word"
+  return pd.seq;
+}
+
 int fused_read(void* dst, const FusedSlots& f, size_t bytes, cudaStream_t s) {
   PK_REQUIRE(bytes <= 32 * kFusedSlotFr, "%zu bytes exceed the fused slots", bytes);
-  PK_CUDA(cudaStreamSynchronize(s));
+  int device = 0;
+  PK_CUDA(cudaGetDevice(&device));
+  const unsigned want = device >= 0 && device < kMaxDevices ? t_res.dev[device].seq : 0;
+  volatile const unsigned* word =
+      reinterpret_cast<volatile const unsigned*>(reinterpret_cast<const uint8_t*>(f.host) +
+                                                 32 * kFusedSlotFr);
+  // Poll the completion word the last fused launch writes after its sums
+  // (a few microseconds sooner than the stream's own completion); the
+  // stream's state is checked now and then, so an error, or a stream that
+  // went idle without the word (a launch that wrote none), ends the poll and
+  // falls back to synchronising.
+  bool seen = false;
+  for (uint32_t i = 1; want != 0; i++) {
+    if (*word == want) {
+      seen = true;
+      break;
+    }
+    if ((i & 255) == 0) {
+      const cudaError_t q = cudaStreamQuery(s);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) return cuda_status(q, "fused_read");
+    }
+  }
+  if (!seen) PK_CUDA(cudaStreamSynchronize(s));
 #ifdef PK_DEBUG_FUSED
   t_res.fused_busy = false;
 #endif

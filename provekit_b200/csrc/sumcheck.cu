@@ -246,7 +246,7 @@ int spartan_round_device(uint64_t* a, uint64_t* b, uint64_t* c, uint64_t* eq, si
   memset(&f, 0, sizeof f);
   size_t q;
   int g;
-  const RedOut ro = {part, ticket, out};
+  const RedOut ro = {part, ticket, out, ticket ? fused_next_seq() : 0u};
   if (fold_host) {
     memcpy(f.v, fold_host, 32);
     q = size / 4;
@@ -354,7 +354,8 @@ static int read_err_flag(uint32_t* d_err, cudaStream_t s, const char* what) {
 int dot_device(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* out, uint64_t* part,
                cudaStream_t s, unsigned* ticket) {
   PK_REQUIRE(ticket && out, "dot_device needs the thread's fused slots");
-  dot_kernel<<<red_grid(n), kRedThreads, 0, s>>>(a, b, n, RedOut{part, ticket, out});
+  dot_kernel<<<red_grid(n), kRedThreads, 0, s>>>(a, b, n,
+                                                 RedOut{part, ticket, out, fused_next_seq()});
   PK_CHECK_LAUNCH("dot_kernel");
   return PKG_OK;
 }

@@ -361,7 +361,8 @@ extern "C" int pkg_poly_eval_many(const uint64_t* coeffs, size_t n, const uint64
       put_param(P, 1 + kEvalTreeLevels + b, sq);
       sq = HostFr::mul(sq, sq);
     }
-    const RedOut ro = {part, fused ? fs.ticket : nullptr, fused ? d_out + 4 * j : nullptr};
+    const RedOut ro = {part, fused ? fs.ticket : nullptr, fused ? d_out + 4 * j : nullptr,
+                       fused ? fused_next_seq() : 0u};
     poly_eval_kernel<<<(unsigned)g, kRedThreads, 0, s>>>(coeffs, n, C, P, ro);
     PK_CHECK_LAUNCH("poly_eval_kernel");
     if (!fused) {
@@ -490,7 +491,7 @@ extern "C" int pkg_whir_sumcheck_round(uint64_t* f, uint64_t* w, size_t size, co
   FrParams<1> A;
   memset(&A, 0, sizeof A);
   if (fold) memcpy(A.v[0], fold, 32);
-  const RedOut ro = {part, fs.ticket, fs.dev};
+  const RedOut ro = {part, fs.ticket, fs.dev, fused_next_seq()};
   if (fold)
     whir_round_kernel<true><<<g, kRedThreads, 0, s>>>(f, w, q, A, ro);
   else
