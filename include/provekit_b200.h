@@ -362,8 +362,16 @@ int pkg_batch_job_info(pkg_batch *batch, size_t job, pkg_batch_job *out);
 /* NTT plan: passes of at most kmax stages (radix 2^kmax), 2^log_elems_per_cta
  * elements staged per CTA.  Re-planning drops a captured graph. */
 int pkg_batch_set_params(pkg_batch *batch, int kmax, int log_elems_per_cta);
-/* Autotuner: times every (kmax in 4..11, elements per CTA) on this batch and
- * keeps the fastest. */
+/* Butterflies each thread of an NTT pass runs per stage: 2^log_bpt (0..2), so
+ * a CTA staging E elements has E / 2^(1 + log_bpt) threads (at least 32, at
+ * most 512).  No counterpart in the reference (its NTT is a CPU crate). */
+int pkg_batch_set_butterflies_per_thread(pkg_batch *batch, int log_bpt);
+/* The plan's current (kmax, log2 elements per CTA, log2 butterflies per
+ * thread), e.g. after pkg_batch_tune.  No counterpart in the reference. */
+int pkg_batch_get_params(pkg_batch *batch, int *kmax, int *log_elems_per_cta,
+                         int *log_butterflies_per_thread);
+/* Autotuner: times every (kmax in 4..11, elements per CTA, butterflies per
+ * thread) on this batch and keeps the fastest. */
 int pkg_batch_tune(pkg_batch *batch, pkg_stream_t stream, int *best_kmax, int *best_log_elems,
                    double *best_ms);
 /* Run the batch on stream.  use_graph: the first call captures the batch as

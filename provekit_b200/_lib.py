@@ -69,6 +69,8 @@ SIGNATURES = {
     "pkg_batch_job_info": [_c_vp, _c_sz, _c_vp],
     "pkg_batch_set_params": [_c_vp, _c_int, _c_int],
     "pkg_batch_tune": [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+    "pkg_batch_set_butterflies_per_thread": [_c_vp, _c_int],
+    "pkg_batch_get_params": [_c_vp, _c_vp, _c_vp, _c_vp],
     "pkg_batch_run": [_c_vp, _c_int, _c_vp],
     "pkg_batch_sumcheck_result": [_c_vp, _c_sz, _c_vp],
     "pkg_copy_to_host": [_c_vp, _c_vp, _c_sz],

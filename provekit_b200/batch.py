@@ -54,10 +54,23 @@ class Batch:
         check(lib().pkg_batch_job_info(self._b, j, ctypes.byref(out)))
         return out
 
-    def set_params(self, kmax: int, log_elems: int):
+    def set_params(self, kmax: int, log_elems: int, log_bpt: int = None):
+        """NTT plan: passes of at most kmax stages, 2^log_elems elements per
+        CTA and (if given) 2^log_bpt butterflies per thread per stage."""
+        if log_bpt is not None:
+            check(lib().pkg_batch_set_butterflies_per_thread(self._b, log_bpt))
         check(lib().pkg_batch_set_params(self._b, kmax, log_elems))
 
+    def params(self):
+        """(kmax, log2 elements per CTA, log2 butterflies per thread)."""
+        k, e, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().pkg_batch_get_params(self._b, ctypes.byref(k), ctypes.byref(e),
+                                         ctypes.byref(t)))
+        return k.value, e.value, t.value
+
     def tune(self, stream=None):
+        """Autotune (kmax, elements per CTA, butterflies per thread); returns
+        (kmax, log2 elements per CTA, best ms); params() gives all three."""
         k, e, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
         s = (stream or torch.cuda.current_stream()).cuda_stream
         check(lib().pkg_batch_tune(self._b, s, ctypes.byref(k), ctypes.byref(e), ctypes.byref(ms)))

@@ -6,8 +6,9 @@
 // Every phase is ONE launch over all jobs: a small device table maps each CTA
 // (or each element) to its job, so 256 jobs cost the same number of launches
 // as one.  NTT passes take their radix (K stages) and CTA shape at run time
-// per job; the autotuner (pkg_batch_tune) sweeps the largest radix 2^4..2^11
-// and the elements per CTA.  The sumcheck's Fiat-Shamir transcript and the
+// per job; the autotuner (pkg_batch_tune) sweeps the largest radix 2^4..2^11,
+// the elements per CTA and the butterflies each thread runs per stage (1, 2
+// or 4: the CTA size for a given tile).  The sumcheck's Fiat-Shamir transcript and the
 // round-polynomial bookkeeping run on the device (one thread per job), so a
 // whole batch has no host round trip and is captured once and replayed.
 //
@@ -415,7 +416,10 @@ struct pkg_batch {
   uint8_t* tables = nullptr;     // descriptor tables (rebuilt by plan())
   size_t tables_bytes = 0;
   const uint64_t* roots = nullptr;
-  int kmax = 9, log_elems = 9;
+  // the autotuner's choice on the 256-job config-4 mix (radix 2^8, 256
+  // elements per CTA) as the default plan
+  int kmax = 8, log_elems = 8;
+  int log_bpt = 0;  // log2 butterflies per thread per stage (CTA size E / 2^(1 + log_bpt))
   // plan
   std::vector<pk::PassLaunch> passes;
   pk::Grouped leaves, eq_half, eq_comb, copy_sc;
@@ -573,7 +577,8 @@ static int batch_plan(pkg_batch* b) {
       maxe = std::max<uint64_t>(maxe, (uint64_t(1) << p[i].K) * p[i].T);
     }
     pl.ctas = acc;
-    pl.threads = (int)std::max<uint64_t>(32, std::min<uint64_t>(maxe / 2, 512));
+    pl.threads =
+        (int)std::max<uint64_t>(32, std::min<uint64_t>((maxe / 2) >> b->log_bpt, 512));
     pl.smem = 32 * maxe;
     pl.d_desc = reinterpret_cast<PassDesc*>(cur);
     cur += align256(sizeof(PassDesc) * p.size());
@@ -848,6 +853,22 @@ extern "C" int pkg_batch_set_params(pkg_batch* b, int kmax, int log_elems_per_ct
   return batch_replan(b);
 }
 
+extern "C" int pkg_batch_set_butterflies_per_thread(pkg_batch* b, int log_bpt) {
+  PK_REQUIRE(b, "null batch");
+  PK_REQUIRE(log_bpt >= 0 && log_bpt <= 2, "butterflies per thread 2^%d out of [1, 4]", log_bpt);
+  b->log_bpt = log_bpt;
+  return batch_replan(b);
+}
+
+extern "C" int pkg_batch_get_params(pkg_batch* b, int* kmax, int* log_elems_per_cta,
+                                    int* log_butterflies_per_thread) {
+  PK_REQUIRE(b, "null batch");
+  if (kmax) *kmax = b->kmax;
+  if (log_elems_per_cta) *log_elems_per_cta = b->log_elems;
+  if (log_butterflies_per_thread) *log_butterflies_per_thread = b->log_bpt;
+  return PKG_OK;
+}
+
 extern "C" int pkg_batch_run(pkg_batch* b, int use_graph, pkg_stream_t stream) {
   PK_REQUIRE(b, "null batch");
   cudaStream_t s = as_stream(stream);
@@ -901,27 +922,32 @@ extern "C" int pkg_batch_tune(pkg_batch* b, pkg_stream_t stream, int* best_kmax,
   PK_CUDA(cudaEventCreate(&e0));
   PK_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
-  int bk = b->kmax, be = b->log_elems;
+  int bk = b->kmax, be = b->log_elems, bb = b->log_bpt;
   for (int k = 4; k <= 11; k++) {
     for (int le = std::max(k, 8); le <= 11; le++) {
-      int rc = pkg_batch_set_params(b, k, le);
-      if (rc) return rc;
-      if ((rc = batch_enqueue(b, s))) return rc;  // warm-up
-      PK_CUDA(cudaEventRecord(e0, s));
-      if ((rc = batch_enqueue(b, s))) return rc;
-      PK_CUDA(cudaEventRecord(e1, s));
-      PK_CUDA(cudaEventSynchronize(e1));
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best) {
-        best = ms;
-        bk = k;
-        be = le;
+      for (int lb = 0; lb <= 2; lb++) {
+        b->log_bpt = lb;
+        int rc = pkg_batch_set_params(b, k, le);
+        if (rc) return rc;
+        if ((rc = batch_enqueue(b, s))) return rc;  // warm-up
+        PK_CUDA(cudaEventRecord(e0, s));
+        if ((rc = batch_enqueue(b, s))) return rc;
+        PK_CUDA(cudaEventRecord(e1, s));
+        PK_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+          best = ms;
+          bk = k;
+          be = le;
+          bb = lb;
+        }
       }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  b->log_bpt = bb;
   int rc = pkg_batch_set_params(b, bk, be);
   if (rc) return rc;
   if (best_kmax) *best_kmax = bk;

@@ -34,13 +34,15 @@ struct HostSky {
     };
     return RC[k];
   }
-  static uint8_t sbox(uint8_t v) {
-    uint8_t nv = (uint8_t)~v;
-    uint8_t r1 = (uint8_t)((nv << 1) | (nv >> 7));
-    uint8_t r2 = (uint8_t)((v << 2) | (v >> 6));
-    uint8_t r3 = (uint8_t)((v << 3) | (v >> 5));
-    uint8_t t = (uint8_t)(v ^ (r1 & r2 & r3));
-    return (uint8_t)((t << 1) | (t >> 7));
+  // sbox (bar.rs:40-42) on the 8 bytes of a word at once: rotations within
+  // each byte, rotl_k(v) = ((v & high k bits) >> (8 - k)) | ((v & low bits) << k)
+  static uint64_t sbox8(uint64_t v) {
+    const uint64_t nv = ~v;
+    const uint64_t r1 = ((nv & 0x8080808080808080ULL) >> 7) | ((nv & 0x7f7f7f7f7f7f7f7fULL) << 1);
+    const uint64_t r2 = ((v & 0xc0c0c0c0c0c0c0c0ULL) >> 6) | ((v & 0x3f3f3f3f3f3f3f3fULL) << 2);
+    const uint64_t r3 = ((v & 0xe0e0e0e0e0e0e0e0ULL) >> 5) | ((v & 0x1f1f1f1f1f1f1f1fULL) << 3);
+    const uint64_t t = v ^ (r1 & r2 & r3);
+    return ((t & 0x8080808080808080ULL) >> 7) | ((t & 0x7f7f7f7f7f7f7f7fULL) << 1);
   }
   // any 256-bit value -> [0, p)
   static HostFr reduce(HostFr x) {
@@ -48,10 +50,12 @@ struct HostSky {
     return x;
   }
   static HostFr bar(const HostFr& x) {
-    uint64_t y[4] = {x.l[2], x.l[3], x.l[0], x.l[1]};
-    uint8_t* b = reinterpret_cast<uint8_t*>(y);
-    for (int i = 0; i < 32; i++) b[i] = sbox(b[i]);
-    return reduce(HostFr::from_limbs(y));
+    HostFr y;
+    y.l[0] = sbox8(x.l[2]);
+    y.l[1] = sbox8(x.l[3]);
+    y.l[2] = sbox8(x.l[0]);
+    y.l[3] = sbox8(x.l[1]);
+    return reduce(y);
   }
   static void round(int k, bool is_bar, HostFr& l, HostFr& r) {
     HostFr f = is_bar ? bar(l) : HostFr::mul(l, l);

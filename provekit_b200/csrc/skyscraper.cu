@@ -27,6 +27,12 @@ namespace pk {
 
 constexpr int kTopNodes = 1024;  // nodes finished inside one CTA
 
+// CTAs of 128 threads per SM the leaf kernel is compiled for (its register
+// budget: 7 -> 72 registers).
+#ifndef PK_LEAF_MIN_CTAS
+#define PK_LEAF_MIN_CTAS 7
+#endif
+
 __device__ __forceinline__ Fr load_raw(const uint8_t* p) {
   const uint4* q = reinterpret_cast<const uint4*>(p);
   uint4 a = __ldg(q), b = __ldg(q + 1);
@@ -71,7 +77,7 @@ __global__ void leaf_fold_kernel(const uint8_t* __restrict__ in, size_t size, si
 // (x*2^256 -> x) before hashing; Montgomery encoding hashes the raw limbs.
 // A one-element leaf is the element itself (hash_many(32) copies).
 template <bool kCanonical>
-__global__ void __launch_bounds__(128, 7) leaf_fold_fr_kernel(const uint64_t* __restrict__ cw, size_t fr_per_leaf,
+__global__ void __launch_bounds__(128, PK_LEAF_MIN_CTAS) leaf_fold_fr_kernel(const uint64_t* __restrict__ cw, size_t fr_per_leaf,
                                     size_t count, uint8_t* __restrict__ out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
        i += (size_t)gridDim.x * blockDim.x) {

@@ -325,6 +325,12 @@ class WhirProver {
     pos_ += 4;
   }
   int sumcheck_phase(unsigned rounds, std::vector<HostFr>& rands, bool last = false);
+  // Moves the staged openings into the proof.  Only call it when the stream
+  // has passed a synchronisation since their copies were enqueued.
+  void place_openings() {
+    for (const Placement& pl : place_) memcpy(out_ + pl.word, stage_->buf + pl.src, pl.bytes);
+    place_.clear();
+  }
   int pow_step(unsigned bits);
   int stir_step(size_t q, size_t L, size_t row, const uint64_t* cw, const uint8_t* layers,
                 std::vector<uint64_t>& idx);
@@ -581,6 +587,9 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
       PK_TRY(pkg_whir_commit(g, size_t(1) << nv, k, p_->log_inv_rate + (r + 1) * (k - 1), nullptr,
                              0, PKG_LEAF_CANONICAL, cw_next.as<uint64_t>(), lay_next.as<uint8_t>(),
                              ps));
+      // the previous round's openings (copied before that round's sumcheck
+      // synchronised) go into the proof while the device encodes and hashes
+      place_openings();
       HostFr root;
       PK_TRY(read_small(root.l, lay_next.as<uint8_t>() + 32 * (2 * Ln - 2), 32, s_));
       put(root);
@@ -662,7 +671,7 @@ int WhirProver::run(const uint64_t* coeffs, const uint64_t* codeword, const uint
     PK_CUDA(cudaStreamSynchronize(s_));
   }
   // the staged openings into their places
-  for (const Placement& pl : place_) memcpy(out_ + pl.word, stage_->buf + pl.src, pl.bytes);
+  place_openings();
   return PKG_OK;
 }
 

@@ -79,6 +79,12 @@ def test_batch_graph_replay_and_params():
     b.run(use_graph=True, stream=s)
     s.synchronize()
     check_batch(b)
+    for lb in (1, 2):                 # 2 and 4 butterflies per thread per stage
+        b.set_params(8, 10, log_bpt=lb)
+        assert b.params() == (8, 10, lb)
+        b.run(use_graph=False, stream=s)
+        s.synchronize()
+        check_batch(b)
     b.close()
 
 
@@ -87,6 +93,8 @@ def test_batch_autotune_keeps_results():
     b = Batch([10, 12, 9, 11], seed=13)
     k, e, ms = b.tune()
     assert 4 <= k <= 11 and k <= e <= 11 and ms > 0
+    kk, ee, lb = b.params()
+    assert (kk, ee) == (k, e) and 0 <= lb <= 2
     b.run(use_graph=False)
     torch.cuda.synchronize()
     check_batch(b)
