@@ -91,6 +91,11 @@ struct FusedSlots {
 };
 constexpr size_t kFusedSlotFr = 64;
 int fused_slots(FusedSlots* f);
+// A spare 32-bit word of the thread's mapped pinned slots buffer (after the
+// slots and the completion word): a caller may copy a device flag there with
+// cudaMemcpyAsync and read it after a later synchronising read on the same
+// stream (fused_read, read_small), which implies the copy completed.
+int fused_aux_word(uint32_t** word);
 // The completion number for the next fused launch of this thread on the
 // current device (its RedOut's seq; never 0).
 unsigned fused_next_seq();

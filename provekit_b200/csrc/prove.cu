@@ -138,14 +138,16 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
     return rc;
   if ((rc = rs_encode_device(poly, M * nb, L, nullptr, 0, cw_len, cw, s))) return rc;
   if ((rc = merkle_tree_fr_device(cw, M * nb, cw_len, PKG_LEAF_CANONICAL, layers, s))) return rc;
-  if ((rc = read_small(out->root, layers + 32 * (2 * cw_len - 2), 32, s))) return rc;
   uint64_t ood_points[4 * 5];
   if (whir) {
-    // whir's commit: the root, then the OOD samples of the committed polynomial
+    // whir's commit: the root (read there, its words are the commitment's
+    // first four), then the OOD samples of the committed polynomial
     if ((rc = pkg_whir_commit_ood(whir, &out->transcript, poly, layers, whir_commit_words,
                                   ood_points, stream)))
       return rc;
+    memcpy(out->root, whir_commit_words, 32);
   } else {
+    if ((rc = read_small(out->root, layers + 32 * (2 * cw_len - 2), 32, s))) return rc;
     HostFr root = HostFr::to_mont(HostFr::from_limbs(reinterpret_cast<const uint64_t*>(out->root)));
     pkg_transcript_absorb(&out->transcript, root.l);
   }
@@ -155,8 +157,6 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   // partial sums of dot_device (<= 4 * SMs CTAs); its results go to the
   // thread's fused slots
   const size_t nparts = 4 * (size_t)sm_count();
-  FusedSlots fs;
-  if ((rc = fused_slots(&fs))) return rc;
   if ((rc = s_misc.alloc(256 + 32 * nparts, s))) return rc;
   uint32_t* err = static_cast<uint32_t*>(s_misc.ptr);
   uint64_t* part = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(s_misc.ptr) + 256);
@@ -164,20 +164,27 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   // a = A w, b = B w, c = a o b, zero-padded to 2^m0: one launch
   if ((rc = witness_bounds_device(r1cs, witness, n0, ta, tb, tc, err, s))) return rc;
 
-  // ---- zk sumcheck (whir_r1cs.rs:519-621)
-  std::vector<uint64_t> wb(16 * m0);
-  {
-    uint32_t h_err = 0;
-    const HostRead reads[2] = {{wb.data(), poly + 4 * w1_size, 32 * 4 * m0}, {&h_err, err, 4}};
-    if ((rc = read_small(reads, 2, s))) return rc;
-    PK_REQUIRE(!h_err, "R1CS column index out of range");
-  }
+  // The witness bounds' error flag goes to a spare word of the thread's
+  // mapped slots without a synchronisation; the sumcheck's first round
+  // trip, which follows the copy in the stream, makes it readable.  The host
+  // meanwhile starts the sumcheck (its challenges, the eq table), so the
+  // device is not left idle for a read here.
+  volatile uint32_t* h_err = nullptr;
+  if ((rc = fused_aux_word(const_cast<uint32_t**>(&h_err)))) return rc;
+  *h_err = 0;
+  PK_CUDA(cudaMemcpyAsync(const_cast<uint32_t*>(h_err), err, 4, cudaMemcpyDeviceToHost, s));
   clk.mark(1);
-  rc = pkg_spartan_sumcheck(ta, tb, tc, m0, g.data(), wb.data(), &out->transcript, &out->r[0][0],
+
+  // ---- zk sumcheck (whir_r1cs.rs:519-621); the blinding coefficients in
+  // w1[offset .. offset + 4 m0] are g, written above
+  rc = pkg_spartan_sumcheck(ta, tb, tc, m0, g.data(), g.data(), &out->transcript, &out->r[0][0],
                             out->rho, out->sum_g, &out->coeffs[0][0], &out->alpha[0][0],
                             out->blinding_eval, stream);
   if (rc) return rc;
+  PK_REQUIRE(!*h_err, "R1CS column index out of range");
   clk.mark(2);
+  FusedSlots fs;  // the dots below write their results to the thread's slots
+  if ((rc = fused_slots(&fs))) return rc;
 
   // ---- eq(alpha) and the transposed products (sumcheck.rs:195-227)
   // The covectors: one nw-entry buffer, or for the WHIR proof the

@@ -192,6 +192,34 @@ void thread_resource_totals(size_t* host_bytes, size_t* device_bytes) {
   *device_bytes = (size_t)std::max<int64_t>(0, g_res_dev.load());
 }
 
+// The thread's mapped pinned buffer: the fused slots, the completion word
+// (byte 32 kFusedSlotFr) and the spare word (16 bytes later).
+static int fused_host_buffer(ThreadResources& tr) {
+  if (tr.fused_host) return PKG_OK;
+  void* p = nullptr;
+  PK_CUDA(cudaHostAlloc(&p, kFusedHostBytes, cudaHostAllocMapped | cudaHostAllocPortable));
+  memset(p, 0, kFusedHostBytes);
+  void* d = nullptr;
+  const cudaError_t e = cudaHostGetDevicePointer(&d, p, 0);
+  if (e != cudaSuccess) {
+    cudaFreeHost(p);
+    return cuda_status(e, "cudaHostGetDevicePointer");
+  }
+  tr.fused_host = static_cast<uint64_t*>(p);
+  tr.fused_dev = static_cast<uint64_t*>(d);
+  g_res_host += (int64_t)kFusedHostBytes;
+  return PKG_OK;
+}
+
+int fused_aux_word(uint32_t** word) {
+  ThreadResources& tr = t_res;
+  const int rc = fused_host_buffer(tr);
+  if (rc) return rc;
+  *word = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(tr.fused_host) +
+                                      32 * kFusedSlotFr + 16);
+  return PKG_OK;
+}
+
 int fused_slots(FusedSlots* f) {
   ThreadResources& tr = t_res;
 #ifdef PK_DEBUG_FUSED
@@ -199,19 +227,9 @@ int fused_slots(FusedSlots* f) {
              "fused slots: a fused use began before the thread's previous one synchronised");
   tr.fused_busy = true;
 #endif
-  if (!tr.fused_host) {
-    void* p = nullptr;
-    PK_CUDA(cudaHostAlloc(&p, kFusedHostBytes, cudaHostAllocMapped | cudaHostAllocPortable));
-    memset(p, 0, kFusedHostBytes);
-    void* d = nullptr;
-    const cudaError_t e = cudaHostGetDevicePointer(&d, p, 0);
-    if (e != cudaSuccess) {
-      cudaFreeHost(p);
-      return cuda_status(e, "cudaHostGetDevicePointer");
-    }
-    tr.fused_host = static_cast<uint64_t*>(p);
-    tr.fused_dev = static_cast<uint64_t*>(d);
-    g_res_host += (int64_t)kFusedHostBytes;
+  {
+    const int rc = fused_host_buffer(tr);
+    if (rc) return rc;
   }
   int device = 0;
   PK_CUDA(cudaGetDevice(&device));
