@@ -32,6 +32,17 @@
 #ifndef PK_NTT_KMAX
 #define PK_NTT_KMAX 8
 #endif
+// Butterflies per thread per stage, log2 (the CTA has E / 2^(1 + this)
+// threads, at least 32).  Two: 2^24 points in 5.01 ms against 5.14 ms with
+// one (a CTA of 256 elements' worth of 128 threads, each with two
+// independent products in flight per stage); four were slower (5.31 ms).
+#ifndef PK_NTT_LOG_BPT
+#define PK_NTT_LOG_BPT 1
+#endif
+// Elements per CTA, log2 (lines of 2^K elements: 2^(this - K) of them).
+#ifndef PK_NTT_LOG_ELEMS
+#define PK_NTT_LOG_ELEMS 9
+#endif
 
 namespace pk {
 
@@ -308,8 +319,8 @@ int ntt_stages(uint64_t* data, size_t N, size_t M, int t_begin, int t_end, const
     int B = log2_exact(N) - t - K;
     uint64_t U = (uint64_t(1) << B) * M;
     uint64_t num_lines = (uint64_t(1) << t) * U;
-    // aim for ~512 elements per CTA
-    int log_tgt = K >= 9 ? 0 : 9 - K;
+    // aim for 2^PK_NTT_LOG_ELEMS elements per CTA
+    int log_tgt = K >= PK_NTT_LOG_ELEMS ? 0 : PK_NTT_LOG_ELEMS - K;
     uint64_t T = uint64_t(1) << log_tgt;
     if (T > num_lines) T = pow2_part(num_lines);
     int mode_b = 0;
@@ -323,7 +334,7 @@ int ntt_stages(uint64_t* data, size_t N, size_t M, int t_begin, int t_end, const
     }
     int log_t = log2_exact(T);
     uint64_t E = (uint64_t(1) << K) * T;
-    int threads = (int)std::min<uint64_t>(E / 2, 512);
+    int threads = (int)std::min<uint64_t>((E / 2) >> PK_NTT_LOG_BPT, 512);
     if (threads < 32) threads = 32;
     size_t smem = 32 * E + (mode_b ? 0 : sizeof(double) * 2 * 11 * (size_t(1) << (K - 1)));
     uint64_t grid = num_lines / T;
