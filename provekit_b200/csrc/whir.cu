@@ -166,8 +166,13 @@ __global__ void gather_rows_kernel(const uint64_t* __restrict__ cw, size_t row_f
 
 // One WHIR sumcheck round over f, w (quarter layout when folding, as the
 // Spartan rounds): pairs (i, i + q); sums f0 w0, f1 w1, (2f1-f0)(2w1-w0).
+// The round kernel's seven products go through one out-of-line call, and the
+// kernel is bounded to two CTAs per SM (128 registers): with them inlined the
+// folding kernel took 172 registers, one CTA of 256 threads per SM.
+static __device__ __noinline__ Fr whir_mul(const Fr a, const Fr b) { return fr_mul_f64(a, b); }
+
 template <bool kFold>
-__global__ void __launch_bounds__(kRedThreads) whir_round_kernel(
+__global__ void __launch_bounds__(kRedThreads, 2) whir_round_kernel(
     uint64_t* __restrict__ f, uint64_t* __restrict__ w, size_t q,
     const __grid_constant__ FrParams<1> A, const RedOut ro) {
   Fr acc[3] = {fr_zero(), fr_zero(), fr_zero()};
@@ -176,19 +181,19 @@ __global__ void __launch_bounds__(kRedThreads) whir_round_kernel(
        i += (size_t)gridDim.x * blockDim.x) {
     Fr f0 = fr_load(f, i), f1 = fr_load(f, i + q), w0 = fr_load(w, i), w1 = fr_load(w, i + q);
     if (kFold) {
-      f0 = fr_add(f0, fr_mul_f64(alpha, fr_sub(fr_load(f, i + 2 * q), f0)));
-      f1 = fr_add(f1, fr_mul_f64(alpha, fr_sub(fr_load(f, i + 3 * q), f1)));
-      w0 = fr_add(w0, fr_mul_f64(alpha, fr_sub(fr_load(w, i + 2 * q), w0)));
-      w1 = fr_add(w1, fr_mul_f64(alpha, fr_sub(fr_load(w, i + 3 * q), w1)));
+      f0 = fr_add(f0, whir_mul(alpha, fr_sub(fr_load(f, i + 2 * q), f0)));
+      f1 = fr_add(f1, whir_mul(alpha, fr_sub(fr_load(f, i + 3 * q), f1)));
+      w0 = fr_add(w0, whir_mul(alpha, fr_sub(fr_load(w, i + 2 * q), w0)));
+      w1 = fr_add(w1, whir_mul(alpha, fr_sub(fr_load(w, i + 3 * q), w1)));
       fr_store(f, i, f0);
       fr_store(f, i + q, f1);
       fr_store(w, i, w0);
       fr_store(w, i + q, w1);
     }
-    acc[0] = fr_add(acc[0], fr_mul_f64(f0, w0));
-    acc[1] = fr_add(acc[1], fr_mul_f64(f1, w1));
+    acc[0] = fr_add(acc[0], whir_mul(f0, w0));
+    acc[1] = fr_add(acc[1], whir_mul(f1, w1));
     const Fr f2 = fr_sub(fr_add(f1, f1), f0), w2 = fr_sub(fr_add(w1, w1), w0);
-    acc[2] = fr_add(acc[2], fr_mul_f64(f2, w2));
+    acc[2] = fr_add(acc[2], whir_mul(f2, w2));
   }
   block_finish<3>(acc, ro);
 }
