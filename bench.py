@@ -1006,7 +1006,8 @@ def batched_compare(sizes, seed, steps, warmup, tune=False):
     tuned = None
     if tune:
         k, e, ms = b.tune(stream)
-        tuned = {"kmax": k, "log_elems_per_cta": e, "ms": ms}
+        tuned = {"kmax": k, "log_elems_per_cta": e,
+                 "log_butterflies_per_thread": b.params()[2], "ms": ms}
     b.run(use_graph=True, stream=stream)  # capture
     for _ in range(warmup):
         b.run(use_graph=True, stream=stream)

@@ -336,3 +336,13 @@ def test_prover_load_bytes_validates_the_layout(L):
         L.pkg_prover_free(out)
     else:
         assert rc == -2 and not out.value  # CUDA: past every host check
+
+
+def test_batch_plan_entry_points_reject_null_batch(L):
+    """The batch plan setters and getter validate their handle before any
+    device work."""
+    from provekit_b200._lib import PKG_ERR_INVALID_ARGUMENT
+    assert L.pkg_batch_set_params(None, 8, 8) == PKG_ERR_INVALID_ARGUMENT
+    assert L.pkg_batch_set_butterflies_per_thread(None, 1) == PKG_ERR_INVALID_ARGUMENT
+    k = ctypes.c_int()
+    assert L.pkg_batch_get_params(None, ctypes.byref(k), None, None) == PKG_ERR_INVALID_ARGUMENT
