@@ -180,7 +180,10 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   rc = pkg_spartan_sumcheck(ta, tb, tc, m0, g.data(), g.data(), &out->transcript, &out->r[0][0],
                             out->rho, out->sum_g, &out->coeffs[0][0], &out->alpha[0][0],
                             out->blinding_eval, stream);
-  if (rc) return rc;
+  if (rc) {
+    cudaStreamSynchronize(s);  // the flag's copy must not land in a later proof's word
+    return rc;
+  }
   PK_REQUIRE(!*h_err, "R1CS column index out of range");
   clk.mark(2);
   FusedSlots fs;  // the dots below write their results to the thread's slots
