@@ -301,7 +301,8 @@ int pkg_spartan_prove(const pkg_r1cs *r1cs, const uint64_t *witness, uint64_t bl
  * pkg_spartan_prove or pkg_prove_r1cs: [0] commit (to the root, and the
  * OOD answers), [1] witness bounds, [2] zk sumcheck, [3] eq(alpha) + public
  * weight, [4] transposed products and evaluations, [5] the WHIR proof (0
- * for pkg_spartan_prove).  Each stage ends with a stream synchronisation.
+ * for pkg_spartan_prove).  The witness bounds are only enqueued (their
+ * device time falls in [2]); every other stage ends with a synchronisation.
  * No counterpart in the reference (diagnostics). */
 #define PKG_PROVE_STAGES 6
 int pkg_last_prove_stages(double ms[PKG_PROVE_STAGES]);

@@ -32,8 +32,9 @@ static size_t ceil_log2(size_t n) {  // utils::next_power_of_two (utils/mod.rs:7
 }
 
 // Host wall-clock of the calling thread's last pkg_spartan_prove, per stage;
-// every stage ends with a stream synchronisation, so these are the stages'
-// device time plus their host work.
+// every stage but the witness bounds (only enqueued; their device time falls
+// in the zk sumcheck's) ends with a synchronisation, so these are the
+// stages' device time plus their host work.
 thread_local double g_stage_ms[PKG_PROVE_STAGES];
 
 // Seed of the WHIR-ZK blinding polynomial: the blinding seed with the first
