@@ -69,7 +69,7 @@ def parse_args():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plugin-e2e", action="store_true")
-    p.add_argument("--no-north-star", action="store_true",
+    p.add_argument("--no-targets", action="store_true",
                    help="prove: skip the 2^24 NTT, batched and served measurements after the "
                         "headline")
     p.add_argument("--workload", choices=["commit", "prove", "batched", "served", "ntt", "whir_ops",
@@ -817,12 +817,12 @@ def run_prove(a):
     proof = last[2]
     proof_bytes = 8 * proof.shape[0]
 
-    # the north star's targets, measured in the same run: the 2^24 NTT
+    # the project's other targets, measured in the same run: the 2^24 NTT
     # against both rooflines, the batched form on the 256-job mix against
     # the same jobs one at a time, and the served form under an open-loop
     # Poisson stream against sequential plain proving
     north = None
-    if a.gpus == 1 and not a.no_north_star:
+    if a.gpus == 1 and not a.no_targets:
         north = {}
         imad = ctypes.c_double(0)
         check(L.pkg_measure_imad_rate(ctypes.byref(imad)))
@@ -912,7 +912,7 @@ def run_prove(a):
                                 "from the first call to the last proof"},
             "gpu_launches": int(launches),
             "clocks": clk,
-            "north_star": north}
+            "targets": north}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -1276,7 +1276,7 @@ def ntt_measure(L, stream, flush, logn, steps, warmup, dfma_rate, imad_rate):
                     "before each; frac_fp64 against the measured binary64 fma rate / "
                     f"{F64_PER_MUL} per product (the butterflies multiply on the FP64 pipe), "
                     f"frac_int against the measured IMAD rate / {IMAD_PER_MONT} per 8x32 CIOS "
-                    "product (the north star's integer roofline)"}
+                    "product (the integer-pipe roofline)"}
 
 
 def run_ntt(a):
