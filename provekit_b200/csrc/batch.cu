@@ -416,7 +416,7 @@ struct pkg_batch {
   uint8_t* tables = nullptr;     // descriptor tables (rebuilt by plan())
   size_t tables_bytes = 0;
   const uint64_t* roots = nullptr;
-  // the autotuner's choice on the 256-job config-4 mix as the default plan:
+  // the autotuner's choice on a mix of 256 jobs of 2^10..2^22 points as the default plan:
   // radix 2^10, 1024 elements per CTA, 4 butterflies per thread per stage
   // (492.6 ms per batch, against 503 ms with radix 2^8, 256 elements and one
   // butterfly per thread)
