@@ -1240,6 +1240,255 @@ int pko_prove_r1cs(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t blind
                               whir->log_inv_rate, out, whir, whir_commit_words, whir_proof);
 }
 
+/* ----------------------------------------------------------------------- */
+/* Two commitments: R1CS with verifier challenges                          */
+/* ----------------------------------------------------------------------- */
+void pko_r1cs_sizing_split(size_t num_constraints, size_t num_witnesses, size_t w1_size,
+                           size_t *m_out, size_t *m0_out) {
+    /* new_for_r1cs (r1cs-compiler/src/whir_r1cs.rs:48-92) */
+    const size_t m1 = ceil_log2(w1_size), m2 = ceil_log2(num_witnesses - w1_size);
+    size_t m = m1 > m2 ? m1 : m2, m0 = ceil_log2(num_constraints);
+    if (m < 13) m = 13;
+    if (m0 < 1) m0 = 1;
+    if (((size_t)1 << m) - w1_size < 4 * m0) m++;
+    *m_out = m;
+    *m0_out = m0;
+}
+
+/* One part's commitment (whir_r1cs.rs commit, :82-140): its nvals values
+ * padded to n, g (4 m0 Fr) at g_offset when given, with batch 2 the mask
+ * polynomial in the second half; RS encode + tree, then the OOD samples. */
+static int dual_commit(const pko_whir_params *whir, pko_transcript *t, const uint64_t *vals,
+                       size_t nvals, const uint64_t *g, size_t g_len, size_t g_offset,
+                       uint64_t mask_seed, uint64_t *poly, uint64_t *cw, uint8_t *layers,
+                       uint8_t root[32], uint64_t *commit_words, uint64_t *ood_points) {
+    const size_t n = (size_t)1 << whir->num_variables, nb = whir->batch_size;
+    const unsigned ff = whir->folding_factor, lr = whir->log_inv_rate;
+    memset(poly, 0, 32 * n * nb);
+    if (nvals) memcpy(poly, vals, 32 * nvals);
+    if (g) memcpy(poly + 4 * g_offset, g, 32 * g_len);
+    if (nb == 2) pko_sample_fr_indexed(mask_seed, 0, n, poly + 4 * n);
+    const size_t cw_len = (n >> ff) << lr;
+    int rc = pko_whir_commit(poly, n * nb, ff + (nb == 2 ? 1 : 0), lr, cw, layers);
+    if (rc) return rc;
+    memcpy(root, layers + 32 * (2 * cw_len - 2), 32);
+    return pko_whir_commit_ood(whir, t, poly, root, commit_words, ood_points);
+}
+
+int pko_prove_r1cs_dual(const pko_r1cs *r1cs, size_t w1_size, const size_t *offs, size_t nchal,
+                        uint64_t *witness, pko_w2_solver solve, void *ctx,
+                        uint64_t blinding_seed, uint64_t domain, const pko_whir_params *whir,
+                        pko_dual_proof *out, uint64_t *challenges, uint64_t *commit_words1,
+                        uint64_t *commit_words2, uint64_t *proof1, uint64_t *proof2) {
+    const size_t nc = r1cs->num_constraints, nw = r1cs->num_witnesses;
+    const size_t np = r1cs->num_public_inputs;
+    if (!whir || !solve || w1_size < np + 1 || w1_size > nw) return -1;
+    size_t m, m0;
+    pko_r1cs_sizing_split(nc, nw, w1_size, &m, &m0);
+    if (m0 > 30 || m > 28 || whir->num_variables != m || whir->folding_factor > m ||
+        whir->ood_samples > 4 || (whir->batch_size != 1 && whir->batch_size != 2))
+        return -1;
+    const size_t n = (size_t)1 << m, nb = whir->batch_size, w2_size = nw - w1_size;
+    for (size_t j = 0; j < nchal; j++)
+        if (offs[j] >= n) return -1; /* SparseCovector::new (prefix_covector.rs:257-266) */
+    memset(out, 0, sizeof *out);
+    pko_spartan_proof *sp = &out->spartan;
+    sp->m = m;
+    sp->m0 = m0;
+    pko_transcript *t = &sp->transcript;
+    const uint64_t dom[4] = {domain, 0, 0, 0};
+    pko_transcript_init(t, dom);
+
+    const size_t cw_len = (n >> whir->folding_factor) << whir->log_inv_rate;
+    const size_t cw_fr = ((size_t)1 << whir->folding_factor) * nb * cw_len;
+    uint64_t *poly1 = malloc(32 * n * nb), *poly2 = malloc(32 * n * nb);
+    uint64_t *cw1 = malloc(32 * cw_fr), *cw2 = malloc(32 * cw_fr);
+    uint8_t *lay1 = malloc(32 * (2 * cw_len - 1)), *lay2 = malloc(32 * (2 * cw_len - 1));
+    uint64_t *g = malloc(32 * 4 * m0);
+    size_t n0 = (size_t)1 << m0;
+    uint64_t *a = calloc(n0, 32), *b = calloc(n0, 32), *cc = calloc(n0, 32);
+    uint64_t *cov = malloc(32 * 3 * (nw ? nw : 1));
+    uint64_t *st1 = malloc(32 * 5 * n), *st2 = malloc(32 * 4 * n);
+    uint64_t ood1[4 * 5], ood2[4 * 5];
+    int rc = -2;
+    if (!poly1 || !poly2 || !cw1 || !cw2 || !lay1 || !lay2 || !g || !a || !b || !cc || !cov ||
+        !st1 || !st2)
+        goto done;
+
+    /* commit w1 with the blinding univariates at w1_size (lib.rs:184-187) */
+    pko_sample_fr(blinding_seed, 4 * m0, g, 1);
+    rc = dual_commit(whir, t, witness, w1_size, g, 4 * m0, w1_size,
+                     blinding_seed ^ 0x243f6a8885a308d3ULL, poly1, cw1, lay1, sp->root,
+                     commit_words1, ood1);
+    if (rc) goto done;
+    /* the challenges (WitnessBuilder::Challenge, witness_builder.rs:167-170),
+     * then the caller's solve of w2 and its commitment (lib.rs:189-217) */
+    for (size_t j = 0; j < nchal; j++) pko_transcript_squeeze(t, challenges + 4 * j);
+    solve(ctx, challenges, nchal, witness);
+    rc = dual_commit(whir, t, witness + 4 * w1_size, w2_size, NULL, 0, 0,
+                     blinding_seed ^ 0x13198a2e03707344ULL, poly2, cw2, lay2, out->root2,
+                     commit_words2, ood2);
+    if (rc) goto done;
+
+    /* witness bounds over the whole witness, the zk sumcheck with w1's
+     * blinding (prove_noir, whir_r1cs.rs:143-187) */
+    pko_spmv(r1cs->row_ptr[0], r1cs->cols[0], r1cs->vals[0], nc, witness, a);
+    pko_spmv(r1cs->row_ptr[1], r1cs->cols[1], r1cs->vals[1], nc, witness, b);
+    for (size_t i = 0; i < nc; i++) pko_fr_mul(cc + 4 * i, a + 4 * i, b + 4 * i);
+    rc = pko_spartan_sumcheck(t, a, b, cc, m0, g, poly1, w1_size, &sp->r[0][0], sp->rho,
+                              sp->sum_g, &sp->coeffs[0][0], &sp->alpha[0][0], sp->blinding_eval);
+    if (rc) goto done;
+    /* get_public_weights (:665-676) */
+    {
+        uint64_t *pv = malloc(32 * (np + 1)), hm[4];
+        if (!pv) { rc = -2; goto done; }
+        memcpy(pv, witness + 4, 32 * np);
+        pko_from_mont_many(pv, np);
+        pko_public_inputs_hash(sp->public_hash, pv, np);
+        free(pv);
+        pko_fr_to_mont(hm, sp->public_hash);
+        pko_transcript_absorb(t, hm);
+    }
+    pko_transcript_squeeze(t, sp->public_x);
+    /* alphas split at w1_size (:311-326); compute_alpha_evals (prefix_covector.rs:212-223) */
+    if ((rc = pko_r1cs_covectors(r1cs, &sp->alpha[0][0], m0, nw, cov))) goto done;
+    for (int k = 0; k < 3; k++) pko_dot(sp->evals[k], cov + 4 * nw * (size_t)k, poly1, w1_size);
+    for (int k = 0; k < 3; k++)
+        pko_dot(out->evals2[k], cov + 4 * (nw * (size_t)k + w1_size), poly2, w2_size);
+    for (int k = 0; k < 3; k++) pko_transcript_absorb(t, sp->evals[k]);
+    for (int k = 0; k < 3; k++) pko_transcript_absorb(t, out->evals2[k]);
+    uint64_t pw[4], x[4];
+    if (np) { /* compute_public_eval (prefix_covector.rs:226-240) on w1 */
+        cpy4(pw, ONE_MONT);
+        for (size_t i = 0; i <= np; i++) {
+            pko_fr_mul(x, pw, poly1 + 4 * i);
+            pko_fr_add(sp->public_eval, sp->public_eval, x);
+            pko_fr_mul(pw, pw, sp->public_x);
+        }
+        pko_transcript_absorb(t, sp->public_eval);
+    }
+    if (nchal) { /* compute_challenge_eval (prefix_covector.rs:326-338) on w2 */
+        cpy4(pw, ONE_MONT);
+        for (size_t j = 0; j < nchal; j++) {
+            pko_fr_mul(x, pw, poly2 + 4 * offs[j]);
+            pko_fr_add(out->challenge_eval, out->challenge_eval, x);
+            pko_fr_mul(pw, pw, sp->public_x);
+        }
+        pko_transcript_absorb(t, out->challenge_eval);
+    }
+
+    /* w1's statements: the public weight first (make_public_weight, :350-356),
+     * the alphas restricted to w1, the blinding covector expand_powers::<4>(alpha)
+     * at w1_size (the whole witness may be longer than 2^m: each part is not) */
+    const size_t base = np ? 1 : 0, ncov1 = base + 4, ncov2 = 3 + (nchal ? 1 : 0);
+    memset(st1, 0, 32 * ncov1 * n);
+    if (np) {
+        cpy4(pw, ONE_MONT);
+        for (size_t i = 0; i <= np; i++) {
+            cpy4(st1 + 4 * i, pw);
+            pko_fr_mul(pw, pw, sp->public_x);
+        }
+    }
+    for (int k = 0; k < 3; k++)
+        memcpy(st1 + 4 * n * (base + (size_t)k), cov + 4 * nw * (size_t)k, 32 * w1_size);
+    for (size_t i = 0; i < m0; i++) {
+        uint64_t *bl = st1 + 4 * (n * (base + 3) + w1_size + 4 * i);
+        cpy4(pw, ONE_MONT);
+        for (int q = 0; q < 4; q++) {
+            cpy4(bl + 4 * q, pw);
+            pko_fr_mul(pw, pw, sp->alpha[i]);
+        }
+    }
+    /* w2's statements: the alphas restricted to w2, the challenge weight
+     * (make_challenge_weight, prefix_covector.rs:311-323; SparseCovector
+     * accumulates, so repeated offsets add) */
+    memset(st2, 0, 32 * ncov2 * n);
+    for (int k = 0; k < 3; k++)
+        memcpy(st2 + 4 * n * (size_t)k, cov + 4 * (nw * (size_t)k + w1_size), 32 * w2_size);
+    if (nchal) {
+        cpy4(pw, ONE_MONT);
+        for (size_t j = 0; j < nchal; j++) {
+            uint64_t *e = st2 + 4 * (3 * n + offs[j]);
+            pko_fr_add(e, e, pw);
+            pko_fr_mul(pw, pw, sp->public_x);
+        }
+    }
+    {
+        pko_transcript tw = *t;
+        rc = pko_whir_prove(whir, &tw, poly1, cw1, lay1, commit_words1, ood1, st1, ncov1, proof1);
+        if (!rc)
+            rc = pko_whir_prove(whir, &tw, poly2, cw2, lay2, commit_words2, ood2, st2, ncov2,
+                                proof2);
+    }
+done:
+    free(poly1); free(poly2); free(cw1); free(cw2); free(lay1); free(lay2); free(g);
+    free(a); free(b); free(cc); free(cov); free(st1); free(st2);
+    return rc;
+}
+
+int pko_synthetic_r1cs_dual(uint64_t seed, size_t nc1, size_t ni, size_t nchal, size_t rows2,
+                            uint64_t *row_ptr[3], uint32_t *cols[3], uint64_t *vals[3],
+                            size_t nnz_out[3], uint64_t *witness, size_t *offs) {
+    const size_t w1 = 1 + ni + nc1, w2 = nchal + rows2;
+    if (w1 + w2 >= ((size_t)1 << 32)) return -1;
+    int rc = pko_synthetic_r1cs(seed, nc1, ni, row_ptr, cols, vals, nnz_out, witness);
+    if (rc) return rc;
+    memset(witness + 4 * w1, 0, 32 * w2);
+    /* w2's layout: challenges spread at multiples of the stride, products
+     * at the remaining offsets in order */
+    const size_t stride = nchal ? w2 / nchal : 0;
+    for (size_t j = 0; j < nchal; j++) offs[j] = j * stride;
+    uint64_t rng = seed ^ 0xd1b54a32d192ed03ULL;
+    uint64_t *coef = malloc(32 * 2 * (rows2 ? rows2 : 1));
+    if (!coef) return -2;
+    pko_sample_fr(seed + 2, 2 * rows2, coef, 1);
+    size_t e[2] = {nnz_out[0], nnz_out[1]}, used = 0, next = 0, j = 0;
+    for (size_t i = 0; i < rows2; i++) {
+        const size_t row = nc1 + i;
+        /* A: the challenge (or the constant) with coefficient 1 */
+        cols[0][e[0]] = (uint32_t)(nchal ? w1 + offs[i % nchal] : 0);
+        cpy4(vals[0] + 4 * e[0], ONE_MONT);
+        e[0]++;
+        row_ptr[0][row + 1] = e[0];
+        /* B: 1-2 uniform w1 columns */
+        const int kb = 1 + (int)splitmix64_below(&rng, 2);
+        for (int q = 0; q < kb; q++) {
+            cols[1][e[1]] = (uint32_t)splitmix64_below(&rng, w1);
+            cpy4(vals[1] + 4 * e[1], coef + 4 * used++);
+            e[1]++;
+        }
+        row_ptr[1][row + 1] = e[1];
+        /* C: the next offset that holds no challenge */
+        while (j < nchal && offs[j] == next) { next++; j++; }
+        cols[2][row] = (uint32_t)(w1 + next);
+        cpy4(vals[2] + 4 * row, ONE_MONT);
+        row_ptr[2][row + 1] = row + 1;
+        next++;
+    }
+    free(coef);
+    nnz_out[0] = e[0];
+    nnz_out[1] = e[1];
+    nnz_out[2] = nc1 + rows2;
+    return 0;
+}
+
+void pko_synthetic_dual_solve(void *ctx, const uint64_t *chal, size_t nchal, uint64_t *w) {
+    const pko_synthetic_dual *d = (const pko_synthetic_dual *)ctx;
+    const pko_r1cs *r = d->r1cs;
+    for (size_t j = 0; j < nchal; j++) cpy4(w + 4 * (d->w1_size + d->challenge_offsets[j]), chal + 4 * j);
+    for (size_t row = d->first_row; row < r->num_constraints; row++) {
+        uint64_t dot[2][4], t[4];
+        for (int k = 0; k < 2; k++) {
+            memset(dot[k], 0, 32);
+            for (uint64_t e = r->row_ptr[k][row]; e < r->row_ptr[k][row + 1]; e++) {
+                pko_fr_mul(t, r->vals[k] + 4 * e, w + 4 * (size_t)r->cols[k][e]);
+                pko_fr_add(dot[k], dot[k], t);
+            }
+        }
+        pko_fr_mul(w + 4 * (size_t)r->cols[2][r->row_ptr[2][row]], dot[0], dot[1]);
+    }
+}
+
 /* ======================================================================= */
 /* Poseidon2, t = 4, rf = 8, rp = 56 (poseidon2/src/permutation.rs)         */
 /* ======================================================================= */

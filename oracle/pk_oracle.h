@@ -317,6 +317,68 @@ int pko_prove_r1cs(const pko_r1cs *r1cs, const uint64_t *witness, uint64_t blind
                    uint64_t domain, const pko_whir_params *whir, pko_spartan_proof *out,
                    uint64_t *whir_commit_words, uint64_t *whir_proof);
 
+/* ---- Two commitments: R1CS with verifier challenges -------------------
+ * Sizing with the witness split at w1_size (WhirR1CSScheme::new_for_r1cs,
+ * provekit/r1cs-compiler/src/whir_r1cs.rs:48-92): m = max(log w1, log w2, 13),
+ * one more when w1's padding cannot hold the 4 m0 blinding coefficients.
+ * w1_size = num_witnesses is pko_r1cs_sizing. */
+void pko_r1cs_sizing_split(size_t num_constraints, size_t num_witnesses, size_t w1_size,
+                           size_t *m, size_t *m0);
+
+/* Fills witness[w1_size .. num_witnesses) from the challenges (Montgomery
+ * form): the caller's witness solver for w2 (provekit/prover/src/lib.rs:189-212). */
+typedef void (*pko_w2_solver)(void *ctx, const uint64_t *challenges, size_t num_challenges,
+                              uint64_t *witness);
+
+typedef struct {
+    pko_spartan_proof spartan;  /* root, evals: w1's; transcript: where w1's WHIR proof starts */
+    uint8_t root2[32];          /* w2's commitment root (canonical bytes)      */
+    uint64_t evals2[3][4];      /* <M^T eq(alpha) restricted to w2, w2>, M = A, B, C */
+    uint64_t challenge_eval[4]; /* <[1, x, ..], w2 at the offsets>; 0 without challenges */
+} pko_dual_proof;
+
+/* The dual-commitment proof (Prove::prove, provekit/prover/src/lib.rs:145-232,
+ * then prove_from_alphas's second branch, provekit/prover/src/whir_r1cs.rs:302-425):
+ *   commit w1 = witness[0, w1_size) with the blinding polynomial at w1_size
+ *   (whir-ZK batch: mask from blinding_seed ^ 0x243f6a8885a308d3), squeeze
+ *   num_challenges challenges, solve(ctx, ..) writes w2, commit w2 (mask from
+ *   blinding_seed ^ 0x13198a2e03707344, no blinding polynomial), zk sumcheck
+ *   over the whole witness, public weights, M^T eq(alpha) split at w1_size,
+ *   messages evals1, evals2, public eval (with public inputs), challenge eval
+ *   (with challenges), then two WHIR proofs on one transcript: w1's of
+ *   [public?, A|w1, B|w1, C|w1, blinding], w2's of [A|w2, B|w2, C|w2,
+ *   challenge weight?] (the challenge weight holds x^j at offsets[j], w2-relative).
+ * challenges: num_challenges Fr out.  Word counts: pko_whir_commit_words and
+ * pko_whir_proof_words(whir, 4 or 5) / (whir, 3 or 4). */
+int pko_prove_r1cs_dual(const pko_r1cs *r1cs, size_t w1_size, const size_t *challenge_offsets,
+                        size_t num_challenges, uint64_t *witness, pko_w2_solver solve, void *ctx,
+                        uint64_t blinding_seed, uint64_t domain, const pko_whir_params *whir,
+                        pko_dual_proof *out, uint64_t *challenges, uint64_t *commit_words1,
+                        uint64_t *commit_words2, uint64_t *proof1, uint64_t *proof2);
+
+/* A synthetic R1CS with challenges: pko_synthetic_r1cs(seed, nc1, ni) as w1
+ * (w1_size = 1 + ni + nc1), then w2 of num_challenges + rows2 entries with
+ * challenge j at w2 offset j * floor(w2_size / num_challenges) and the
+ * products at the other offsets in order; row nc1 + i: A = the challenge
+ * i mod num_challenges (the constant w[0] without challenges), B = 1-2 w1
+ * columns with coefficients from pko_sample_fr(seed + 2), C = product i.
+ * Capacities: row_ptr nc1 + rows2 + 1; cols/vals 3 (nc1 + rows2) for A and
+ * B, nc1 + rows2 for C; witness 1 + ni + nc1 + num_challenges + rows2 Fr
+ * (w2 zeroed); offsets num_challenges.  Returns 0 or -1 (too large). */
+int pko_synthetic_r1cs_dual(uint64_t seed, size_t nc1, size_t ni, size_t num_challenges,
+                            size_t rows2, uint64_t *row_ptr[3], uint32_t *cols[3],
+                            uint64_t *vals[3], size_t nnz_out[3], uint64_t *witness,
+                            size_t *challenge_offsets);
+/* The solver of that instance (a pko_w2_solver): the challenges at their
+ * offsets, then for rows first_row.. in order w[C col] = (A w)(B w). */
+typedef struct {
+    const pko_r1cs *r1cs;
+    size_t w1_size, first_row;
+    const size_t *challenge_offsets;
+} pko_synthetic_dual;
+void pko_synthetic_dual_solve(void *ctx, const uint64_t *challenges, size_t num_challenges,
+                              uint64_t *witness);
+
 int pko_num_threads(void);
 
 #ifdef __cplusplus

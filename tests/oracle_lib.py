@@ -107,6 +107,199 @@ def prove_r1cs(h, blinding_seed, domain, wp):
     return _spartan_dict(out), cwords, proof
 
 
+class DualProof(ctypes.Structure):
+    _fields_ = [("spartan", SpartanProof), ("root2", ctypes.c_uint8 * 32),
+                ("evals2", ctypes.c_uint64 * 12), ("challenge_eval", ctypes.c_uint64 * 4)]
+
+
+def dual_dict(out):
+    d = _spartan_dict(out.spartan)
+    d["root2"] = bytes(out.root2)
+    d["evals2"] = np.array(out.evals2, np.uint64).reshape(3, 4)
+    d["challenge_eval"] = np.array(out.challenge_eval, np.uint64)
+    return d
+
+
+class SyntheticDualR1CS:
+    """pko_synthetic_r1cs_dual: w1 = the synthetic R1CS of nc1 rows over ni
+    inputs, w2 = num_challenges challenges spread over it plus rows2 products
+    challenge x w1 terms; the witness's w2 part is zero until solve()."""
+
+    def __init__(self, seed: int, nc1: int, ni: int, num_challenges: int, rows2: int,
+                 num_public_inputs: int = 0):
+        nc = nc1 + rows2
+        self.num_constraints, self.num_public_inputs = nc, num_public_inputs
+        self.w1_size = 1 + ni + nc1
+        self.num_witnesses = self.w1_size + num_challenges + rows2
+        self.first_row = nc1
+        self.row_ptr = [np.zeros(nc + 1, np.uint64) for _ in range(3)]
+        caps = [3 * nc, 3 * nc, nc]
+        cols = [np.zeros(max(c, 1), np.uint32) for c in caps]
+        vals = [np.zeros((max(c, 1), 4), np.uint64) for c in caps]
+        self.witness = np.zeros((self.num_witnesses, 4), np.uint64)
+        self.challenge_offsets = np.zeros(max(num_challenges, 1), np.uint64)
+        nnz = (ctypes.c_size_t * 3)()
+        rp = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.row_ptr])
+        cl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in cols])
+        vl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in vals])
+        rc = lib().pko_synthetic_r1cs_dual(seed, nc1, ni, num_challenges, rows2, rp, cl, vl, nnz,
+                                           p64(self.witness), p64(self.challenge_offsets))
+        assert rc == 0, rc
+        self.challenge_offsets = self.challenge_offsets[:num_challenges]
+        self.nnz = list(nnz)
+        self.cols = [np.ascontiguousarray(c[:n]) for c, n in zip(cols, self.nnz)]
+        self.vals = [np.ascontiguousarray(v[:n]) for v, n in zip(vals, self.nnz)]
+
+    def solver_ctx(self):
+        """(pko_synthetic_dual, the objects it points into) for pko_prove_r1cs_dual."""
+        r = _r1cs_c(self)
+        offs = np.ascontiguousarray(self.challenge_offsets, dtype=np.uint64)
+        ctx = SyntheticDual(ctypes.pointer(r), self.w1_size, self.first_row,
+                            offs.ctypes.data if offs.size else None)
+        return ctx, (r, offs)
+
+    def solve(self, challenges: np.ndarray) -> np.ndarray:
+        """w2 for these challenges (num_challenges x 4 Montgomery words)."""
+        w = np.ascontiguousarray(self.witness.copy())
+        ctx, keep = self.solver_ctx()
+        ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 4)
+        lib().pko_synthetic_dual_solve(ctypes.byref(ctx), p64(ch) if ch.size else None,
+                                       len(self.challenge_offsets), p64(w))
+        del keep
+        return w[self.w1_size:]
+
+
+class SyntheticDual(ctypes.Structure):
+    _fields_ = [("r1cs", ctypes.POINTER(R1CS)), ("w1_size", ctypes.c_size_t),
+                ("first_row", ctypes.c_size_t), ("challenge_offsets", ctypes.c_void_p)]
+
+
+def r1cs_sizing_split(nc, nw, w1_size):
+    m, m0 = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    lib().pko_r1cs_sizing_split(nc, nw, w1_size, ctypes.byref(m), ctypes.byref(m0))
+    return m.value, m0.value
+
+
+def dual_statement_counts(h):
+    npub = getattr(h, "num_public_inputs", 0)
+    return 4 + (1 if npub else 0), 3 + (1 if len(h.challenge_offsets) else 0)
+
+
+def prove_r1cs_dual(h, blinding_seed, domain, wp):
+    """pko_prove_r1cs_dual with the instance's own solver: (dual dict,
+    challenges, commit words 1 and 2, proofs 1 and 2, the solved witness)."""
+    n1, n2 = dual_statement_counts(h)
+    r = _r1cs_c(h)
+    ctx, keep = h.solver_ctx()
+    out = DualProof()
+    k = len(h.challenge_offsets)
+    ch = np.zeros((max(k, 1), 4), np.uint64)
+    cw1 = np.zeros(lib().pko_whir_commit_words(ctypes.byref(wp)), np.uint64)
+    cw2 = np.zeros_like(cw1)
+    pr1 = np.zeros(lib().pko_whir_proof_words(ctypes.byref(wp), n1), np.uint64)
+    pr2 = np.zeros(lib().pko_whir_proof_words(ctypes.byref(wp), n2), np.uint64)
+    w = np.ascontiguousarray(h.witness.copy())
+    offs = np.zeros(max(k, 1), np.uint64)
+    offs[:k] = h.challenge_offsets
+    solve = ctypes.cast(lib().pko_synthetic_dual_solve, ctypes.c_void_p)
+    rc = lib().pko_prove_r1cs_dual(ctypes.byref(r), h.w1_size, p64(offs), k, p64(w), solve,
+                                   ctypes.byref(ctx), blinding_seed, domain, ctypes.byref(wp),
+                                   ctypes.byref(out), p64(ch), p64(cw1), p64(cw2), p64(pr1),
+                                   p64(pr2))
+    del keep
+    assert rc == 0, rc
+    return dual_dict(out), ch[:k], cw1, cw2, pr1, pr2, w
+
+
+MONT_ONE = np.array([0xac96341c4ffffffb, 0x36fc76959f60cd29, 0x666ea36f7879462e,
+                     0x0e0a77c19a07df2f], np.uint64)  # 2^256 mod p
+
+
+def _powers(x, n):
+    out = np.zeros((n, 4), np.uint64)
+    if n:
+        out[0] = MONT_ONE
+    for i in range(1, n):
+        lib().pko_fr_mul(p64(out[i]), p64(out[i - 1]), p64(np.ascontiguousarray(x, np.uint64)))
+    return out
+
+
+def dual_statement_covectors(h, d):
+    """(w1's statements, w2's statements) of a dual proof, as the verifier
+    builds them from the transcript's alpha and x: [public?, A|w1, B|w1,
+    C|w1, blinding] and [A|w2, B|w2, C|w2, challenge weight?]."""
+    n, m0, w1 = 1 << d["m"], d["m0"], h.w1_size
+    nw = h.num_witnesses
+    full = r1cs_covectors(h, d["alpha"], m0, nw).reshape(3, nw, 4)
+    npub = getattr(h, "num_public_inputs", 0)
+    n1, n2 = dual_statement_counts(h)
+    s1 = np.zeros((n1, n, 4), np.uint64)
+    b = 1 if npub else 0
+    if npub:
+        s1[0, : npub + 1] = _powers(d["public_x"], npub + 1)
+    s1[b: b + 3, :w1] = full[:, :w1]
+    for i in range(m0):
+        s1[b + 3, w1 + 4 * i: w1 + 4 * i + 4] = _powers(d["alpha"][i], 4)
+    s2 = np.zeros((n2, n, 4), np.uint64)
+    s2[:3, : nw - w1] = full[:, w1:]
+    if n2 == 4:
+        pw = _powers(d["public_x"], len(h.challenge_offsets))
+        for j, o in enumerate(h.challenge_offsets):
+            e = np.ascontiguousarray(s2[3, int(o)])
+            lib().pko_fr_add(p64(e), p64(e.copy()), p64(pw[j]))
+            s2[3, int(o)] = e
+    return s1.reshape(-1, 4), s2.reshape(-1, 4)
+
+
+def verify_r1cs_dual(h, wp, domain, d, challenges, cw1, cw2, pr1, pr2):
+    """0 when a dual proof is accepted: both commitments with the challenges
+    between them on a fresh transcript, both WHIR proofs from the state the
+    first WHIR prover started from, each proof's claimed statement values
+    equal to the Spartan messages, and the challenge binding
+    <[1, x, ..], challenges> = the challenge evaluation.  Else a negative
+    WHIR code, or 1 (wrong challenges), 2 (values differ), 3 (binding)."""
+    t0 = transcript(domain)
+    z1, z2 = np.zeros((5, 4), np.uint64), np.zeros((5, 4), np.uint64)
+    rc = lib().pko_whir_verify_commit(ctypes.byref(wp), ctypes.byref(t0), p64(cw1), p64(z1))
+    if rc:
+        return rc
+    k = len(h.challenge_offsets)
+    got = np.zeros((max(k, 1), 4), np.uint64)
+    for j in range(k):
+        lib().pko_transcript_squeeze(ctypes.byref(t0), p64(got[j]))
+    if not np.array_equal(got[:k], np.asarray(challenges).reshape(-1, 4)[:k]):
+        return 1
+    rc = lib().pko_whir_verify_commit(ctypes.byref(wp), ctypes.byref(t0), p64(cw2), p64(z2))
+    if rc:
+        return rc
+    t = Transcript()
+    t.l[:], t.r[:] = d["transcript"]
+    s1, s2 = dual_statement_covectors(h, d)
+    n = 1 << d["m"]
+    n1, n2 = s1.shape[0] // n, s2.shape[0] // n
+    for s, nc, cw, z, pr in ((s1, n1, cw1, z1, pr1), (s2, n2, cw2, z2, pr2)):
+        rc = lib().pko_whir_verify_proof(ctypes.byref(wp), ctypes.byref(t), p64(s), nc, p64(cw),
+                                         p64(z), p64(np.ascontiguousarray(pr)), pr.shape[0])
+        if rc:
+            return rc
+    npub = getattr(h, "num_public_inputs", 0)
+    want1 = ([d["public_eval"]] if npub else []) + list(d["evals"]) + [d["blinding_eval"]]
+    want2 = list(d["evals2"]) + ([d["challenge_eval"]] if k else [])
+    if not (np.array_equal(pr1[: 4 * n1].reshape(-1, 4), np.array(want1, np.uint64))
+            and np.array_equal(pr2[: 4 * n2].reshape(-1, 4), np.array(want2, np.uint64))):
+        return 2
+    if k:
+        pw = _powers(d["public_x"], k)
+        acc = np.zeros(4, np.uint64)
+        for j in range(k):
+            x = np.zeros(4, np.uint64)
+            lib().pko_fr_mul(p64(x), p64(pw[j]), p64(np.ascontiguousarray(got[j])))
+            lib().pko_fr_add(p64(acc), p64(acc.copy()), p64(x))
+        if not np.array_equal(acc, d["challenge_eval"]):
+            return 3
+    return 0
+
+
 def r1cs_covectors(h, alpha, m0, length):
     out = np.zeros((3 * length, 4), np.uint64)
     rc = lib().pko_r1cs_covectors(ctypes.byref(_r1cs_c(h)), p64(np.ascontiguousarray(alpha)), m0,
@@ -239,6 +432,17 @@ def lib():
         L.pko_public_inputs_hash.argtypes = [_u64p, _u64p, _sz]
         L.pko_prove_r1cs.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_uint64, wp,
                                      ctypes.c_void_p, _u64p, _u64p]
+        L.pko_fr_add.argtypes = [_u64p, _u64p, _u64p]
+        L.pko_r1cs_sizing_split.argtypes = [_sz, _sz, _sz, ctypes.POINTER(_sz),
+                                            ctypes.POINTER(_sz)]
+        L.pko_synthetic_r1cs_dual.argtypes = [ctypes.c_uint64, _sz, _sz, _sz, _sz,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p, _u64p, _u64p]
+        L.pko_synthetic_dual_solve.argtypes = [ctypes.c_void_p, _u64p, _sz, _u64p]
+        L.pko_prove_r1cs_dual.argtypes = [ctypes.c_void_p, _sz, _u64p, _sz, _u64p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.c_uint64, wp, ctypes.c_void_p, _u64p, _u64p,
+                                          _u64p, _u64p, _u64p]
     return _lib
 
 
