@@ -595,6 +595,73 @@ int pkg_prove_r1cs(const pkg_r1cs *r1cs, const uint64_t *witness, uint64_t blind
                    pkg_spartan_proof *out, uint64_t *whir_commit_words, uint64_t *whir_proof,
                    pkg_stream_t stream);
 
+/* ---- Two commitments: R1CS with verifier challenges ----------------------
+ * The witness is split at w1_size.  w1 = witness[0, w1_size) is committed
+ * first, verifier challenges are drawn from the transcript, the caller
+ * solves w2 = witness[w1_size, num_witnesses) with them, w2 is committed,
+ * and the proof ends with two WHIR proofs on one transcript.  This is
+ * Prove::prove's flow (provekit/prover/src/lib.rs:145-232: commit w1, solve
+ * w2 whose WitnessBuilder::Challenge entries squeeze the transcript,
+ * prover/src/witness/witness_builder.rs:167-170, commit w2) and
+ * prove_from_alphas's dual-commitment branch
+ * (provekit/prover/src/whir_r1cs.rs:302-425).  It is split in two calls
+ * because witness solving stays with the caller:
+ *
+ *   pkg_dual_prove_begin   w1's commitment (with the blinding polynomial at
+ *                          w1_size; whir-ZK mask from blinding_seed as in
+ *                          pkg_prove_r1cs), then num_challenges challenges
+ *   (caller)               solves w2; the challenge values sit in w2 at
+ *                          challenge_offsets (w2-relative, scheme.challenge_offsets)
+ *   pkg_dual_prove_finish  w2's commitment (no blinding polynomial; its mask
+ *                          from blinding_seed ^ 0x13198a2e03707344), the zk
+ *                          sumcheck over the whole witness, public weights,
+ *                          A^T eq, B^T eq, C^T eq split at w1_size, messages
+ *                          evals (w1), evals2 (w2), public eval (public
+ *                          inputs, on w1), challenge eval (challenges, on
+ *                          w2), then WHIR proof 1 of w1's statements
+ *                          [public weight?, A|w1, B|w1, C|w1, blinding] and
+ *                          WHIR proof 2 of w2's [A|w2, B|w2, C|w2,
+ *                          challenge weight?] (make_challenge_weight:
+ *                          x^j at challenge_offsets[j], repeated offsets add)
+ *   pkg_dual_prove_free    releases the state (any time; NULL is a no-op)
+ *
+ * Sizing: pkg_r1cs_sizing_split.  whir: parameters for its m; batch_size 1,
+ * or 2 for whir-ZK (each commitment with its own mask polynomial). */
+typedef struct pkg_dual_prove pkg_dual_prove;
+typedef struct {
+  pkg_spartan_proof spartan; /* root, evals: w1's; transcript: where WHIR proof 1 starts */
+  uint8_t root2[32];         /* w2's commitment root                       */
+  uint64_t evals2[3][4];     /* <M^T eq(alpha) restricted to w2, w2>, M = A, B, C */
+  uint64_t challenge_eval[4];/* <[1, x, ..], w2 at the offsets> (0 without challenges) */
+} pkg_dual_proof;
+/* WhirR1CSScheme::new_for_r1cs with w1_size (r1cs-compiler/src/whir_r1cs.rs:48-92):
+ * m = max(ceil log2 w1_size, ceil log2 (num_witnesses - w1_size), 13), plus
+ * one when fewer than 4 m0 entries of w1's padding are free; m0 as in
+ * pkg_r1cs_sizing.  w1_size = num_witnesses gives pkg_r1cs_sizing. */
+int pkg_r1cs_sizing_split(size_t num_constraints, size_t num_witnesses, size_t w1_size,
+                          size_t *m, size_t *m0);
+/* r1cs: device arrays as for pkg_prove_r1cs; the struct is copied, the
+ * arrays it points to must stay valid until finish returns.  w1: device,
+ * w1_size Fr (16-byte aligned), copied.  Requires num_public_inputs + 1 <=
+ * w1_size <= num_witnesses and every offset < 2^m.  Outputs (host):
+ * whir_commit_words1 (pkg_whir_commit_words), challenges (num_challenges
+ * Fr, Montgomery form: the values w2 holds at the offsets), *state.
+ * Synchronous; device memory for both commitments is held until free. */
+int pkg_dual_prove_begin(const pkg_r1cs *r1cs, size_t w1_size, const size_t *challenge_offsets,
+                         size_t num_challenges, const uint64_t *w1, uint64_t blinding_seed,
+                         uint64_t transcript_domain, const pkg_whir_params *whir,
+                         uint64_t *whir_commit_words1, uint64_t *challenges,
+                         pkg_dual_prove **state, pkg_stream_t stream);
+/* w2: device, num_witnesses - w1_size Fr (16-byte aligned; NULL when
+ * empty).  Outputs (host): out, whir_commit_words2, whir_proof1
+ * (pkg_whir_proof_words(whir, 4 + (public inputs > 0)) words), whir_proof2
+ * (pkg_whir_proof_words(whir, 3 + (num_challenges > 0))).  Once per state;
+ * on the stream given to begin.  Synchronous. */
+int pkg_dual_prove_finish(pkg_dual_prove *state, const uint64_t *w2, pkg_dual_proof *out,
+                          uint64_t *whir_commit_words2, uint64_t *whir_proof1,
+                          uint64_t *whir_proof2);
+void pkg_dual_prove_free(pkg_dual_prove *state);
+
 /* ---- Prover handles (tooling/provekit-ffi/src/ffi.rs, types.rs) ----------
  * The reference's FFI hands out an opaque PKProver (a prepared circuit) and
  * returns proofs in a PKBuf that the library allocated and pk_free_buf

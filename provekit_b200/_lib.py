@@ -115,6 +115,10 @@ SIGNATURES = {
     "pkg_prover_serialize": [_c_vp, _c_vp],
     "pkg_prover_load_bytes": [_c_vp, _c_sz, _c_vp],
     "pkg_thread_resource_bytes": [_c_vp, _c_vp],
+    "pkg_r1cs_sizing_split": [_c_sz, _c_sz, _c_sz, _c_vp, _c_vp],
+    "pkg_dual_prove_begin": [_c_vp, _c_sz, _c_vp, _c_sz, _c_vp, ctypes.c_uint64, ctypes.c_uint64,
+                             _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+    "pkg_dual_prove_finish": [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
 }
 
 
@@ -156,6 +160,8 @@ def lib():
         L.pkg_free_buf.restype = None
         L.pkg_prover_free.argtypes = [_c_vp]
         L.pkg_prover_free.restype = None
+        L.pkg_dual_prove_free.argtypes = [_c_vp]
+        L.pkg_dual_prove_free.restype = None
         L.pkg_r1cs_transposes_bytes.argtypes = [_c_vp]
         L.pkg_r1cs_transposes_bytes.restype = ctypes.c_size_t
         for name in ("pkg_whir_commit_words", "pkg_whir_proof_words"):
@@ -182,4 +188,4 @@ def exported_symbols():
     return sorted(SIGNATURES) + ["pkg_last_error", "pkg_kernel_launches", "pkg_batch_destroy",
                                   "pkg_server_destroy", "pkg_whir_commit_words",
                                   "pkg_whir_proof_words", "pkg_r1cs_transposes_bytes",
-                                  "pkg_free_buf", "pkg_prover_free"]
+                                  "pkg_free_buf", "pkg_prover_free", "pkg_dual_prove_free"]

@@ -54,4 +54,24 @@ int whir_prove_device(const pkg_whir_params* p, pkg_transcript* t, const uint64_
 // In place v[b | 2^i] += v[b] over 2^n entries (pkg_subset_transform's zeta).
 int subset_zeta_device(uint64_t* v, unsigned n, cudaStream_t s);
 
+// ---- the R1CS prove paths (prove.cu, dual_prove.cu) -----------------------
+// Seeds of the whir-ZK mask polynomials: the blinding seed with the first
+// and the second 64 fraction bits of pi (fixed, arbitrary separators), the
+// first for the (first) witness commitment, the second for w2's.
+constexpr uint64_t kMaskSeed = 0x243f6a8885a308d3ULL;
+constexpr uint64_t kMaskSeed2 = 0x13198a2e03707344ULL;
+// get_public_weights (provekit/prover/src/whir_r1cs.rs:665-676): w[0 ..= np]
+// read from the device witness into pubw (host, 4 (np + 1) words), the
+// hash of w[1 ..= np] (PublicInputs::hash, common/src/witness/mod.rs:86-97;
+// canonical, 0 without public inputs) absorbed, the challenge x squeezed.
+int public_challenge(const uint64_t* witness, size_t np, uint64_t* pubw, pkg_transcript* t,
+                     uint64_t hash[4], uint64_t x[4], cudaStream_t s);
+// make_public_weight's entries [1, x, .., x^np] (prefix_covector.rs:173-186)
+// into xpow (4 (np + 1) words) and <xpow, pubw> into eval (Montgomery form).
+void public_weight_host(const uint64_t* pubw, size_t np, const uint64_t x[4], uint64_t* xpow,
+                        uint64_t eval[4]);
+// The blinding covector expand_powers::<4>(alpha) (whir_r1cs.rs:184):
+// [1, a_i, a_i^2, a_i^3] for each of the m0 challenges; bw: 16 m0 words.
+void blinding_weights_host(const uint64_t* alpha, size_t m0, uint64_t* bw);
+
 }  // namespace pk

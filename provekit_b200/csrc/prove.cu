@@ -37,10 +37,6 @@ static size_t ceil_log2(size_t n) {  // utils::next_power_of_two (utils/mod.rs:7
 // stages' device time plus their host work.
 thread_local double g_stage_ms[PKG_PROVE_STAGES];
 
-// Seed of the WHIR-ZK blinding polynomial: the blinding seed with the first
-// 64 fraction bits of pi (a fixed, arbitrary domain separator).
-constexpr uint64_t kMaskSeed = 0x243f6a8885a308d3ULL;
-
 struct StageClock {
   std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
   void mark(int k) {
@@ -49,6 +45,45 @@ struct StageClock {
     t = now;
   }
 };
+
+int public_challenge(const uint64_t* witness, size_t np, uint64_t* pubw, pkg_transcript* t,
+                     uint64_t hash[4], uint64_t x[4], cudaStream_t s) {
+  memset(hash, 0, 32);
+  if (np) {
+    int rc = read_small(pubw, witness, 32 * (np + 1), s);
+    if (rc) return rc;
+    auto w = [pubw](size_t i) { return HostFr::from_mont(HostFr::from_limbs(pubw + 4 * i)); };
+    HostFr h = HostSky::compress(w(1), np > 1 ? w(2) : HostFr::zero());
+    for (size_t i = 3; i <= np; i++) h = HostSky::compress(h, w(i));
+    memcpy(hash, h.l, 32);
+  }
+  const HostFr hm = HostFr::to_mont(HostFr::from_limbs(hash));
+  pkg_transcript_absorb(t, hm.l);
+  return pkg_transcript_squeeze(t, x);
+}
+
+void public_weight_host(const uint64_t* pubw, size_t np, const uint64_t x_words[4], uint64_t* xpow,
+                        uint64_t eval[4]) {
+  const HostFr x = HostFr::from_limbs(x_words);
+  HostFr pw = HostFr::one(), acc = HostFr::zero();
+  for (size_t i = 0; i <= np; i++) {
+    memcpy(xpow + 4 * i, pw.l, 32);
+    acc = HostFr::add(acc, HostFr::mul(pw, HostFr::from_limbs(pubw + 4 * i)));
+    pw = HostFr::mul(pw, x);
+  }
+  memcpy(eval, acc.l, 32);
+}
+
+void blinding_weights_host(const uint64_t* alpha, size_t m0, uint64_t* bw) {
+  for (size_t i = 0; i < m0; i++) {
+    HostFr pw = HostFr::one();
+    const HostFr a = HostFr::from_limbs(alpha + 4 * i);
+    for (int k = 0; k < 4; k++) {
+      memcpy(bw + 4 * (4 * i + k), pw.l, 32);
+      pw = HostFr::mul(pw, a);
+    }
+  }
+}
 
 }  // namespace pk
 
@@ -204,22 +239,11 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   if (whir) PK_CUDA(cudaMemsetAsync(cov, 0, 32 * nstm * n, s));
   // out->alpha stays valid and unchanged until the evaluations' read below
   if ((rc = eq_hypercube_device(&out->alpha[0][0], m0, nc, eq, s, false))) return rc;
-  // public weights (get_public_weights, whir_r1cs.rs:665-676): the hash of
-  // the public inputs (PublicInputs::hash, common/src/witness/mod.rs:86-97)
-  // into the transcript, then the challenge x
-  std::vector<HostFr> pubw(np + 1);  // w[0 ..= np], Montgomery form
-  if (np) {
-    if ((rc = read_small(pubw[0].l, witness, 32 * (np + 1), s))) return rc;
-    HostFr h = HostSky::compress(HostFr::from_mont(pubw[1]),
-                                 np > 1 ? HostFr::from_mont(pubw[2]) : HostFr::zero());
-    for (size_t i = 3; i <= np; i++) h = HostSky::compress(h, HostFr::from_mont(pubw[i]));
-    memcpy(out->public_hash, h.l, 32);
-  }
-  {
-    const HostFr hm = HostFr::to_mont(HostFr::from_limbs(out->public_hash));
-    pkg_transcript_absorb(&out->transcript, hm.l);
-  }
-  pkg_transcript_squeeze(&out->transcript, out->public_x);
+  // public weights: the public inputs' hash into the transcript, then x
+  std::vector<uint64_t> pubw(4 * (np + 1));  // w[0 ..= np], Montgomery form
+  if ((rc = public_challenge(witness, np, pubw.data(), &out->transcript, out->public_hash,
+                             out->public_x, s)))
+    return rc;
   clk.mark(3);
   // the transposes: the resident circuit's (built once), else built here
   const bool cached = r1cs->row_ptr_t[0] && r1cs->row_ptr_t[1] && r1cs->row_ptr_t[2];
@@ -256,34 +280,20 @@ static int spartan_prove_impl(const pkg_r1cs* r1cs, const uint64_t* witness,
   for (int k = 0; k < 3; k++) pkg_transcript_absorb(&out->transcript, out->evals[k]);
   // the public weight's evaluation <[1, x, .., x^np], w> and its message
   // (compute_public_weight_evaluation, :654-663, :275-282)
-  std::vector<HostFr> xpow(np + 1);
+  std::vector<uint64_t> xpow(4 * (np + 1));
   if (np) {
-    const HostFr x = HostFr::from_limbs(out->public_x);
-    HostFr pw = HostFr::one(), acc = HostFr::zero();
-    for (size_t i = 0; i <= np; i++) {
-      xpow[i] = pw;
-      acc = HostFr::add(acc, HostFr::mul(pw, pubw[i]));
-      pw = HostFr::mul(pw, x);
-    }
-    memcpy(out->public_eval, acc.l, 32);
-    pkg_transcript_absorb(&out->transcript, acc.l);
+    public_weight_host(pubw.data(), np, out->public_x, xpow.data(), out->public_eval);
+    pkg_transcript_absorb(&out->transcript, out->public_eval);
   }
   clk.mark(4);
   if (whir) {
     // the public weight and the blinding covector expand_powers::<4>(alpha)
     // at the blinding offset (OffsetCovector, prefix_covector.rs:90-112)
     if (np)
-      PK_CUDA(cudaMemcpyAsync(cov, xpow[0].l, 32 * (np + 1), cudaMemcpyHostToDevice, s));
-    std::vector<HostFr> bw(4 * m0);
-    for (size_t i = 0; i < m0; i++) {
-      HostFr pw = HostFr::one();
-      const HostFr a = HostFr::from_limbs(out->alpha[i]);
-      for (int k = 0; k < 4; k++) {
-        bw[4 * i + k] = pw;
-        pw = HostFr::mul(pw, a);
-      }
-    }
-    PK_CUDA(cudaMemcpyAsync(cov + 4 * n * (sbase + 3) + 4 * w1_size, bw[0].l, 32 * 4 * m0,
+      PK_CUDA(cudaMemcpyAsync(cov, xpow.data(), 32 * (np + 1), cudaMemcpyHostToDevice, s));
+    std::vector<uint64_t> bw(16 * m0);
+    blinding_weights_host(&out->alpha[0][0], m0, bw.data());
+    PK_CUDA(cudaMemcpyAsync(cov + 4 * n * (sbase + 3) + 4 * w1_size, bw.data(), 32 * 4 * m0,
                             cudaMemcpyHostToDevice, s));
     // statement values of w: [public_eval?, evals, blinding_eval]; for
     // whir-ZK also every statement's value on the blinding polynomial g

@@ -1,6 +1,7 @@
 """Prover-level entry points: the synthetic R1CS workload, the Spartan
-prove core (provekit/prover/src/whir_r1cs.rs up to WHIR's prove call) and
-the whole proof with WHIR's rounds (pkg_prove_r1cs)."""
+prove core (provekit/prover/src/whir_r1cs.rs up to WHIR's prove call), the
+whole proof with WHIR's rounds (pkg_prove_r1cs) and the two-commitment
+proof of an R1CS with verifier challenges (pkg_dual_prove_*)."""
 import ctypes
 
 import numpy as np
@@ -150,3 +151,76 @@ def statement_count(r1cs) -> int:
     provekit/prover/src/whir_r1cs.rs:258-301): the public weight when there
     are public inputs, A^T eq, B^T eq, C^T eq, and the blinding covector."""
     return 4 + (1 if getattr(r1cs, "num_public_inputs", 0) else 0)
+
+
+class DualProofC(ctypes.Structure):
+    _fields_ = [("spartan", SpartanProofC), ("root2", ctypes.c_uint8 * 32),
+                ("evals2", ctypes.c_uint64 * 12), ("challenge_eval", ctypes.c_uint64 * 4)]
+
+    def as_dict(self):
+        d = self.spartan.as_dict()
+        d["root2"] = bytes(self.root2)
+        d["evals2"] = np.array(self.evals2, np.uint64).reshape(3, 4)
+        d["challenge_eval"] = np.array(self.challenge_eval, np.uint64)
+        return d
+
+
+def r1cs_sizing_split(num_constraints: int, num_witnesses: int, w1_size: int):
+    """(m, m0) of WhirR1CSScheme::new_for_r1cs with the witness split at w1_size."""
+    m, m0 = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    check(lib().pkg_r1cs_sizing_split(num_constraints, num_witnesses, w1_size, ctypes.byref(m),
+                                      ctypes.byref(m0)))
+    return m.value, m0.value
+
+
+def dual_statement_counts(num_public_inputs: int, num_challenges: int):
+    """WHIR statements of the two proofs (prove_from_alphas's dual branch,
+    provekit/prover/src/whir_r1cs.rs:302-425): [public?, A|w1, B|w1, C|w1,
+    blinding] and [A|w2, B|w2, C|w2, challenge weight?]."""
+    return 4 + (1 if num_public_inputs else 0), 3 + (1 if num_challenges else 0)
+
+
+def prove_r1cs_dual(r1cs: DeviceR1CS, w1_size: int, challenge_offsets, solve_w2, whir=None,
+                    blinding_seed=1, transcript_domain=3, stream=None):
+    """A proof of an R1CS with verifier challenges (two commitments):
+    pkg_dual_prove_begin commits w1 = the resident witness's first w1_size
+    entries and draws the challenges; solve_w2(challenges) -- challenges a
+    (k, 4) uint64 array of Montgomery words -- returns w2 (the witness's
+    remaining entries: a device tensor or a host array of (n, 4) words, the
+    challenge values at challenge_offsets); pkg_dual_prove_finish commits it
+    and proves.  Returns (fields dict, challenges, commitment words of w1
+    and w2, WHIR proofs 1 and 2)."""
+    from .whir import WhirParams
+    offs = np.ascontiguousarray(np.asarray(challenge_offsets, dtype=np.uint64).reshape(-1))
+    k = offs.shape[0]
+    m, _ = r1cs_sizing_split(r1cs.num_constraints, r1cs.num_witnesses, w1_size)
+    p = WhirParams.new(m, 3, 2, 128, 10, batch_size=2) if whir is None else whir
+    n1, n2 = dual_statement_counts(r1cs.num_public_inputs, k)
+    ch = np.zeros((max(k, 1), 4), np.uint64)
+    cw1 = np.zeros(p.commit_words(), np.uint64)
+    cw2 = np.zeros_like(cw1)
+    pr1 = np.zeros(p.proof_words(n1), np.uint64)
+    pr2 = np.zeros(p.proof_words(n2), np.uint64)
+    st = ctypes.c_void_p()
+    strm = stream if stream is not None else torch.cuda.current_stream()
+    w = r1cs.witness
+    check(lib().pkg_dual_prove_begin(ctypes.byref(r1cs.c), w1_size,
+                                     offs.ctypes.data if k else None, k, w.data_ptr(),
+                                     blinding_seed, transcript_domain, ctypes.byref(p),
+                                     cw1.ctypes.data, ch.ctypes.data, ctypes.byref(st),
+                                     strm.cuda_stream))
+    try:
+        w2 = solve_w2(ch[:k].copy())
+        n2w = r1cs.num_witnesses - w1_size
+        if not torch.is_tensor(w2):
+            w2 = torch.from_numpy(np.ascontiguousarray(w2, dtype=np.uint64).view(np.int64))
+        w2 = w2.reshape(-1, 4).to(w.device).contiguous()
+        if w2.shape[0] != n2w:
+            raise ValueError(f"w2 has {w2.shape[0]} entries, the R1CS needs {n2w}")
+        out = DualProofC()
+        strm.wait_stream(torch.cuda.current_stream())
+        check(lib().pkg_dual_prove_finish(st, w2.data_ptr() if n2w else None, ctypes.byref(out),
+                                          cw2.ctypes.data, pr1.ctypes.data, pr2.ctypes.data))
+    finally:
+        lib().pkg_dual_prove_free(st)
+    return out.as_dict(), ch[:k], cw1, cw2, pr1, pr2

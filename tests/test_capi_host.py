@@ -217,6 +217,59 @@ def test_prove_r1cs_validation_needs_no_device(L):
                             None) == PKG_ERR_INVALID_ARGUMENT  # unaligned witness
 
 
+@pytest.mark.parametrize("nc,nw,w1", [(1, 1, 1), (100, 300, 150), (1 << 14, 1 << 13, 1 << 12),
+                                      (1 << 14, (1 << 14) + 5, 5), (1 << 20, 1 << 21, 1 << 20),
+                                      (1 << 20, 3 << 13, (1 << 13) - 80), (1000, 5000, 5000)])
+def test_r1cs_sizing_split_matches_oracle(L, nc, nw, w1):
+    from provekit_b200.prover import r1cs_sizing, r1cs_sizing_split
+    assert r1cs_sizing_split(nc, nw, w1) == O.r1cs_sizing_split(nc, nw, w1)
+    if w1 == nw:
+        assert r1cs_sizing_split(nc, nw, w1) == r1cs_sizing(nc, nw)
+
+
+def test_dual_prove_validation_needs_no_device(L):
+    """pkg_dual_prove_begin refuses bad arguments before any device work: a
+    w1 without the public inputs or longer than the witness, an offset
+    outside 2^m, parameters for another m, a batch of 4, null outputs, an
+    unaligned w1; finish refuses a null state; free accepts NULL."""
+    from provekit_b200._lib import PKG_ERR_INVALID_ARGUMENT
+    from provekit_b200.prover import DualProofC, R1csC, r1cs_sizing_split
+    from provekit_b200.whir import WhirParams
+    nc, nw, w1 = 1 << 10, 3000, 2000
+    m, _ = r1cs_sizing_split(nc, nw, w1)
+    r = R1csC(nc, nw)
+    r.num_public_inputs = 2
+    w = np.zeros(4 * 16, np.uint64)
+    wptr = (w.ctypes.data + 15) // 16 * 16
+    buf = np.zeros(64, np.uint64)
+    good = WhirParams.new(m, 3, 2, 64, 4, batch_size=2)
+
+    def begin(w1_size=w1, offs=(0, 5), p=good, wp=wptr, words=buf.ctypes.data,
+              chal=buf.ctypes.data, state=True):
+        o = np.array(offs, np.uint64)
+        st = ctypes.c_void_p(1)
+        rc = L.pkg_dual_prove_begin(ctypes.byref(r), w1_size, o.ctypes.data if len(o) else None,
+                                    len(o), wp, 1, 2, None if p is None else ctypes.byref(p),
+                                    words, chal, ctypes.byref(st) if state else None, None)
+        assert st.value is None or not state  # the state output is reset on entry
+        return rc
+
+    assert begin(w1_size=2) == PKG_ERR_INVALID_ARGUMENT          # public inputs outside w1
+    assert begin(w1_size=nw + 1) == PKG_ERR_INVALID_ARGUMENT     # w1 longer than the witness
+    assert begin(offs=(0, 1 << m)) == PKG_ERR_INVALID_ARGUMENT   # offset outside 2^m
+    assert begin(p=WhirParams.new(m + 1, 3, 2, 64, 4)) == PKG_ERR_INVALID_ARGUMENT
+    assert begin(p=WhirParams.new(m, 3, 2, 64, 4, batch_size=4)) == PKG_ERR_INVALID_ARGUMENT
+    assert begin(p=None) == PKG_ERR_INVALID_ARGUMENT
+    assert begin(words=None) == PKG_ERR_INVALID_ARGUMENT
+    assert begin(chal=None) == PKG_ERR_INVALID_ARGUMENT
+    assert begin(wp=wptr + 8) == PKG_ERR_INVALID_ARGUMENT        # unaligned w1
+    assert begin(state=False) == PKG_ERR_INVALID_ARGUMENT
+    out = DualProofC()
+    assert L.pkg_dual_prove_finish(None, wptr, ctypes.byref(out), buf.ctypes.data,
+                                   buf.ctypes.data, buf.ctypes.data) == PKG_ERR_INVALID_ARGUMENT
+    L.pkg_dual_prove_free(None)
+
+
 @pytest.mark.parametrize("seed,log_nc,log_ni,npub", [(1, 0, 0, 0), (3, 6, 4, 2), (7, 12, 10, 0),
                                                      (1003, 16, 14, 5)])
 def test_synthetic_r1cs_matches_oracle_generator(L, seed, log_nc, log_ni, npub):
