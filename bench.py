@@ -70,8 +70,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plugin-e2e", action="store_true")
     p.add_argument("--no-targets", action="store_true",
-                   help="prove: skip the 2^24 NTT, batched and served measurements after the "
-                        "headline")
+                   help="prove: skip the 2^24 NTT, batched, two-commitment and served "
+                        "measurements after the headline")
     p.add_argument("--workload", choices=["commit", "prove", "batched", "served", "ntt", "whir_ops",
                                           "poseidon2"],
                    default="prove",
@@ -836,6 +836,8 @@ def run_prove(a):
                        "(ff 3, rate 1/4), zk-sumcheck; one CUDA graph, replayed")
         north["batched_256_jobs"] = b
         torch.cuda.empty_cache()
+        north["dual_2p20"] = dual_measure(L, stream, flush, a.seed, 5, 2)
+        torch.cuda.empty_cache()
         t0 = time.perf_counter()
         logs, reqs, rng = make_requests(a.seed, 32, 14, 20)
         sgen_s = time.perf_counter() - t0
@@ -1213,6 +1215,73 @@ def run_served(a):
                        "hbm_budget_gb": budget / 1e9, "max_inflight": 8, "generation_s": gen_s},
             "sequential_capacity_per_s": cap, "sweeps": sweeps}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Two commitments: an R1CS with verifier challenges of the headline's size
+# ---------------------------------------------------------------------------
+def dual_measure(L, stream, flush, seed, steps, warmup):
+    """pkg_dual_prove_begin + _finish on a 2^20-constraint R1CS with 16
+    challenges (w1: 2^19 rows over 2^18 inputs; w2: the challenges and
+    2^19 - 16 challenge products; 1 310 721 witnesses, as the headline's),
+    whir-ZK ff 3, rate 1/4, 128 bits, 10 PoW bits on both commitments.  w2
+    is solved once on the host before the timed steps (the caller's witness
+    solving is not this path); each step is device-timed from begin's first
+    copy to finish's last proof word, L2 flushed before each."""
+    import numpy as np
+    import torch
+
+    from provekit_b200._lib import check
+    from provekit_b200.prover import (DualProofC, HostDualR1CS, dual_statement_counts,
+                                      r1cs_sizing_split)
+    from provekit_b200.whir import WhirParams
+    t0 = time.perf_counter()
+    nchal = 16
+    h = HostDualR1CS(seed + 11, 1 << 19, 1 << 18, nchal, (1 << 19) - nchal)
+    gen_s = time.perf_counter() - t0
+    d = h.to_device()
+    m, m0 = r1cs_sizing_split(h.num_constraints, h.num_witnesses, h.w1_size)
+    p = WhirParams.new(m, 3, 2, 128, 10, batch_size=2)
+    n1, n2 = dual_statement_counts(0, nchal)
+    offs = np.ascontiguousarray(h.challenge_offsets, dtype=np.uint64)
+    ch = np.zeros((nchal, 4), np.uint64)
+    cw1, cw2 = np.zeros(p.commit_words(), np.uint64), np.zeros(p.commit_words(), np.uint64)
+    pr1, pr2 = np.zeros(p.proof_words(n1), np.uint64), np.zeros(p.proof_words(n2), np.uint64)
+    out = DualProofC()
+    sh = stream.cuda_stream
+    w2 = None
+    proofs, times = [], []
+    for i in range(warmup + steps):
+        st = ctypes.c_void_p()
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record(stream)
+            check(L.pkg_dual_prove_begin(ctypes.byref(d.c), h.w1_size, offs.ctypes.data, nchal,
+                                         d.witness.data_ptr(), 1, 3, ctypes.byref(p),
+                                         cw1.ctypes.data, ch.ctypes.data, ctypes.byref(st), sh))
+            try:
+                if w2 is None:  # the caller's solve, once (the challenges repeat)
+                    w2 = torch.from_numpy(h.solve(ch).view(np.int64)).to(d.witness.device)
+                check(L.pkg_dual_prove_finish(st, w2.data_ptr(), ctypes.byref(out),
+                                              cw2.ctypes.data, pr1.ctypes.data, pr2.ctypes.data))
+            finally:
+                L.pkg_dual_prove_free(st)
+            ev[1].record(stream)
+        stream.synchronize()
+        if i >= warmup:
+            times.append(ev[0].elapsed_time(ev[1]))
+            proofs.append(np.concatenate([cw1, cw2, pr1, pr2]))
+    ms = statistics.mean(times)
+    return {"config": "2^20 constraints (w1: 2^19 rows over 2^18 inputs; w2: 16 challenges and "
+                      "2^19 - 16 challenge products), 1310721 witnesses, m = %d per commitment, "
+                      "whir-ZK ff 3, rate 1/4, 128 bits, 10 PoW bits" % m,
+            "ms": ms, "proofs_per_s": 1e3 / ms, "p99_ms": max(times), "steps": steps,
+            "generation_s": gen_s, "proof_words": int(proofs[0].shape[0]),
+            "deterministic": all(np.array_equal(x, proofs[0]) for x in proofs),
+            "note": "CUDA events around begin + finish (the host solve of w2 is the caller's and "
+                    "runs once before the timed steps); parity with the oracle is tested "
+                    "(tests/test_gpu_dual.py), not repeated here"}
 
 
 # ---------------------------------------------------------------------------

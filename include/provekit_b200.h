@@ -325,6 +325,29 @@ int pkg_r1cs_sizing(size_t num_constraints, size_t num_witnesses, size_t *m, siz
 int pkg_synthetic_r1cs(uint64_t seed, size_t num_constraints, size_t num_inputs,
                        uint64_t *row_ptr[3], uint32_t *cols[3], uint64_t *vals[3],
                        size_t nnz_out[3], uint64_t *witness);
+/* Synthetic R1CS with verifier challenges (host memory), the workload of
+ * the two-commitment prove: pkg_synthetic_r1cs(seed, nc1, num_inputs) as
+ * w1 (w1_size = 1 + num_inputs + nc1), then w2 of num_challenges + rows2
+ * entries: challenge j at w2 offset j * floor(w2_size / num_challenges)
+ * (offsets out), products at the other offsets in order.  Row nc1 + i: A =
+ * the challenge i mod num_challenges (w[0] without challenges), B = 1-2
+ * uniform w1 columns (splitmix64(seed ^ 0xd1b54a32d192ed03)) with
+ * coefficients from pkg_sample_fr(seed + 2), C = product i.  Capacities:
+ * row_ptr nc1 + rows2 + 1; cols/vals 3 (nc1 + rows2) for A and B,
+ * nc1 + rows2 for C; witness w1_size + num_challenges + rows2 Fr (w2
+ * zeroed).  No reference counterpart (the reference compiles such circuits
+ * from Noir programs). */
+int pkg_synthetic_r1cs_dual(uint64_t seed, size_t nc1, size_t num_inputs, size_t num_challenges,
+                            size_t rows2, uint64_t *row_ptr[3], uint32_t *cols[3],
+                            uint64_t *vals[3], size_t nnz_out[3], uint64_t *witness,
+                            size_t *offsets);
+/* That instance's w2 from the challenges (host, in place in witness): the
+ * challenges at w1_size + offsets[j], then for rows first_row.. in order
+ * w[C's column] = <A_row, w> <B_row, w>. */
+int pkg_synthetic_dual_solve(size_t num_constraints, size_t first_row,
+                             const uint64_t *const row_ptr[3], const uint32_t *const cols[3],
+                             const uint64_t *const vals[3], size_t w1_size, const size_t *offsets,
+                             size_t num_challenges, const uint64_t *challenges, uint64_t *witness);
 
 /* ---- Batched form ----------------------------------------------------------- */
 /* A batch of independent jobs of uneven sizes.  Job j (size n = 2^log_n,

@@ -119,6 +119,10 @@ SIGNATURES = {
     "pkg_dual_prove_begin": [_c_vp, _c_sz, _c_vp, _c_sz, _c_vp, ctypes.c_uint64, ctypes.c_uint64,
                              _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
     "pkg_dual_prove_finish": [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+    "pkg_synthetic_r1cs_dual": [ctypes.c_uint64, _c_sz, _c_sz, _c_sz, _c_sz, _c_vp, _c_vp, _c_vp,
+                                _c_vp, _c_vp, _c_vp],
+    "pkg_synthetic_dual_solve": [_c_sz, _c_sz, _c_vp, _c_vp, _c_vp, _c_sz, _c_vp, _c_sz, _c_vp,
+                                 _c_vp],
 }
 
 

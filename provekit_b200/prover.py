@@ -70,6 +70,55 @@ class HostR1CS:
         return DeviceR1CS(self, device, transposes)
 
 
+class HostDualR1CS:
+    """Synthetic R1CS with verifier challenges in host memory
+    (pkg_synthetic_r1cs_dual): w1 = a HostR1CS-like instance of nc1 rows,
+    w2 = num_challenges challenges and rows2 products challenge x w1 terms;
+    the witness's w2 part is zero until solve() fills it."""
+
+    def __init__(self, seed: int, nc1: int, num_inputs: int, num_challenges: int, rows2: int,
+                 num_public_inputs: int = 0):
+        if num_public_inputs > num_inputs:
+            raise ValueError("more public inputs than inputs")
+        nc = nc1 + rows2
+        self.num_constraints, self.num_public_inputs, self.first_row = nc, num_public_inputs, nc1
+        self.w1_size = 1 + num_inputs + nc1
+        self.num_witnesses = self.w1_size + num_challenges + rows2
+        self.row_ptr = [np.zeros(nc + 1, np.uint64) for _ in range(3)]
+        caps = [3 * nc, 3 * nc, nc]
+        cols = [np.zeros(max(c, 1), np.uint32) for c in caps]
+        vals = [np.zeros((max(c, 1), 4), np.uint64) for c in caps]
+        self.witness = np.zeros((self.num_witnesses, 4), np.uint64)
+        offs = np.zeros(max(num_challenges, 1), np.uint64)
+        nnz = (ctypes.c_size_t * 3)()
+        rp = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.row_ptr])
+        cl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in cols])
+        vl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in vals])
+        check(lib().pkg_synthetic_r1cs_dual(seed, nc1, num_inputs, num_challenges, rows2, rp, cl,
+                                            vl, nnz, self.witness.ctypes.data, offs.ctypes.data))
+        self.challenge_offsets = offs[:num_challenges]
+        self.nnz = list(nnz)
+        self.cols = [np.ascontiguousarray(c[:n]) for c, n in zip(cols, self.nnz)]
+        self.vals = [np.ascontiguousarray(v[:n]) for v, n in zip(vals, self.nnz)]
+
+    def solve(self, challenges) -> np.ndarray:
+        """w2 for these challenges ((k, 4) Montgomery words), on the host."""
+        w = np.ascontiguousarray(self.witness.copy())
+        ch = np.ascontiguousarray(np.asarray(challenges, dtype=np.uint64).reshape(-1, 4))
+        k = len(self.challenge_offsets)
+        offs = np.ascontiguousarray(self.challenge_offsets, dtype=np.uint64)
+        rp = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.row_ptr])
+        cl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.cols])
+        vl = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in self.vals])
+        check(lib().pkg_synthetic_dual_solve(self.num_constraints, self.first_row, rp, cl, vl,
+                                             self.w1_size, offs.ctypes.data if k else None, k,
+                                             ch.ctypes.data if k else None, w.ctypes.data))
+        return w[self.w1_size:]
+
+    def to_device(self, device="cuda", transposes=True):
+        return DeviceR1CS(self, device, transposes)
+
+
 class DeviceR1CS:
     """An R1CS resident on the device.  transposes: build A^T, B^T, C^T once
     (pkg_r1cs_build_transposes) so that proofs of this circuit skip the

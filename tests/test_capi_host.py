@@ -302,6 +302,26 @@ def test_synthetic_r1cs_matches_oracle_generator(L, seed, log_nc, log_ni, npub):
         assert np.array_equal(ab, ys[2][i]), i
 
 
+@pytest.mark.parametrize("nc1,ni,nchal,rows2", [(1, 1, 0, 0), (64, 20, 3, 77), (100, 30, 0, 50),
+                                                (50, 10, 5, 0), (4096, 1024, 16, 5000)])
+def test_synthetic_dual_matches_oracle_generator(L, nc1, ni, nchal, rows2):
+    """pkg_synthetic_r1cs_dual and pkg_synthetic_dual_solve (the library's
+    generator and w2 solve of the two-commitment workload) equal the
+    oracle's entry for entry, for the same challenges."""
+    from provekit_b200.prover import HostDualR1CS
+    got = HostDualR1CS(9, nc1, ni, nchal, rows2)
+    exp = O.SyntheticDualR1CS(9, nc1, ni, nchal, rows2)
+    assert (got.w1_size, got.num_witnesses, got.nnz) == (exp.w1_size, exp.num_witnesses, exp.nnz)
+    assert np.array_equal(got.challenge_offsets, exp.challenge_offsets)
+    for k in range(3):
+        assert np.array_equal(got.row_ptr[k], exp.row_ptr[k]), k
+        assert np.array_equal(got.cols[k], exp.cols[k]), k
+        assert np.array_equal(got.vals[k], exp.vals[k]), k
+    assert np.array_equal(got.witness, exp.witness)
+    ch = O.sample_fr(5, nchal).reshape(-1, 4)
+    assert np.array_equal(got.solve(ch), exp.solve(ch))
+
+
 def prover_bytes(h, folding_factor=3, log_inv_rate=2, security_bits=128, pow_bits=10, zk=1,
                  domain=0) -> bytes:
     """The pkg_prover_serialize layout written independently from the header's
