@@ -646,7 +646,9 @@ int pkg_prove_r1cs(const pkg_r1cs *r1cs, const uint64_t *witness, uint64_t blind
  *                          WHIR proof 2 of w2's [A|w2, B|w2, C|w2,
  *                          challenge weight?] (make_challenge_weight:
  *                          x^j at challenge_offsets[j], repeated offsets add)
- *   pkg_dual_prove_free    releases the state (any time; NULL is a no-op)
+ *   pkg_dual_prove_free    releases the state (any time; NULL is a no-op;
+ *                          it synchronises the stream given to begin, which
+ *                          must still exist)
  *
  * Sizing: pkg_r1cs_sizing_split.  whir: parameters for its m; batch_size 1,
  * or 2 for whir-ZK (each commitment with its own mask polynomial). */
