@@ -78,6 +78,31 @@ def test_dual_proof_matches_oracle_and_verifies(shape, transposes):
     assert O.verify_r1cs_dual(h, wp, 33, got, ch, cw1, cw2, pr1, pr2) == 0
 
 
+def test_dual_proof_at_the_measured_configuration_matches_oracle():
+    """The two-commitment instance the default bench line times: 2^20
+    constraints (w1 2^19 rows over 2^18 inputs, w2 16 challenges and
+    2^19 - 16 products), m = 20 per commitment, whir-ZK ff 3, rate 1/4,
+    128 bits, 10 PoW bits, blinding seed 1, domain 3; generated by the
+    library (pkg_synthetic_r1cs_dual, equal to the oracle's generator) and
+    proved on the device, word for word equal to the oracle's proof."""
+    from provekit_b200.prover import HostDualR1CS, prove_r1cs_dual
+    seed = 2 + 11
+    h = HostDualR1CS(seed, 1 << 19, 1 << 18, 16, (1 << 19) - 16)
+    eh = O.SyntheticDualR1CS(seed, 1 << 19, 1 << 18, 16, (1 << 19) - 16)
+    m, _ = O.r1cs_sizing_split(h.num_constraints, h.num_witnesses, h.w1_size)
+    assert m == 20
+    got, ch, cw1, cw2, pr1, pr2 = prove_r1cs_dual(h.to_device(), h.w1_size, h.challenge_offsets,
+                                                  h.solve, device_params(m, 128, 10, 2),
+                                                  blinding_seed=1, transcript_domain=3)
+    wp = O.whir_params(m, 3, 2, 128, 10, batch_size=2)
+    ed, ech, ecw1, ecw2, epr1, epr2, _ = O.prove_r1cs_dual(eh, 1, 3, wp)
+    assert np.array_equal(ch, ech)
+    assert_same(got, ed)
+    for a, b in ((cw1, ecw1), (cw2, ecw2), (pr1, epr1), (pr2, epr2)):
+        assert np.array_equal(a, b)
+    assert O.verify_r1cs_dual(eh, wp, 3, got, ch, cw1, cw2, pr1, pr2) == 0
+
+
 def test_dual_proof_with_a_wrong_challenge_value_fails_the_binding():
     """w2 whose challenge entry differs from the drawn challenge: the device
     proves it (the prover does not check the witness), and the verifier's
