@@ -1110,16 +1110,31 @@ def served_compare(reqs, mults, budget, rng, max_inflight=8):
     max_inflight slots (warmed once), against sequential proving under the
     same arrivals (FIFO, the measured service times).  Latency is from submit
     to completion; proofs/s is the stream's requests over its first submit
-    to its last completion."""
+    to its last completion.  Every served proof is compared with the same
+    request's sequential proof (same seeds, so the same words)."""
+    import hashlib
+
     import numpy as np
 
     from provekit_b200.server import ProofServer
+
+    def digest(res):  # every field of a whole proof, in key order
+        h = hashlib.sha256()
+        for k in sorted(res):
+            v = res[k]
+            h.update(k.encode())
+            if isinstance(v, np.ndarray):
+                v = np.ascontiguousarray(v).tobytes()
+            h.update(v if isinstance(v, bytes) else repr(v).encode())
+        return h.digest()
+
     srv = ProofServer(budget, max_inflight=1)
     srv.wait(srv.submit(reqs[0], whole_proof=True, blinding_seed=0, transcript_domain=0))  # warm-up
-    service = []
+    service, want = [], []
     for i, h in enumerate(reqs):
-        _, tm = srv.wait(srv.submit(h, whole_proof=True, blinding_seed=i, transcript_domain=i))
+        res, tm = srv.wait(srv.submit(h, whole_proof=True, blinding_seed=i, transcript_domain=i))
         service.append((tm["done_ns"] - tm["submit_ns"]) * 1e-9)
+        want.append(digest(res))
     srv.close()
     cap = len(service) / sum(service)
     sweeps = []
@@ -1146,8 +1161,10 @@ def served_compare(reqs, mults, budget, rng, max_inflight=8):
                 time.sleep(delay)
             ids[i] = srv.submit(h, whole_proof=True, blinding_seed=i, transcript_domain=i)
         lat, qwait, svc, t_sub, t_done = [], [], [], [], []
-        for rid in ids:
-            _, tm = srv.wait(rid)
+        mismatches = 0
+        for i, rid in enumerate(ids):
+            res, tm = srv.wait(rid)
+            mismatches += digest(res) != want[i]
             lat.append((tm["done_ns"] - tm["submit_ns"]) * 1e-9)
             qwait.append((tm["admit_ns"] - tm["submit_ns"]) * 1e-9)
             svc.append((tm["done_ns"] - tm["admit_ns"]) * 1e-9)
@@ -1167,6 +1184,7 @@ def served_compare(reqs, mults, budget, rng, max_inflight=8):
             "sequential": {"proofs_per_s": len(reqs) / fin, "p50_ms": 1e3 * _pct(seq_lat, 0.5),
                            "p99_ms": 1e3 * _pct(seq_lat, 0.99),
                            "p999_ms": 1e3 * _pct(seq_lat, 0.999)},
+            "proofs_differing_from_sequential": mismatches,
         })
         s = sweeps[-1]
         s["served_beats_sequential"] = bool(

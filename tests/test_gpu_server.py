@@ -121,3 +121,25 @@ def test_served_mix_of_public_inputs_and_zk_equals_alone_results():
         assert np.array_equal(got.pop("whir_proof"), proof)
         same(got, sp)
     srv.close()
+
+
+def test_served_large_whole_proofs_equal_alone_results():
+    """Requests of 2^18 and 2^20 constraints (the latter the headline's size)
+    with a small one, served two at a time under a budget that admits both
+    large ones together: whole whir-ZK proofs equal to the same requests
+    proved alone."""
+    from provekit_b200.prover import HostR1CS, prove_r1cs
+    from provekit_b200.server import ProofServer
+    sizes = [(20, 18), (18, 16), (14, 12), (18, 17)]
+    reqs = [HostR1CS(900 + i, 1 << lc, 1 << li) for i, (lc, li) in enumerate(sizes)]
+    alone = [prove_r1cs(h.to_device(), blinding_seed=7 + i, transcript_domain=70 + i)
+             for i, h in enumerate(reqs)]
+    srv = ProofServer(hbm_budget_bytes=24 << 30, max_inflight=2)
+    ids = [srv.submit(h, whole_proof=True, blinding_seed=7 + i, transcript_domain=70 + i)
+           for i, h in enumerate(reqs)]
+    for rid, (sp, cw, proof) in zip(ids, alone):
+        got, _ = srv.wait(rid)
+        assert np.array_equal(got.pop("whir_commit_words"), cw)
+        assert np.array_equal(got.pop("whir_proof"), proof)
+        same(got, sp)
+    srv.close()
