@@ -47,13 +47,13 @@ F64_PER_SQR = 11 + 66 + 10 + 140 + 69  # 296
 # so the leaf kernel's multiply work is its squarings plus these.
 IMAD_PER_REDC = 8 * (1 + 16)  # 136
 # dram__bytes_read.sum + dram__bytes_write.sum of one leaf_fold_fr_kernel launch
-# from an ncu capture of this workload (profiles/leaf_fold_fr_kernel_whir_commit_2p20.md),
-# keyed by (log2 coeffs, folding factor, log inv rate).
+# from an ncu capture of this workload (the leaf kernel's WHIR-commit profile
+# summary under profiles/), keyed by (log2 coeffs, folding factor, log inv rate).
 LEAF_TRAFFIC_BYTES = {(20, 4, 2): 134.264064e6 + 6.855168e6}
 # the same for the whole proof's witness commitment (whir-ZK: 2^20 leaves of
 # 16 Fr, the witness and blinding polynomials of m = 21 at rate 1/4), from an
-# ncu capture of the default command
-# (profiles/leaf_fold_fr_kernel_whole_proof_2p20_constraints.md).
+# ncu capture of the default command (the leaf kernel's whole-proof profile
+# summary under profiles/).
 LEAF_TRAFFIC_PROVE_BYTES = 537195264 + 33959680
 
 

@@ -694,8 +694,10 @@ void pkg_dual_prove_free(pkg_dual_prove *state);
  * the circuit resident on the device that was current at creation, with its
  * transposes built once; a proof comes back in a pkg_buf.  Calls on one
  * handle are serialised (one proof at a time, synchronous); different
- * handles prove concurrently.  Statuses are this header's PKG_* codes (the
- * reference's PKStatus values are positive: INTEGRATION.md maps them). */
+ * handles prove concurrently.  Statuses are this header's PKG_* codes; the
+ * reference's PKStatus values are positive, and map as PKG_OK = PK_SUCCESS,
+ * PKG_ERR_INVALID_ARGUMENT = InvalidInput or SchemeReadError, the other
+ * PKG_ERR_* codes = ProofError. */
 /* PKBuf (tooling/provekit-ffi/src/types.rs:8-40, include/provekit_ffi.h:14-22):
  * library-allocated bytes, released exactly once by pkg_free_buf. */
 typedef struct {
