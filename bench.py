@@ -8,7 +8,7 @@ zk-sumcheck, the covector evaluations and WHIR's prove rounds -- bit-exact
 with the CPU restatement; proofs/s and p50/p99 latency.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload prove|commit|batched|served|ntt|whir_ops|poseidon2]
+                    [--workload prove|commit|batched|served|ntt|whir_ops|poseidon2|dual]
 
 N > 1 runs under torchrun: every rank proves its own instance (independent
 replicas, no data-path collective); time = max over ranks.  Prints one JSON
@@ -73,12 +73,13 @@ def parse_args():
                    help="prove: skip the 2^24 NTT, batched, two-commitment and served "
                         "measurements after the headline")
     p.add_argument("--workload", choices=["commit", "prove", "batched", "served", "ntt", "whir_ops",
-                                          "poseidon2"],
+                                          "poseidon2", "dual"],
                    default="prove",
                    help="prove (default, the headline line): whole proofs of a 2^20-constraint "
                         "R1CS; commit: WHIR commit of 2^20 coefficients; batched: 256 uneven "
                         "jobs as one CUDA graph vs the same jobs one at a time; served: Poisson "
-                        "stream of whole proofs")
+                        "stream of whole proofs; dual: two-commitment proofs of a 2^20-constraint "
+                        "R1CS with 16 verifier challenges")
     p.add_argument("--jobs", type=int, default=256)
     p.add_argument("--tune", action="store_true", help="batched: run the NTT radix autotuner first")
     p.add_argument("--requests", type=int, default=32, help="served: requests per arrival rate")
@@ -1402,6 +1403,31 @@ def run_ntt(a):
     print(json.dumps(line), flush=True)
 
 
+def run_dual(a):
+    """The two-commitment proof of an R1CS with verifier challenges on its own
+    line (dual_measure: 2^20 constraints, 16 challenges, whir-ZK)."""
+    import torch
+
+    from provekit_b200 import _lib
+
+    L = _lib.lib()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    r = dual_measure(L, stream, flush, a.seed, a.steps, a.warmup)
+    line = {"metric": "two-commitment proofs/s (R1CS with verifier challenges: w1 committed, "
+                      "challenges drawn, w2 committed, zk-sumcheck, two WHIR proofs)",
+            "value": r["proofs_per_s"], "unit": "proofs/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": r["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32/f64 (BN254 Fr: 8x32-bit limbs, products on the FP64 pipe)",
+            "data": "synthetic R1CS with challenges (pkg_synthetic_r1cs_dual, seeded)",
+            "config": {"workload": "dual", "description": r["config"],
+                       "l2": "flushed: 256 MiB device write before each step"},
+            "dual_2p20": r}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------------------
 # WHIR prove-round operations at the prove core's first-round sizes
 # (m = 21 variables, folding factor 3, rate 1/4).
@@ -1576,6 +1602,8 @@ def main():
         run_whir_ops(a)
     elif a.workload == "poseidon2":
         run_poseidon2(a)
+    elif a.workload == "dual":
+        run_dual(a)
     else:
         run_b200(a)
 
