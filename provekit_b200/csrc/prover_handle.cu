@@ -27,6 +27,7 @@
 #include <new>
 #include <vector>
 
+#include "fr_host.hpp"
 #include "host_stage.cuh"
 #include "pk_common.cuh"
 
@@ -80,9 +81,11 @@ void free_handle(pkg_prover* p) {
 }
 
 // CSR checks the device kernels rely on: row pointers start at 0, never
-// decrease and end at nnz; every column is a witness index.
+// decrease and end at nnz; every column is a witness index; every
+// coefficient is a canonical field element (below p, as ark-ff's validating
+// deserialisation requires and the device arithmetic assumes).
 int check_csr(int k, size_t rows, size_t cols, const uint64_t* rp, const uint32_t* cl,
-              size_t nnz) {
+              const uint64_t* vl, size_t nnz) {
   PK_REQUIRE(rp, "matrix %d: null row pointers", k);
   PK_REQUIRE(nnz == 0 || cl, "matrix %d: null columns", k);
   PK_REQUIRE(rp[0] == 0, "matrix %d: row pointers must start at 0", k);
@@ -93,6 +96,9 @@ int check_csr(int k, size_t rows, size_t cols, const uint64_t* rp, const uint32_
   for (size_t e = 0; e < nnz; e++)
     PK_REQUIRE(cl[e] < cols, "matrix %d: column %u of entry %zu is not a witness index (< %zu)",
                k, cl[e], e, cols);
+  for (size_t e = 0; e < nnz; e++)
+    PK_REQUIRE(HostFr::from_limbs(vl + 4 * e).is_canonical(),
+               "matrix %d: coefficient %zu is not a canonical field element (>= p)", k, e);
   return PKG_OK;
 }
 
@@ -220,7 +226,8 @@ extern "C" int pkg_prover_create(size_t num_constraints, size_t num_witnesses,
   PK_REQUIRE(m <= 28 && m0 <= 30, "instance too large (m = %zu, m0 = %zu)", m, m0);
   for (int k = 0; k < 3; k++) {
     PK_REQUIRE(nnz[k] == 0 || vals[k], "matrix %d: null values", k);
-    if ((rc = check_csr(k, num_constraints, num_witnesses, row_ptr[k], cols[k], nnz[k])))
+    if ((rc = check_csr(k, num_constraints, num_witnesses, row_ptr[k], cols[k], vals[k],
+                        nnz[k])))
       return rc;
   }
   pkg_whir_params whir;

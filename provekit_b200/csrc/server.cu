@@ -309,6 +309,16 @@ extern "C" int pkg_server_submit(pkg_server* s, const pkg_prove_request* req, ui
   for (int k = 0; k < 3; k++) {
     PK_REQUIRE(req->row_ptr[k] && (req->nnz[k] == 0 || (req->cols[k] && req->vals[k])),
                "null matrix array");
+    // the row pointers bound every device walk over a row's entries: they
+    // start at 0, never decrease and end at nnz (column indices are checked
+    // on the device, where an out-of-range one is skipped and reported)
+    const uint64_t* rp = req->row_ptr[k];
+    PK_REQUIRE(rp[0] == 0 && rp[r->nc] == req->nnz[k],
+               "matrix %d: row pointers run from %llu to %llu, nnz is %zu", k,
+               (unsigned long long)rp[0], (unsigned long long)rp[r->nc], req->nnz[k]);
+    bool monotone = true;
+    for (size_t i = 0; i < r->nc; i++) monotone &= rp[i + 1] >= rp[i];
+    PK_REQUIRE(monotone, "matrix %d: row pointers decrease", k);
     r->nnz[k] = req->nnz[k];
     r->row_ptr[k] = req->row_ptr[k];
     r->cols[k] = req->cols[k];

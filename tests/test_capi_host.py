@@ -348,11 +348,14 @@ def test_get_last_error_takes_and_clears(L):
     assert last_error_taken() == ""  # cleared by the first take
 
 
+P_LIMBS = [0x43e1f593f0000001, 0x2833e84879b97091, 0xb85045b68181585d, 0x30644e72e131a029]
+
+
 def _bad_variants(h):
     """(description, mutated HostR1CS-like copy) with one malformed matrix each."""
     import copy
     out = []
-    for what in ("start", "decrease", "end", "column"):
+    for what in ("start", "decrease", "end", "column", "coefficient p", "coefficient max"):
         g = copy.deepcopy(h)
         if what == "start":
             g.row_ptr[1] = g.row_ptr[1].copy()
@@ -363,16 +366,21 @@ def _bad_variants(h):
         elif what == "end":
             g.nnz = list(g.nnz)
             g.nnz[2] += 1
-        else:
+        elif what == "column":
             g.cols[0] = g.cols[0].copy()
             g.cols[0][3] = g.num_witnesses
+        else:  # a coefficient that is not a canonical field element
+            k = 1 if what == "coefficient p" else 2
+            g.vals[k] = g.vals[k].copy()
+            g.vals[k][-1] = P_LIMBS if what == "coefficient p" else [2**64 - 1] * 4
         out.append((what, g))
     return out
 
 
 def test_prover_create_rejects_malformed_circuits_before_device_work(L):
     """Row pointers that do not start at 0, decrease or do not end at nnz,
-    and columns that are not witness indices, are rejected on the host:
+    columns that are not witness indices and coefficients that are not
+    canonical field elements (p itself, 2^256 - 1) are rejected on the host:
     the kernels that walk the rows never see them."""
     from provekit_b200._lib import PkgError
     from provekit_b200.handle import Prover

@@ -143,3 +143,30 @@ def test_served_large_whole_proofs_equal_alone_results():
         assert np.array_equal(got.pop("whir_proof"), proof)
         same(got, sp)
     srv.close()
+
+
+def test_malformed_request_is_rejected_at_submit():
+    """Row pointers that decrease or do not end at nnz are refused by
+    pkg_server_submit before the request is queued (device walks over a
+    row's entries are bounded by them); a well-formed request on the same
+    server still proves."""
+    import copy
+
+    from provekit_b200._lib import PKG_ERR_INVALID_ARGUMENT, PkgError
+    from provekit_b200.prover import HostR1CS, spartan_prove
+    from provekit_b200.server import ProofServer
+    h = HostR1CS(950, 1 << 10, 1 << 8)
+    srv = ProofServer(hbm_budget_bytes=1 << 30, max_inflight=1)
+    dec = copy.deepcopy(h)
+    dec.row_ptr[1] = dec.row_ptr[1].copy()
+    dec.row_ptr[1][3] = dec.row_ptr[1][4] + 1  # row 3 starts after row 4 does
+    end = copy.deepcopy(h)
+    end.row_ptr[2] = end.row_ptr[2].copy()
+    end.row_ptr[2][-1] += 1  # past nnz
+    for bad in (dec, end):
+        with pytest.raises(PkgError) as e:
+            srv.submit(bad, blinding_seed=2, transcript_domain=5)
+        assert e.value.code == PKG_ERR_INVALID_ARGUMENT
+    got, _ = srv.wait(srv.submit(h, blinding_seed=2, transcript_domain=5))
+    same(got, spartan_prove(h.to_device(), blinding_seed=2, transcript_domain=5))
+    srv.close()
