@@ -447,7 +447,10 @@ int pkg_server_create(size_t hbm_budget_bytes, int max_inflight, pkg_server **ou
 /* Queues the request without copying it: the caller's host buffers must stay
  * valid and unchanged until pkg_server_wait returns for the returned id (the
  * worker uploads them when the request is admitted).  A request whose
- * estimate exceeds the whole budget returns PKG_ERR_OUT_OF_MEMORY. */
+ * estimate exceeds the whole budget returns PKG_ERR_OUT_OF_MEMORY; row
+ * pointers that do not start at 0, decrease or do not end at nnz return
+ * PKG_ERR_INVALID_ARGUMENT (column indices are checked on the device: an
+ * out-of-range one fails the request). */
 int pkg_server_submit(pkg_server *server, const pkg_prove_request *req, uint64_t *request_id);
 /* Blocks until the request is done; returns its status. */
 int pkg_server_wait(pkg_server *server, uint64_t request_id, pkg_spartan_proof *proof,
@@ -732,8 +735,9 @@ int pkg_prover_config_default(pkg_prover_config *cfg);
  * (ffi.rs:160-265) as far as the prover goes: the reference compiles a Noir
  * circuit or reads a .pkp file, which is outside this library (Noir
  * compilation and the .pkp serde layout of the un-vendored whir / spongefish
- * types).  Row pointers and column indices are validated on the host.
- * Synchronous; the handle is freed by pkg_prover_free. */
+ * types).  Row pointers, column indices and coefficients (canonical field
+ * elements, below p) are validated on the host.  Synchronous; the handle is
+ * freed by pkg_prover_free. */
 int pkg_prover_create(size_t num_constraints, size_t num_witnesses, size_t num_public_inputs,
                       const uint64_t *const row_ptr[3], const uint32_t *const cols[3],
                       const uint64_t *const vals[3], const size_t nnz[3],
