@@ -186,3 +186,29 @@ def test_dual_argument_errors():
     assert call(h.num_witnesses + 1, [0, 1]) == -1         # w1 longer than the witness
     assert call(h.w1_size, [0, 1], O.whir_params(m + 1, 3, 2, 40, 4)) == -1  # wrong m
     del keep
+
+
+def test_dual_proofs_verify_over_random_shapes():
+    """Seeded random shapes (rows of w1 and w2, inputs, challenges, public
+    inputs, batch, folding factor): every oracle dual proof is accepted, and
+    the proof of another seed's instance is not."""
+    rng = np.random.default_rng(2024)
+    for case in range(12):
+        nc1 = int(rng.integers(1, 300))
+        ni = int(rng.integers(1, 120))
+        nchal = int(rng.integers(0, 9))
+        rows2 = int(rng.integers(0, 400))
+        npub = int(rng.integers(0, min(ni, 4) + 1))
+        nb = int(rng.integers(1, 3))
+        ff = int(rng.integers(1, 5))
+        h = O.SyntheticDualR1CS(100 + case, nc1, ni, nchal, rows2, num_public_inputs=npub)
+        m, _ = O.r1cs_sizing_split(h.num_constraints, h.num_witnesses, h.w1_size)
+        wp = O.whir_params(m, ff, 2, 40, 3, batch_size=nb)
+        d, ch, cw1, cw2, pr1, pr2, w = O.prove_r1cs_dual(h, case, 7, wp)
+        assert satisfied(h, w), case
+        assert O.verify_r1cs_dual(h, wp, 7, d, ch, cw1, cw2, pr1, pr2) == 0, case
+        if case:  # the previous case's proof does not verify against this instance
+            pd, pch, pcw1, pcw2, ppr1, ppr2 = prev
+            if pcw1.shape == cw1.shape and ppr1.shape == pr1.shape and ppr2.shape == pr2.shape:
+                assert O.verify_r1cs_dual(h, wp, 7, pd, pch, pcw1, pcw2, ppr1, ppr2) != 0, case
+        prev = (d, ch, cw1, cw2, pr1, pr2)
